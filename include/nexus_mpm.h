@@ -1,0 +1,277 @@
+/*
+ * nexus_mpm.h — C ABI of the B200 (sm_100a) MLS-MPM step.
+ *
+ * A drop-in for nexus_mpm's `MpmPipeline::step` and the `MpmState` /
+ * `GpuParticles` calls around it (reference crate nexus_mpm3d 0.5.0).
+ * Every entry point below names the reference interface it replaces
+ * (path:line within the reference project).  Plain pointers and sizes
+ * only; the library owns all device memory.
+ *
+ * Conventions
+ *   - Return value: 0 (NXM_OK) or a negative NXM_E_* code.
+ *   - Matrices are column-major, 9 floats (glam Mat3 layout).
+ *   - A state is used by one host thread at a time; calls on one state are
+ *     ordered on that state's CUDA stream.  nxm_step enqueues and returns;
+ *     readbacks synchronize the state's stream.
+ *   - Particle indices are stable: particle i stays at index i until it is
+ *     removed (the sort reorders an index list, never the particle arrays).
+ */
+#ifndef NEXUS_MPM_H
+#define NEXUS_MPM_H
+
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define NXM_API __attribute__((visibility("default")))
+#else
+#define NXM_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- error codes ------------------------------------------------------- */
+#define NXM_OK 0
+#define NXM_E_INVALID (-1)      /* bad argument (null pointer, out-of-range index, ...) */
+#define NXM_E_CUDA (-2)         /* a CUDA runtime call failed */
+#define NXM_E_CAPACITY (-3)     /* more active grid blocks than the grid capacity */
+#define NXM_E_HASH_FULL (-4)    /* the block hash map is full */
+#define NXM_E_NO_DEVICE (-5)    /* no CUDA device / the library cannot run here */
+#define NXM_E_UNSUPPORTED (-6)  /* a feature this build does not implement */
+#define NXM_E_OOM (-7)          /* device allocation failed */
+
+/* Device status bits reported by nxm_state_status (sticky until cleared). */
+#define NXM_STATUS_HASH_FULL 1u
+#define NXM_STATUS_BLOCK_CAPACITY 2u
+#define NXM_STATUS_MISSING_BLOCK 4u
+#define NXM_STATUS_SORT_CAPACITY 8u
+
+/* ---- plain data -------------------------------------------------------- */
+
+/* SimulationParams (src_mpm_shaders/solver/params.rs:9-17). */
+typedef struct nxm_simulation_params {
+    float gravity[3];
+    float dt;
+} nxm_simulation_params;
+
+/* MpmCapacities (src_mpm/pipeline.rs:27-43): grid_size = grid blocks to
+ * reserve (rounded up to a power of two, as GpuGrid::with_capacity does). */
+typedef struct nxm_capacities {
+    uint32_t grid_size;
+    uint32_t particles_capacity;
+} nxm_capacities;
+
+/* GpuParticleModel (src_mpm_shaders/models/default.rs:41-44): tag + 24 words,
+ * 100 bytes, bit-identical to the reference's host packing
+ * (src_mpm/solver/particle_model.rs:282-325). */
+typedef struct nxm_particle_model {
+    uint32_t tag;
+    uint32_t data[24];
+} nxm_particle_model;
+
+/* Particle + ParticleDynamics (src_mpm/solver/particle.rs:26-122). */
+typedef struct nxm_particle {
+    float position[3];
+    float velocity[3];
+    float def_grad[9];
+    float affine[9];
+    float force_dt[3];
+    float vel_grad_det;
+    float init_volume;
+    float init_radius;
+    float mass;
+    float damping;
+    float phase;
+    float boundary_friction;
+    uint32_t group_id;
+    uint32_t enabled;
+    uint32_t fixed;
+    nxm_particle_model model;
+} nxm_particle;
+
+/* Structure-of-arrays view of n particles, for bulk upload (the same fields
+ * as nxm_particle; any pointer except position and model may be NULL to
+ * take the Particle::new default: zero velocity/affine/force/vel_grad_det,
+ * identity F, damping 0, phase 1, boundary_friction 1, group 0, enabled 1,
+ * fixed 0; init_volume/mass are then required). */
+typedef struct nxm_particles_soa {
+    const float* position;        /* n*3 */
+    const float* velocity;        /* n*3 */
+    const float* def_grad;        /* n*9 */
+    const float* affine;          /* n*9 */
+    const float* vel_grad_det;    /* n   */
+    const float* init_volume;     /* n   */
+    const float* init_radius;     /* n   */
+    const float* mass;            /* n   */
+    const float* damping;         /* n   */
+    const float* phase;           /* n   */
+    const float* boundary_friction; /* n */
+    const uint32_t* group_id;     /* n   */
+    const uint32_t* enabled;      /* n   */
+    const uint32_t* fixed;        /* n   */
+    const nxm_particle_model* model; /* n */
+} nxm_particles_soa;
+
+/* BoundaryCondition (src_mpm_shaders/solver/boundary_condition.rs:105-115). */
+#define NXM_BC_STICK 0u
+#define NXM_BC_SLIP 1u
+#define NXM_BC_SEPARATE 2u
+#define NXM_BC_NON_REFLECTING 3u
+
+/* One coupled collider (128 bytes): Shape (src_rbd_shaders/shapes/shape.rs:29-73;
+ * shape_a[3] holds the bit pattern of the shape type: 0 ball, 1 cuboid,
+ * 2 capsule, 6 trimesh), Pose3 (rotation quaternion x,y,z,w + translation),
+ * Velocity (src_rbd_shaders/dynamics/body.rs:216-225), local centre of mass,
+ * BoundaryCondition, and for a trimesh the range of its triangles in the
+ * triangle buffer passed to nxm_state_set_colliders. */
+typedef struct nxm_collider {
+    float shape_a[4];
+    float shape_b[4];
+    float shape_c[4];
+    float rotation[4];
+    float translation[3];
+    float linvel[3];
+    float angvel[3];
+    float local_com[3];
+    uint32_t bc_type;
+    float bc_friction;
+    uint32_t tri_first;
+    uint32_t tri_count;
+} nxm_collider;
+
+/* Per-phase device times of the last timed step (GpuTimestamps,
+ * src_mpm/pipeline.rs:389-524), milliseconds. */
+typedef struct nxm_timestamps {
+    float sort_ms;
+    float p2g_ms;
+    float grid_update_ms;
+    float g2p_ms;   /* G2P and particle update (one fused kernel) */
+    float total_ms;
+} nxm_timestamps;
+
+typedef struct nxm_pipeline nxm_pipeline;
+typedef struct nxm_state nxm_state;
+
+/* ---- pipeline ------------------------------------------------------------ */
+
+/* MpmPipeline::new (src_mpm/pipeline.rs:366-382).  Checks for an sm_100
+ * device; there is no CPU fallback. */
+NXM_API int nxm_pipeline_create(nxm_pipeline** out);
+NXM_API void nxm_pipeline_destroy(nxm_pipeline* pipeline);
+
+/* MpmPipeline::step (src_mpm/pipeline.rs:385-526): sort, P2G, grid update
+ * (with collider projection unless CPIC is on), G2P + particle update,
+ * body integration.  Enqueued on the state's stream; returns immediately.
+ * `timestamps` may be NULL; when given, the call waits and fills it. */
+NXM_API int nxm_step(nxm_pipeline* pipeline, nxm_state* state, nxm_timestamps* timestamps);
+
+/* ---- state -------------------------------------------------------------- */
+
+/* MpmState::empty (src_mpm/pipeline.rs:107-165): no particles, cell width
+ * 1, dt = 1/60, zero gravity. */
+NXM_API int nxm_state_create(const nxm_capacities* capacities, nxm_state** out);
+NXM_API void nxm_state_destroy(nxm_state* state);
+
+/* MpmState::set_simulation_params (src_mpm/pipeline.rs:169-178). */
+NXM_API int nxm_state_set_simulation_params(nxm_state* state, const nxm_simulation_params* params);
+
+/* MpmState::write_substep_params (src_mpm/pipeline.rs:183-196): dt = base_dt / max(substeps, 1). */
+NXM_API int nxm_state_write_substep_params(nxm_state* state, uint32_t num_substeps);
+
+/* MpmState::set_cell_width (src_mpm/pipeline.rs:200-209). */
+NXM_API int nxm_state_set_cell_width(nxm_state* state, float cell_width, uint32_t grid_capacity);
+
+/* MpmState::set_coupling (src_mpm/pipeline.rs:220-247) for one-way coupled
+ * colliders given directly (at most 16).  `tri_vertices` holds 3 vertices
+ * (9 floats) per triangle, in the local frame of the owning trimesh.  Unlike
+ * the reference, this does not switch CPIC on; see nxm_state_set_use_cpic. */
+NXM_API int nxm_state_set_colliders(nxm_state* state, const nxm_collider* colliders, uint32_t num_colliders,
+                            const float* tri_vertices, uint32_t num_triangles);
+
+/* Overwrites the velocity of collider i (kinematic driving, e.g. velocity =
+ * d(pose)/dt each step; the step integrates the pose from it). */
+NXM_API int nxm_state_set_collider_velocity(nxm_state* state, uint32_t index, const float linvel[3], const float angvel[3]);
+
+/* Reads collider i's pose: quaternion x,y,z,w then translation (7 floats). */
+NXM_API int nxm_state_read_collider_pose(nxm_state* state, uint32_t index, float out[7]);
+
+/* MpmState::use_cpic (src_mpm/pipeline.rs:69).  CPIC coupling is not built
+ * yet: enabling it returns NXM_E_UNSUPPORTED. */
+NXM_API int nxm_state_set_use_cpic(nxm_state* state, int enabled);
+
+/* Deterministic mode: canonical sort order (ascending id inside every sort
+ * bucket) and the reference's atomic-free, gather-form P2G with its
+ * summation order.  Off by default (the fast path scatters with atomics). */
+NXM_API int nxm_state_set_deterministic(nxm_state* state, int enabled);
+
+/* ---- particles -------------------------------------------------------- */
+
+/* GpuParticles::append (src_mpm/solver/particle.rs:533-565). */
+NXM_API int nxm_particles_append(nxm_state* state, const nxm_particle* particles, uint32_t count);
+/* Same, from structure-of-arrays host buffers. */
+NXM_API int nxm_particles_append_soa(nxm_state* state, const nxm_particles_soa* particles, uint32_t count);
+
+/* GpuParticles::swap_remove (src_mpm/solver/particle.rs:579-631).  Writes up
+ * to `count` (from, to) relocation pairs to `remaps` (may be NULL) and their
+ * number to `num_remaps`. */
+NXM_API int nxm_particles_swap_remove(nxm_state* state, const uint32_t* slots, uint32_t count, uint32_t* remaps,
+                              uint32_t* num_remaps);
+
+/* GpuParticles::shift_remove (src_mpm/solver/particle.rs:505-531) for [start, end). */
+NXM_API int nxm_particles_shift_remove(nxm_state* state, uint32_t start, uint32_t end);
+
+/* GpuParticles::len (src_mpm/solver/particle.rs:374-377). */
+NXM_API uint32_t nxm_particles_len(const nxm_state* state);
+
+/* GpuParticles::read_positions (src_mpm/solver/particle.rs:634-647) and the
+ * other per-particle fields (n*3, n*3, n*9, n*9, n, n, n, n*25 words). */
+NXM_API int nxm_read_positions(nxm_state* state, float* out);
+NXM_API int nxm_read_velocities(nxm_state* state, float* out);
+NXM_API int nxm_read_affine(nxm_state* state, float* out);
+NXM_API int nxm_read_def_grad(nxm_state* state, float* out);
+NXM_API int nxm_read_vel_grad_det(nxm_state* state, float* out);
+NXM_API int nxm_read_mass(nxm_state* state, float* out);
+NXM_API int nxm_read_enabled(nxm_state* state, uint32_t* out);
+NXM_API int nxm_read_models(nxm_state* state, nxm_particle_model* out);
+
+/* ---- grid inspection (parity tests, debugging) -------------------------- */
+
+/* Number of active blocks of the last sort. */
+NXM_API int nxm_grid_num_blocks(nxm_state* state, uint32_t* out);
+/* Per block, in this build's header order, 23 int32: virtual id xyz,
+ * first_particle, num_particles, num_particles_with_extras,
+ * sort_bucket_cursors[10] (as left by the sort: bucket ends), nbh_block_ids[7]
+ * (ActiveBlockHeader, src_mpm_shaders/grid/grid.rs:318-341). */
+NXM_API int nxm_grid_read_headers(nxm_state* state, int32_t* out, uint32_t max_blocks);
+/* Sorted particle ids with extras (GpuParticles::sorted_ids). */
+NXM_API int nxm_grid_sorted_len(nxm_state* state, uint32_t* out);
+NXM_API int nxm_grid_read_sorted_ids(nxm_state* state, uint32_t* out, uint32_t max_len);
+/* Nodes after the last step's grid update, 4 floats per node (velocity xyz,
+ * mass), 64 per block in header order (Node, grid.rs:401-421). */
+NXM_API int nxm_grid_read_nodes(nxm_state* state, float* out, uint32_t max_blocks);
+
+/* Runs only the sort (+ P2G when `with_p2g`) of the next step on the current
+ * particles, leaving the grid readable; particles are not advanced. */
+NXM_API int nxm_debug_sort(nxm_pipeline* pipeline, nxm_state* state, int with_p2g);
+
+/* ---- synchronisation and status ------------------------------------------ */
+
+NXM_API int nxm_synchronize(nxm_state* state);
+/* Device status bits (NXM_STATUS_*); synchronizes.  `clear` resets them. */
+NXM_API int nxm_state_status(nxm_state* state, uint32_t* bits, int clear);
+NXM_API const char* nxm_error_string(int code);
+
+/* The CUDA stream (cudaStream_t) every call on this state is ordered on,
+ * so that a caller can record events or order its own work against it. */
+NXM_API void* nxm_state_cuda_stream(const nxm_state* state);
+
+/* Launches of this library's own kernels issued since the state was created
+ * (each graph replay counts its kernel nodes). */
+NXM_API uint64_t nxm_state_kernel_launches(const nxm_state* state);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* NEXUS_MPM_H */

@@ -1,0 +1,475 @@
+// Device-side types and math of the nexus_mpm MLS-MPM step for sm_100a.
+//
+// Arithmetic follows the reference shaders operation by operation (glam's
+// column-major Mat3, left-to-right accumulation) so that a build with
+// --fmad=false reproduces the reference's f32 rounding; the fast build lets
+// the compiler contract multiply-adds.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "nxm_layout.h"
+
+namespace nxm {
+
+// ---------------------------------------------------------------------------
+// Small vector / matrix helpers (glam order).
+// ---------------------------------------------------------------------------
+
+struct v3 {
+    float x, y, z;
+};
+struct m3 {
+    v3 c0, c1, c2;  // columns
+};
+
+__device__ __forceinline__ v3 mk(float x, float y, float z) { return v3{x, y, z}; }
+__device__ __forceinline__ v3 operator+(v3 a, v3 b) { return mk(a.x + b.x, a.y + b.y, a.z + b.z); }
+__device__ __forceinline__ v3 operator-(v3 a, v3 b) { return mk(a.x - b.x, a.y - b.y, a.z - b.z); }
+__device__ __forceinline__ v3 operator*(v3 a, float s) { return mk(a.x * s, a.y * s, a.z * s); }
+__device__ __forceinline__ v3 operator/(v3 a, float s) { return mk(a.x / s, a.y / s, a.z / s); }
+__device__ __forceinline__ float dot(v3 a, v3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ v3 cross(v3 a, v3 b) {
+    return mk(a.y * b.z - b.y * a.z, a.z * b.x - b.z * a.x, a.x * b.y - b.x * a.y);
+}
+__device__ __forceinline__ float length(v3 a) { return sqrtf(dot(a, a)); }
+__device__ __forceinline__ v3 vabs(v3 a) { return mk(fabsf(a.x), fabsf(a.y), fabsf(a.z)); }
+__device__ __forceinline__ float vget(v3 a, int i) { return i == 0 ? a.x : (i == 1 ? a.y : a.z); }
+__device__ __forceinline__ v3 splat(float s) { return mk(s, s, s); }
+// glam Vec3::clamp = max(min).min(max) with NaN-ignoring f32::max / f32::min.
+__device__ __forceinline__ v3 vclamp(v3 a, float lo, float hi) {
+    return mk(fminf(fmaxf(a.x, lo), hi), fminf(fmaxf(a.y, lo), hi), fminf(fmaxf(a.z, lo), hi));
+}
+// Rust f32::clamp: NaN-preserving comparison chain.
+__device__ __forceinline__ float rclamp(float a, float lo, float hi) { return a < lo ? lo : (a > hi ? hi : a); }
+
+__device__ __forceinline__ m3 mkm(v3 a, v3 b, v3 c) { return m3{a, b, c}; }
+__device__ __forceinline__ m3 mzero() { return mkm(splat(0.f), splat(0.f), splat(0.f)); }
+__device__ __forceinline__ m3 mident() { return mkm(mk(1, 0, 0), mk(0, 1, 0), mk(0, 0, 1)); }
+__device__ __forceinline__ v3 operator*(const m3& m, v3 v) {
+    v3 r = m.c0 * v.x;
+    r = r + m.c1 * v.y;
+    r = r + m.c2 * v.z;
+    return r;
+}
+__device__ __forceinline__ m3 operator*(const m3& a, const m3& b) { return mkm(a * b.c0, a * b.c1, a * b.c2); }
+__device__ __forceinline__ m3 operator+(const m3& a, const m3& b) { return mkm(a.c0 + b.c0, a.c1 + b.c1, a.c2 + b.c2); }
+__device__ __forceinline__ m3 operator-(const m3& a, const m3& b) { return mkm(a.c0 - b.c0, a.c1 - b.c1, a.c2 - b.c2); }
+__device__ __forceinline__ m3 operator*(const m3& a, float s) { return mkm(a.c0 * s, a.c1 * s, a.c2 * s); }
+__device__ __forceinline__ m3 transpose(const m3& a) {
+    return mkm(mk(a.c0.x, a.c1.x, a.c2.x), mk(a.c0.y, a.c1.y, a.c2.y), mk(a.c0.z, a.c1.z, a.c2.z));
+}
+__device__ __forceinline__ float det(const m3& a) { return dot(a.c2, cross(a.c0, a.c1)); }
+__device__ __forceinline__ m3 diag(v3 d) { return mkm(mk(d.x, 0, 0), mk(0, d.y, 0), mk(0, 0, d.z)); }
+__device__ __forceinline__ float trace(const m3& a) { return a.c0.x + a.c1.y + a.c2.z; }
+__device__ __forceinline__ m3 outer(v3 a, v3 b) { return mkm(a * b.x, a * b.y, a * b.z); }
+
+struct quat {
+    float x, y, z, w;
+};
+// glam Quat::mul_vec3.
+__device__ __forceinline__ v3 qrot(quat q, v3 v) {
+    v3 b = mk(q.x, q.y, q.z);
+    float b2 = dot(b, b);
+    v3 r = v * (q.w * q.w - b2);
+    r = r + b * (dot(v, b) * 2.0f);
+    r = r + cross(b, v) * (q.w * 2.0f);
+    return r;
+}
+__device__ __forceinline__ quat qconj(quat q) { return quat{-q.x, -q.y, -q.z, q.w}; }
+
+// ---------------------------------------------------------------------------
+// Sparse-grid keys (src_mpm_shaders/grid/grid.rs:101-134, solver/particle.rs:208-225).
+// ---------------------------------------------------------------------------
+
+__device__ __forceinline__ uint32_t pack_key(int x, int y, int z) {
+    return ((uint32_t)(x + 0x3FF) & 0x7FFu) | (((uint32_t)(y + 0x1FF) & 0x3FFu) << 11) |
+           (((uint32_t)(z + 0x3FF) & 0x7FFu) << 21);
+}
+__device__ __forceinline__ int key_x(uint32_t k) { return (int)(k & 0x7FFu) - 0x3FF; }
+__device__ __forceinline__ int key_y(uint32_t k) { return (int)((k >> 11) & 0x3FFu) - 0x1FF; }
+__device__ __forceinline__ int key_z(uint32_t k) { return (int)((k >> 21) & 0x7FFu) - 0x3FF; }
+
+__device__ __forceinline__ uint32_t hash_key(uint32_t k) {
+    k *= 0xCC9E2D51u;
+    k = (k << 15) | (k >> 17);
+    k *= 0x1B873593u;
+    return k;
+}
+
+// assoc_cell = round(pt / dx) - 1, with an IEEE division as in the reference.
+__device__ __forceinline__ v3 assoc_cell_of(float dx, v3 pt) {
+    return mk(roundf(__fdiv_rn(pt.x, dx)) - 1.0f, roundf(__fdiv_rn(pt.y, dx)) - 1.0f,
+              roundf(__fdiv_rn(pt.z, dx)) - 1.0f);
+}
+// float -> int32 conversion truncating toward zero, saturating, NaN -> 0 (Rust `as i32`).
+__device__ __forceinline__ int f2i_sat(float f) { return __float2int_rz(f); }
+
+struct CellInfo {
+    int bx, by, bz;       // primary block
+    uint32_t ax, ay, az;  // associated cell inside the block, in [0, 3]
+};
+
+__device__ __forceinline__ CellInfo cell_info(float dx, v3 pt) {
+    v3 a = assoc_cell_of(dx, pt);
+    float fx = floorf(a.x / 4.0f), fy = floorf(a.y / 4.0f), fz = floorf(a.z / 4.0f);
+    CellInfo c;
+    c.bx = f2i_sat(fx);
+    c.by = f2i_sat(fy);
+    c.bz = f2i_sat(fz);
+    // a - floor(a / 4) * 4 is an exact small integer; negative or NaN -> 0 like `as u32`.
+    float dxl = a.x - fx * 4.0f, dyl = a.y - fy * 4.0f, dzl = a.z - fz * 4.0f;
+    c.ax = (uint32_t)__float2uint_rz(dxl);
+    c.ay = (uint32_t)__float2uint_rz(dyl);
+    c.az = (uint32_t)__float2uint_rz(dzl);
+    return c;
+}
+
+// ---------------------------------------------------------------------------
+// Quadratic B-spline (src_mpm_shaders/grid/kernel.rs:118-142).
+// ---------------------------------------------------------------------------
+
+__device__ __forceinline__ float kernel_eval(float x) {
+    float x_abs = fabsf(x);
+    float part1 = 0.75f - x_abs * x_abs;
+    float part2 = 0.5f * (1.5f - x_abs) * (1.5f - x_abs);
+    float lt05 = x_abs < 0.5f ? 1.0f : 0.0f;
+    float lt15 = x_abs < 1.5f ? 1.0f : 0.0f;
+    return lt05 * part1 + (1.0f - lt05) * lt15 * part2;
+}
+__device__ __forceinline__ v3 kernel_eval_all(float x) {
+    return mk(0.5f * (1.5f - x) * (1.5f - x), 0.75f - (x - 1.0f) * (x - 1.0f), 0.5f * (x - 0.5f) * (x - 0.5f));
+}
+
+// Stencil order of the reference's G2P (kernel.rs:42-70): z in (2,0,1) outer,
+// x in (2,0,1), y in (2,0,1) inner.
+__device__ __forceinline__ void nbh_shift(int i, int& sx, int& sy, int& sz) {
+    const int ord[3] = {2, 0, 1};
+    sz = ord[i / 9];
+    sx = ord[(i / 3) % 3];
+    sy = ord[i % 3];
+}
+
+// ---------------------------------------------------------------------------
+// 3x3 SVD: one-sided Jacobi (Hestenes) on the columns of F, in float.
+// ---------------------------------------------------------------------------
+
+struct Svd {
+    m3 u;
+    v3 s;
+    m3 vt;
+};
+
+__device__ __forceinline__ void jacobi_pair(float (&a)[3][3], float (&v)[3][3], int p, int q) {
+    float alpha = a[0][p] * a[0][p] + a[1][p] * a[1][p] + a[2][p] * a[2][p];
+    float beta = a[0][q] * a[0][q] + a[1][q] * a[1][q] + a[2][q] * a[2][q];
+    float gamma = a[0][p] * a[0][q] + a[1][p] * a[1][q] + a[2][p] * a[2][q];
+    if (fabsf(gamma) <= 1.0e-30f || fabsf(gamma) <= 1.0e-9f * sqrtf(alpha * beta)) return;
+    float zeta = (beta - alpha) / (2.0f * gamma);
+    float t = copysignf(1.0f, zeta) / (fabsf(zeta) + sqrtf(1.0f + zeta * zeta));
+    float c = rsqrtf(1.0f + t * t);
+    float s = c * t;
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+        float ap = a[r][p], aq = a[r][q];
+        a[r][p] = c * ap - s * aq;
+        a[r][q] = s * ap + c * aq;
+        float vp = v[r][p], vq = v[r][q];
+        v[r][p] = c * vp - s * vq;
+        v[r][q] = s * vp + c * vq;
+    }
+}
+
+__device__ __forceinline__ Svd svd3(const m3& f) {
+    float a[3][3] = {{f.c0.x, f.c1.x, f.c2.x}, {f.c0.y, f.c1.y, f.c2.y}, {f.c0.z, f.c1.z, f.c2.z}};
+    float v[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
+#pragma unroll 1
+    for (int sweep = 0; sweep < 6; ++sweep) {
+        jacobi_pair(a, v, 0, 1);
+        jacobi_pair(a, v, 0, 2);
+        jacobi_pair(a, v, 1, 2);
+    }
+    float sig[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) sig[c] = sqrtf(a[0][c] * a[0][c] + a[1][c] * a[1][c] + a[2][c] * a[2][c]);
+    // sort decreasing (3-element network), swapping columns of a and v
+    auto swapc = [&](int i, int j) {
+        float t = sig[i]; sig[i] = sig[j]; sig[j] = t;
+#pragma unroll
+        for (int r = 0; r < 3; ++r) {
+            float ta = a[r][i]; a[r][i] = a[r][j]; a[r][j] = ta;
+            float tv = v[r][i]; v[r][i] = v[r][j]; v[r][j] = tv;
+        }
+    };
+    if (sig[1] > sig[0]) swapc(0, 1);
+    if (sig[2] > sig[0]) swapc(0, 2);
+    if (sig[2] > sig[1]) swapc(1, 2);
+    float u[3][3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        float inv = sig[c] > 1.0e-30f ? 1.0f / sig[c] : 0.0f;
+#pragma unroll
+        for (int r = 0; r < 3; ++r) u[r][c] = a[r][c] * inv;
+    }
+    if (!(sig[1] > 1.0e-30f)) {
+        float ux = u[0][0], uy = u[1][0], uz = u[2][0];
+        float ox, oy, oz;
+        if (fabsf(ux) < 0.9f) { ox = 0; oy = -uz; oz = uy; } else { ox = uz; oy = 0; oz = -ux; }
+        float on = sqrtf(ox * ox + oy * oy + oz * oz);
+        if (on == 0.0f) { ox = 1; oy = 0; oz = 0; on = 1; }
+        u[0][1] = ox / on; u[1][1] = oy / on; u[2][1] = oz / on;
+    }
+    if (!(sig[2] > 1.0e-30f)) {
+        u[0][2] = u[1][0] * u[2][1] - u[2][0] * u[1][1];
+        u[1][2] = u[2][0] * u[0][1] - u[0][0] * u[2][1];
+        u[2][2] = u[0][0] * u[1][1] - u[1][0] * u[0][1];
+    }
+    Svd out;
+    out.u = mkm(mk(u[0][0], u[1][0], u[2][0]), mk(u[0][1], u[1][1], u[2][1]), mk(u[0][2], u[1][2], u[2][2]));
+    out.s = mk(sig[0], sig[1], sig[2]);
+    out.vt = mkm(mk(v[0][0], v[0][1], v[0][2]), mk(v[1][0], v[1][1], v[1][2]), mk(v[2][0], v[2][1], v[2][2]));
+    return out;
+}
+
+// ---------------------------------------------------------------------------
+// Constitutive models (src_mpm_shaders/models/*.rs).
+// ---------------------------------------------------------------------------
+
+// linear_elasticity.rs:114-138
+__device__ __forceinline__ m3 linear_stress(float lambda, float mu, const m3& F) {
+    Svd d = svd3(F);
+    float j = d.s.x * d.s.y * d.s.z;
+    v3 ms = d.s - splat(1.0f);
+    m3 rec = (d.u * diag(ms)) * d.vt;
+    float diag_val = lambda * (j - 1.0f) * j;
+    m3 res = (rec * transpose(F)) * (2.0f * mu);
+    res.c0.x += diag_val;
+    res.c1.y += diag_val;
+    res.c2.z += diag_val;
+    return res;
+}
+
+// neo_hookean_elasticity.rs:26-39
+__device__ __forceinline__ m3 neo_hookean_stress(float lambda, float mu, const m3& F) {
+    float j = fmaxf(det(F), 1.0e-10f);
+    float diag_val = lambda * logf(j) - mu;
+    m3 st = (F * transpose(F)) * mu;
+    st.c0.x += diag_val;
+    st.c1.y += diag_val;
+    st.c2.z += diag_val;
+    return st;
+}
+
+// fluid.rs:54-85; p = [bulk_modulus, gamma, viscosity, cfl_coeff, tensile_stiffness]
+__device__ __forceinline__ float fluid_pressure(const float* p, float j) {
+    j = fmaxf(j, 1.0e-6f);
+    if (j <= 1.0f) {
+        float ratio = expf(-p[1] * logf(j));
+        return p[0] * (ratio - 1.0f);
+    }
+    return -p[0] * p[4] * (j - 1.0f);
+}
+__device__ __forceinline__ m3 fluid_stress(const float* p, const m3& F, const m3& strain_rate) {
+    float j = fmaxf(det(F), 1.0e-6f);
+    float sph = trace(strain_rate) / 3.0f;
+    m3 dev = strain_rate;
+    dev.c0.x -= sph;
+    dev.c1.y -= sph;
+    dev.c2.z -= sph;
+    m3 st = dev * (2.0f * p[2] * j);
+    float diag_val = -fluid_pressure(p, j) * j;
+    st.c0.x += diag_val;
+    st.c1.y += diag_val;
+    st.c2.z += diag_val;
+    return st;
+}
+
+// drucker_prager.rs:64-67; pl = [ha, hb, hc, hd, lambda, mu, cohesion]
+__device__ __forceinline__ float dp_alpha(const float* pl, float q) {
+    float angle = pl[0] + (pl[1] * q - pl[3]) * expf(-pl[2] * q);
+    float s_angle = sinf(angle);
+    return sqrtf(2.0f / 3.0f) * (2.0f * s_angle) / (3.0f - s_angle);
+}
+
+// drucker_prager.rs:121-167 and :224-267; state = [pdet, hardening, log_vol_gain]
+__device__ __forceinline__ m3 dp_project(const float* pl, float* state, const m3& F) {
+    if (pl[4] == 0.0f) return F;
+    Svd d = svd3(F);
+    float alpha = dp_alpha(pl, state[1]);
+    const float dd = 3.0f;
+    v3 strain = mk(logf(d.s.x), logf(d.s.y), logf(d.s.z)) + splat(state[2] / dd);
+    float tr = strain.x + strain.y + strain.z;
+    v3 dev = strain - splat(tr / dd);
+    float shifted = tr - pl[6];
+    v3 sv;
+    float hard;
+    if (shifted > 0.0f || (dev.x == 0.0f && dev.y == 0.0f && dev.z == 0.0f)) {
+        sv = splat(expf(pl[6] / dd));
+        hard = length(strain);
+    } else {
+        float dnorm = length(dev);
+        float gamma = dnorm + (dd * pl[4] + 2.0f * pl[5]) / (2.0f * pl[5]) * shifted * alpha;
+        if (gamma <= 0.0f) return F;  // invalid projection: state and F unchanged
+        v3 h = strain - dev * (gamma / dnorm);
+        sv = mk(expf(h.x), expf(h.y), expf(h.z));
+        hard = gamma;
+    }
+    float prev_det = d.s.x * d.s.y * d.s.z;
+    float new_det = sv.x * sv.y * sv.z;
+    float npdet = state[0] * prev_det / new_det;
+    float nlvg = state[2] + logf(prev_det) - logf(new_det);
+    float nhard = state[1] + hard;
+    state[0] = npdet;
+    state[1] = nhard;
+    state[2] = nlvg;
+    return (d.u * diag(sv)) * d.vt;
+}
+
+// snow.rs:452-488; state = [plastic_det]; pl = [critical_compression, critical_stretch, hardening]
+__device__ __forceinline__ m3 snow_project(const float* pl, float* state, const m3& F, float* hardening) {
+    if (pl[0] <= 0.0f && pl[1] <= 0.0f) {
+        *hardening = expf(pl[2] * (1.0f - state[0]));
+        return F;
+    }
+    Svd d = svd3(F);
+    float lo = 1.0f - pl[0];
+    float hi = 1.0f + pl[1];
+    v3 cl = vclamp(d.s, lo, hi);
+    float prev_det = d.s.x * d.s.y * d.s.z;
+    float new_det = cl.x * cl.y * cl.z;
+    float pdet = rclamp(state[0] * prev_det / new_det, 0.1f, 4.0f);
+    state[0] = pdet;
+    *hardening = expf(pl[2] * (1.0f - pdet));
+    return (d.u * diag(cl)) * d.vt;
+}
+
+// models/default.rs:208-264.  `w` holds the material's 24 model words; the
+// per-particle state words (Drucker-Prager words 0..2, snow word 0) are in `st`
+// and updated in place.
+__device__ __forceinline__ m3 model_update(uint32_t tag, const float* w, float* st, m3& F, const m3& vel_grad) {
+    switch (tag) {
+    case MODEL_ELASTIC_LINEAR:
+        return linear_stress(w[0], w[1], F);
+    case MODEL_ELASTIC_NEO_HOOKEAN:
+        return neo_hookean_stress(w[0], w[1], F);
+    case MODEL_SAND_LINEAR:
+        F = dp_project(&w[3], st, F);
+        return linear_stress(w[10], w[11], F);
+    case MODEL_SAND_NEO_HOOKEAN:
+        F = dp_project(&w[3], st, F);
+        return neo_hookean_stress(w[10], w[11], F);
+    case MODEL_FLUID: {
+        m3 sr = (vel_grad + transpose(vel_grad)) * 0.5f;
+        return fluid_stress(&w[0], F, sr);
+    }
+    case MODEL_SNOW: {
+        float hard;
+        F = snow_project(&w[1], st, F, &hard);
+        return linear_stress(w[4] * hard, w[5] * hard, F);
+    }
+    default:
+        return mzero();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Colliders (grid_update_collide.rs:30-99, shapes, boundary_condition.rs:165-201).
+// ---------------------------------------------------------------------------
+
+struct Proj {
+    v3 point;
+    bool inside;
+};
+
+__device__ __forceinline__ Proj ball_project_local(float radius, v3 pt) {
+    float d2 = dot(pt, pt);
+    Proj r;
+    r.inside = d2 <= radius * radius;
+    r.point = pt * (radius / sqrtf(d2));
+    return r;
+}
+
+// parry3d Aabb::project_local_point, solid = false.
+__device__ __forceinline__ Proj cuboid_project_local(v3 half, v3 pt) {
+    v3 mins_pt = mk(-half.x, -half.y, -half.z) - pt;
+    v3 pt_maxs = pt - half;
+    v3 shift = mk(fmaxf(mins_pt.x, 0.f), fmaxf(mins_pt.y, 0.f), fmaxf(mins_pt.z, 0.f)) -
+               mk(fmaxf(pt_maxs.x, 0.f), fmaxf(pt_maxs.y, 0.f), fmaxf(pt_maxs.z, 0.f));
+    Proj r;
+    if (!(shift.x == 0.f && shift.y == 0.f && shift.z == 0.f)) {
+        r.inside = false;
+        r.point = pt + shift;
+        return r;
+    }
+    float best = -3.0e38f;
+    bool is_mins = false;
+    int best_id = 0;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        float mp = vget(mins_pt, i), pm = vget(pt_maxs, i);
+        if (mp < pm) {
+            if (pm > best) { best_id = i; is_mins = false; best = pm; }
+        } else if (mp > best) {
+            best_id = i; is_mins = true; best = mp;
+        }
+    }
+    float val = is_mins ? best : -best;
+    v3 s = mk(best_id == 0 ? val : 0.f, best_id == 1 ? val : 0.f, best_id == 2 ? val : 0.f);
+    r.inside = true;
+    r.point = pt + s;
+    return r;
+}
+
+__device__ __forceinline__ v3 segment_project_local(v3 a, v3 b, v3 pt) {
+    v3 ab = b - a;
+    v3 ap = pt - a;
+    float ab_ap = dot(ab, ap);
+    float sqnab = dot(ab, ab);
+    if (ab_ap <= 0.f) return a;
+    if (ab_ap >= sqnab) return b;
+    float u = ab_ap / sqnab;
+    return a + ab * u;
+}
+
+__device__ __forceinline__ Proj capsule_project_local(v3 a, v3 b, float radius, v3 pt) {
+    v3 pa = segment_project_local(a, b, pt);
+    v3 dproj = pt - pa;
+    float d = length(dproj);
+    Proj r;
+    if (d > 0.f) {
+        r.inside = d <= radius;
+        r.point = pa + dproj * (radius / d);
+    } else {
+        v3 axis = b - a;
+        v3 n = axis / length(axis);
+        v3 o = fabsf(n.x) > fabsf(n.y) ? mk(-n.z, 0.f, n.x) : mk(0.f, n.z, -n.y);
+        o = o / length(o);
+        r.inside = true;
+        r.point = pa + o * radius;
+    }
+    return r;
+}
+
+__device__ __forceinline__ v3 bc_project(uint32_t ty, float friction, v3 vel, v3 n) {
+    if (ty == BC_STICK) return splat(0.f);
+    if (ty == BC_SLIP) {
+        float nv = dot(vel, n);
+        return vel - n * nv;
+    }
+    if (ty == BC_SEPARATE) {
+        float nv = dot(vel, n);
+        if (nv < 0.f) {
+            v3 t = vel - n * nv;
+            float tl = length(t);
+            v3 tdir = tl > 1.0e-8f ? t / tl : splat(0.f);
+            float pl = tl + friction * nv;
+            pl = pl > 0.f ? pl : 0.f;
+            return tdir * pl;
+        }
+        return vel;
+    }
+    return vel;
+}
+
+}  // namespace nxm

@@ -1,0 +1,114 @@
+// Memory layout of one MPM state in HBM (shared by the host library and the kernels).
+//
+// Particles are stored as two 16-byte-aligned records so that a particle
+// gathered through the sorted index costs whole 32-byte sectors:
+//   PKin (80 B): x, mass | v, flags | C columns (c0.w = vel_grad_det)
+//   PDef (48 B): F columns | (f0.w = V0, f1.w = damping, f2.w = material id)
+// plus, for plastic models only, a float4 of model state words.
+// The grid is a hash of 4x4x4-node blocks: packed block keys, per-block
+// headers (struct-of-arrays), 64 float4 nodes per block (momentum + mass,
+// then velocity + mass after the grid update).
+#pragma once
+
+#include <cstdint>
+
+namespace nxm {
+
+constexpr uint32_t NONE = 0xFFFFFFFFu;
+constexpr int NUM_PRIMARY_BUCKETS = 4;
+constexpr int NUM_EXTRA_BUCKETS = 6;
+constexpr int NUM_BUCKETS = 10;
+constexpr int NUM_NBH = 7;
+constexpr int MODEL_WORDS = 24;
+constexpr float MAX_FLT = 1.0e18f;  // nexus_rbd_shaders::MAX_FLT
+constexpr int MAX_COLLIDERS = 16;   // solver/boundary_condition.rs:132
+
+enum : uint32_t {
+    MODEL_ELASTIC_LINEAR = 0,
+    MODEL_ELASTIC_NEO_HOOKEAN = 1,
+    MODEL_SAND_LINEAR = 2,
+    MODEL_SAND_NEO_HOOKEAN = 3,
+    MODEL_FLUID = 4,
+    MODEL_SNOW = 5,
+};
+
+enum : uint32_t { BC_STICK = 0, BC_SLIP = 1, BC_SEPARATE = 2, BC_NON_REFLECTING = 3 };
+enum : uint32_t { SHAPE_BALL = 0, SHAPE_CUBOID = 1, SHAPE_CAPSULE = 2, SHAPE_TRIMESH = 6 };
+
+// Particle flag bits (PKin.flags as u32 bits).
+enum : uint32_t { PFLAG_ENABLED = 1u, PFLAG_FIXED = 2u };
+
+// Device status bits (sticky until read by the host).
+enum : uint32_t {
+    STATUS_HASH_FULL = 1u,        // a block could not be inserted into the hash
+    STATUS_BLOCK_CAPACITY = 2u,   // more active blocks than the grid capacity
+    STATUS_MISSING_BLOCK = 4u,    // a particle's block was not found (follows 1 or 2)
+    STATUS_SORT_CAPACITY = 8u,    // sorted-id list longer than its buffer
+};
+
+struct alignas(16) PKin {
+    float x, y, z, mass;
+    float vx, vy, vz, flags;     // flags: PFLAG_* as u32 bits
+    float c00, c10, c20, vgd;    // C column 0; w = vel_grad_det
+    float c01, c11, c21, pad1;   // C column 1
+    float c02, c12, c22, pad2;   // C column 2
+};
+static_assert(sizeof(PKin) == 80, "PKin layout");
+
+struct alignas(16) PDef {
+    float f00, f10, f20, init_volume;
+    float f01, f11, f21, damping;
+    float f02, f12, f22, material;  // material index (u32 bits)
+};
+static_assert(sizeof(PDef) == 48, "PDef layout");
+
+// One deduplicated material: tag + the 24 model words as floats.  State
+// words (Drucker-Prager words 0..2, snow word 0) live per particle.
+struct alignas(16) Material {
+    uint32_t tag;
+    uint32_t has_state;  // 1 if the model mutates per-particle state words
+    uint32_t pad[2];
+    float w[MODEL_WORDS];
+};
+static_assert(sizeof(Material) == 112, "Material layout");
+
+// Device form of a collider.
+struct alignas(16) DevCollider {
+    float a[4], b[4], c[4];
+    float rot[4];   // quaternion x, y, z, w
+    float tra[4];
+    float linvel[4];
+    float angvel[4];
+    float local_com[4];
+    float com[4];   // world centre of mass (refreshed at the start of a step)
+    uint32_t type, bc_type, tri_first, tri_count;
+    float bc_friction, pad[3];
+};
+static_assert(sizeof(DevCollider) == 176, "DevCollider layout");
+
+// Per-step parameters read by every kernel from device memory (so a captured
+// CUDA graph stays valid when they change).
+struct alignas(16) Params {
+    float gravity[3];
+    float dt;
+    float dx;
+    float inv_dx;
+    uint32_t n;              // particles
+    uint32_t ncol;           // colliders
+    uint32_t block_capacity; // headers / node blocks
+    uint32_t hash_capacity;  // slots, power of two
+    uint32_t sorted_capacity;
+    uint32_t use_cpic;
+};
+
+// Device counters (reset each step by the sort).
+struct alignas(16) Counters {
+    uint32_t num_primary;   // blocks inserted by the primary pass
+    uint32_t num_extra;     // blocks inserted by the neighbour pass
+    uint32_t num_blocks;    // num_primary + num_extra (written by the scan)
+    uint32_t sorted_len;    // total sorted ids, extras included
+    uint32_t status;        // STATUS_* bits
+    uint32_t pad[3];
+};
+
+}  // namespace nxm

@@ -1,0 +1,358 @@
+// Block activation and particle sort (src_mpm/grid/grid.rs:26-191,
+// src_mpm_shaders/grid/sort.rs:104-491, src_mpm_shaders/grid/grid.rs:447-578).
+//
+// Same results as the reference: the set of active blocks (every particle's
+// 2x2x2 block neighbourhood), the per-block slab buckets (4 primary z-slabs,
+// 6 extra buckets), the +1 neighbour header ids and the sorted id list with
+// extras.  Header order and the order inside a bucket come from atomics, as
+// in the reference; the canonical pass (deterministic mode) orders every
+// bucket by ascending particle id.
+//
+// B200 specifics: every particle pass is a persistent grid-stride loop that
+// keeps whole warps together, so that __match_any_sync can merge the atomics
+// of lanes that hit the same block (or the same block bucket): one hash probe
+// or one atomicAdd per distinct key per warp instead of one per particle.
+// Counters, headers and the hash live in L2 (a 2M-particle scene has a few
+// thousand blocks).
+#include "nxm_device.cuh"
+#include "nxm_kernels.h"
+
+namespace nxm {
+namespace {
+
+__device__ __forceinline__ void set_status(Counters* c, uint32_t bit) { atomicOr(&c->status, bit); }
+
+__device__ __forceinline__ void assoc_shift(int i, int& dx, int& dy, int& dz) {
+    // grid.rs:175-212 blocks_associated_to_block: z fastest.
+    dx = (i >> 2) & 1;
+    dy = (i >> 1) & 1;
+    dz = i & 1;
+}
+
+// Insert `key` (block kx,ky,kz); allocates a header on first insertion.
+// Primary blocks take ids [0, num_primary); neighbour-pass blocks take ids
+// base + [0, num_extra) with base = num_primary.
+__device__ void hash_insert(const DevPtrs& P, uint32_t key, int kx, int ky, int kz, bool primary, uint32_t base,
+                            uint32_t hash_mask, uint32_t block_cap) {
+    uint32_t slot = hash_key(key) & hash_mask;
+    for (uint32_t it = 0; it <= hash_mask; ++it) {
+        uint32_t cur = __ldcg(&P.hkey[slot]);
+        if (cur == key) return;
+        if (cur == NONE) {
+            uint32_t old = atomicCAS(&P.hkey[slot], NONE, key);
+            if (old == NONE) {
+                uint32_t id = primary ? atomicAdd(&P.counters->num_primary, 1u)
+                                      : base + atomicAdd(&P.counters->num_extra, 1u);
+                if (id >= block_cap) {
+                    set_status(P.counters, STATUS_BLOCK_CAPACITY);
+                    P.hval[slot] = NONE;
+                    return;
+                }
+                P.bvid[id] = make_int4(kx, ky, kz, (int)key);
+                P.hval[slot] = id;
+                return;
+            }
+            if (old == key) return;
+        }
+        slot = (slot + 1) & hash_mask;
+    }
+    set_status(P.counters, STATUS_HASH_FULL);
+}
+
+__device__ __forceinline__ uint32_t hash_find(const DevPtrs& P, uint32_t key, uint32_t hash_mask) {
+    uint32_t slot = hash_key(key) & hash_mask;
+    for (uint32_t it = 0; it <= hash_mask; ++it) {
+        uint32_t cur = __ldg(&P.hkey[slot]);
+        if (cur == key) return __ldg(&P.hval[slot]);
+        if (cur == NONE) return NONE;
+        slot = (slot + 1) & hash_mask;
+    }
+    return NONE;
+}
+
+// Warp-aggregated atomicAdd: lanes with equal `key` (NONE = no-op) share one
+// atomic; each gets base + its rank among the equal lanes (lane order).
+__device__ __forceinline__ uint32_t warp_agg_add(uint32_t key, uint32_t* addr) {
+    const uint32_t lane = threadIdx.x & 31u;
+    uint32_t peers = __match_any_sync(0xFFFFFFFFu, key);
+    uint32_t leader = __ffs(peers) - 1;
+    uint32_t rank = __popc(peers & ((1u << lane) - 1u));
+    uint32_t base = 0;
+    if (key != NONE && lane == leader) base = atomicAdd(addr, (uint32_t)__popc(peers));
+    base = __shfl_sync(peers, base, leader);
+    return base + rank;
+}
+
+__device__ __forceinline__ bool spills(uint32_t ax, uint32_t ay, uint32_t az, int sx, int sy, int sz) {
+    // sort.rs:320-329, EXTRA_PARTICLE_MIN_SHIFT = 2
+    return (sx == 0 || ax >= 2) && (sy == 0 || ay >= 2) && (sz == 0 || az >= 2);
+}
+__device__ __forceinline__ uint32_t extra_bucket(uint32_t az, int sz) {
+    // sort.rs:56-62
+    int local = (int)az - sz * 4;
+    if (local < -2) local = -2;
+    return NUM_PRIMARY_BUCKETS + (uint32_t)(local + 2);
+}
+
+// ---------------------------------------------------------------------------
+
+__global__ void k_sort_reset(DevPtrs P, uint32_t hash_cap) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < hash_cap; i += gridDim.x * blockDim.x)
+        P.hkey[i] = NONE;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        P.counters->num_primary = 0;
+        P.counters->num_extra = 0;
+        P.counters->num_blocks = 0;
+        P.counters->sorted_len = 0;
+    }
+}
+
+// sort.rs:104-121 gpu_touch_primary_blocks (+ per-particle key cache).
+__global__ void __launch_bounds__(256) k_touch_primary(DevPtrs P) {
+    const uint32_t n = P.params->n;
+    const float dx = P.params->dx;
+    const uint32_t hmask = P.params->hash_capacity - 1;
+    const uint32_t bcap = P.params->block_capacity;
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t base = warp * 32u; base < n; base += nwarps * 32u) {
+        const uint32_t p = base + lane;
+        const bool active = p < n;
+        uint32_t key = NONE;
+        CellInfo ci{};
+        if (active) {
+            float4 xm = __ldg(reinterpret_cast<const float4*>(&P.kin[p]));
+            ci = cell_info(dx, mk(xm.x, xm.y, xm.z));
+            key = pack_key(ci.bx, ci.by, ci.bz);
+            P.pcode[p] = make_uint2(key, ci.ax | (ci.ay << 2) | (ci.az << 4));
+        }
+        uint32_t peers = __match_any_sync(0xFFFFFFFFu, key);
+        if (active && lane == (uint32_t)(__ffs(peers) - 1)) hash_insert(P, key, ci.bx, ci.by, ci.bz, true, 0, hmask, bcap);
+    }
+}
+
+// sort.rs:133-163 gpu_touch_neighbor_blocks.
+__global__ void __launch_bounds__(256) k_touch_nbh(DevPtrs P) {
+    const uint32_t hmask = P.params->hash_capacity - 1;
+    const uint32_t bcap = P.params->block_capacity;
+    const uint32_t nprim = min(__ldcg(&P.counters->num_primary), bcap);
+    for (uint32_t b = blockIdx.x * blockDim.x + threadIdx.x; b < nprim; b += gridDim.x * blockDim.x) {
+        int4 v = P.bvid[b];
+        for (int i = 1; i < 8; ++i) {
+            int sx, sy, sz;
+            assoc_shift(i, sx, sy, sz);
+            int kx = v.x + sx, ky = v.y + sy, kz = v.z + sz;
+            hash_insert(P, pack_key(kx, ky, kz), kx, ky, kz, false, nprim, hmask, bcap);
+        }
+    }
+}
+
+// sort.rs:261-279 gpu_update_nbh_block_ids, plus zeroing of the block's
+// bucket counters and P2G accumulation nodes.  One thread per node.
+__global__ void __launch_bounds__(256) k_block_prep(DevPtrs P) {
+    const uint32_t hmask = P.params->hash_capacity - 1;
+    const uint32_t bcap = P.params->block_capacity;
+    const uint32_t nprim = min(__ldcg(&P.counters->num_primary), bcap);
+    const uint32_t total = min(nprim + __ldcg(&P.counters->num_extra), bcap);
+    if (blockIdx.x == 0 && threadIdx.x == 0) P.counters->num_blocks = total;
+    const uint32_t nthreads = total * 64u;
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < nthreads; t += gridDim.x * blockDim.x) {
+        const uint32_t b = t >> 6, k = t & 63u;
+        P.nodes[t] = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (k < NUM_NBH) {
+            int4 v = P.bvid[b];
+            int sx, sy, sz;
+            assoc_shift((int)k + 1, sx, sy, sz);
+            P.nbh[b * NUM_NBH + k] = hash_find(P, pack_key(v.x + sx, v.y + sy, v.z + sz), hmask);
+        } else if (k < NUM_NBH + NUM_BUCKETS) {
+            P.cursors[b * NUM_BUCKETS + (k - NUM_NBH)] = 0;
+        }
+    }
+}
+
+// sort.rs:287-349 gpu_update_block_particle_count.
+__global__ void __launch_bounds__(256) k_count(DevPtrs P) {
+    const uint32_t n = P.params->n;
+    const uint32_t hmask = P.params->hash_capacity - 1;
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t base = warp * 32u; base < n; base += nwarps * 32u) {
+        const uint32_t p = base + lane;
+        uint32_t h0 = NONE;
+        uint2 code = make_uint2(NONE, 0);
+        if (p < n) {
+            code = P.pcode[p];
+            h0 = hash_find(P, code.x, hmask);
+            P.phdr[p] = h0;
+            if (h0 == NONE) set_status(P.counters, STATUS_MISSING_BLOCK);
+        }
+        const uint32_t ax = code.y & 3u, ay = (code.y >> 2) & 3u, az = (code.y >> 4) & 3u;
+        uint32_t key = (h0 != NONE) ? h0 * 16u + az : NONE;
+        warp_agg_add(key, key != NONE ? &P.cursors[h0 * NUM_BUCKETS + az] : nullptr);
+        for (int i = 1; i < 8; ++i) {
+            int sx, sy, sz;
+            assoc_shift(i, sx, sy, sz);
+            uint32_t hi = NONE, e = 0;
+            if (h0 != NONE && spills(ax, ay, az, sx, sy, sz)) {
+                hi = P.nbh[h0 * NUM_NBH + (i - 1)];
+                if (hi == NONE) set_status(P.counters, STATUS_MISSING_BLOCK);
+                e = extra_bucket(az, sz);
+            }
+            uint32_t k2 = (hi != NONE) ? hi * 16u + e : NONE;
+            warp_agg_add(k2, k2 != NONE ? &P.cursors[hi * NUM_BUCKETS + e] : nullptr);
+        }
+    }
+}
+
+// prefix sum (src_rbd/utils/prefix_sum.rs) over the block totals, then
+// sort.rs:382-420 gpu_copy_scan_values_to_first_particles.  One CTA of 1024.
+__global__ void __launch_bounds__(1024) k_scan(DevPtrs P) {
+    __shared__ uint32_t warp_tot[32];
+    __shared__ uint32_t carry_s;
+    const uint32_t total = P.counters->num_blocks;
+    const uint32_t tid = threadIdx.x, lane = tid & 31u, wid = tid >> 5;
+    if (tid == 0) carry_s = 0;
+    __syncthreads();
+    for (uint32_t tile = 0; tile < total; tile += 1024u) {
+        const uint32_t b = tile + tid;
+        uint32_t cnt[NUM_BUCKETS];
+        uint32_t t = 0;
+        if (b < total) {
+#pragma unroll
+            for (int k = 0; k < NUM_BUCKETS; ++k) {
+                cnt[k] = P.cursors[b * NUM_BUCKETS + k];
+                t += cnt[k];
+            }
+        }
+        uint32_t incl = t;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+            if (lane >= (uint32_t)o) incl += y;
+        }
+        if (lane == 31) warp_tot[wid] = incl;
+        __syncthreads();
+        if (wid == 0) {
+            uint32_t w = warp_tot[lane];
+            uint32_t wi = w;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                uint32_t y = __shfl_up_sync(0xFFFFFFFFu, wi, o);
+                if (lane >= (uint32_t)o) wi += y;
+            }
+            warp_tot[lane] = wi - w;  // exclusive warp offsets
+        }
+        __syncthreads();
+        const uint32_t carry = carry_s;
+        const uint32_t excl = carry + warp_tot[wid] + incl - t;
+        if (b < total) {
+            P.first[b] = excl;
+            uint32_t running = excl;
+#pragma unroll
+            for (int k = 0; k < NUM_BUCKETS; ++k) {
+                if (k == NUM_PRIMARY_BUCKETS) P.nprim[b] = running - excl;
+                P.cursors[b * NUM_BUCKETS + k] = running;
+                running += cnt[k];
+            }
+            P.nwx[b] = running - excl;
+        }
+        __syncthreads();
+        if (tid == 1023) carry_s = excl + t;
+        __syncthreads();
+    }
+    if (tid == 0) {
+        P.counters->sorted_len = carry_s;
+        if (carry_s > P.params->sorted_capacity) set_status(P.counters, STATUS_SORT_CAPACITY);
+    }
+}
+
+// sort.rs:430-491 gpu_finalize_particles_sort.
+__global__ void __launch_bounds__(256) k_finalize(DevPtrs P) {
+    const uint32_t n = P.params->n;
+    const uint32_t scap = P.params->sorted_capacity;
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t base = warp * 32u; base < n; base += nwarps * 32u) {
+        const uint32_t p = base + lane;
+        uint32_t h0 = NONE;
+        uint32_t code = 0;
+        if (p < n) {
+            h0 = P.phdr[p];
+            code = P.pcode[p].y;
+        }
+        const uint32_t ax = code & 3u, ay = (code >> 2) & 3u, az = (code >> 4) & 3u;
+        uint32_t key = (h0 != NONE) ? h0 * 16u + az : NONE;
+        uint32_t slot = warp_agg_add(key, key != NONE ? &P.cursors[h0 * NUM_BUCKETS + az] : nullptr);
+        if (key != NONE && slot < scap) P.sorted[slot] = p;
+        for (int i = 1; i < 8; ++i) {
+            int sx, sy, sz;
+            assoc_shift(i, sx, sy, sz);
+            uint32_t hi = NONE, e = 0;
+            if (h0 != NONE && spills(ax, ay, az, sx, sy, sz)) {
+                hi = P.nbh[h0 * NUM_NBH + (i - 1)];
+                e = extra_bucket(az, sz);
+            }
+            uint32_t k2 = (hi != NONE) ? hi * 16u + e : NONE;
+            uint32_t s2 = warp_agg_add(k2, k2 != NONE ? &P.cursors[hi * NUM_BUCKETS + e] : nullptr);
+            if (k2 != NONE && s2 < scap) P.sorted[s2] = p;
+        }
+    }
+}
+
+// Canonical order: every (block, bucket) segment sorted by ascending id.
+// Rank sort in shared memory (particle ids are distinct inside a block).
+constexpr uint32_t kSegMax = 4096;
+__global__ void __launch_bounds__(256) k_sort_segments(DevPtrs P) {
+    __shared__ uint32_t buf[kSegMax];
+    const uint32_t total = P.counters->num_blocks;
+    for (uint32_t b = blockIdx.x; b < total; b += gridDim.x) {
+        uint32_t start = P.first[b];
+        for (int k = 0; k < NUM_BUCKETS; ++k) {
+            const uint32_t end = P.cursors[b * NUM_BUCKETS + k];
+            const uint32_t len = end - start;
+            if (len > 1 && len <= kSegMax) {
+                for (uint32_t i = threadIdx.x; i < len; i += blockDim.x) buf[i] = P.sorted[start + i];
+                __syncthreads();
+                for (uint32_t i = threadIdx.x; i < len; i += blockDim.x) {
+                    const uint32_t v = buf[i];
+                    uint32_t rank = 0;
+                    for (uint32_t j = 0; j < len; ++j) rank += buf[j] < v ? 1u : 0u;
+                    P.sorted[start + rank] = v;
+                }
+                __syncthreads();
+            } else if (len > kSegMax && threadIdx.x == 0) {
+                set_status(P.counters, STATUS_SORT_CAPACITY);
+            }
+            start = end;
+        }
+    }
+}
+
+inline int grid_for(int sm_count, int per_sm) { return sm_count * per_sm; }
+
+}  // namespace
+
+int sort_launches(bool canonical) { return canonical ? 8 : 7; }
+
+namespace fast {
+
+void launch_sort(const DevPtrs& P, const LaunchCfg& c, bool canonical, cudaStream_t s) {
+    const int g = grid_for(c.sm_count, 8);
+    int reset_grid = (int)((c.hash_capacity + 255u) / 256u);
+    if (reset_grid > g) reset_grid = g;
+    if (reset_grid < 1) reset_grid = 1;
+    k_sort_reset<<<reset_grid, 256, 0, s>>>(P, c.hash_capacity);
+    k_touch_primary<<<g, 256, 0, s>>>(P);
+    k_touch_nbh<<<g, 256, 0, s>>>(P);
+    k_block_prep<<<g, 256, 0, s>>>(P);
+    k_count<<<g, 256, 0, s>>>(P);
+    k_scan<<<1, 1024, 0, s>>>(P);
+    k_finalize<<<g, 256, 0, s>>>(P);
+    if (canonical) k_sort_segments<<<grid_for(c.sm_count, 4), 256, 0, s>>>(P);
+}
+
+}  // namespace fast
+}  // namespace nxm

@@ -1,0 +1,939 @@
+// Host side of the library: MpmState / MpmPipeline equivalents behind the C
+// ABI of include/nexus_mpm.h (src_mpm/pipeline.rs, src_mpm/solver/particle.rs,
+// src_mpm/grid/grid.rs).
+//
+// A state owns its device buffers and one CUDA stream.  The step's kernels
+// read every size and parameter from device memory (Params, Counters) and
+// loop grid-stride over device-side counts, so the whole step is captured
+// once as a CUDA graph and replayed; the graph is rebuilt only when a
+// buffer is reallocated or the mode changes.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <new>
+#include <vector>
+
+#include "../../include/nexus_mpm.h"
+#include "nxm_kernels.h"
+#include "nxm_layout.h"
+
+using namespace nxm;
+
+namespace {
+
+uint32_t next_pow2(uint32_t v) {
+    uint32_t c = 1;
+    while (c < v && c < 0x80000000u) c <<= 1;
+    return c;
+}
+
+#define NXM_TRY(expr)                                   \
+    do {                                                \
+        cudaError_t e_ = (expr);                        \
+        if (e_ != cudaSuccess) {                        \
+            (void)cudaGetLastError();                   \
+            return e_ == cudaErrorMemoryAllocation ? NXM_E_OOM : NXM_E_CUDA; \
+        }                                               \
+    } while (0)
+
+template <class T>
+cudaError_t dalloc(T** p, size_t count) {
+    *p = nullptr;
+    if (count == 0) count = 1;
+    return cudaMalloc(reinterpret_cast<void**>(p), count * sizeof(T));
+}
+template <class T>
+void dfree(T*& p) {
+    if (p) cudaFree(p);
+    p = nullptr;
+}
+
+float bits_f(uint32_t u) {
+    float f;
+    std::memcpy(&f, &u, 4);
+    return f;
+}
+uint32_t f_bits(float f) {
+    uint32_t u;
+    std::memcpy(&u, &f, 4);
+    return u;
+}
+
+bool model_has_state(uint32_t tag) {
+    return tag == MODEL_SAND_LINEAR || tag == MODEL_SAND_NEO_HOOKEAN || tag == MODEL_SNOW;
+}
+int model_state_words(uint32_t tag) {
+    if (tag == MODEL_SAND_LINEAR || tag == MODEL_SAND_NEO_HOOKEAN) return 3;
+    if (tag == MODEL_SNOW) return 1;
+    return 0;
+}
+
+// Packs selected 4-byte fields of per-particle records into a dense array.
+__global__ void k_pack_fields(const uint32_t* __restrict__ src, uint32_t stride_words, uint32_t n,
+                              const int* __restrict__ offsets, int nfields, uint32_t* __restrict__ dst) {
+    const uint32_t total = n * (uint32_t)nfields;
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+        const uint32_t p = t / (uint32_t)nfields, f = t % (uint32_t)nfields;
+        dst[t] = src[(size_t)p * stride_words + offsets[f]];
+    }
+}
+
+}  // namespace
+
+struct nxm_pipeline {
+    int device = 0;
+    int sm_count = 0;
+};
+
+struct nxm_state {
+    int device = 0;
+    int sm_count = 148;
+    cudaStream_t stream = nullptr;
+
+    // parameters
+    float base_dt = 1.0f / 60.0f;
+    float gravity[3] = {0.f, 0.f, 0.f};
+    float dt = 1.0f / 60.0f;
+    float dx = 1.0f;
+    bool use_cpic = false;
+    bool deterministic = false;
+
+    // particles
+    uint32_t n = 0, pcap = 0;
+    PKin* kin = nullptr;
+    PDef* def = nullptr;
+    float4* pstate = nullptr;
+    uint2* pcode = nullptr;
+    uint32_t* phdr = nullptr;
+    uint32_t* sorted = nullptr;
+    std::vector<float> init_radius, phase, boundary_friction;
+    std::vector<uint32_t> group_id;
+
+    // materials (deduplicated model words)
+    std::vector<Material> materials;
+    std::map<std::vector<uint32_t>, uint32_t> material_index;
+    Material* d_materials = nullptr;
+    uint32_t mat_cap = 0;
+    bool materials_dirty = false;
+
+    // grid
+    uint32_t block_cap = 0, hash_cap = 0;
+    uint32_t* hkey = nullptr;
+    uint32_t* hval = nullptr;
+    int4* bvid = nullptr;
+    uint32_t *first = nullptr, *nprim = nullptr, *nwx = nullptr, *cursors = nullptr, *nbh = nullptr;
+    float4* nodes = nullptr;
+
+    // colliders
+    std::vector<DevCollider> colliders;
+    DevCollider* d_colliders = nullptr;
+    float4* d_tri = nullptr;
+
+    // control
+    Params* d_params = nullptr;
+    Counters* d_counters = nullptr;
+    Counters* h_counters = nullptr;  // pinned
+    bool params_dirty = true;
+
+    // graph
+    cudaGraphExec_t graph = nullptr;
+    bool graph_valid = false;
+    int graph_kernels = 0;
+    uint64_t launches = 0;
+
+    // scratch for readback packing
+    uint32_t* d_pack = nullptr;
+    size_t pack_cap = 0;
+    int* d_offsets = nullptr;
+};
+
+namespace {
+
+DevPtrs dev_ptrs(nxm_state* s) {
+    DevPtrs P{};
+    P.kin = s->kin;
+    P.def = s->def;
+    P.pstate = s->pstate;
+    P.materials = s->d_materials;
+    P.colliders = s->d_colliders;
+    P.tri = s->d_tri;
+    P.params = s->d_params;
+    P.counters = s->d_counters;
+    P.hkey = s->hkey;
+    P.hval = s->hval;
+    P.bvid = s->bvid;
+    P.first = s->first;
+    P.nprim = s->nprim;
+    P.nwx = s->nwx;
+    P.cursors = s->cursors;
+    P.nbh = s->nbh;
+    P.nodes = s->nodes;
+    P.sorted = s->sorted;
+    P.pcode = s->pcode;
+    P.phdr = s->phdr;
+    return P;
+}
+
+LaunchCfg launch_cfg(nxm_state* s) {
+    LaunchCfg c{};
+    c.sm_count = s->sm_count;
+    c.hash_capacity = s->hash_cap;
+    c.block_capacity = s->block_cap;
+    c.particle_capacity = s->pcap;
+    return c;
+}
+
+void invalidate_graph(nxm_state* s) {
+    if (s->graph) cudaGraphExecDestroy(s->graph);
+    s->graph = nullptr;
+    s->graph_valid = false;
+}
+
+int free_grid(nxm_state* s) {
+    dfree(s->hkey); dfree(s->hval); dfree(s->bvid); dfree(s->first); dfree(s->nprim); dfree(s->nwx);
+    dfree(s->cursors); dfree(s->nbh); dfree(s->nodes);
+    return NXM_OK;
+}
+
+int alloc_grid(nxm_state* s, uint32_t grid_capacity) {
+    free_grid(s);
+    s->block_cap = next_pow2(std::max<uint32_t>(grid_capacity, 1));
+    s->hash_cap = next_pow2(std::max<uint32_t>(2u * s->block_cap, 1024u));
+    NXM_TRY(dalloc(&s->hkey, s->hash_cap));
+    NXM_TRY(dalloc(&s->hval, s->hash_cap));
+    NXM_TRY(dalloc(&s->bvid, s->block_cap));
+    NXM_TRY(dalloc(&s->first, s->block_cap));
+    NXM_TRY(dalloc(&s->nprim, s->block_cap));
+    NXM_TRY(dalloc(&s->nwx, s->block_cap));
+    NXM_TRY(dalloc(&s->cursors, (size_t)s->block_cap * NUM_BUCKETS));
+    NXM_TRY(dalloc(&s->nbh, (size_t)s->block_cap * NUM_NBH));
+    NXM_TRY(dalloc(&s->nodes, (size_t)s->block_cap * 64));
+    NXM_TRY(cudaMemsetAsync(s->hkey, 0xFF, sizeof(uint32_t) * s->hash_cap, s->stream));
+    invalidate_graph(s);
+    s->params_dirty = true;
+    return NXM_OK;
+}
+
+int reserve_particles(nxm_state* s, uint32_t need) {
+    if (need <= s->pcap) return NXM_OK;
+    uint32_t cap = std::max<uint32_t>(need, s->pcap ? s->pcap * 2 : 1024);
+    PKin* kin; PDef* def; float4* pstate; uint2* pcode; uint32_t* phdr; uint32_t* sorted;
+    NXM_TRY(dalloc(&kin, cap));
+    NXM_TRY(dalloc(&def, cap));
+    NXM_TRY(dalloc(&pstate, cap));
+    NXM_TRY(dalloc(&pcode, cap));
+    NXM_TRY(dalloc(&phdr, cap));
+    NXM_TRY(dalloc(&sorted, (size_t)cap * 8));
+    if (s->n) {
+        NXM_TRY(cudaMemcpyAsync(kin, s->kin, sizeof(PKin) * s->n, cudaMemcpyDeviceToDevice, s->stream));
+        NXM_TRY(cudaMemcpyAsync(def, s->def, sizeof(PDef) * s->n, cudaMemcpyDeviceToDevice, s->stream));
+        NXM_TRY(cudaMemcpyAsync(pstate, s->pstate, sizeof(float4) * s->n, cudaMemcpyDeviceToDevice, s->stream));
+    }
+    NXM_TRY(cudaStreamSynchronize(s->stream));
+    dfree(s->kin); dfree(s->def); dfree(s->pstate); dfree(s->pcode); dfree(s->phdr); dfree(s->sorted);
+    s->kin = kin; s->def = def; s->pstate = pstate; s->pcode = pcode; s->phdr = phdr; s->sorted = sorted;
+    s->pcap = cap;
+    invalidate_graph(s);
+    s->params_dirty = true;
+    return NXM_OK;
+}
+
+// Deduplicates a model's static words; returns the material index.
+uint32_t material_of(nxm_state* s, const nxm_particle_model& m) {
+    std::vector<uint32_t> key(1 + MODEL_WORDS);
+    key[0] = m.tag;
+    const int ns = model_state_words(m.tag);
+    for (int k = 0; k < MODEL_WORDS; ++k) key[1 + k] = (k < ns) ? 0u : m.data[k];
+    auto it = s->material_index.find(key);
+    if (it != s->material_index.end()) return it->second;
+    Material mat{};
+    mat.tag = m.tag;
+    mat.has_state = model_has_state(m.tag) ? 1u : 0u;
+    for (int k = 0; k < MODEL_WORDS; ++k) mat.w[k] = bits_f(key[1 + k]);
+    const uint32_t idx = (uint32_t)s->materials.size();
+    s->materials.push_back(mat);
+    s->material_index.emplace(std::move(key), idx);
+    s->materials_dirty = true;
+    return idx;
+}
+
+int sync_materials(nxm_state* s) {
+    if (!s->materials_dirty) return NXM_OK;
+    const uint32_t need = (uint32_t)s->materials.size();
+    if (need > s->mat_cap) {
+        uint32_t cap = std::max<uint32_t>(need, s->mat_cap ? s->mat_cap * 2 : 16);
+        Material* m;
+        NXM_TRY(dalloc(&m, cap));
+        NXM_TRY(cudaStreamSynchronize(s->stream));
+        dfree(s->d_materials);
+        s->d_materials = m;
+        s->mat_cap = cap;
+        invalidate_graph(s);
+    }
+    NXM_TRY(cudaMemcpyAsync(s->d_materials, s->materials.data(), sizeof(Material) * need, cudaMemcpyHostToDevice,
+                            s->stream));
+    NXM_TRY(cudaStreamSynchronize(s->stream));
+    s->materials_dirty = false;
+    return NXM_OK;
+}
+
+int sync_params(nxm_state* s) {
+    if (!s->params_dirty) return NXM_OK;
+    Params p{};
+    p.gravity[0] = s->gravity[0];
+    p.gravity[1] = s->gravity[1];
+    p.gravity[2] = s->gravity[2];
+    p.dt = s->dt;
+    p.dx = s->dx;
+    p.inv_dx = 1.0f / s->dx;
+    p.n = s->n;
+    p.ncol = (uint32_t)s->colliders.size();
+    p.block_capacity = s->block_cap;
+    p.hash_capacity = s->hash_cap;
+    p.sorted_capacity = s->pcap * 8u;
+    p.use_cpic = s->use_cpic ? 1u : 0u;
+    NXM_TRY(cudaMemcpyAsync(s->d_params, &p, sizeof(Params), cudaMemcpyHostToDevice, s->stream));
+    NXM_TRY(cudaStreamSynchronize(s->stream));
+    s->params_dirty = false;
+    return NXM_OK;
+}
+
+// Issues the kernels of one step on stream `st`; returns how many.
+int enqueue_step(nxm_state* s, cudaStream_t st, cudaEvent_t* ev /* 5 events or null */) {
+    DevPtrs P = dev_ptrs(s);
+    LaunchCfg c = launch_cfg(s);
+    int k = 0;
+    const bool has_col = !s->colliders.empty();
+    if (ev) cudaEventRecord(ev[0], st);
+    if (has_col) { fast::launch_colliders_begin(P, st); ++k; }
+    fast::launch_sort(P, c, s->deterministic, st);
+    k += sort_launches(s->deterministic);
+    if (ev) cudaEventRecord(ev[1], st);
+    if (s->deterministic) exact::launch_p2g_gather(P, c, st);
+    else fast::launch_p2g(P, c, st);
+    k += kP2gLaunches;
+    if (ev) cudaEventRecord(ev[2], st);
+    if (s->deterministic) exact::launch_grid_update(P, c, st);
+    else fast::launch_grid_update(P, c, st);
+    k += kGridLaunches;
+    if (ev) cudaEventRecord(ev[3], st);
+    if (s->deterministic) exact::launch_g2p_update(P, c, st);
+    else fast::launch_g2p_update(P, c, st);
+    k += kG2pLaunches;
+    if (has_col) { fast::launch_colliders_end(P, st); ++k; }
+    if (ev) cudaEventRecord(ev[4], st);
+    return k;
+}
+
+int ensure_ready(nxm_state* s) {
+    int rc = sync_materials(s);
+    if (rc) return rc;
+    return sync_params(s);
+}
+
+int build_graph(nxm_state* s) {
+    invalidate_graph(s);
+    cudaGraph_t g = nullptr;
+    NXM_TRY(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+    int k = enqueue_step(s, s->stream, nullptr);
+    cudaError_t e = cudaStreamEndCapture(s->stream, &g);
+    if (e != cudaSuccess) {
+        (void)cudaGetLastError();
+        if (g) cudaGraphDestroy(g);
+        return NXM_E_CUDA;
+    }
+    e = cudaGraphInstantiate(&s->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+        (void)cudaGetLastError();
+        s->graph = nullptr;
+        return NXM_E_CUDA;
+    }
+    s->graph_kernels = k;
+    s->graph_valid = true;
+    return NXM_OK;
+}
+
+int pack_read(nxm_state* s, const void* records, uint32_t stride_bytes, const int* offsets, int nfields, void* out) {
+    if (!out) return NXM_E_INVALID;
+    if (s->n == 0) return NXM_OK;
+    const size_t words = (size_t)s->n * nfields;
+    if (words > s->pack_cap) {
+        dfree(s->d_pack);
+        NXM_TRY(dalloc(&s->d_pack, words));
+        s->pack_cap = words;
+    }
+    if (!s->d_offsets) NXM_TRY(dalloc(&s->d_offsets, 32));
+    NXM_TRY(cudaMemcpyAsync(s->d_offsets, offsets, sizeof(int) * nfields, cudaMemcpyHostToDevice, s->stream));
+    int grid = std::min<int>((int)((words + 255) / 256), s->sm_count * 8);
+    if (grid < 1) grid = 1;
+    k_pack_fields<<<grid, 256, 0, s->stream>>>(reinterpret_cast<const uint32_t*>(records), stride_bytes / 4, s->n,
+                                                 s->d_offsets, nfields, s->d_pack);
+    s->launches += 1;
+    NXM_TRY(cudaGetLastError());
+    NXM_TRY(cudaMemcpyAsync(out, s->d_pack, words * 4, cudaMemcpyDeviceToHost, s->stream));
+    NXM_TRY(cudaStreamSynchronize(s->stream));
+    return NXM_OK;
+}
+
+int upload_particles(nxm_state* s, const nxm_particles_soa* p, uint32_t count) {
+    if (count == 0) return NXM_OK;
+    if (!p || !p->position || !p->model) return NXM_E_INVALID;
+    if ((!p->init_volume || !p->mass)) return NXM_E_INVALID;
+    uint64_t need = (uint64_t)s->n + count;
+    if (need > 0x7FFFFFFFull / 8) return NXM_E_INVALID;
+    int rc = reserve_particles(s, (uint32_t)need);
+    if (rc) return rc;
+    std::vector<PKin> hk(count);
+    std::vector<PDef> hd(count);
+    std::vector<float4> hs(count);
+    static const float I9[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+    for (uint32_t i = 0; i < count; ++i) {
+        const float* x = p->position + 3 * (size_t)i;
+        const float* v = p->velocity ? p->velocity + 3 * (size_t)i : nullptr;
+        const float* a = p->affine ? p->affine + 9 * (size_t)i : nullptr;
+        const float* F = p->def_grad ? p->def_grad + 9 * (size_t)i : I9;
+        uint32_t flags = 0;
+        if (!p->enabled || p->enabled[i]) flags |= PFLAG_ENABLED;
+        if (p->fixed && p->fixed[i]) flags |= PFLAG_FIXED;
+        PKin& k = hk[i];
+        k.x = x[0]; k.y = x[1]; k.z = x[2];
+        k.mass = p->mass[i];
+        k.vx = v ? v[0] : 0.f; k.vy = v ? v[1] : 0.f; k.vz = v ? v[2] : 0.f;
+        k.flags = bits_f(flags);
+        k.c00 = a ? a[0] : 0.f; k.c10 = a ? a[1] : 0.f; k.c20 = a ? a[2] : 0.f;
+        k.c01 = a ? a[3] : 0.f; k.c11 = a ? a[4] : 0.f; k.c21 = a ? a[5] : 0.f;
+        k.c02 = a ? a[6] : 0.f; k.c12 = a ? a[7] : 0.f; k.c22 = a ? a[8] : 0.f;
+        k.vgd = p->vel_grad_det ? p->vel_grad_det[i] : 0.f;
+        k.pad1 = 0.f; k.pad2 = 0.f;
+        const nxm_particle_model& m = p->model[i];
+        const uint32_t mid = material_of(s, m);
+        PDef& d = hd[i];
+        d.f00 = F[0]; d.f10 = F[1]; d.f20 = F[2];
+        d.f01 = F[3]; d.f11 = F[4]; d.f21 = F[5];
+        d.f02 = F[6]; d.f12 = F[7]; d.f22 = F[8];
+        d.init_volume = p->init_volume[i];
+        d.damping = p->damping ? p->damping[i] : 0.f;
+        d.material = bits_f(mid);
+        const int ns = model_state_words(m.tag);
+        float st[4] = {0, 0, 0, 0};
+        for (int w = 0; w < ns; ++w) st[w] = bits_f(m.data[w]);
+        hs[i] = make_float4(st[0], st[1], st[2], st[3]);
+        s->init_radius.push_back(p->init_radius ? p->init_radius[i] : 0.f);
+        s->phase.push_back(p->phase ? p->phase[i] : 1.f);
+        s->boundary_friction.push_back(p->boundary_friction ? p->boundary_friction[i] : 1.f);
+        s->group_id.push_back(p->group_id ? p->group_id[i] : 0u);
+    }
+    rc = sync_materials(s);
+    if (rc) return rc;
+    NXM_TRY(cudaMemcpyAsync(s->kin + s->n, hk.data(), sizeof(PKin) * count, cudaMemcpyHostToDevice, s->stream));
+    NXM_TRY(cudaMemcpyAsync(s->def + s->n, hd.data(), sizeof(PDef) * count, cudaMemcpyHostToDevice, s->stream));
+    NXM_TRY(cudaMemcpyAsync(s->pstate + s->n, hs.data(), sizeof(float4) * count, cudaMemcpyHostToDevice, s->stream));
+    NXM_TRY(cudaStreamSynchronize(s->stream));
+    s->n += count;
+    s->params_dirty = true;
+    return NXM_OK;
+}
+
+bool device_ok(int* dev, int* sms) {
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+        (void)cudaGetLastError();
+        return false;
+    }
+    int d = 0;
+    if (cudaGetDevice(&d) != cudaSuccess) return false;
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, d) != cudaSuccess) return false;
+    if (prop.major != 10) return false;  // kernels are built for sm_100a only
+    *dev = d;
+    *sms = prop.multiProcessorCount;
+    return true;
+}
+
+}  // namespace
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+
+extern "C" {
+
+const char* nxm_error_string(int code) {
+    switch (code) {
+    case NXM_OK: return "ok";
+    case NXM_E_INVALID: return "invalid argument";
+    case NXM_E_CUDA: return "CUDA runtime error";
+    case NXM_E_CAPACITY: return "more active grid blocks than the grid capacity";
+    case NXM_E_HASH_FULL: return "grid block hash map full";
+    case NXM_E_NO_DEVICE: return "no sm_100 CUDA device available";
+    case NXM_E_UNSUPPORTED: return "unsupported feature";
+    case NXM_E_OOM: return "device out of memory";
+    default: return "unknown error";
+    }
+}
+
+int nxm_pipeline_create(nxm_pipeline** out) {
+    if (!out) return NXM_E_INVALID;
+    *out = nullptr;
+    int dev = 0, sms = 0;
+    if (!device_ok(&dev, &sms)) return NXM_E_NO_DEVICE;
+    nxm_pipeline* p = new (std::nothrow) nxm_pipeline();
+    if (!p) return NXM_E_OOM;
+    p->device = dev;
+    p->sm_count = sms;
+    *out = p;
+    return NXM_OK;
+}
+
+void nxm_pipeline_destroy(nxm_pipeline* p) { delete p; }
+
+int nxm_state_create(const nxm_capacities* caps, nxm_state** out) {
+    if (!out) return NXM_E_INVALID;
+    *out = nullptr;
+    int dev = 0, sms = 0;
+    if (!device_ok(&dev, &sms)) return NXM_E_NO_DEVICE;
+    nxm_capacities c = caps ? *caps : nxm_capacities{32768u, 65536u};
+    nxm_state* s = new (std::nothrow) nxm_state();
+    if (!s) return NXM_E_OOM;
+    s->device = dev;
+    s->sm_count = sms;
+    int rc = NXM_OK;
+    if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess) rc = NXM_E_CUDA;
+    if (!rc && dalloc(&s->d_params, 1) != cudaSuccess) rc = NXM_E_OOM;
+    if (!rc && dalloc(&s->d_counters, 1) != cudaSuccess) rc = NXM_E_OOM;
+    if (!rc && cudaMallocHost(reinterpret_cast<void**>(&s->h_counters), sizeof(Counters)) != cudaSuccess) rc = NXM_E_OOM;
+    if (!rc && dalloc(&s->d_colliders, MAX_COLLIDERS) != cudaSuccess) rc = NXM_E_OOM;
+    if (!rc && cudaMemsetAsync(s->d_counters, 0, sizeof(Counters), s->stream) != cudaSuccess) rc = NXM_E_CUDA;
+    if (!rc) rc = alloc_grid(s, c.grid_size);
+    if (!rc) rc = reserve_particles(s, std::max<uint32_t>(c.particles_capacity, 1));
+    if (!rc) rc = sync_params(s);
+    if (rc) {
+        nxm_state_destroy(s);
+        (void)cudaGetLastError();
+        return rc;
+    }
+    *out = s;
+    return NXM_OK;
+}
+
+void nxm_state_destroy(nxm_state* s) {
+    if (!s) return;
+    if (s->stream) cudaStreamSynchronize(s->stream);
+    invalidate_graph(s);
+    free_grid(s);
+    dfree(s->kin); dfree(s->def); dfree(s->pstate); dfree(s->pcode); dfree(s->phdr); dfree(s->sorted);
+    dfree(s->d_materials); dfree(s->d_colliders); dfree(s->d_tri); dfree(s->d_params); dfree(s->d_counters);
+    dfree(s->d_pack); dfree(s->d_offsets);
+    if (s->h_counters) cudaFreeHost(s->h_counters);
+    if (s->stream) cudaStreamDestroy(s->stream);
+    delete s;
+}
+
+int nxm_state_set_simulation_params(nxm_state* s, const nxm_simulation_params* p) {
+    if (!s || !p) return NXM_E_INVALID;
+    if (!(p->dt > 0.f)) return NXM_E_INVALID;
+    std::memcpy(s->gravity, p->gravity, sizeof(s->gravity));
+    s->base_dt = p->dt;
+    s->dt = p->dt;
+    s->params_dirty = true;
+    return NXM_OK;
+}
+
+int nxm_state_write_substep_params(nxm_state* s, uint32_t num_substeps) {
+    if (!s) return NXM_E_INVALID;
+    s->dt = s->base_dt / (float)std::max<uint32_t>(num_substeps, 1u);
+    s->params_dirty = true;
+    return NXM_OK;
+}
+
+int nxm_state_set_cell_width(nxm_state* s, float cell_width, uint32_t grid_capacity) {
+    if (!s || !(cell_width > 0.f) || grid_capacity == 0 || grid_capacity > (1u << 26)) return NXM_E_INVALID;
+    s->dx = cell_width;
+    int rc = alloc_grid(s, grid_capacity);
+    if (rc) return rc;
+    NXM_TRY(cudaStreamSynchronize(s->stream));
+    s->params_dirty = true;
+    return NXM_OK;
+}
+
+int nxm_state_set_colliders(nxm_state* s, const nxm_collider* cols, uint32_t ncol, const float* tri, uint32_t ntri) {
+    if (!s) return NXM_E_INVALID;
+    if (ncol > (uint32_t)MAX_COLLIDERS) return NXM_E_INVALID;
+    if (ncol && !cols) return NXM_E_INVALID;
+    std::vector<DevCollider> dc(ncol);
+    for (uint32_t i = 0; i < ncol; ++i) {
+        const nxm_collider& c = cols[i];
+        DevCollider& d = dc[i];
+        std::memset(&d, 0, sizeof(d));
+        std::memcpy(d.a, c.shape_a, 16);
+        std::memcpy(d.b, c.shape_b, 16);
+        std::memcpy(d.c, c.shape_c, 16);
+        std::memcpy(d.rot, c.rotation, 16);
+        std::memcpy(d.tra, c.translation, 12);
+        std::memcpy(d.linvel, c.linvel, 12);
+        std::memcpy(d.angvel, c.angvel, 12);
+        std::memcpy(d.local_com, c.local_com, 12);
+        d.type = f_bits(c.shape_a[3]);
+        d.bc_type = c.bc_type;
+        d.bc_friction = c.bc_friction;
+        d.tri_first = c.tri_first;
+        d.tri_count = c.tri_count;
+        if (d.type != SHAPE_BALL && d.type != SHAPE_CUBOID && d.type != SHAPE_CAPSULE) return NXM_E_UNSUPPORTED;
+    }
+    (void)tri;
+    (void)ntri;
+    NXM_TRY(cudaStreamSynchronize(s->stream));
+    if (ncol)
+        NXM_TRY(cudaMemcpyAsync(s->d_colliders, dc.data(), sizeof(DevCollider) * ncol, cudaMemcpyHostToDevice,
+                                s->stream));
+    NXM_TRY(cudaStreamSynchronize(s->stream));
+    const bool had = !s->colliders.empty();
+    s->colliders = dc;
+    if (had != !s->colliders.empty()) invalidate_graph(s);
+    s->params_dirty = true;
+    return NXM_OK;
+}
+
+int nxm_state_set_collider_velocity(nxm_state* s, uint32_t index, const float linvel[3], const float angvel[3]) {
+    if (!s || !linvel || !angvel || index >= s->colliders.size()) return NXM_E_INVALID;
+    float buf[8] = {linvel[0], linvel[1], linvel[2], 0.f, angvel[0], angvel[1], angvel[2], 0.f};
+    char* base = reinterpret_cast<char*>(s->d_colliders + index);
+    NXM_TRY(cudaMemcpyAsync(base + offsetof(DevCollider, linvel), buf, 32, cudaMemcpyHostToDevice, s->stream));
+    NXM_TRY(cudaStreamSynchronize(s->stream));
+    return NXM_OK;
+}
+
+int nxm_state_read_collider_pose(nxm_state* s, uint32_t index, float out[7]) {
+    if (!s || !out || index >= s->colliders.size()) return NXM_E_INVALID;
+    DevCollider c;
+    NXM_TRY(cudaMemcpyAsync(&c, s->d_colliders + index, sizeof(c), cudaMemcpyDeviceToHost, s->stream));
+    NXM_TRY(cudaStreamSynchronize(s->stream));
+    std::memcpy(out, c.rot, 16);
+    std::memcpy(out + 4, c.tra, 12);
+    return NXM_OK;
+}
+
+int nxm_state_set_use_cpic(nxm_state* s, int enabled) {
+    if (!s) return NXM_E_INVALID;
+    if (enabled) return NXM_E_UNSUPPORTED;
+    s->use_cpic = false;
+    s->params_dirty = true;
+    return NXM_OK;
+}
+
+int nxm_state_set_deterministic(nxm_state* s, int enabled) {
+    if (!s) return NXM_E_INVALID;
+    if (s->deterministic != (enabled != 0)) invalidate_graph(s);
+    s->deterministic = enabled != 0;
+    return NXM_OK;
+}
+
+int nxm_particles_append_soa(nxm_state* s, const nxm_particles_soa* p, uint32_t count) {
+    if (!s) return NXM_E_INVALID;
+    return upload_particles(s, p, count);
+}
+
+int nxm_particles_append(nxm_state* s, const nxm_particle* particles, uint32_t count) {
+    if (!s || (count && !particles)) return NXM_E_INVALID;
+    if (count == 0) return NXM_OK;
+    std::vector<float> pos(3 * (size_t)count), vel(3 * (size_t)count), F(9 * (size_t)count), A(9 * (size_t)count);
+    std::vector<float> vgd(count), v0(count), rad(count), mass(count), damp(count), phase(count), bf(count);
+    std::vector<uint32_t> gid(count), en(count), fx(count);
+    std::vector<nxm_particle_model> models(count);
+    for (uint32_t i = 0; i < count; ++i) {
+        const nxm_particle& q = particles[i];
+        std::memcpy(&pos[3 * (size_t)i], q.position, 12);
+        std::memcpy(&vel[3 * (size_t)i], q.velocity, 12);
+        std::memcpy(&F[9 * (size_t)i], q.def_grad, 36);
+        std::memcpy(&A[9 * (size_t)i], q.affine, 36);
+        vgd[i] = q.vel_grad_det; v0[i] = q.init_volume; rad[i] = q.init_radius; mass[i] = q.mass;
+        damp[i] = q.damping; phase[i] = q.phase; bf[i] = q.boundary_friction;
+        gid[i] = q.group_id; en[i] = q.enabled; fx[i] = q.fixed; models[i] = q.model;
+    }
+    nxm_particles_soa soa{pos.data(), vel.data(), F.data(), A.data(), vgd.data(), v0.data(), rad.data(), mass.data(),
+                          damp.data(), phase.data(), bf.data(), gid.data(), en.data(), fx.data(), models.data()};
+    return upload_particles(s, &soa, count);
+}
+
+uint32_t nxm_particles_len(const nxm_state* s) { return s ? s->n : 0u; }
+
+int nxm_particles_swap_remove(nxm_state* s, const uint32_t* slots, uint32_t count, uint32_t* remaps,
+                              uint32_t* num_remaps) {
+    if (!s || (count && !slots)) return NXM_E_INVALID;
+    std::vector<uint32_t> t(slots, slots + count);
+    std::sort(t.begin(), t.end(), [](uint32_t a, uint32_t b) { return a > b; });
+    t.erase(std::unique(t.begin(), t.end()), t.end());
+    uint32_t nr = 0;
+    NXM_TRY(cudaStreamSynchronize(s->stream));
+    for (uint32_t slot : t) {
+        if (slot >= s->n) continue;
+        const uint32_t last = s->n - 1;
+        if (slot != last) {
+            NXM_TRY(cudaMemcpyAsync(s->kin + slot, s->kin + last, sizeof(PKin), cudaMemcpyDeviceToDevice, s->stream));
+            NXM_TRY(cudaMemcpyAsync(s->def + slot, s->def + last, sizeof(PDef), cudaMemcpyDeviceToDevice, s->stream));
+            NXM_TRY(cudaMemcpyAsync(s->pstate + slot, s->pstate + last, sizeof(float4), cudaMemcpyDeviceToDevice,
+                                    s->stream));
+            s->init_radius[slot] = s->init_radius[last];
+            s->phase[slot] = s->phase[last];
+            s->boundary_friction[slot] = s->boundary_friction[last];
+            s->group_id[slot] = s->group_id[last];
+            if (remaps && nr < count) {
+                remaps[2 * nr] = last;
+                remaps[2 * nr + 1] = slot;
+            }
+            ++nr;
+        }
+        s->init_radius.pop_back();
+        s->phase.pop_back();
+        s->boundary_friction.pop_back();
+        s->group_id.pop_back();
+        s->n -= 1;
+    }
+    NXM_TRY(cudaStreamSynchronize(s->stream));
+    if (num_remaps) *num_remaps = nr;
+    s->params_dirty = true;
+    return NXM_OK;
+}
+
+int nxm_particles_shift_remove(nxm_state* s, uint32_t start, uint32_t end) {
+    if (!s || start > end || end > s->n) return NXM_E_INVALID;
+    const uint32_t removed = end - start;
+    if (removed == 0) return NXM_OK;
+    const uint32_t tail = s->n - end;
+    if (tail) {
+        PKin* tk; PDef* td; float4* ts;
+        NXM_TRY(dalloc(&tk, tail));
+        NXM_TRY(dalloc(&td, tail));
+        NXM_TRY(dalloc(&ts, tail));
+        NXM_TRY(cudaMemcpyAsync(tk, s->kin + end, sizeof(PKin) * tail, cudaMemcpyDeviceToDevice, s->stream));
+        NXM_TRY(cudaMemcpyAsync(td, s->def + end, sizeof(PDef) * tail, cudaMemcpyDeviceToDevice, s->stream));
+        NXM_TRY(cudaMemcpyAsync(ts, s->pstate + end, sizeof(float4) * tail, cudaMemcpyDeviceToDevice, s->stream));
+        NXM_TRY(cudaMemcpyAsync(s->kin + start, tk, sizeof(PKin) * tail, cudaMemcpyDeviceToDevice, s->stream));
+        NXM_TRY(cudaMemcpyAsync(s->def + start, td, sizeof(PDef) * tail, cudaMemcpyDeviceToDevice, s->stream));
+        NXM_TRY(cudaMemcpyAsync(s->pstate + start, ts, sizeof(float4) * tail, cudaMemcpyDeviceToDevice, s->stream));
+        NXM_TRY(cudaStreamSynchronize(s->stream));
+        cudaFree(tk); cudaFree(td); cudaFree(ts);
+    }
+    auto erase = [&](auto& v) { v.erase(v.begin() + start, v.begin() + end); };
+    erase(s->init_radius);
+    erase(s->phase);
+    erase(s->boundary_friction);
+    erase(s->group_id);
+    s->n -= removed;
+    s->params_dirty = true;
+    return NXM_OK;
+}
+
+int nxm_step(nxm_pipeline* pipeline, nxm_state* s, nxm_timestamps* ts) {
+    if (!pipeline || !s) return NXM_E_INVALID;
+    int rc = ensure_ready(s);
+    if (rc) return rc;
+    if (s->n == 0) return NXM_OK;
+    if (ts) {
+        cudaEvent_t ev[5];
+        for (auto& e : ev) NXM_TRY(cudaEventCreate(&e));
+        int k = enqueue_step(s, s->stream, ev);
+        s->launches += (uint64_t)k;
+        cudaError_t e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaEventSynchronize(ev[4]);
+        if (e == cudaSuccess) {
+            cudaEventElapsedTime(&ts->sort_ms, ev[0], ev[1]);
+            cudaEventElapsedTime(&ts->p2g_ms, ev[1], ev[2]);
+            cudaEventElapsedTime(&ts->grid_update_ms, ev[2], ev[3]);
+            cudaEventElapsedTime(&ts->g2p_ms, ev[3], ev[4]);
+            cudaEventElapsedTime(&ts->total_ms, ev[0], ev[4]);
+        }
+        for (auto& x : ev) cudaEventDestroy(x);
+        return e == cudaSuccess ? NXM_OK : NXM_E_CUDA;
+    }
+    if (!s->graph_valid) {
+        rc = build_graph(s);
+        if (rc) return rc;
+    }
+    NXM_TRY(cudaGraphLaunch(s->graph, s->stream));
+    s->launches += (uint64_t)s->graph_kernels;
+    return NXM_OK;
+}
+
+int nxm_debug_sort(nxm_pipeline* pipeline, nxm_state* s, int with_p2g) {
+    if (!pipeline || !s) return NXM_E_INVALID;
+    int rc = ensure_ready(s);
+    if (rc) return rc;
+    if (s->n == 0) return NXM_OK;
+    DevPtrs P = dev_ptrs(s);
+    LaunchCfg c = launch_cfg(s);
+    fast::launch_sort(P, c, s->deterministic, s->stream);
+    s->launches += (uint64_t)sort_launches(s->deterministic);
+    if (with_p2g) {
+        if (s->deterministic) exact::launch_p2g_gather(P, c, s->stream);
+        else fast::launch_p2g(P, c, s->stream);
+        s->launches += 1;
+    }
+    NXM_TRY(cudaGetLastError());
+    NXM_TRY(cudaStreamSynchronize(s->stream));
+    return NXM_OK;
+}
+
+int nxm_synchronize(nxm_state* s) {
+    if (!s) return NXM_E_INVALID;
+    NXM_TRY(cudaStreamSynchronize(s->stream));
+    uint32_t bits = 0;
+    int rc = nxm_state_status(s, &bits, 0);
+    if (rc) return rc;
+    if (bits & NXM_STATUS_HASH_FULL) return NXM_E_HASH_FULL;
+    if (bits & (NXM_STATUS_BLOCK_CAPACITY | NXM_STATUS_MISSING_BLOCK | NXM_STATUS_SORT_CAPACITY)) return NXM_E_CAPACITY;
+    return NXM_OK;
+}
+
+int nxm_state_status(nxm_state* s, uint32_t* bits, int clear) {
+    if (!s || !bits) return NXM_E_INVALID;
+    NXM_TRY(cudaMemcpyAsync(s->h_counters, s->d_counters, sizeof(Counters), cudaMemcpyDeviceToHost, s->stream));
+    NXM_TRY(cudaStreamSynchronize(s->stream));
+    *bits = s->h_counters->status;
+    if (clear) {
+        uint32_t z = 0;
+        NXM_TRY(cudaMemcpyAsync(reinterpret_cast<char*>(s->d_counters) + offsetof(Counters, status), &z, 4,
+                                cudaMemcpyHostToDevice, s->stream));
+        NXM_TRY(cudaStreamSynchronize(s->stream));
+    }
+    return NXM_OK;
+}
+
+uint64_t nxm_state_kernel_launches(const nxm_state* s) { return s ? s->launches : 0; }
+
+void* nxm_state_cuda_stream(const nxm_state* s) { return s ? reinterpret_cast<void*>(s->stream) : nullptr; }
+
+// ---- readback ---------------------------------------------------------------
+
+int nxm_read_positions(nxm_state* s, float* out) {
+    if (!s) return NXM_E_INVALID;
+    static const int off[3] = {0, 1, 2};
+    return pack_read(s, s->kin, sizeof(PKin), off, 3, out);
+}
+int nxm_read_velocities(nxm_state* s, float* out) {
+    if (!s) return NXM_E_INVALID;
+    static const int off[3] = {4, 5, 6};
+    return pack_read(s, s->kin, sizeof(PKin), off, 3, out);
+}
+int nxm_read_affine(nxm_state* s, float* out) {
+    if (!s) return NXM_E_INVALID;
+    static const int off[9] = {8, 9, 10, 12, 13, 14, 16, 17, 18};
+    return pack_read(s, s->kin, sizeof(PKin), off, 9, out);
+}
+int nxm_read_vel_grad_det(nxm_state* s, float* out) {
+    if (!s) return NXM_E_INVALID;
+    static const int off[1] = {11};
+    return pack_read(s, s->kin, sizeof(PKin), off, 1, out);
+}
+int nxm_read_mass(nxm_state* s, float* out) {
+    if (!s) return NXM_E_INVALID;
+    static const int off[1] = {3};
+    return pack_read(s, s->kin, sizeof(PKin), off, 1, out);
+}
+int nxm_read_enabled(nxm_state* s, uint32_t* out) {
+    if (!s || !out) return NXM_E_INVALID;
+    static const int off[1] = {7};
+    int rc = pack_read(s, s->kin, sizeof(PKin), off, 1, out);
+    if (rc) return rc;
+    for (uint32_t i = 0; i < s->n; ++i) out[i] = (out[i] & PFLAG_ENABLED) ? 1u : 0u;
+    return NXM_OK;
+}
+int nxm_read_def_grad(nxm_state* s, float* out) {
+    if (!s) return NXM_E_INVALID;
+    static const int off[9] = {0, 1, 2, 4, 5, 6, 8, 9, 10};
+    return pack_read(s, s->def, sizeof(PDef), off, 9, out);
+}
+int nxm_read_models(nxm_state* s, nxm_particle_model* out) {
+    if (!s || !out) return NXM_E_INVALID;
+    if (s->n == 0) return NXM_OK;
+    std::vector<uint32_t> mid(s->n);
+    static const int off_m[1] = {11};
+    int rc = pack_read(s, s->def, sizeof(PDef), off_m, 1, mid.data());
+    if (rc) return rc;
+    std::vector<float> st(4 * (size_t)s->n);
+    static const int off_s[4] = {0, 1, 2, 3};
+    rc = pack_read(s, s->pstate, sizeof(float4), off_s, 4, st.data());
+    if (rc) return rc;
+    for (uint32_t i = 0; i < s->n; ++i) {
+        if (mid[i] >= s->materials.size()) return NXM_E_INVALID;
+        const Material& m = s->materials[mid[i]];
+        out[i].tag = m.tag;
+        const int ns = model_state_words(m.tag);
+        for (int k = 0; k < MODEL_WORDS; ++k) out[i].data[k] = k < ns ? f_bits(st[4 * (size_t)i + k]) : f_bits(m.w[k]);
+    }
+    return NXM_OK;
+}
+
+// ---- grid inspection ----------------------------------------------------------
+
+int nxm_grid_num_blocks(nxm_state* s, uint32_t* out) {
+    if (!s || !out) return NXM_E_INVALID;
+    NXM_TRY(cudaMemcpyAsync(s->h_counters, s->d_counters, sizeof(Counters), cudaMemcpyDeviceToHost, s->stream));
+    NXM_TRY(cudaStreamSynchronize(s->stream));
+    *out = s->h_counters->num_blocks;
+    return NXM_OK;
+}
+
+int nxm_grid_sorted_len(nxm_state* s, uint32_t* out) {
+    if (!s || !out) return NXM_E_INVALID;
+    NXM_TRY(cudaMemcpyAsync(s->h_counters, s->d_counters, sizeof(Counters), cudaMemcpyDeviceToHost, s->stream));
+    NXM_TRY(cudaStreamSynchronize(s->stream));
+    *out = s->h_counters->sorted_len;
+    return NXM_OK;
+}
+
+int nxm_grid_read_headers(nxm_state* s, int32_t* out, uint32_t max_blocks) {
+    if (!s || !out) return NXM_E_INVALID;
+    uint32_t nb = 0;
+    int rc = nxm_grid_num_blocks(s, &nb);
+    if (rc) return rc;
+    nb = std::min(nb, max_blocks);
+    if (nb == 0) return NXM_OK;
+    std::vector<int4> v(nb);
+    std::vector<uint32_t> f(nb), np(nb), nw(nb), cur((size_t)nb * NUM_BUCKETS), nbh((size_t)nb * NUM_NBH);
+    NXM_TRY(cudaMemcpyAsync(v.data(), s->bvid, sizeof(int4) * nb, cudaMemcpyDeviceToHost, s->stream));
+    NXM_TRY(cudaMemcpyAsync(f.data(), s->first, 4 * nb, cudaMemcpyDeviceToHost, s->stream));
+    NXM_TRY(cudaMemcpyAsync(np.data(), s->nprim, 4 * nb, cudaMemcpyDeviceToHost, s->stream));
+    NXM_TRY(cudaMemcpyAsync(nw.data(), s->nwx, 4 * nb, cudaMemcpyDeviceToHost, s->stream));
+    NXM_TRY(cudaMemcpyAsync(cur.data(), s->cursors, 4 * cur.size(), cudaMemcpyDeviceToHost, s->stream));
+    NXM_TRY(cudaMemcpyAsync(nbh.data(), s->nbh, 4 * nbh.size(), cudaMemcpyDeviceToHost, s->stream));
+    NXM_TRY(cudaStreamSynchronize(s->stream));
+    for (uint32_t b = 0; b < nb; ++b) {
+        int32_t* o = out + 23 * (size_t)b;
+        o[0] = v[b].x; o[1] = v[b].y; o[2] = v[b].z;
+        o[3] = (int32_t)f[b]; o[4] = (int32_t)np[b]; o[5] = (int32_t)nw[b];
+        for (int k = 0; k < NUM_BUCKETS; ++k) o[6 + k] = (int32_t)cur[(size_t)b * NUM_BUCKETS + k];
+        for (int k = 0; k < NUM_NBH; ++k) o[16 + k] = (int32_t)nbh[(size_t)b * NUM_NBH + k];
+    }
+    return NXM_OK;
+}
+
+int nxm_grid_read_sorted_ids(nxm_state* s, uint32_t* out, uint32_t max_len) {
+    if (!s || !out) return NXM_E_INVALID;
+    uint32_t len = 0;
+    int rc = nxm_grid_sorted_len(s, &len);
+    if (rc) return rc;
+    len = std::min(len, std::min(max_len, s->pcap * 8u));
+    if (len == 0) return NXM_OK;
+    NXM_TRY(cudaMemcpyAsync(out, s->sorted, 4 * (size_t)len, cudaMemcpyDeviceToHost, s->stream));
+    NXM_TRY(cudaStreamSynchronize(s->stream));
+    return NXM_OK;
+}
+
+int nxm_grid_read_nodes(nxm_state* s, float* out, uint32_t max_blocks) {
+    if (!s || !out) return NXM_E_INVALID;
+    uint32_t nb = 0;
+    int rc = nxm_grid_num_blocks(s, &nb);
+    if (rc) return rc;
+    nb = std::min(nb, max_blocks);
+    if (nb == 0) return NXM_OK;
+    NXM_TRY(cudaMemcpyAsync(out, s->nodes, sizeof(float4) * 64 * (size_t)nb, cudaMemcpyDeviceToHost, s->stream));
+    NXM_TRY(cudaStreamSynchronize(s->stream));
+    return NXM_OK;
+}
+
+}  // extern "C"

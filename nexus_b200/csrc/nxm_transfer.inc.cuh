@@ -1,0 +1,240 @@
+// Grid update and G2P + particle update kernels, included twice: by
+// nxm_transfer_fast.cu (multiply-adds may fuse) and by nxm_transfer_det.cu
+// (built with --fmad=false, every multiply and add rounded separately in the
+// reference's order).  NXM_NS names the namespace of the instantiation.
+#include "nxm_device.cuh"
+#include "nxm_kernels.h"
+
+#ifndef NXM_NS
+#error "define NXM_NS before including nxm_transfer.inc.cuh"
+#endif
+
+namespace nxm {
+namespace NXM_NS {
+namespace {
+
+__device__ __forceinline__ void set_status(Counters* c, uint32_t bit) { atomicOr(&c->status, bit); }
+
+__device__ __forceinline__ v3 col_vel_at(const DevCollider& c, v3 p) {
+    // dynamics/body.rs:239-250 velocity_at_point
+    v3 lin = mk(c.linvel[0], c.linvel[1], c.linvel[2]);
+    v3 ang = mk(c.angvel[0], c.angvel[1], c.angvel[2]);
+    v3 com = mk(c.com[0], c.com[1], c.com[2]);
+    return lin + cross(ang, p - com);
+}
+
+struct Collision {
+    v3 normal;
+    float distance;
+    uint32_t closest;
+};
+
+// grid_update_collide.rs:30-99 collide() for analytic shapes (ball, cuboid,
+// capsule).  Trimesh colliders are rejected on the host for now.
+__device__ __forceinline__ Collision collide(const DevCollider* cols, uint32_t ncol, float dx, v3 point) {
+    const float cap = dx * 1.5f;
+    Collision col;
+    col.normal = splat(0.f);
+    col.distance = MAX_FLT;
+    col.closest = 0;
+    for (uint32_t i = 0; i < ncol; ++i) {
+        const DevCollider& c = cols[i];
+        quat q = quat{c.rot[0], c.rot[1], c.rot[2], c.rot[3]};
+        v3 tra = mk(c.tra[0], c.tra[1], c.tra[2]);
+        v3 local = qrot(qconj(q), point - tra);
+        Proj pr;
+        if (c.type == SHAPE_BALL) pr = ball_project_local(c.a[0], local);
+        else if (c.type == SHAPE_CUBOID) pr = cuboid_project_local(mk(c.a[0], c.a[1], c.a[2]), local);
+        else if (c.type == SHAPE_CAPSULE)
+            pr = capsule_project_local(mk(c.a[0], c.a[1], c.a[2]), mk(c.b[0], c.b[1], c.b[2]), c.b[3], local);
+        else { pr.point = local; pr.inside = false; }
+        pr.point = qrot(q, pr.point) + tra;
+        v3 dpt = pr.point - point;
+        v3 ad = vabs(dpt);
+        bool within = ad.x <= cap && ad.y <= cap && ad.z <= cap;
+        if (pr.inside || within) {
+            float sign = pr.inside ? -1.0f : 1.0f;
+            float distance = length(dpt);
+            v3 normal = dpt / (distance * -sign);
+            float sd = sign * distance;
+            if (sd < col.distance) {
+                col.distance = sd;
+                col.normal = normal;
+                col.closest = i;
+            }
+        }
+    }
+    return col;
+}
+
+// grid_update.rs:21-88 + grid_update_collide.rs:102-183, one thread per node.
+__global__ void __launch_bounds__(256) k_grid_update(DevPtrs P) {
+    __shared__ DevCollider scol[MAX_COLLIDERS];
+    const Params prm = *P.params;
+    const uint32_t ncol = prm.use_cpic ? 0u : min(prm.ncol, (uint32_t)MAX_COLLIDERS);
+    for (uint32_t i = threadIdx.x; i < ncol * (sizeof(DevCollider) / 4); i += blockDim.x)
+        reinterpret_cast<uint32_t*>(scol)[i] = reinterpret_cast<const uint32_t*>(P.colliders)[i];
+    __syncthreads();
+    const float dx = prm.dx, dt = prm.dt;
+    const v3 g = mk(prm.gravity[0], prm.gravity[1], prm.gravity[2]);
+    const float lim = dx / dt;
+    const uint32_t total = P.counters->num_blocks * 64u;
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+        float4 nd = P.nodes[t];
+        const float mass = nd.w;
+        const float inv_mass = mass > 0.f ? 1.0f / mass : 0.0f;
+        v3 v = (mk(nd.x, nd.y, nd.z) + g * (mass * dt)) * inv_mass;
+        v = vclamp(v, -lim, lim);
+        if (ncol > 0) {
+            const uint32_t b = t >> 6, k = t & 63u;
+            int4 vid = P.bvid[b];
+            v3 cell_pt = mk((float)(vid.x * 4 + (int)(k & 3u)), (float)(vid.y * 4 + (int)((k >> 2) & 3u)),
+                            (float)(vid.z * 4 + (int)(k >> 4))) * dx;
+            Collision c = collide(scol, ncol, dx, cell_pt);
+            if (c.distance != MAX_FLT) {
+                const DevCollider& cc = scol[c.closest];
+                v3 bv = col_vel_at(cc, cell_pt);
+                v3 delta = v - bv;
+                float nv = dot(delta, c.normal);
+                const float margin = dx;
+                if (c.distance <= margin) {
+                    v = bv + bc_project(cc.bc_type, cc.bc_friction, delta, c.normal);
+                } else if (-nv * dt > c.distance - margin) {
+                    v3 excess = c.normal * (nv + (c.distance - margin) / dt);
+                    v = v - excess;
+                }
+            }
+        }
+        P.nodes[t] = make_float4(v.x, v.y, v.z, mass);
+    }
+}
+
+// g2p.rs:42-347 (non-CPIC) fused with particle_update.rs:60-201.
+// One CTA per active block (grid-stride): the 6x6x6 node-velocity halo of the
+// block and its +1 neighbours is staged in shared memory, then each thread
+// gathers and updates one of the block's primary particles.
+__global__ void __launch_bounds__(256) k_g2p_update(DevPtrs P) {
+    __shared__ float4 halo[216];
+    const Params prm = *P.params;
+    const float dx = prm.dx, dt = prm.dt;
+    const float inv_d = 4.0f / (dx * dx);
+    const uint32_t nb = P.counters->num_blocks;
+    for (uint32_t b = blockIdx.x; b < nb; b += gridDim.x) {
+        for (uint32_t t = threadIdx.x; t < 216u; t += blockDim.x) {
+            const uint32_t tx = t % 6u, ty = (t / 6u) % 6u, tz = t / 36u;
+            const uint32_t ox = tx >= 4u, oy = ty >= 4u, oz = tz >= 4u;
+            const uint32_t oct = ox * 4u + oy * 2u + oz;
+            const uint32_t blk = oct == 0 ? b : P.nbh[b * NUM_NBH + oct - 1u];
+            float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (blk != NONE) {
+                float4 nd = P.nodes[blk * 64u + (tx - 4u * ox) + 4u * (ty - 4u * oy) + 16u * (tz - 4u * oz)];
+                v = make_float4(nd.x, nd.y, nd.z, 0.f);
+            }
+            halo[t] = v;
+        }
+        __syncthreads();
+        const uint32_t first = P.first[b], np = P.nprim[b];
+        for (uint32_t k = threadIdx.x; k < np; k += blockDim.x) {
+            const uint32_t pid = P.sorted[first + k];
+            float4* kr = reinterpret_cast<float4*>(&P.kin[pid]);
+            const float4 xm = kr[0];
+            const float4 vf = kr[1];
+            uint32_t flags = __float_as_uint(vf.w);
+            const v3 pt = mk(xm.x, xm.y, xm.z);
+            float mass = xm.w;
+
+            // ---- G2P (g2p.rs:150-270)
+            v3 velocity = splat(0.f);
+            m3 grad = mzero();
+            float vgd = 0.f;
+            if (flags & PFLAG_ENABLED) {
+                const v3 ref = assoc_cell_of(dx, pt) * dx - pt;
+                const v3 w0 = kernel_eval_all(-ref.x / dx);
+                const v3 w1 = kernel_eval_all(-ref.y / dx);
+                const v3 w2 = kernel_eval_all(-ref.z / dx);
+                const CellInfo ci = cell_info(dx, pt);
+                const uint32_t packed = ci.ax + 6u * ci.ay + 36u * ci.az;
+#pragma unroll
+                for (int i = 0; i < 27; ++i) {
+                    int sx, sy, sz;
+                    nbh_shift(i, sx, sy, sz);
+                    const float4 h = halo[packed + (uint32_t)(sx + 6 * sy + 36 * sz)];
+                    const v3 cv = mk(h.x, h.y, h.z);
+                    const v3 dpt = ref + mk((float)sx, (float)sy, (float)sz) * dx;
+                    const float weight = vget(w0, sx) * vget(w1, sy) * vget(w2, sz);
+                    velocity = velocity + cv * weight;
+                    grad = grad + outer(cv, dpt) * (weight * inv_d);
+                    vgd += weight * inv_d * dot(cv, dpt);
+                }
+            }
+
+            // ---- particle update (particle_update.rs:60-201, non-CPIC: Cdf = 0)
+            const float4* dr = reinterpret_cast<const float4*>(&P.def[pid]);
+            const float4 d0 = dr[0], d1 = dr[1], d2 = dr[2];
+            m3 F = mkm(mk(d0.x, d0.y, d0.z), mk(d1.x, d1.y, d1.z), mk(d2.x, d2.y, d2.z));
+            const float init_volume = d0.w, damping = d1.w;
+            const uint32_t mid = __float_as_uint(d2.w);
+            const Material& mat = P.materials[mid];
+            const uint32_t tag = mat.tag;
+
+            v3 v = velocity;
+            const float vl = length(v);
+            if (vl > dx / dt) v = ((v / vl) * dx) / dt;
+            v = v / (1.0f + damping * dt);
+            if (flags & PFLAG_FIXED) v = splat(0.f);
+            const v3 np_ = pt + v * dt;
+            const m3 A = grad;
+            if (tag != MODEL_FLUID) {
+                F = F + (A * dt) * F;
+            } else {
+                const float fd0 = F.c0.x;
+                float rate = vgd * dt / 3.0f;
+                rate = rclamp(rate, -0.1f, 0.1f);
+                const float nd = rclamp(fd0 + rate * fd0, 0.5f, 2.0f);
+                F = diag(splat(nd));
+            }
+            float st[4] = {0.f, 0.f, 0.f, 0.f};
+            if (mat.has_state) {
+                float4 s4 = P.pstate[pid];
+                st[0] = s4.x; st[1] = s4.y; st[2] = s4.z; st[3] = s4.w;
+            }
+            const m3 tau = model_update(tag, mat.w, st, F, A);
+            m3 aff = A * mass - tau * (init_volume * inv_d * dt);
+            v3 new_pos = pt;
+            const bool nan = (np_.x != np_.x) || (np_.y != np_.y) || (np_.z != np_.z);
+            if (!nan && det(F) > 0.0f) {
+                new_pos = np_;
+            } else {
+                flags &= ~PFLAG_ENABLED;
+                v = splat(0.f);
+                F = mident();
+                aff = mzero();
+                mass = 0.f;
+            }
+            kr[0] = make_float4(new_pos.x, new_pos.y, new_pos.z, mass);
+            kr[1] = make_float4(v.x, v.y, v.z, __uint_as_float(flags));
+            kr[2] = make_float4(aff.c0.x, aff.c0.y, aff.c0.z, vgd);
+            kr[3] = make_float4(aff.c1.x, aff.c1.y, aff.c1.z, 0.f);
+            kr[4] = make_float4(aff.c2.x, aff.c2.y, aff.c2.z, 0.f);
+            float4* dw = reinterpret_cast<float4*>(&P.def[pid]);
+            dw[0] = make_float4(F.c0.x, F.c0.y, F.c0.z, init_volume);
+            dw[1] = make_float4(F.c1.x, F.c1.y, F.c1.z, damping);
+            dw[2] = make_float4(F.c2.x, F.c2.y, F.c2.z, d2.w);
+            if (mat.has_state) P.pstate[pid] = make_float4(st[0], st[1], st[2], st[3]);
+        }
+        __syncthreads();
+    }
+}
+
+}  // namespace
+
+void launch_grid_update(const DevPtrs& P, const LaunchCfg& c, cudaStream_t s) {
+    k_grid_update<<<c.sm_count * 8, 256, 0, s>>>(P);
+}
+
+void launch_g2p_update(const DevPtrs& P, const LaunchCfg& c, cudaStream_t s) {
+    k_g2p_update<<<c.sm_count * 4, 256, 0, s>>>(P);
+}
+
+}  // namespace NXM_NS
+}  // namespace nxm

@@ -1,0 +1,337 @@
+"""Python front-end over the C ABI (include/nexus_mpm.h), mirroring nexus_mpm.
+
+``MpmPipeline`` / ``MpmState`` follow ``src_mpm/pipeline.rs`` (``MpmPipeline::new``,
+``step``; ``MpmState::empty``, ``set_simulation_params``, ``write_substep_params``,
+``set_cell_width``, ``set_coupling``, ``use_cpic``) and ``GpuParticles``
+(``src_mpm/solver/particle.rs``: ``append``, ``swap_remove``, ``shift_remove``,
+``read_positions``).  All work happens in libnexus_mpm.so on an sm_100 GPU;
+loading fails loudly if the library or the GPU is missing.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from .particles import ParticleBatch, COLLIDER_DTYPE
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libnexus_mpm.so")
+
+NXM_OK = 0
+NXM_E_INVALID = -1
+NXM_E_CUDA = -2
+NXM_E_CAPACITY = -3
+NXM_E_HASH_FULL = -4
+NXM_E_NO_DEVICE = -5
+NXM_E_UNSUPPORTED = -6
+NXM_E_OOM = -7
+
+HEADER_FIELDS = 23
+
+# Every function the header declares, with its ctypes signature.
+_vp = C.c_void_p
+_f = C.POINTER(C.c_float)
+_u = C.POINTER(C.c_uint32)
+_i = C.POINTER(C.c_int32)
+_pp = C.POINTER(C.c_void_p)
+
+
+class SimulationParamsC(C.Structure):
+    _fields_ = [("gravity", C.c_float * 3), ("dt", C.c_float)]
+
+
+class CapacitiesC(C.Structure):
+    _fields_ = [("grid_size", C.c_uint32), ("particles_capacity", C.c_uint32)]
+
+
+class ParticlesSoAC(C.Structure):
+    _fields_ = [(name, C.c_void_p) for name in (
+        "position", "velocity", "def_grad", "affine", "vel_grad_det", "init_volume", "init_radius", "mass",
+        "damping", "phase", "boundary_friction", "group_id", "enabled", "fixed", "model")]
+
+
+class TimestampsC(C.Structure):
+    _fields_ = [("sort_ms", C.c_float), ("p2g_ms", C.c_float), ("grid_update_ms", C.c_float),
+                ("g2p_ms", C.c_float), ("total_ms", C.c_float)]
+
+
+SIGNATURES = {
+    "nxm_pipeline_create": (C.c_int, [_pp]),
+    "nxm_pipeline_destroy": (None, [_vp]),
+    "nxm_step": (C.c_int, [_vp, _vp, C.POINTER(TimestampsC)]),
+    "nxm_state_create": (C.c_int, [C.POINTER(CapacitiesC), _pp]),
+    "nxm_state_destroy": (None, [_vp]),
+    "nxm_state_set_simulation_params": (C.c_int, [_vp, C.POINTER(SimulationParamsC)]),
+    "nxm_state_write_substep_params": (C.c_int, [_vp, C.c_uint32]),
+    "nxm_state_set_cell_width": (C.c_int, [_vp, C.c_float, C.c_uint32]),
+    "nxm_state_set_colliders": (C.c_int, [_vp, _vp, C.c_uint32, _f, C.c_uint32]),
+    "nxm_state_set_collider_velocity": (C.c_int, [_vp, C.c_uint32, _f, _f]),
+    "nxm_state_read_collider_pose": (C.c_int, [_vp, C.c_uint32, _f]),
+    "nxm_state_set_use_cpic": (C.c_int, [_vp, C.c_int]),
+    "nxm_state_set_deterministic": (C.c_int, [_vp, C.c_int]),
+    "nxm_particles_append": (C.c_int, [_vp, _vp, C.c_uint32]),
+    "nxm_particles_append_soa": (C.c_int, [_vp, C.POINTER(ParticlesSoAC), C.c_uint32]),
+    "nxm_particles_swap_remove": (C.c_int, [_vp, _u, C.c_uint32, _u, _u]),
+    "nxm_particles_shift_remove": (C.c_int, [_vp, C.c_uint32, C.c_uint32]),
+    "nxm_particles_len": (C.c_uint32, [_vp]),
+    "nxm_read_positions": (C.c_int, [_vp, _f]),
+    "nxm_read_velocities": (C.c_int, [_vp, _f]),
+    "nxm_read_affine": (C.c_int, [_vp, _f]),
+    "nxm_read_def_grad": (C.c_int, [_vp, _f]),
+    "nxm_read_vel_grad_det": (C.c_int, [_vp, _f]),
+    "nxm_read_mass": (C.c_int, [_vp, _f]),
+    "nxm_read_enabled": (C.c_int, [_vp, _u]),
+    "nxm_read_models": (C.c_int, [_vp, _u]),
+    "nxm_grid_num_blocks": (C.c_int, [_vp, _u]),
+    "nxm_grid_read_headers": (C.c_int, [_vp, _i, C.c_uint32]),
+    "nxm_grid_sorted_len": (C.c_int, [_vp, _u]),
+    "nxm_grid_read_sorted_ids": (C.c_int, [_vp, _u, C.c_uint32]),
+    "nxm_grid_read_nodes": (C.c_int, [_vp, _f, C.c_uint32]),
+    "nxm_debug_sort": (C.c_int, [_vp, _vp, C.c_int]),
+    "nxm_synchronize": (C.c_int, [_vp]),
+    "nxm_state_status": (C.c_int, [_vp, _u, C.c_int]),
+    "nxm_error_string": (C.c_char_p, [C.c_int]),
+    "nxm_state_kernel_launches": (C.c_uint64, [_vp]),
+    "nxm_state_cuda_stream": (C.c_void_p, [_vp]),
+}
+
+_LIB = None
+
+
+class NexusError(RuntimeError):
+    def __init__(self, code: int, what: str):
+        self.code = code
+        msg = load().nxm_error_string(code).decode() if _LIB is not None else str(code)
+        super().__init__(f"{what}: {msg} ({code})")
+
+
+def load(path: str = LIB_PATH):
+    """Loads libnexus_mpm.so (no fallback: a missing library is an error)."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not os.path.exists(path):
+        raise FileNotFoundError(f"{path} not built: run python -m nexus_b200.build")
+    lib = C.CDLL(path)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _LIB = lib
+    return lib
+
+
+def _check(rc: int, what: str):
+    if rc != NXM_OK:
+        raise NexusError(rc, what)
+
+
+def _p(a, t=_f):
+    return a.ctypes.data_as(t)
+
+
+class MpmPipeline:
+    """``MpmPipeline::new`` (src_mpm/pipeline.rs:366-382)."""
+
+    def __init__(self):
+        self.lib = load()
+        h = C.c_void_p()
+        _check(self.lib.nxm_pipeline_create(C.byref(h)), "nxm_pipeline_create")
+        self.h = h
+
+    def step(self, state: "MpmState", timestamps: bool = False):
+        """``MpmPipeline::step`` (src_mpm/pipeline.rs:385-526).  Enqueued; with
+        ``timestamps`` it waits and returns the per-phase device times (ms)."""
+        if timestamps:
+            ts = TimestampsC()
+            _check(self.lib.nxm_step(self.h, state.h, C.byref(ts)), "nxm_step")
+            return {k: getattr(ts, k) for k, _ in TimestampsC._fields_}
+        _check(self.lib.nxm_step(self.h, state.h, None), "nxm_step")
+        return None
+
+    def debug_sort(self, state: "MpmState", with_p2g: bool = False):
+        _check(self.lib.nxm_debug_sort(self.h, state.h, int(with_p2g)), "nxm_debug_sort")
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.lib.nxm_pipeline_destroy(self.h)
+            self.h = None
+
+
+class MpmState:
+    """``MpmState::empty`` (src_mpm/pipeline.rs:107-165) plus its setters."""
+
+    def __init__(self, grid_size: int = 32768, particles_capacity: int = 65536):
+        self.lib = load()
+        caps = CapacitiesC(grid_size, particles_capacity)
+        h = C.c_void_p()
+        _check(self.lib.nxm_state_create(C.byref(caps), C.byref(h)), "nxm_state_create")
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.nxm_state_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    # -- parameters -----------------------------------------------------------
+    def set_simulation_params(self, gravity, dt):
+        p = SimulationParamsC((C.c_float * 3)(*gravity), dt)
+        _check(self.lib.nxm_state_set_simulation_params(self.h, C.byref(p)), "set_simulation_params")
+
+    def write_substep_params(self, num_substeps: int):
+        _check(self.lib.nxm_state_write_substep_params(self.h, num_substeps), "write_substep_params")
+
+    def set_cell_width(self, cell_width: float, grid_capacity: int):
+        _check(self.lib.nxm_state_set_cell_width(self.h, cell_width, grid_capacity), "set_cell_width")
+
+    def set_colliders(self, colliders: np.ndarray, tri_vertices=None):
+        cols = np.ascontiguousarray(colliders, dtype=COLLIDER_DTYPE)
+        tri = (np.zeros((0,), np.float32) if tri_vertices is None
+               else np.ascontiguousarray(tri_vertices, np.float32).reshape(-1))
+        _check(self.lib.nxm_state_set_colliders(self.h, cols.ctypes.data_as(C.c_void_p), len(cols), _p(tri),
+                                                tri.size // 9), "set_colliders")
+
+    def set_collider_velocity(self, index: int, linvel, angvel):
+        lv = np.asarray(linvel, np.float32)
+        av = np.asarray(angvel, np.float32)
+        _check(self.lib.nxm_state_set_collider_velocity(self.h, index, _p(lv), _p(av)), "set_collider_velocity")
+
+    def collider_pose(self, index: int) -> np.ndarray:
+        out = np.zeros(7, np.float32)
+        _check(self.lib.nxm_state_read_collider_pose(self.h, index, _p(out)), "read_collider_pose")
+        return out
+
+    def set_use_cpic(self, enabled: bool):
+        _check(self.lib.nxm_state_set_use_cpic(self.h, int(enabled)), "set_use_cpic")
+
+    def set_deterministic(self, enabled: bool):
+        _check(self.lib.nxm_state_set_deterministic(self.h, int(enabled)), "set_deterministic")
+
+    # -- particles --------------------------------------------------------------
+    def append(self, batch: ParticleBatch):
+        """``GpuParticles::append`` (src_mpm/solver/particle.rs:533-565), bulk SoA form."""
+        keep = {}
+
+        def arr(name, dtype):
+            a = np.ascontiguousarray(getattr(batch, name), dtype=dtype)
+            keep[name] = a
+            return a.ctypes.data_as(C.c_void_p)
+
+        soa = ParticlesSoAC(
+            arr("pos", np.float32), arr("vel", np.float32), arr("def_grad", np.float32), arr("aff", np.float32),
+            arr("vel_grad_det", np.float32), arr("init_volume", np.float32), arr("init_radius", np.float32),
+            arr("mass", np.float32), arr("damping", np.float32), arr("phase", np.float32),
+            arr("boundary_friction", np.float32), arr("group_id", np.uint32), arr("enabled", np.uint32),
+            arr("fixed", np.uint32), arr("model", np.uint32))
+        _check(self.lib.nxm_particles_append_soa(self.h, C.byref(soa), batch.n), "append")
+
+    def swap_remove(self, slots):
+        s = np.ascontiguousarray(slots, np.uint32)
+        remaps = np.zeros((max(len(s), 1), 2), np.uint32)
+        nr = C.c_uint32()
+        _check(self.lib.nxm_particles_swap_remove(self.h, _p(s, _u), len(s), _p(remaps, _u), C.byref(nr)),
+               "swap_remove")
+        return [tuple(r) for r in remaps[:nr.value]]
+
+    def shift_remove(self, start: int, end: int):
+        _check(self.lib.nxm_particles_shift_remove(self.h, start, end), "shift_remove")
+
+    def __len__(self):
+        return int(self.lib.nxm_particles_len(self.h))
+
+    # -- readback -----------------------------------------------------------------
+    def _read(self, fn, shape, dtype=np.float32, t=_f):
+        out = np.zeros(shape, dtype)
+        _check(getattr(self.lib, fn)(self.h, _p(out, t)), fn)
+        return out
+
+    def read_positions(self) -> np.ndarray:
+        return self._read("nxm_read_positions", (len(self), 3))
+
+    def read_positions_into(self, out: np.ndarray):
+        """Positions into a caller-provided (n, 3) float32 host array (e.g. pinned)."""
+        assert out.dtype == np.float32 and out.shape == (len(self), 3) and out.flags.c_contiguous
+        _check(self.lib.nxm_read_positions(self.h, _p(out)), "nxm_read_positions")
+
+    def read_velocities(self) -> np.ndarray:
+        return self._read("nxm_read_velocities", (len(self), 3))
+
+    def read_affine(self) -> np.ndarray:
+        return self._read("nxm_read_affine", (len(self), 9))
+
+    def read_def_grad(self) -> np.ndarray:
+        return self._read("nxm_read_def_grad", (len(self), 9))
+
+    def read_vel_grad_det(self) -> np.ndarray:
+        return self._read("nxm_read_vel_grad_det", (len(self),))
+
+    def read_mass(self) -> np.ndarray:
+        return self._read("nxm_read_mass", (len(self),))
+
+    def read_enabled(self) -> np.ndarray:
+        return self._read("nxm_read_enabled", (len(self),), np.uint32, _u)
+
+    def read_models(self) -> np.ndarray:
+        return self._read("nxm_read_models", (len(self), 25), np.uint32, _u)
+
+    def read_particles(self) -> dict:
+        return dict(pos=self.read_positions(), vel=self.read_velocities(), aff=self.read_affine(),
+                    def_grad=self.read_def_grad(), vel_grad_det=self.read_vel_grad_det(), mass=self.read_mass(),
+                    enabled=self.read_enabled(), model=self.read_models())
+
+    # -- grid ------------------------------------------------------------------------
+    def num_blocks(self) -> int:
+        v = C.c_uint32()
+        _check(self.lib.nxm_grid_num_blocks(self.h, C.byref(v)), "grid_num_blocks")
+        return v.value
+
+    def headers(self) -> np.ndarray:
+        nb = self.num_blocks()
+        out = np.zeros((nb, HEADER_FIELDS), np.int32)
+        _check(self.lib.nxm_grid_read_headers(self.h, _p(out, _i), nb), "grid_read_headers")
+        return out
+
+    def sorted_ids(self) -> np.ndarray:
+        v = C.c_uint32()
+        _check(self.lib.nxm_grid_sorted_len(self.h, C.byref(v)), "grid_sorted_len")
+        out = np.zeros(v.value, np.uint32)
+        _check(self.lib.nxm_grid_read_sorted_ids(self.h, _p(out, _u), v.value), "grid_read_sorted_ids")
+        return out
+
+    def nodes(self) -> np.ndarray:
+        nb = self.num_blocks()
+        out = np.zeros((nb, 64, 4), np.float32)
+        _check(self.lib.nxm_grid_read_nodes(self.h, _p(out), nb), "grid_read_nodes")
+        return out
+
+    # -- status ------------------------------------------------------------------------
+    def synchronize(self):
+        _check(self.lib.nxm_synchronize(self.h), "synchronize")
+
+    def status(self, clear: bool = False) -> int:
+        v = C.c_uint32()
+        _check(self.lib.nxm_state_status(self.h, C.byref(v), int(clear)), "state_status")
+        return v.value
+
+    def kernel_launches(self) -> int:
+        return int(self.lib.nxm_state_kernel_launches(self.h))
+
+    def cuda_stream(self) -> int:
+        """The cudaStream_t (as an integer) all of this state's work runs on."""
+        return int(self.lib.nxm_state_cuda_stream(self.h) or 0)
+
+
+def state_from_scene(scene, deterministic: bool = False, grid_capacity: int | None = None) -> MpmState:
+    """Builds a device state for a ``nexus_b200.scenes.Scene``."""
+    st = MpmState(grid_size=grid_capacity or scene.grid_capacity, particles_capacity=scene.n)
+    st.set_cell_width(scene.dx, grid_capacity or scene.grid_capacity)
+    st.set_simulation_params(scene.gravity, scene.dt)
+    st.set_colliders(scene.colliders, scene.tri_vertices if scene.tri_vertices.size else None)
+    st.set_deterministic(deterministic)
+    st.append(scene.particles)
+    return st

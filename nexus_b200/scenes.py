@@ -1,0 +1,137 @@
+"""Seeded synthetic MPM scenes (the benchmark and test workloads).
+
+Random numbers come from SplitMix64 (Steele, Lea & Flood 2014) evaluated on a
+counter, so a scene is a pure function of its seed and sizes; the same arrays
+go to the CPU oracle and to the GPU.
+
+Workloads (all 3D, unit domain, FP32 state):
+  * ``elastic_cube``: dx = 1/64, a 32^3 lattice (2 particles per cell and
+    axis, 32,768 particles) at 0.4 + (i + 1/2) dx/2 with +-dx/4 jitter,
+    neo-Hookean E = 1e5, nu = 0.3, rho = 1000, gravity -9.81 z, slip walls on
+    the six faces, dt = 1e-4.
+  * ``sand_water``: dx = 1/256, a Drucker-Prager sand column (friction 30
+    deg, E = 3.5e5, nu = 0.3, rho = 2700, 100 x 100 x 150 particles =
+    1.5 M) and a weakly compressible water block (bulk modulus 1e5, rho =
+    1000, 100 x 100 x 50 = 0.5 M), 8 particles per cell with +-dx/4 jitter,
+    sticky floor, slip side walls and ceiling, dt = 5e-5.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from .models import ParticleModel, BoundaryCondition
+from .particles import ParticleBatch, box_walls, collider_array
+
+_GOLDEN = np.uint64(0x9E3779B97F4A7C15)
+_M1 = np.uint64(0xBF58476D1CE4E5B9)
+_M2 = np.uint64(0x94D049BB133111EB)
+
+
+def splitmix64(seed: int, count: int, offset: int = 0) -> np.ndarray:
+    """``count`` SplitMix64 outputs for stream ``seed`` starting at ``offset``."""
+    with np.errstate(over="ignore"):
+        i = np.arange(offset + 1, offset + count + 1, dtype=np.uint64)
+        z = np.uint64(seed) + i * _GOLDEN
+        z = (z ^ (z >> np.uint64(30))) * _M1
+        z = (z ^ (z >> np.uint64(27))) * _M2
+        z = z ^ (z >> np.uint64(31))
+    return z
+
+
+def uniform(seed: int, count: int, offset: int = 0) -> np.ndarray:
+    """Uniform doubles in [0, 1) with 53 random bits."""
+    return (splitmix64(seed, count, offset) >> np.uint64(11)).astype(np.float64) * (1.0 / (1 << 53))
+
+
+@dataclass
+class Scene:
+    name: str
+    dx: float
+    dt: float
+    gravity: tuple
+    particles: ParticleBatch
+    colliders: np.ndarray
+    steps: int
+    grid_capacity: int
+    tri_vertices: np.ndarray = field(default_factory=lambda: np.zeros((0, 3), np.float32))
+
+    @property
+    def n(self) -> int:
+        return self.particles.n
+
+
+def lattice_block(origin, counts, dx, seed, stream_offset=0) -> np.ndarray:
+    """Particles at origin + (i + 1/2) dx/2 for i in [0, counts) per axis, each
+    jittered by U(-dx/4, dx/4) per axis; x varies fastest."""
+    nx, ny, nz = counts
+    k, j, i = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    base = np.stack([i.ravel(), j.ravel(), k.ravel()], axis=1).astype(np.float64)
+    pos = np.asarray(origin, np.float64)[None, :] + (base + 0.5) * (dx * 0.5)
+    u = uniform(seed, pos.size, stream_offset).reshape(pos.shape)
+    pos += (u * 2.0 - 1.0) * (0.25 * dx)
+    return pos.astype(np.float32)
+
+
+def grid_capacity_for(n_particles: int, ppc: float = 8.0, slack: float = 4.0) -> int:
+    """Blocks (and hash slots) to reserve: active blocks are roughly the
+    primary blocks (n / (64 ppc)) plus their +1 neighbours; ``slack`` covers
+    both and thin or spread-out scenes."""
+    blocks = max(64, int(n_particles / (64.0 * ppc) * slack) + 64)
+    cap = 1
+    while cap < blocks:
+        cap <<= 1
+    return cap
+
+
+def elastic_cube(n_side: int = 32, seed: int = 1, steps: int = 100) -> Scene:
+    dx = 1.0 / 64.0
+    pos = lattice_block((0.4, 0.4, 0.4), (n_side, n_side, n_side), dx, seed)
+    model = ParticleModel.elastic_neo_hookean(1.0e5, 0.3)
+    batch = ParticleBatch.from_positions(pos, np.float32(dx) / np.float32(4.0), 1000.0, model)
+    cols = collider_array(box_walls(0.0, 1.0, BoundaryCondition.slip(), BoundaryCondition.slip()))
+    return Scene("elastic_cube", dx, 1.0e-4, (0.0, 0.0, -9.81), batch, cols, steps,
+                 grid_capacity_for(batch.n))
+
+
+def sand_water(scale: float = 1.0, seed: int = 2, steps: int = 500) -> Scene:
+    """The 2 M-particle sand + water scene; ``scale`` < 1 shrinks each
+    particle count per axis (for CPU-sized tests) at the same dx."""
+    dx = 1.0 / 256.0
+    s = lambda v: max(2, int(round(v * scale)))
+    sand_counts = (s(100), s(100), s(150))
+    water_counts = (s(100), s(100), s(50))
+    z0 = 4 * dx
+    sand_pos = lattice_block((0.20, 0.40, z0), sand_counts, dx, seed, 0)
+    water_pos = lattice_block((0.45, 0.40, z0), water_counts, dx, seed, sand_pos.size)
+    sand = ParticleBatch.from_positions(sand_pos, np.float32(dx) / np.float32(4.0), 2700.0,
+                                        ParticleModel.sand_with_friction_angle(3.5e5, 0.3, 30.0))
+    water = ParticleBatch.from_positions(water_pos, np.float32(dx) / np.float32(4.0), 1000.0,
+                                         ParticleModel.water(1.0e5))
+    batch = ParticleBatch.concat([sand, water])
+    cols = collider_array(box_walls(0.0, 1.0, BoundaryCondition.stick(), BoundaryCondition.slip()))
+    return Scene("sand_water", dx, 5.0e-5, (0.0, 0.0, -9.81), batch, cols, steps, grid_capacity_for(batch.n))
+
+
+def mixed_materials(n_side: int = 12, seed: int = 7, dx: float = 1.0 / 64.0) -> Scene:
+    """Small test scene with every model on a stack of blocks: linear and
+    neo-Hookean elastic, sand (both backbones), fluid and snow, with random
+    initial velocities so every branch of the update is exercised."""
+    models = [ParticleModel.elastic(2.0e4, 0.25), ParticleModel.elastic_neo_hookean(5.0e4, 0.3),
+              ParticleModel.sand(3.5e5, 0.3), ParticleModel.sand_neo_hookean(2.0e5, 0.3),
+              ParticleModel.water(5.0e4), ParticleModel.snow(1.4e5, 0.2)]
+    batches = []
+    off = 0
+    for m, model in enumerate(models):
+        ox = 0.15 + 0.12 * (m % 3)
+        oz = 0.2 + 0.15 * (m // 3)
+        pos = lattice_block((ox, 0.4, oz), (n_side, n_side, n_side), dx, seed, off)
+        off += pos.size
+        b = ParticleBatch.from_positions(pos, np.float32(dx) / np.float32(4.0), 1000.0, model)
+        u = uniform(seed + 101, pos.size, off).reshape(-1, 3)
+        b.vel[:] = ((u * 2.0 - 1.0) * 0.5).astype(np.float32)
+        batches.append(b)
+    batch = ParticleBatch.concat(batches)
+    cols = collider_array(box_walls(0.0, 1.0, BoundaryCondition.stick(), BoundaryCondition.separate(0.5)))
+    return Scene("mixed_materials", dx, 1.0e-4, (0.0, 0.0, -9.81), batch, cols, 50, grid_capacity_for(batch.n))

@@ -1,0 +1,274 @@
+"""Known-answer and property tests of the CPU oracle (no GPU).
+
+The reference ships no MPM tests or fixtures, so these pin the oracle to the
+mathematics of the cited shader code instead: closed forms, conservation
+laws and brute-force recomputations.  The one pin against the reference's own
+code is the prefix-sum CPU semantics (src_rbd/utils/prefix_sum.rs:112-136).
+"""
+import math
+
+import numpy as np
+import pytest
+
+from nexus_b200 import scenes
+from nexus_b200.models import ParticleModel, lame_lambda_mu
+from nexus_b200.particles import ParticleBatch, Collider, collider_array
+from nexus_b200.models import BoundaryCondition
+
+
+def test_prefix_sum_matches_reference_cpu_semantics(oracle_built):
+    o = oracle_built
+    v = np.array([3, 0, 5, 1, 7, 2], np.uint32)
+    # inclusive wrapping sum, shifted right, leading 0
+    assert o.prefix_sum(v).tolist() == [0, 3, 3, 8, 9, 16]
+    big = np.array([0xFFFFFFFF, 2, 1], np.uint32)
+    assert o.prefix_sum(big).tolist() == [0, 0xFFFFFFFF, 1]
+
+
+def test_pack_key_and_hash(oracle_built):
+    o = oracle_built
+    # grid.rs:101-106: 11/10/11 bits with offsets 1023/511/1023
+    assert o.pack_key(0, 0, 0) == 0x3FF | (0x1FF << 11) | (0x3FF << 21)
+    assert o.pack_key(-1023, -511, -1023) == 0
+    k = o.pack_key(5, -3, 7)
+    assert (k & 0x7FF) - 0x3FF == 5 and ((k >> 11) & 0x3FF) - 0x1FF == -3 and ((k >> 21) & 0x7FF) - 0x3FF == 7
+    # Murmur3 fmix-style mix of grid.rs:430-436
+    kk = 12345
+    ref = (kk * 0xCC9E2D51) & 0xFFFFFFFF
+    ref = ((ref << 15) | (ref >> 17)) & 0xFFFFFFFF
+    ref = (ref * 0x1B873593) & 0xFFFFFFFF
+    assert o.hash_key(kk) == ref
+
+
+def test_quadratic_kernel_partition_of_unity(oracle_built):
+    o = oracle_built
+    for x in np.linspace(0.5, 1.5, 41):
+        w = o.kernel_eval_all(float(x), "f64")
+        assert abs(w.sum() - 1.0) < 1e-12
+        # first moment: sum_i w_i (i - x) = 0 with nodes at 0, 1, 2
+        assert abs(sum(w[i] * (i - x) for i in range(3))) < 1e-12
+        # eval_all agrees with the branchless single-node eval
+        for i in range(3):
+            assert abs(w[i] - o.kernel_eval(i - x, "f64")) < 1e-12
+    assert o.kernel_eval(1.5, "f64") == 0.0 and o.kernel_eval(-1.5, "f64") == 0.0
+    assert o.kernel_eval(0.0, "f64") == 0.75
+
+
+def test_block_of_point(oracle_built):
+    o = oracle_built
+    dx = 1.0 / 64.0
+    # x = 10.4 dx -> round 10 -> assoc 9 -> block 2, cell 1; y = 0.6 dx -> assoc 0;
+    # z = -3.2 dx -> round -3 -> assoc -4 -> block -1, cell 0
+    b, a = o.block_of_point(dx, [10.4 * dx, 0.6 * dx, -3.2 * dx])
+    assert b.tolist() == [2, 0, -1] and a.tolist() == [1, 0, 0]
+    # round half away from zero: 2.5 -> 3
+    b, a = o.block_of_point(1.0, [2.5, -2.5, 4.49])
+    assert b.tolist() == [0, -1, 0] and a.tolist() == [2, 0, 3]
+
+
+def _rot(axis, ang):
+    axis = np.asarray(axis, np.float64) / np.linalg.norm(axis)
+    K = np.array([[0, -axis[2], axis[1]], [axis[2], 0, -axis[0]], [-axis[1], axis[0], 0]])
+    return np.eye(3) + math.sin(ang) * K + (1 - math.cos(ang)) * K @ K
+
+
+def _cm(m):  # row-major 3x3 -> column-major 9
+    return np.asarray(m, np.float32).T.reshape(9)
+
+
+def _from_cm(v):
+    return np.asarray(v, np.float64).reshape(3, 3).T
+
+
+def test_neo_hookean_rest_and_rotation(oracle_built):
+    o = oracle_built
+    m = ParticleModel.elastic_neo_hookean(1e5, 0.3).gpu_words()
+    tau, _, _ = o.model_update(m, _cm(np.eye(3)), np.zeros(9), "f64")
+    assert np.abs(tau).max() < 1e-6
+    # a rotation stores no energy; F enters as f32, so det F = 1 +- 1e-7 and
+    # tau is zero up to (lambda + mu) * 1e-7
+    tau, _, _ = o.model_update(m, _cm(_rot([1, 2, 3], 0.7)), np.zeros(9), "f64")
+    assert np.abs(tau).max() < 1e-6 * 1e5
+    # uniform stretch: tau = mu (s^2 - 1) I + lambda ln(s^3) I
+    lam, mu = lame_lambda_mu(1e5, 0.3)
+    s = 1.01
+    tau, _, _ = o.model_update(m, _cm(np.eye(3) * s), np.zeros(9), "f64")
+    expect = float(mu) * (s * s - 1) + float(lam) * math.log(s ** 3)
+    assert np.allclose(_from_cm(tau), np.eye(3) * expect, rtol=1e-5, atol=1e-3)
+
+
+def test_linear_corotated_rest_and_rotation(oracle_built):
+    o = oracle_built
+    m = ParticleModel.elastic(2e4, 0.25).gpu_words()
+    for F in (np.eye(3), _rot([0, 0, 1], 1.2), _rot([1, -1, 0.5], -0.4)):
+        tau, _, _ = o.model_update(m, _cm(F), np.zeros(9), "f64")
+        assert np.abs(tau).max() < 2e-6 * 2e4
+
+
+def test_svd_reconstructs(oracle_built):
+    o = oracle_built
+    rng = np.random.default_rng(3)
+    for _ in range(50):
+        F = np.eye(3) + 0.3 * rng.standard_normal((3, 3))
+        u, s, vt = o.svd(_cm(F), "f64")
+        U, Vt = _from_cm(u), _from_cm(vt)
+        assert np.allclose(U @ np.diag(s) @ Vt, F, atol=1e-5)
+        assert np.allclose(U.T @ U, np.eye(3), atol=1e-5)
+        assert np.all(np.diff(s) <= 1e-7) and np.all(s >= 0)
+
+
+def test_drucker_prager_tensile_and_inside_cone(oracle_built):
+    o = oracle_built
+    m = ParticleModel.sand(3.5e5, 0.3).gpu_words()
+    # pure tension (positive volumetric strain, no cohesion): projected to exp(0/3) = I
+    _, F, w = o.model_update(m, _cm(np.eye(3) * 1.05), np.zeros(9), "f64")
+    assert np.allclose(_from_cm(F), np.eye(3), atol=1e-6)
+    # compression with a small deviatoric part sits inside the cone: F unchanged
+    # (gamma <= 0 -> invalid projection) and the plastic state untouched
+    Fc = np.diag([0.98, 0.981, 0.979])
+    _, F, w2 = o.model_update(m, _cm(Fc), np.zeros(9), "f64")
+    assert np.allclose(_from_cm(F), Fc, atol=1e-6)
+    assert np.array_equal(w2, m)
+    # exactly hydrostatic strain (zero deviatoric part) is the degenerate case of
+    # drucker_prager.rs:139: projected to the tip, exp(cohesion/3) I = I
+    _, F, _ = o.model_update(m, _cm(np.eye(3) * 0.98), np.zeros(9), "f64")
+    assert np.allclose(_from_cm(F), np.eye(3), atol=1e-6)
+    # large shear is pulled back onto the cone: det and trace change, state advances
+    Fs = np.array([[1.0, 0.2, 0.0], [0.0, 1.0, 0.0], [0.0, 0.0, 1.0]]) @ np.diag([0.99, 0.99, 0.99])
+    _, F, w3 = o.model_update(m, _cm(Fs), np.zeros(9), "f64")
+    assert not np.allclose(_from_cm(F), Fs, atol=1e-4)
+    assert w3.view(np.float32)[2] > 1.0  # plastic hardening grew
+    # cohesive sand: tensile projection goes to exp(cohesion/3) I
+    mc = ParticleModel.cohesive_sand(3.5e5, 0.3, 0.003).gpu_words()
+    _, F, _ = o.model_update(mc, _cm(np.eye(3) * 1.05), np.zeros(9), "f64")
+    assert np.allclose(_from_cm(F), np.eye(3) * math.exp(0.001), atol=1e-6)
+
+
+def test_fluid_pressure_and_volume_only(oracle_built):
+    o = oracle_built
+    m = ParticleModel.water(1e5).gpu_words()
+    tau, _, _ = o.model_update(m, _cm(np.eye(3)), np.zeros(9), "f64")
+    assert np.abs(tau).max() < 1e-6  # p(1) = 0, no strain rate
+    j = 0.97 ** 3
+    tau, _, _ = o.model_update(m, _cm(np.eye(3) * 0.97), np.zeros(9), "f64")
+    p = 1e5 * (j ** -7 - 1)
+    assert np.allclose(_from_cm(tau), -p * j * np.eye(3), rtol=1e-5)
+
+
+def test_boundary_condition_projection(oracle_built):
+    o = oracle_built
+    n = np.array([0, 0, 1], np.float32)
+    v = np.array([1.0, -2.0, -3.0], np.float32)
+    assert np.allclose(o.bc_project(0, 0.0, v, n), 0)
+    assert np.allclose(o.bc_project(1, 0.0, v, n), [1, -2, 0])
+    # separate with friction 0.5: tangent |(1,-2)| reduced by 0.5*3
+    t = math.sqrt(5.0)
+    assert np.allclose(o.bc_project(2, 0.5, v, n), np.array([1, -2, 0]) / t * (t - 1.5), atol=1e-6)
+    assert np.allclose(o.bc_project(2, 0.5, np.array([1, 1, 2], np.float32), n), [1, 1, 2])
+    assert np.allclose(o.bc_project(3, 0.0, v, n), v)
+
+
+def _scene_with(colliders, n=8):
+    pos = np.full((n, 3), 0.5, np.float32)
+    b = ParticleBatch.from_positions(pos, 0.01, 1000.0, ParticleModel.elastic(1e3, 0.2))
+    return scenes.Scene("probe", 1.0 / 64, 1e-4, (0, 0, 0), b, collider_array(colliders), 1, 64)
+
+
+def test_shape_projections(oracle_built):
+    from oracle.oracle import OracleScene
+    cols = [Collider.cuboid((0.2, 0.1, 0.3), (0.5, 0.5, 0.5), BoundaryCondition.slip()),
+            Collider.ball(0.25, (0.1, 0.2, 0.3), BoundaryCondition.slip()),
+            Collider.capsule((0.0, 0.0, -0.2), (0.0, 0.0, 0.2), 0.1, (0.7, 0.7, 0.7), BoundaryCondition.slip())]
+    sc = OracleScene(_scene_with(cols))
+    # cuboid: outside point clamps to the box; inside point goes to the nearest face
+    p, inside = sc.project_point(0, [0.9, 0.5, 0.5])
+    assert inside == 0 and np.allclose(p, [0.7, 0.5, 0.5], atol=1e-6)
+    p, inside = sc.project_point(0, [0.5, 0.58, 0.5])
+    assert inside == 1 and np.allclose(p, [0.5, 0.6, 0.5], atol=1e-6)
+    # ball
+    p, inside = sc.project_point(1, [0.1, 0.2, 0.9])
+    assert inside == 0 and np.allclose(p, [0.1, 0.2, 0.55], atol=1e-6)
+    p, inside = sc.project_point(1, [0.1, 0.3, 0.3])
+    assert inside == 1 and np.allclose(p, [0.1, 0.45, 0.3], atol=1e-6)
+    # capsule: beside the segment and beyond a cap
+    p, inside = sc.project_point(2, [0.9, 0.7, 0.7])
+    assert inside == 0 and np.allclose(p, [0.8, 0.7, 0.7], atol=1e-6)
+    p, inside = sc.project_point(2, [0.7, 0.7, 1.2])
+    assert inside == 0 and np.allclose(p, [0.7, 0.7, 1.0], atol=1e-6)
+
+
+def test_activation_set_is_every_particles_block_neighbourhood(oracle_built):
+    from oracle.oracle import OracleScene
+    sc = scenes.mixed_materials(n_side=6)
+    o = OracleScene(sc)
+    o.sort()
+    h = o.headers()
+    got = {tuple(r[:3]) for r in h}
+    dx = sc.dx
+    pos = sc.particles.pos.astype(np.float32)
+    assoc = np.round(pos / np.float32(dx)) - 1
+    blk = np.floor(assoc / 4).astype(np.int64)
+    want = set()
+    for b in {tuple(r) for r in blk}:
+        for s in range(8):
+            want.add((b[0] + (s >> 2 & 1), b[1] + (s >> 1 & 1), b[2] + (s & 1)))
+    assert got == want
+    # every particle is the primary of exactly one block, and appears as extra
+    # exactly where its stencil spills (bucket invariants)
+    sorted_ids = o.sorted_ids()
+    prim = np.concatenate([sorted_ids[r[3]:r[3] + r[4]] for r in h])
+    assert np.array_equal(np.sort(prim), np.arange(sc.n))
+    total_extras = int(h[:, 5].sum() - h[:, 4].sum())
+    a_local = (assoc - blk * 4).astype(np.int64)
+    spill = (a_local >= 2)
+    expect = sum(int(np.prod([1 + int(s) for s in row])) - 1 for row in spill)
+    assert total_extras == expect
+    # within a block's primaries, the ids are grouped by ascending z-slab
+    for r in h:
+        seg = sorted_ids[r[3]:r[3] + r[4]]
+        slabs = a_local[seg, 2]
+        assert np.all(np.diff(slabs) >= 0)
+
+
+def test_p2g_conserves_mass_and_momentum_fp64(oracle_built):
+    from oracle.oracle import OracleScene
+    sc = scenes.mixed_materials(n_side=5)
+    rng = np.random.default_rng(0)
+    sc.particles.aff[:] = rng.standard_normal(sc.particles.aff.shape).astype(np.float32)
+    o = OracleScene(sc, "f64")
+    o.sort()
+    o.p2g()
+    nodes = o.nodes().reshape(-1, 8).astype(np.float64)
+    m = sc.particles.mass.astype(np.float64)
+    # (node values come back rounded to f32, hence the 1e-6 relative bound)
+    assert abs(nodes[:, 3].sum() - m.sum()) < 1e-6 * m.sum()
+    # APIC: the affine term has zero net momentum (first moment of the kernel vanishes)
+    mom = (sc.particles.vel.astype(np.float64) * m[:, None]).sum(0)
+    assert np.allclose(nodes[:, :3].sum(0), mom, rtol=1e-6, atol=1e-9)
+
+
+def test_free_fall_and_uniform_translation(oracle_built):
+    from oracle.oracle import OracleScene
+    sc = scenes.elastic_cube(n_side=8, steps=10)
+    sc.colliders = sc.colliders[:0]
+    sc.particles.vel[:] = np.array([0.3, -0.2, 0.0], np.float32)
+    o = OracleScene(sc, "f64")
+    o.step(10)
+    p = o.particles()
+    t = 10 * sc.dt
+    assert np.allclose(p["vel"], [0.3, -0.2, -9.81 * t], atol=1e-6)
+    assert p["enabled"].all()
+    x0 = sc.particles.pos.astype(np.float64)
+    disp = p["pos"].astype(np.float64) - x0
+    # uniform translation: every particle moves by the same amount (rigid motion)
+    assert np.abs(disp - disp.mean(0)).max() < 1e-6
+
+
+def test_fp32_and_fp64_oracles_agree_on_elastic_cube(oracle_built):
+    from oracle.oracle import OracleScene
+    sc = scenes.elastic_cube(n_side=12, steps=20)
+    a, b = OracleScene(sc, "f32"), OracleScene(sc, "f64")
+    a.step(20)
+    b.step(20)
+    pa, pb = a.particles()["pos"], b.positions_f64()
+    assert np.linalg.norm(pa - pb) / np.linalg.norm(pb) < 1e-6
