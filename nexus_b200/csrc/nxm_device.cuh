@@ -161,11 +161,13 @@ struct Svd {
     m3 vt;
 };
 
-__device__ __forceinline__ void jacobi_pair(float (&a)[3][3], float (&v)[3][3], int p, int q) {
+// One Jacobi rotation of columns p, q; returns |a_p . a_q| / (|a_p| |a_q|)
+// before the rotation (0 when the pair is already orthogonal to 1e-6).
+__device__ __forceinline__ float jacobi_pair(float (&a)[3][3], float (&v)[3][3], int p, int q) {
     float alpha = a[0][p] * a[0][p] + a[1][p] * a[1][p] + a[2][p] * a[2][p];
     float beta = a[0][q] * a[0][q] + a[1][q] * a[1][q] + a[2][q] * a[2][q];
     float gamma = a[0][p] * a[0][q] + a[1][p] * a[1][q] + a[2][p] * a[2][q];
-    if (fabsf(gamma) <= 1.0e-30f || fabsf(gamma) <= 1.0e-9f * sqrtf(alpha * beta)) return;
+    if (fabsf(gamma) <= 1.0e-30f || fabsf(gamma) <= 1.0e-6f * sqrtf(alpha * beta)) return 0.0f;
     float zeta = (beta - alpha) / (2.0f * gamma);
     float t = copysignf(1.0f, zeta) / (fabsf(zeta) + sqrtf(1.0f + zeta * zeta));
     float c = rsqrtf(1.0f + t * t);
@@ -179,16 +181,20 @@ __device__ __forceinline__ void jacobi_pair(float (&a)[3][3], float (&v)[3][3], 
         v[r][p] = c * vp - s * vq;
         v[r][q] = s * vp + c * vq;
     }
+    return fabsf(gamma) * rsqrtf(alpha * beta);
 }
 
 __device__ __forceinline__ Svd svd3(const m3& f) {
     float a[3][3] = {{f.c0.x, f.c1.x, f.c2.x}, {f.c0.y, f.c1.y, f.c2.y}, {f.c0.z, f.c1.z, f.c2.z}};
     float v[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
 #pragma unroll 1
-    for (int sweep = 0; sweep < 6; ++sweep) {
-        jacobi_pair(a, v, 0, 1);
-        jacobi_pair(a, v, 0, 2);
-        jacobi_pair(a, v, 1, 2);
+    // cyclic sweeps until every column pair is orthogonal to 1e-6 (two or
+    // three sweeps for the near-rotation deformation gradients of MPM; at most 10)
+    for (int sweep = 0; sweep < 10; ++sweep) {
+        float off = jacobi_pair(a, v, 0, 1);
+        off = fmaxf(off, jacobi_pair(a, v, 0, 2));
+        off = fmaxf(off, jacobi_pair(a, v, 1, 2));
+        if (off == 0.0f) break;
     }
     float sig[3];
 #pragma unroll
@@ -236,9 +242,8 @@ __device__ __forceinline__ Svd svd3(const m3& f) {
 // Constitutive models (src_mpm_shaders/models/*.rs).
 // ---------------------------------------------------------------------------
 
-// linear_elasticity.rs:114-138
-__device__ __forceinline__ m3 linear_stress(float lambda, float mu, const m3& F) {
-    Svd d = svd3(F);
+// linear_elasticity.rs:114-138, given the SVD of F.
+__device__ __forceinline__ m3 linear_stress_svd(float lambda, float mu, const m3& F, const Svd& d) {
     float j = d.s.x * d.s.y * d.s.z;
     v3 ms = d.s - splat(1.0f);
     m3 rec = (d.u * diag(ms)) * d.vt;
@@ -248,6 +253,9 @@ __device__ __forceinline__ m3 linear_stress(float lambda, float mu, const m3& F)
     res.c1.y += diag_val;
     res.c2.z += diag_val;
     return res;
+}
+__device__ __forceinline__ m3 linear_stress(float lambda, float mu, const m3& F) {
+    return linear_stress_svd(lambda, mu, F, svd3(F));
 }
 
 // neo_hookean_elasticity.rs:26-39
@@ -292,10 +300,12 @@ __device__ __forceinline__ float dp_alpha(const float* pl, float q) {
     return sqrtf(2.0f / 3.0f) * (2.0f * s_angle) / (3.0f - s_angle);
 }
 
-// drucker_prager.rs:121-167 and :224-267; state = [pdet, hardening, log_vol_gain]
-__device__ __forceinline__ m3 dp_project(const float* pl, float* state, const m3& F) {
+// drucker_prager.rs:121-167 and :224-267; state = [pdet, hardening, log_vol_gain].
+// `d` receives an SVD of the returned F: the projected F is U diag(sv) V^T,
+// so its SVD is known without recomputing it.
+__device__ __forceinline__ m3 dp_project_svd(const float* pl, float* state, const m3& F, Svd& d) {
+    d = svd3(F);
     if (pl[4] == 0.0f) return F;
-    Svd d = svd3(F);
     float alpha = dp_alpha(pl, state[1]);
     const float dd = 3.0f;
     v3 strain = mk(logf(d.s.x), logf(d.s.y), logf(d.s.z)) + splat(state[2] / dd);
@@ -323,7 +333,12 @@ __device__ __forceinline__ m3 dp_project(const float* pl, float* state, const m3
     state[0] = npdet;
     state[1] = nhard;
     state[2] = nlvg;
+    d.s = sv;
     return (d.u * diag(sv)) * d.vt;
+}
+__device__ __forceinline__ m3 dp_project(const float* pl, float* state, const m3& F) {
+    Svd d;
+    return dp_project_svd(pl, state, F, d);
 }
 
 // snow.rs:452-488; state = [plastic_det]; pl = [critical_compression, critical_stretch, hardening]
@@ -346,7 +361,11 @@ __device__ __forceinline__ m3 snow_project(const float* pl, float* state, const 
 
 // models/default.rs:208-264.  `w` holds the material's 24 model words; the
 // per-particle state words (Drucker-Prager words 0..2, snow word 0) are in `st`
-// and updated in place.
+// and updated in place.  With kReuseSvd, Drucker-Prager sand on a linear
+// backbone computes the stress from the projection's SVD instead of taking
+// the SVD of the projected F a second time (the reference recomputes it; the
+// two agree to rounding).
+template <bool kReuseSvd>
 __device__ __forceinline__ m3 model_update(uint32_t tag, const float* w, float* st, m3& F, const m3& vel_grad) {
     switch (tag) {
     case MODEL_ELASTIC_LINEAR:
@@ -354,8 +373,14 @@ __device__ __forceinline__ m3 model_update(uint32_t tag, const float* w, float* 
     case MODEL_ELASTIC_NEO_HOOKEAN:
         return neo_hookean_stress(w[0], w[1], F);
     case MODEL_SAND_LINEAR:
-        F = dp_project(&w[3], st, F);
-        return linear_stress(w[10], w[11], F);
+        if (kReuseSvd) {
+            Svd d;
+            F = dp_project_svd(&w[3], st, F, d);
+            return linear_stress_svd(w[10], w[11], F, d);
+        } else {
+            F = dp_project(&w[3], st, F);
+            return linear_stress(w[10], w[11], F);
+        }
     case MODEL_SAND_NEO_HOOKEAN:
         F = dp_project(&w[3], st, F);
         return neo_hookean_stress(w[10], w[11], F);

@@ -31,7 +31,11 @@ struct DevPtrs {
     uint32_t* sorted;        // sorted ids with extras
     uint2* pcode;            // per particle: packed block key, assoc code (ax | ay<<2 | az<<4)
     uint32_t* phdr;          // per particle: primary header id
+    uint32_t* scan_tmp;      // per block: offset inside its scan tile
+    uint32_t* tile_sums;     // per scan tile of kScanTile blocks: its total
 };
+
+constexpr uint32_t kScanTile = 1024;  // blocks per scan tile
 
 struct LaunchCfg {
     int sm_count;
@@ -49,7 +53,11 @@ struct StepLaunches {
 };
 
 namespace fast {
-void launch_sort(const DevPtrs& P, const LaunchCfg& c, bool canonical, cudaStream_t s);
+// `with_extras`: also list every particle as an "extra" in the +1 neighbour
+// blocks its stencil reaches (the reference's full sorted-id layout, used by
+// the gather-form P2G); the scatter P2G needs the primaries only.
+// `canonical`: order each bucket by ascending particle id.
+void launch_sort(const DevPtrs& P, const LaunchCfg& c, bool with_extras, bool canonical, cudaStream_t s);
 void launch_p2g(const DevPtrs& P, const LaunchCfg& c, cudaStream_t s);
 void launch_grid_update(const DevPtrs& P, const LaunchCfg& c, cudaStream_t s);
 void launch_g2p_update(const DevPtrs& P, const LaunchCfg& c, cudaStream_t s);

@@ -108,7 +108,8 @@ struct alignas(16) Counters {
     uint32_t num_blocks;    // num_primary + num_extra (written by the scan)
     uint32_t sorted_len;    // total sorted ids, extras included
     uint32_t status;        // STATUS_* bits
-    uint32_t pad[3];
+    uint32_t codes_valid;   // 1 when pcode holds the block key of every particle's current position
+    uint32_t pad[2];
 };
 
 }  // namespace nxm

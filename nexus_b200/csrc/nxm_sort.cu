@@ -3,19 +3,25 @@
 //
 // Same results as the reference: the set of active blocks (every particle's
 // 2x2x2 block neighbourhood), the per-block slab buckets (4 primary z-slabs,
-// 6 extra buckets), the +1 neighbour header ids and the sorted id list with
-// extras.  Header order and the order inside a bucket come from atomics, as
-// in the reference; the canonical pass (deterministic mode) orders every
-// bucket by ascending particle id.
+// 6 extra buckets), the +1 neighbour header ids and the sorted id list.
+// Header order and the order inside a bucket come from atomics, as in the
+// reference; the canonical pass (deterministic mode) orders every bucket by
+// ascending particle id.  The extras (a particle listed again in each +1
+// neighbour block its stencil reaches) are only built when asked for: the
+// gather-form P2G reads them, the scatter-form P2G does not.
 //
 // B200 specifics: every particle pass is a persistent grid-stride loop that
 // keeps whole warps together, so that __match_any_sync can merge the atomics
 // of lanes that hit the same block (or the same block bucket): one hash probe
 // or one atomicAdd per distinct key per warp instead of one per particle.
-// Counters, headers and the hash live in L2 (a 2M-particle scene has a few
-// thousand blocks).
+// The block key of each particle is cached in `pcode` (8 bytes) by the
+// previous step's G2P, so activation does not re-read the 80-byte particle
+// records.  Counters, headers and the hash live in L2.
 #include "nxm_device.cuh"
 #include "nxm_kernels.h"
+
+// k_count<false> / k_finalize<false> skip the extras loop by design.
+#pragma nv_diag_suppress 128
 
 namespace nxm {
 namespace {
@@ -107,12 +113,14 @@ __global__ void k_sort_reset(DevPtrs P, uint32_t hash_cap) {
     }
 }
 
-// sort.rs:104-121 gpu_touch_primary_blocks (+ per-particle key cache).
+// sort.rs:104-121 gpu_touch_primary_blocks.  Block keys come from the cache
+// written by the previous step (or from the positions after an upload).
 __global__ void __launch_bounds__(256) k_touch_primary(DevPtrs P) {
     const uint32_t n = P.params->n;
     const float dx = P.params->dx;
     const uint32_t hmask = P.params->hash_capacity - 1;
     const uint32_t bcap = P.params->block_capacity;
+    const bool cached = P.counters->codes_valid != 0;
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
@@ -120,31 +128,35 @@ __global__ void __launch_bounds__(256) k_touch_primary(DevPtrs P) {
         const uint32_t p = base + lane;
         const bool active = p < n;
         uint32_t key = NONE;
-        CellInfo ci{};
         if (active) {
-            float4 xm = __ldg(reinterpret_cast<const float4*>(&P.kin[p]));
-            ci = cell_info(dx, mk(xm.x, xm.y, xm.z));
-            key = pack_key(ci.bx, ci.by, ci.bz);
-            P.pcode[p] = make_uint2(key, ci.ax | (ci.ay << 2) | (ci.az << 4));
+            if (cached) {
+                key = __ldg(&P.pcode[p].x);
+            } else {
+                float4 xm = __ldg(reinterpret_cast<const float4*>(&P.kin[p]));
+                CellInfo ci = cell_info(dx, mk(xm.x, xm.y, xm.z));
+                key = pack_key(ci.bx, ci.by, ci.bz);
+                P.pcode[p] = make_uint2(key, ci.ax | (ci.ay << 2) | (ci.az << 4));
+            }
         }
         uint32_t peers = __match_any_sync(0xFFFFFFFFu, key);
-        if (active && lane == (uint32_t)(__ffs(peers) - 1)) hash_insert(P, key, ci.bx, ci.by, ci.bz, true, 0, hmask, bcap);
+        if (active && lane == (uint32_t)(__ffs(peers) - 1))
+            hash_insert(P, key, key_x(key), key_y(key), key_z(key), true, 0, hmask, bcap);
     }
 }
 
-// sort.rs:133-163 gpu_touch_neighbor_blocks.
+// sort.rs:133-163 gpu_touch_neighbor_blocks: one thread per (base block, neighbour).
 __global__ void __launch_bounds__(256) k_touch_nbh(DevPtrs P) {
     const uint32_t hmask = P.params->hash_capacity - 1;
     const uint32_t bcap = P.params->block_capacity;
     const uint32_t nprim = min(__ldcg(&P.counters->num_primary), bcap);
-    for (uint32_t b = blockIdx.x * blockDim.x + threadIdx.x; b < nprim; b += gridDim.x * blockDim.x) {
-        int4 v = P.bvid[b];
-        for (int i = 1; i < 8; ++i) {
-            int sx, sy, sz;
-            assoc_shift(i, sx, sy, sz);
-            int kx = v.x + sx, ky = v.y + sy, kz = v.z + sz;
-            hash_insert(P, pack_key(kx, ky, kz), kx, ky, kz, false, nprim, hmask, bcap);
-        }
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < nprim * 7u; t += gridDim.x * blockDim.x) {
+        const uint32_t b = t / 7u;
+        const int i = (int)(t % 7u) + 1;
+        const int4 v = P.bvid[b];
+        int sx, sy, sz;
+        assoc_shift(i, sx, sy, sz);
+        const int kx = v.x + sx, ky = v.y + sy, kz = v.z + sz;
+        hash_insert(P, pack_key(kx, ky, kz), kx, ky, kz, false, nprim, hmask, bcap);
     }
 }
 
@@ -172,6 +184,7 @@ __global__ void __launch_bounds__(256) k_block_prep(DevPtrs P) {
 }
 
 // sort.rs:287-349 gpu_update_block_particle_count.
+template <bool kExtras>
 __global__ void __launch_bounds__(256) k_count(DevPtrs P) {
     const uint32_t n = P.params->n;
     const uint32_t hmask = P.params->hash_capacity - 1;
@@ -191,6 +204,7 @@ __global__ void __launch_bounds__(256) k_count(DevPtrs P) {
         const uint32_t ax = code.y & 3u, ay = (code.y >> 2) & 3u, az = (code.y >> 4) & 3u;
         uint32_t key = (h0 != NONE) ? h0 * 16u + az : NONE;
         warp_agg_add(key, key != NONE ? &P.cursors[h0 * NUM_BUCKETS + az] : nullptr);
+        if (!kExtras) continue;
         for (int i = 1; i < 8; ++i) {
             int sx, sy, sz;
             assoc_shift(i, sx, sy, sz);
@@ -207,68 +221,109 @@ __global__ void __launch_bounds__(256) k_count(DevPtrs P) {
 }
 
 // prefix sum (src_rbd/utils/prefix_sum.rs) over the block totals, then
-// sort.rs:382-420 gpu_copy_scan_values_to_first_particles.  One CTA of 1024.
-__global__ void __launch_bounds__(1024) k_scan(DevPtrs P) {
-    __shared__ uint32_t warp_tot[32];
-    __shared__ uint32_t carry_s;
-    const uint32_t total = P.counters->num_blocks;
-    const uint32_t tid = threadIdx.x, lane = tid & 31u, wid = tid >> 5;
-    if (tid == 0) carry_s = 0;
-    __syncthreads();
-    for (uint32_t tile = 0; tile < total; tile += 1024u) {
-        const uint32_t b = tile + tid;
-        uint32_t cnt[NUM_BUCKETS];
-        uint32_t t = 0;
-        if (b < total) {
+// sort.rs:382-420 gpu_copy_scan_values_to_first_particles, as a two-pass
+// tiled scan: pass 1 gives each block its offset inside a tile of kScanTile
+// blocks and each tile its total; pass 2 adds the tile's offset (the sum of
+// the tile totals before it) and turns the bucket counts into cursors.
+constexpr uint32_t kScanThreads = 256;
+constexpr uint32_t kScanPer = kScanTile / kScanThreads;  // blocks per thread
+
+// Exclusive CTA-wide scan of one value per thread; returns the CTA total in *total.
+__device__ __forceinline__ uint32_t cta_exclusive_scan(uint32_t v, uint32_t* warp_tot, uint32_t* total) {
+    const uint32_t lane = threadIdx.x & 31u, wid = threadIdx.x >> 5;
+    uint32_t incl = v;
 #pragma unroll
-            for (int k = 0; k < NUM_BUCKETS; ++k) {
-                cnt[k] = P.cursors[b * NUM_BUCKETS + k];
-                t += cnt[k];
-            }
-        }
-        uint32_t incl = t;
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+        if (lane >= (uint32_t)o) incl += y;
+    }
+    if (lane == 31) warp_tot[wid] = incl;
+    __syncthreads();
+    if (wid == 0) {
+        const uint32_t nw = blockDim.x >> 5;
+        uint32_t w = lane < nw ? warp_tot[lane] : 0u;
+        uint32_t wi = w;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
-            uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
-            if (lane >= (uint32_t)o) incl += y;
+            uint32_t y = __shfl_up_sync(0xFFFFFFFFu, wi, o);
+            if (lane >= (uint32_t)o) wi += y;
         }
-        if (lane == 31) warp_tot[wid] = incl;
-        __syncthreads();
-        if (wid == 0) {
-            uint32_t w = warp_tot[lane];
-            uint32_t wi = w;
+        if (lane < nw) warp_tot[lane] = wi - w;
+        if (lane == 31) warp_tot[32] = wi;
+    }
+    __syncthreads();
+    const uint32_t out = warp_tot[wid] + incl - v;
+    *total = warp_tot[32];
+    __syncthreads();
+    return out;
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_scan_tiles(DevPtrs P) {
+    __shared__ uint32_t warp_tot[33];
+    const uint32_t total = P.counters->num_blocks;
+    const uint32_t ntiles = (total + kScanTile - 1) / kScanTile;
+    for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const uint32_t b0 = tile * kScanTile + threadIdx.x * kScanPer;
+        uint32_t bt[kScanPer];
+        uint32_t t = 0;
 #pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                uint32_t y = __shfl_up_sync(0xFFFFFFFFu, wi, o);
-                if (lane >= (uint32_t)o) wi += y;
+        for (uint32_t j = 0; j < kScanPer; ++j) {
+            const uint32_t b = b0 + j;
+            uint32_t s = 0;
+            if (b < total) {
+#pragma unroll
+                for (int k = 0; k < NUM_BUCKETS; ++k) s += P.cursors[b * NUM_BUCKETS + k];
             }
-            warp_tot[lane] = wi - w;  // exclusive warp offsets
+            bt[j] = s;
+            t += s;
         }
-        __syncthreads();
-        const uint32_t carry = carry_s;
-        const uint32_t excl = carry + warp_tot[wid] + incl - t;
-        if (b < total) {
-            P.first[b] = excl;
-            uint32_t running = excl;
+        uint32_t tile_total;
+        uint32_t run = cta_exclusive_scan(t, warp_tot, &tile_total);
+#pragma unroll
+        for (uint32_t j = 0; j < kScanPer; ++j) {
+            const uint32_t b = b0 + j;
+            if (b < total) P.scan_tmp[b] = run;
+            run += bt[j];
+        }
+        if (threadIdx.x == 0) P.tile_sums[tile] = tile_total;
+    }
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_scan_apply(DevPtrs P) {
+    __shared__ uint32_t warp_tot[33];
+    const uint32_t total = P.counters->num_blocks;
+    const uint32_t ntiles = (total + kScanTile - 1) / kScanTile;
+    for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        uint32_t part = 0;
+        for (uint32_t i = threadIdx.x; i < tile; i += kScanThreads) part += P.tile_sums[i];
+        uint32_t offset;
+        cta_exclusive_scan(part, warp_tot, &offset);
+        const uint32_t b0 = tile * kScanTile + threadIdx.x * kScanPer;
+#pragma unroll
+        for (uint32_t j = 0; j < kScanPer; ++j) {
+            const uint32_t b = b0 + j;
+            if (b >= total) break;
+            const uint32_t first = offset + P.scan_tmp[b];
+            uint32_t running = first;
+            P.first[b] = first;
 #pragma unroll
             for (int k = 0; k < NUM_BUCKETS; ++k) {
-                if (k == NUM_PRIMARY_BUCKETS) P.nprim[b] = running - excl;
+                if (k == NUM_PRIMARY_BUCKETS) P.nprim[b] = running - first;
+                const uint32_t c = P.cursors[b * NUM_BUCKETS + k];
                 P.cursors[b * NUM_BUCKETS + k] = running;
-                running += cnt[k];
+                running += c;
             }
-            P.nwx[b] = running - excl;
+            P.nwx[b] = running - first;
+            if (b == total - 1) {
+                P.counters->sorted_len = running;
+                if (running > P.params->sorted_capacity) set_status(P.counters, STATUS_SORT_CAPACITY);
+            }
         }
-        __syncthreads();
-        if (tid == 1023) carry_s = excl + t;
-        __syncthreads();
-    }
-    if (tid == 0) {
-        P.counters->sorted_len = carry_s;
-        if (carry_s > P.params->sorted_capacity) set_status(P.counters, STATUS_SORT_CAPACITY);
     }
 }
 
 // sort.rs:430-491 gpu_finalize_particles_sort.
+template <bool kExtras>
 __global__ void __launch_bounds__(256) k_finalize(DevPtrs P) {
     const uint32_t n = P.params->n;
     const uint32_t scap = P.params->sorted_capacity;
@@ -287,6 +342,7 @@ __global__ void __launch_bounds__(256) k_finalize(DevPtrs P) {
         uint32_t key = (h0 != NONE) ? h0 * 16u + az : NONE;
         uint32_t slot = warp_agg_add(key, key != NONE ? &P.cursors[h0 * NUM_BUCKETS + az] : nullptr);
         if (key != NONE && slot < scap) P.sorted[slot] = p;
+        if (!kExtras) continue;
         for (int i = 1; i < 8; ++i) {
             int sx, sy, sz;
             assoc_shift(i, sx, sy, sz);
@@ -335,11 +391,11 @@ inline int grid_for(int sm_count, int per_sm) { return sm_count * per_sm; }
 
 }  // namespace
 
-int sort_launches(bool canonical) { return canonical ? 8 : 7; }
+int sort_launches(bool canonical) { return canonical ? 9 : 8; }
 
 namespace fast {
 
-void launch_sort(const DevPtrs& P, const LaunchCfg& c, bool canonical, cudaStream_t s) {
+void launch_sort(const DevPtrs& P, const LaunchCfg& c, bool with_extras, bool canonical, cudaStream_t s) {
     const int g = grid_for(c.sm_count, 8);
     int reset_grid = (int)((c.hash_capacity + 255u) / 256u);
     if (reset_grid > g) reset_grid = g;
@@ -348,9 +404,12 @@ void launch_sort(const DevPtrs& P, const LaunchCfg& c, bool canonical, cudaStrea
     k_touch_primary<<<g, 256, 0, s>>>(P);
     k_touch_nbh<<<g, 256, 0, s>>>(P);
     k_block_prep<<<g, 256, 0, s>>>(P);
-    k_count<<<g, 256, 0, s>>>(P);
-    k_scan<<<1, 1024, 0, s>>>(P);
-    k_finalize<<<g, 256, 0, s>>>(P);
+    if (with_extras) k_count<true><<<g, 256, 0, s>>>(P);
+    else k_count<false><<<g, 256, 0, s>>>(P);
+    k_scan_tiles<<<c.sm_count, kScanThreads, 0, s>>>(P);
+    k_scan_apply<<<c.sm_count, kScanThreads, 0, s>>>(P);
+    if (with_extras) k_finalize<true><<<g, 256, 0, s>>>(P);
+    else k_finalize<false><<<g, 256, 0, s>>>(P);
     if (canonical) k_sort_segments<<<grid_for(c.sm_count, 4), 256, 0, s>>>(P);
 }
 

@@ -126,6 +126,8 @@ struct nxm_state {
     int4* bvid = nullptr;
     uint32_t *first = nullptr, *nprim = nullptr, *nwx = nullptr, *cursors = nullptr, *nbh = nullptr;
     float4* nodes = nullptr;
+    uint32_t* scan_tmp = nullptr;
+    uint32_t* tile_sums = nullptr;
 
     // colliders
     std::vector<DevCollider> colliders;
@@ -174,6 +176,8 @@ DevPtrs dev_ptrs(nxm_state* s) {
     P.sorted = s->sorted;
     P.pcode = s->pcode;
     P.phdr = s->phdr;
+    P.scan_tmp = s->scan_tmp;
+    P.tile_sums = s->tile_sums;
     return P;
 }
 
@@ -194,7 +198,7 @@ void invalidate_graph(nxm_state* s) {
 
 int free_grid(nxm_state* s) {
     dfree(s->hkey); dfree(s->hval); dfree(s->bvid); dfree(s->first); dfree(s->nprim); dfree(s->nwx);
-    dfree(s->cursors); dfree(s->nbh); dfree(s->nodes);
+    dfree(s->cursors); dfree(s->nbh); dfree(s->nodes); dfree(s->scan_tmp); dfree(s->tile_sums);
     return NXM_OK;
 }
 
@@ -211,6 +215,8 @@ int alloc_grid(nxm_state* s, uint32_t grid_capacity) {
     NXM_TRY(dalloc(&s->cursors, (size_t)s->block_cap * NUM_BUCKETS));
     NXM_TRY(dalloc(&s->nbh, (size_t)s->block_cap * NUM_NBH));
     NXM_TRY(dalloc(&s->nodes, (size_t)s->block_cap * 64));
+    NXM_TRY(dalloc(&s->scan_tmp, s->block_cap));
+    NXM_TRY(dalloc(&s->tile_sums, s->block_cap / kScanTile + 2));
     NXM_TRY(cudaMemsetAsync(s->hkey, 0xFF, sizeof(uint32_t) * s->hash_cap, s->stream));
     invalidate_graph(s);
     s->params_dirty = true;
@@ -280,6 +286,14 @@ int sync_materials(nxm_state* s) {
     return NXM_OK;
 }
 
+// The cached block keys (written by the G2P epilogue) no longer match the
+// particle positions: the next sort recomputes them from the positions.
+int invalidate_codes(nxm_state* s) {
+    NXM_TRY(cudaMemsetAsync(reinterpret_cast<char*>(s->d_counters) + offsetof(Counters, codes_valid), 0, 4,
+                            s->stream));
+    return NXM_OK;
+}
+
 int sync_params(nxm_state* s) {
     if (!s->params_dirty) return NXM_OK;
     Params p{};
@@ -309,7 +323,7 @@ int enqueue_step(nxm_state* s, cudaStream_t st, cudaEvent_t* ev /* 5 events or n
     const bool has_col = !s->colliders.empty();
     if (ev) cudaEventRecord(ev[0], st);
     if (has_col) { fast::launch_colliders_begin(P, st); ++k; }
-    fast::launch_sort(P, c, s->deterministic, st);
+    fast::launch_sort(P, c, /*with_extras=*/s->deterministic, /*canonical=*/s->deterministic, st);
     k += sort_launches(s->deterministic);
     if (ev) cudaEventRecord(ev[1], st);
     if (s->deterministic) exact::launch_p2g_gather(P, c, st);
@@ -435,7 +449,7 @@ int upload_particles(nxm_state* s, const nxm_particles_soa* p, uint32_t count) {
     NXM_TRY(cudaStreamSynchronize(s->stream));
     s->n += count;
     s->params_dirty = true;
-    return NXM_OK;
+    return invalidate_codes(s);
 }
 
 bool device_ok(int* dev, int* sms) {
@@ -557,7 +571,7 @@ int nxm_state_set_cell_width(nxm_state* s, float cell_width, uint32_t grid_capac
     if (rc) return rc;
     NXM_TRY(cudaStreamSynchronize(s->stream));
     s->params_dirty = true;
-    return NXM_OK;
+    return invalidate_codes(s);
 }
 
 int nxm_state_set_colliders(nxm_state* s, const nxm_collider* cols, uint32_t ncol, const float* tri, uint32_t ntri) {
@@ -696,7 +710,7 @@ int nxm_particles_swap_remove(nxm_state* s, const uint32_t* slots, uint32_t coun
     NXM_TRY(cudaStreamSynchronize(s->stream));
     if (num_remaps) *num_remaps = nr;
     s->params_dirty = true;
-    return NXM_OK;
+    return invalidate_codes(s);
 }
 
 int nxm_particles_shift_remove(nxm_state* s, uint32_t start, uint32_t end) {
@@ -725,7 +739,7 @@ int nxm_particles_shift_remove(nxm_state* s, uint32_t start, uint32_t end) {
     erase(s->group_id);
     s->n -= removed;
     s->params_dirty = true;
-    return NXM_OK;
+    return invalidate_codes(s);
 }
 
 int nxm_step(nxm_pipeline* pipeline, nxm_state* s, nxm_timestamps* ts) {
@@ -766,7 +780,7 @@ int nxm_debug_sort(nxm_pipeline* pipeline, nxm_state* s, int with_p2g) {
     if (s->n == 0) return NXM_OK;
     DevPtrs P = dev_ptrs(s);
     LaunchCfg c = launch_cfg(s);
-    fast::launch_sort(P, c, s->deterministic, s->stream);
+    fast::launch_sort(P, c, /*with_extras=*/true, /*canonical=*/s->deterministic, s->stream);
     s->launches += (uint64_t)sort_launches(s->deterministic);
     if (with_p2g) {
         if (s->deterministic) exact::launch_p2g_gather(P, c, s->stream);

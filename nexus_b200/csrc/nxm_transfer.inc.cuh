@@ -8,6 +8,9 @@
 #ifndef NXM_NS
 #error "define NXM_NS before including nxm_transfer.inc.cuh"
 #endif
+#ifndef NXM_FAST
+#error "define NXM_FAST (true: fast build, false: reference operation order)"
+#endif
 
 namespace nxm {
 namespace NXM_NS {
@@ -113,13 +116,25 @@ __global__ void __launch_bounds__(256) k_grid_update(DevPtrs P) {
 // One CTA per active block (grid-stride): the 6x6x6 node-velocity halo of the
 // block and its +1 neighbours is staged in shared memory, then each thread
 // gathers and updates one of the block's primary particles.
-__global__ void __launch_bounds__(256) k_g2p_update(DevPtrs P) {
+#ifndef NXM_G2P_MIN_CTAS
+#define NXM_G2P_MIN_CTAS 4  // CTAs of 256 threads per SM the register budget is sized for
+#endif
+__global__ void __launch_bounds__(256, NXM_G2P_MIN_CTAS) k_g2p_update(DevPtrs P) {
     __shared__ float4 halo[216];
     const Params prm = *P.params;
     const float dx = prm.dx, dt = prm.dt;
     const float inv_d = 4.0f / (dx * dx);
     const uint32_t nb = P.counters->num_blocks;
     for (uint32_t b = blockIdx.x; b < nb; b += gridDim.x) {
+        const uint32_t first = P.first[b], np = P.nprim[b];
+        if (np == 0) continue;  // neighbour-only block: no primary particles to update
+        // issue this thread's first particle loads before the halo barrier
+        uint32_t pid_next = threadIdx.x < np ? P.sorted[first + threadIdx.x] : 0u;
+        float4 xm_next = make_float4(0.f, 0.f, 0.f, 0.f), vf_next = xm_next;
+        if (threadIdx.x < np) {
+            xm_next = reinterpret_cast<const float4*>(&P.kin[pid_next])[0];
+            vf_next = reinterpret_cast<const float4*>(&P.kin[pid_next])[1];
+        }
         for (uint32_t t = threadIdx.x; t < 216u; t += blockDim.x) {
             const uint32_t tx = t % 6u, ty = (t / 6u) % 6u, tz = t / 36u;
             const uint32_t ox = tx >= 4u, oy = ty >= 4u, oz = tz >= 4u;
@@ -133,12 +148,16 @@ __global__ void __launch_bounds__(256) k_g2p_update(DevPtrs P) {
             halo[t] = v;
         }
         __syncthreads();
-        const uint32_t first = P.first[b], np = P.nprim[b];
         for (uint32_t k = threadIdx.x; k < np; k += blockDim.x) {
-            const uint32_t pid = P.sorted[first + k];
+            const uint32_t pid = pid_next;
             float4* kr = reinterpret_cast<float4*>(&P.kin[pid]);
-            const float4 xm = kr[0];
-            const float4 vf = kr[1];
+            const float4 xm = xm_next;
+            const float4 vf = vf_next;
+            if (k + blockDim.x < np) {  // prefetch the next particle of this thread
+                pid_next = P.sorted[first + k + blockDim.x];
+                xm_next = reinterpret_cast<const float4*>(&P.kin[pid_next])[0];
+                vf_next = reinterpret_cast<const float4*>(&P.kin[pid_next])[1];
+            }
             uint32_t flags = __float_as_uint(vf.w);
             const v3 pt = mk(xm.x, xm.y, xm.z);
             float mass = xm.w;
@@ -147,7 +166,38 @@ __global__ void __launch_bounds__(256) k_g2p_update(DevPtrs P) {
             v3 velocity = splat(0.f);
             m3 grad = mzero();
             float vgd = 0.f;
-            if (flags & PFLAG_ENABLED) {
+            if ((flags & PFLAG_ENABLED) && NXM_FAST) {
+                // Same sums, factored: with dpt_i = ref + s_i dx,
+                //   grad = inv_d (v (x) ref + dx [Sx Sy Sz]),  S_a = sum_i w_i v_i s_i,a
+                //   vgd  = inv_d (v . ref + dx (Sx.x + Sy.y + Sz.z))
+                // so each node costs one weight product and 3 + (s != 0) FMAs.
+                const float inv_dx = prm.inv_dx;
+                const v3 ref = assoc_cell_of(dx, pt) * dx - pt;
+                const v3 wx = kernel_eval_all(-ref.x * inv_dx);
+                const v3 wy = kernel_eval_all(-ref.y * inv_dx);
+                const v3 wz = kernel_eval_all(-ref.z * inv_dx);
+                const CellInfo ci = cell_info(dx, pt);
+                const uint32_t packed = ci.ax + 6u * ci.ay + 36u * ci.az;
+                v3 sxv = splat(0.f), syv = splat(0.f), szv = splat(0.f);
+#pragma unroll
+                for (int sz = 0; sz < 3; ++sz) {
+#pragma unroll
+                    for (int sy = 0; sy < 3; ++sy) {
+                        const float wyz = vget(wy, sy) * vget(wz, sz);
+#pragma unroll
+                        for (int sx = 0; sx < 3; ++sx) {
+                            const float4 h = halo[packed + (uint32_t)(sx + 6 * sy + 36 * sz)];
+                            const v3 wc = mk(h.x, h.y, h.z) * (vget(wx, sx) * wyz);
+                            velocity = velocity + wc;
+                            if (sx) sxv = sxv + wc * (float)sx;
+                            if (sy) syv = syv + wc * (float)sy;
+                            if (sz) szv = szv + wc * (float)sz;
+                        }
+                    }
+                }
+                grad = (outer(velocity, ref) + mkm(sxv, syv, szv) * dx) * inv_d;
+                vgd = (dot(velocity, ref) + dx * (sxv.x + syv.y + szv.z)) * inv_d;
+            } else if (flags & PFLAG_ENABLED) {
                 const v3 ref = assoc_cell_of(dx, pt) * dx - pt;
                 const v3 w0 = kernel_eval_all(-ref.x / dx);
                 const v3 w1 = kernel_eval_all(-ref.y / dx);
@@ -198,7 +248,7 @@ __global__ void __launch_bounds__(256) k_g2p_update(DevPtrs P) {
                 float4 s4 = P.pstate[pid];
                 st[0] = s4.x; st[1] = s4.y; st[2] = s4.z; st[3] = s4.w;
             }
-            const m3 tau = model_update(tag, mat.w, st, F, A);
+            const m3 tau = model_update<NXM_FAST>(tag, mat.w, st, F, A);
             m3 aff = A * mass - tau * (init_volume * inv_d * dt);
             v3 new_pos = pt;
             const bool nan = (np_.x != np_.x) || (np_.y != np_.y) || (np_.z != np_.z);
@@ -221,9 +271,13 @@ __global__ void __launch_bounds__(256) k_g2p_update(DevPtrs P) {
             dw[1] = make_float4(F.c1.x, F.c1.y, F.c1.z, damping);
             dw[2] = make_float4(F.c2.x, F.c2.y, F.c2.z, d2.w);
             if (mat.has_state) P.pstate[pid] = make_float4(st[0], st[1], st[2], st[3]);
+            // block key of the new position, for the next step's activation
+            const CellInfo nc = cell_info(dx, new_pos);
+            P.pcode[pid] = make_uint2(pack_key(nc.bx, nc.by, nc.bz), nc.ax | (nc.ay << 2) | (nc.az << 4));
         }
         __syncthreads();
     }
+    if (blockIdx.x == 0 && threadIdx.x == 0) P.counters->codes_valid = 1u;
 }
 
 }  // namespace
@@ -233,7 +287,7 @@ void launch_grid_update(const DevPtrs& P, const LaunchCfg& c, cudaStream_t s) {
 }
 
 void launch_g2p_update(const DevPtrs& P, const LaunchCfg& c, cudaStream_t s) {
-    k_g2p_update<<<c.sm_count * 4, 256, 0, s>>>(P);
+    k_g2p_update<<<c.sm_count * NXM_G2P_MIN_CTAS, 256, 0, s>>>(P);
 }
 
 }  // namespace NXM_NS

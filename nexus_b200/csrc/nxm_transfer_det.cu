@@ -5,6 +5,7 @@
 // sort order these reproduce the CPU oracle's f32 arithmetic operation by
 // operation (up to the last bits of logf/expf/sinf).
 #define NXM_NS exact
+#define NXM_FAST false
 #include "nxm_transfer.inc.cuh"
 
 namespace nxm {

@@ -107,11 +107,13 @@ class NexusError(RuntimeError):
         super().__init__(f"{what}: {msg} ({code})")
 
 
-def load(path: str = LIB_PATH):
-    """Loads libnexus_mpm.so (no fallback: a missing library is an error)."""
+def load(path: str | None = None):
+    """Loads libnexus_mpm.so (no fallback: a missing library is an error).
+    NXM_LIB in the environment selects another build of the same library."""
     global _LIB
     if _LIB is not None:
         return _LIB
+    path = path or os.environ.get("NXM_LIB") or LIB_PATH
     if not os.path.exists(path):
         raise FileNotFoundError(f"{path} not built: run python -m nexus_b200.build")
     lib = C.CDLL(path)
