@@ -25,6 +25,7 @@ UNITS = {
     "nxm_sort.cu": [],
     "nxm_transfer_fast.cu": [],
     "nxm_transfer_det.cu": ["--fmad=false"],
+    "nxm_noalloc.cu": [],
 }
 
 HEADERS = ["nxm_device.cuh", "nxm_layout.h", "nxm_kernels.h", "nxm_transfer.inc.cuh"]

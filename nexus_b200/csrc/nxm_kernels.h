@@ -71,6 +71,11 @@ void launch_grid_update(const DevPtrs& P, const LaunchCfg& c, cudaStream_t s);
 void launch_g2p_update(const DevPtrs& P, const LaunchCfg& c, cudaStream_t s);
 }  // namespace exact
 
+// Primary-only block sort of plain float4 positions (x, y, z, unused): no
+// per-particle scratch; P.sorted receives the ids, P.nodes may be null.
+void launch_sort_positions(const DevPtrs& P, const LaunchCfg& c, const float4* pos, cudaStream_t s);
+constexpr int kSortPositionsLaunches = 8;
+
 // Kernels issued per phase (sort counts the canonical segment sort when on).
 int sort_launches(bool canonical);
 constexpr int kP2gLaunches = 1;

@@ -171,7 +171,7 @@ __global__ void __launch_bounds__(256) k_block_prep(DevPtrs P) {
     const uint32_t nthreads = total * 64u;
     for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < nthreads; t += gridDim.x * blockDim.x) {
         const uint32_t b = t >> 6, k = t & 63u;
-        P.nodes[t] = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (P.nodes) P.nodes[t] = make_float4(0.f, 0.f, 0.f, 0.f);
         if (k < NUM_NBH) {
             int4 v = P.bvid[b];
             int sx, sy, sz;
@@ -389,9 +389,79 @@ __global__ void __launch_bounds__(256) k_sort_segments(DevPtrs P) {
 
 inline int grid_for(int sm_count, int per_sm) { return sm_count * per_sm; }
 
+
+// ---------------------------------------------------------------------------
+// Primary-only sort of plain float4 positions (no per-particle scratch: the
+// key is recomputed from the position in each pass and the primary block is
+// found again through the hash).  Used by the allocation-free entry point.
+
+__device__ __forceinline__ uint32_t key_of(const float4* pos, uint32_t p, float dx, uint32_t* assoc) {
+    const float4 x = __ldg(&pos[p]);
+    const CellInfo ci = cell_info(dx, mk(x.x, x.y, x.z));
+    *assoc = ci.ax | (ci.ay << 2) | (ci.az << 4);
+    return pack_key(ci.bx, ci.by, ci.bz);
+}
+
+__global__ void __launch_bounds__(256) k_touch_primary_pos(DevPtrs P, const float4* __restrict__ pos) {
+    const uint32_t n = P.params->n;
+    const float dx = P.params->dx;
+    const uint32_t hmask = P.params->hash_capacity - 1;
+    const uint32_t bcap = P.params->block_capacity;
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t base = warp * 32u; base < n; base += nwarps * 32u) {
+        const uint32_t p = base + lane;
+        uint32_t assoc = 0, key = NONE;
+        if (p < n) key = key_of(pos, p, dx, &assoc);
+        uint32_t peers = __match_any_sync(0xFFFFFFFFu, key);
+        if (p < n && lane == (uint32_t)(__ffs(peers) - 1))
+            hash_insert(P, key, key_x(key), key_y(key), key_z(key), true, 0, hmask, bcap);
+    }
+}
+
+template <bool kScatter>
+__global__ void __launch_bounds__(256) k_bucket_pos(DevPtrs P, const float4* __restrict__ pos) {
+    const uint32_t n = P.params->n;
+    const float dx = P.params->dx;
+    const uint32_t hmask = P.params->hash_capacity - 1;
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t base = warp * 32u; base < n; base += nwarps * 32u) {
+        const uint32_t p = base + lane;
+        uint32_t h0 = NONE, assoc = 0;
+        if (p < n) {
+            h0 = hash_find(P, key_of(pos, p, dx, &assoc), hmask);
+            if (h0 == NONE) set_status(P.counters, STATUS_MISSING_BLOCK);
+        }
+        const uint32_t az = (assoc >> 4) & 3u;
+        const uint32_t key = (h0 != NONE) ? h0 * 16u + az : NONE;
+        const uint32_t slot = warp_agg_add(key, key != NONE ? &P.cursors[h0 * NUM_BUCKETS + az] : nullptr);
+        if (kScatter && key != NONE && slot < P.params->sorted_capacity) P.sorted[slot] = p;
+    }
+}
+
 }  // namespace
 
 int sort_launches(bool canonical) { return canonical ? 9 : 8; }
+
+void launch_sort_positions(const DevPtrs& P, const LaunchCfg& c, const float4* pos, cudaStream_t s) {
+    const int g = grid_for(c.sm_count, 8);
+    int reset_grid = (int)((c.hash_capacity + 255u) / 256u);
+    if (reset_grid > g) reset_grid = g;
+    if (reset_grid < 1) reset_grid = 1;
+    k_sort_reset<<<reset_grid, 256, 0, s>>>(P, c.hash_capacity);
+    k_touch_primary_pos<<<g, 256, 0, s>>>(P, pos);
+    k_touch_nbh<<<g, 256, 0, s>>>(P);
+    k_block_prep<<<g, 256, 0, s>>>(P);
+    k_bucket_pos<false><<<g, 256, 0, s>>>(P, pos);
+    k_scan_tiles<<<c.sm_count, kScanThreads, 0, s>>>(P);
+    k_scan_apply<<<c.sm_count, kScanThreads, 0, s>>>(P);
+    k_bucket_pos<true><<<g, 256, 0, s>>>(P, pos);
+}
+
+
 
 namespace fast {
 

@@ -95,6 +95,7 @@ SIGNATURES = {
     "nxm_error_string": (C.c_char_p, [C.c_int]),
     "nxm_state_kernel_launches": (C.c_uint64, [_vp]),
     "nxm_state_cuda_stream": (C.c_void_p, [_vp]),
+    "nxm_sort_blocks_noalloc": (C.c_int, [_vp, C.c_uint32, C.c_float, _vp, _vp, _vp, C.c_uint32, _u, _vp]),
 }
 
 _LIB = None
