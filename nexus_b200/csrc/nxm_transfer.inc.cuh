@@ -112,168 +112,166 @@ __global__ void __launch_bounds__(256) k_grid_update(DevPtrs P) {
     }
 }
 
-// g2p.rs:42-347 (non-CPIC) fused with particle_update.rs:60-201.
-// One CTA per active block (grid-stride): the 6x6x6 node-velocity halo of the
-// block and its +1 neighbours is staged in shared memory, then each thread
-// gathers and updates one of the block's primary particles.
+// Velocity of shared-halo node t (t = x + 6 y + 36 z, x, y, z in [0, 6)) of
+// block b: node (x mod 4, ...) of the block itself or of one of its +1
+// neighbours; zero where that neighbour is not active.
+__device__ __forceinline__ float4 halo_node(const DevPtrs& P, uint32_t b, uint32_t t) {
+    const uint32_t tx = t % 6u, ty = (t / 6u) % 6u, tz = t / 36u;
+    const uint32_t ox = tx >= 4u, oy = ty >= 4u, oz = tz >= 4u;
+    const uint32_t oct = ox * 4u + oy * 2u + oz;
+    const uint32_t blk = oct == 0 ? b : P.nbh[b * NUM_NBH + oct - 1u];
+    if (blk == NONE) return make_float4(0.f, 0.f, 0.f, 0.f);
+    const float4 nd = P.nodes[blk * 64u + (tx - 4u * ox) + 4u * (ty - 4u * oy) + 16u * (tz - 4u * oz)];
+    return make_float4(nd.x, nd.y, nd.z, 0.f);
+}
+
+// g2p.rs:150-270 (non-CPIC) fused with particle_update.rs:60-201 for one
+// particle: gathers velocity and velocity gradient from the 6x6x6 halo of its
+// block (shared memory), then advects, updates F and the model, and writes the
+// particle back together with the block key of its new position.
+__device__ __forceinline__ void g2p_particle(const DevPtrs& P, const Params& prm, const float4* __restrict__ halo,
+                                             uint32_t pid, float4 xm, float4 vf) {
+    const float dx = prm.dx, dt = prm.dt;
+    const float inv_d = 4.0f / (dx * dx);
+    float4* kr = reinterpret_cast<float4*>(&P.kin[pid]);
+    uint32_t flags = __float_as_uint(vf.w);
+    const v3 pt = mk(xm.x, xm.y, xm.z);
+    float mass = xm.w;
+
+    // ---- G2P (g2p.rs:150-270)
+    v3 velocity = splat(0.f);
+    m3 grad = mzero();
+    float vgd = 0.f;
+    if ((flags & PFLAG_ENABLED) && NXM_FAST) {
+        // Same sums, factored: with dpt_i = ref + s_i dx,
+        //   grad = inv_d (v (x) ref + dx [Sx Sy Sz]),  S_a = sum_i w_i v_i s_i,a
+        //   vgd  = inv_d (v . ref + dx (Sx.x + Sy.y + Sz.z))
+        // so each node costs one weight product and 3 + (s != 0) FMAs.
+        const float inv_dx = prm.inv_dx;
+        const v3 ref = assoc_cell_of(dx, pt) * dx - pt;
+        const v3 wx = kernel_eval_all(-ref.x * inv_dx);
+        const v3 wy = kernel_eval_all(-ref.y * inv_dx);
+        const v3 wz = kernel_eval_all(-ref.z * inv_dx);
+        const CellInfo ci = cell_info(dx, pt);
+        const uint32_t packed = ci.ax + 6u * ci.ay + 36u * ci.az;
+        v3 sxv = splat(0.f), syv = splat(0.f), szv = splat(0.f);
+#pragma unroll
+        for (int sz = 0; sz < 3; ++sz) {
+#pragma unroll
+            for (int sy = 0; sy < 3; ++sy) {
+                const float wyz = vget(wy, sy) * vget(wz, sz);
+#pragma unroll
+                for (int sx = 0; sx < 3; ++sx) {
+                    const float4 h = halo[packed + (uint32_t)(sx + 6 * sy + 36 * sz)];
+                    const v3 wc = mk(h.x, h.y, h.z) * (vget(wx, sx) * wyz);
+                    velocity = velocity + wc;
+                    if (sx) sxv = sxv + wc * (float)sx;
+                    if (sy) syv = syv + wc * (float)sy;
+                    if (sz) szv = szv + wc * (float)sz;
+                }
+            }
+        }
+        grad = (outer(velocity, ref) + mkm(sxv, syv, szv) * dx) * inv_d;
+        vgd = (dot(velocity, ref) + dx * (sxv.x + syv.y + szv.z)) * inv_d;
+    } else if (flags & PFLAG_ENABLED) {
+        const v3 ref = assoc_cell_of(dx, pt) * dx - pt;
+        const v3 w0 = kernel_eval_all(-ref.x / dx);
+        const v3 w1 = kernel_eval_all(-ref.y / dx);
+        const v3 w2 = kernel_eval_all(-ref.z / dx);
+        const CellInfo ci = cell_info(dx, pt);
+        const uint32_t packed = ci.ax + 6u * ci.ay + 36u * ci.az;
+#pragma unroll
+        for (int i = 0; i < 27; ++i) {
+            int sx, sy, sz;
+            nbh_shift(i, sx, sy, sz);
+            const float4 h = halo[packed + (uint32_t)(sx + 6 * sy + 36 * sz)];
+            const v3 cv = mk(h.x, h.y, h.z);
+            const v3 dpt = ref + mk((float)sx, (float)sy, (float)sz) * dx;
+            const float weight = vget(w0, sx) * vget(w1, sy) * vget(w2, sz);
+            velocity = velocity + cv * weight;
+            grad = grad + outer(cv, dpt) * (weight * inv_d);
+            vgd += weight * inv_d * dot(cv, dpt);
+        }
+    }
+
+    // ---- particle update (particle_update.rs:60-201, non-CPIC: Cdf = 0)
+    const float4* dr = reinterpret_cast<const float4*>(&P.def[pid]);
+    const float4 d0 = dr[0], d1 = dr[1], d2 = dr[2];
+    m3 F = mkm(mk(d0.x, d0.y, d0.z), mk(d1.x, d1.y, d1.z), mk(d2.x, d2.y, d2.z));
+    const float init_volume = d0.w, damping = d1.w;
+    const uint32_t mid = __float_as_uint(d2.w);
+    const Material& mat = P.materials[mid];
+    const uint32_t tag = mat.tag;
+
+    v3 v = velocity;
+    const float vl = length(v);
+    if (vl > dx / dt) v = ((v / vl) * dx) / dt;
+    v = v / (1.0f + damping * dt);
+    if (flags & PFLAG_FIXED) v = splat(0.f);
+    const v3 np_ = pt + v * dt;
+    const m3 A = grad;
+    if (tag != MODEL_FLUID) {
+        F = F + (A * dt) * F;
+    } else {
+        const float fd0 = F.c0.x;
+        float rate = vgd * dt / 3.0f;
+        rate = rclamp(rate, -0.1f, 0.1f);
+        const float nd = rclamp(fd0 + rate * fd0, 0.5f, 2.0f);
+        F = diag(splat(nd));
+    }
+    float st[4] = {0.f, 0.f, 0.f, 0.f};
+    if (mat.has_state) {
+        float4 s4 = P.pstate[pid];
+        st[0] = s4.x; st[1] = s4.y; st[2] = s4.z; st[3] = s4.w;
+    }
+    const m3 tau = model_update<NXM_FAST>(tag, mat.w, st, F, A);
+    m3 aff = A * mass - tau * (init_volume * inv_d * dt);
+    v3 new_pos = pt;
+    const bool nan = (np_.x != np_.x) || (np_.y != np_.y) || (np_.z != np_.z);
+    if (!nan && det(F) > 0.0f) {
+        new_pos = np_;
+    } else {
+        flags &= ~PFLAG_ENABLED;
+        v = splat(0.f);
+        F = mident();
+        aff = mzero();
+        mass = 0.f;
+    }
+    kr[0] = make_float4(new_pos.x, new_pos.y, new_pos.z, mass);
+    kr[1] = make_float4(v.x, v.y, v.z, __uint_as_float(flags));
+    kr[2] = make_float4(aff.c0.x, aff.c0.y, aff.c0.z, vgd);
+    kr[3] = make_float4(aff.c1.x, aff.c1.y, aff.c1.z, 0.f);
+    kr[4] = make_float4(aff.c2.x, aff.c2.y, aff.c2.z, 0.f);
+    float4* dw = reinterpret_cast<float4*>(&P.def[pid]);
+    dw[0] = make_float4(F.c0.x, F.c0.y, F.c0.z, init_volume);
+    dw[1] = make_float4(F.c1.x, F.c1.y, F.c1.z, damping);
+    dw[2] = make_float4(F.c2.x, F.c2.y, F.c2.z, d2.w);
+    if (mat.has_state) P.pstate[pid] = make_float4(st[0], st[1], st[2], st[3]);
+    // block key of the new position, for the next step's activation
+    const CellInfo nc = cell_info(dx, new_pos);
+    P.pcode[pid] = make_uint2(pack_key(nc.bx, nc.by, nc.bz), nc.ax | (nc.ay << 2) | (nc.az << 4));
+}
+
 #ifndef NXM_G2P_MIN_CTAS
 #define NXM_G2P_MIN_CTAS 4  // CTAs of 256 threads per SM the register budget is sized for
 #endif
+
+// One CTA per active block (grid-stride): the halo of the block and its +1
+// neighbours is staged in shared memory, then each thread gathers and
+// updates one of the block's primary particles.
 __global__ void __launch_bounds__(256, NXM_G2P_MIN_CTAS) k_g2p_update(DevPtrs P) {
     __shared__ float4 halo[216];
     const Params prm = *P.params;
-    const float dx = prm.dx, dt = prm.dt;
-    const float inv_d = 4.0f / (dx * dx);
     const uint32_t nb = P.counters->num_blocks;
     for (uint32_t b = blockIdx.x; b < nb; b += gridDim.x) {
         const uint32_t first = P.first[b], np = P.nprim[b];
         if (np == 0) continue;  // neighbour-only block: no primary particles to update
-        // issue this thread's first particle loads before the halo barrier
-        uint32_t pid_next = threadIdx.x < np ? P.sorted[first + threadIdx.x] : 0u;
-        float4 xm_next = make_float4(0.f, 0.f, 0.f, 0.f), vf_next = xm_next;
-        if (threadIdx.x < np) {
-            xm_next = reinterpret_cast<const float4*>(&P.kin[pid_next])[0];
-            vf_next = reinterpret_cast<const float4*>(&P.kin[pid_next])[1];
-        }
-        for (uint32_t t = threadIdx.x; t < 216u; t += blockDim.x) {
-            const uint32_t tx = t % 6u, ty = (t / 6u) % 6u, tz = t / 36u;
-            const uint32_t ox = tx >= 4u, oy = ty >= 4u, oz = tz >= 4u;
-            const uint32_t oct = ox * 4u + oy * 2u + oz;
-            const uint32_t blk = oct == 0 ? b : P.nbh[b * NUM_NBH + oct - 1u];
-            float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-            if (blk != NONE) {
-                float4 nd = P.nodes[blk * 64u + (tx - 4u * ox) + 4u * (ty - 4u * oy) + 16u * (tz - 4u * oz)];
-                v = make_float4(nd.x, nd.y, nd.z, 0.f);
-            }
-            halo[t] = v;
-        }
+        for (uint32_t t = threadIdx.x; t < 216u; t += blockDim.x) halo[t] = halo_node(P, b, t);
         __syncthreads();
         for (uint32_t k = threadIdx.x; k < np; k += blockDim.x) {
-            const uint32_t pid = pid_next;
-            float4* kr = reinterpret_cast<float4*>(&P.kin[pid]);
-            const float4 xm = xm_next;
-            const float4 vf = vf_next;
-            if (k + blockDim.x < np) {  // prefetch the next particle of this thread
-                pid_next = P.sorted[first + k + blockDim.x];
-                xm_next = reinterpret_cast<const float4*>(&P.kin[pid_next])[0];
-                vf_next = reinterpret_cast<const float4*>(&P.kin[pid_next])[1];
-            }
-            uint32_t flags = __float_as_uint(vf.w);
-            const v3 pt = mk(xm.x, xm.y, xm.z);
-            float mass = xm.w;
-
-            // ---- G2P (g2p.rs:150-270)
-            v3 velocity = splat(0.f);
-            m3 grad = mzero();
-            float vgd = 0.f;
-            if ((flags & PFLAG_ENABLED) && NXM_FAST) {
-                // Same sums, factored: with dpt_i = ref + s_i dx,
-                //   grad = inv_d (v (x) ref + dx [Sx Sy Sz]),  S_a = sum_i w_i v_i s_i,a
-                //   vgd  = inv_d (v . ref + dx (Sx.x + Sy.y + Sz.z))
-                // so each node costs one weight product and 3 + (s != 0) FMAs.
-                const float inv_dx = prm.inv_dx;
-                const v3 ref = assoc_cell_of(dx, pt) * dx - pt;
-                const v3 wx = kernel_eval_all(-ref.x * inv_dx);
-                const v3 wy = kernel_eval_all(-ref.y * inv_dx);
-                const v3 wz = kernel_eval_all(-ref.z * inv_dx);
-                const CellInfo ci = cell_info(dx, pt);
-                const uint32_t packed = ci.ax + 6u * ci.ay + 36u * ci.az;
-                v3 sxv = splat(0.f), syv = splat(0.f), szv = splat(0.f);
-#pragma unroll
-                for (int sz = 0; sz < 3; ++sz) {
-#pragma unroll
-                    for (int sy = 0; sy < 3; ++sy) {
-                        const float wyz = vget(wy, sy) * vget(wz, sz);
-#pragma unroll
-                        for (int sx = 0; sx < 3; ++sx) {
-                            const float4 h = halo[packed + (uint32_t)(sx + 6 * sy + 36 * sz)];
-                            const v3 wc = mk(h.x, h.y, h.z) * (vget(wx, sx) * wyz);
-                            velocity = velocity + wc;
-                            if (sx) sxv = sxv + wc * (float)sx;
-                            if (sy) syv = syv + wc * (float)sy;
-                            if (sz) szv = szv + wc * (float)sz;
-                        }
-                    }
-                }
-                grad = (outer(velocity, ref) + mkm(sxv, syv, szv) * dx) * inv_d;
-                vgd = (dot(velocity, ref) + dx * (sxv.x + syv.y + szv.z)) * inv_d;
-            } else if (flags & PFLAG_ENABLED) {
-                const v3 ref = assoc_cell_of(dx, pt) * dx - pt;
-                const v3 w0 = kernel_eval_all(-ref.x / dx);
-                const v3 w1 = kernel_eval_all(-ref.y / dx);
-                const v3 w2 = kernel_eval_all(-ref.z / dx);
-                const CellInfo ci = cell_info(dx, pt);
-                const uint32_t packed = ci.ax + 6u * ci.ay + 36u * ci.az;
-#pragma unroll
-                for (int i = 0; i < 27; ++i) {
-                    int sx, sy, sz;
-                    nbh_shift(i, sx, sy, sz);
-                    const float4 h = halo[packed + (uint32_t)(sx + 6 * sy + 36 * sz)];
-                    const v3 cv = mk(h.x, h.y, h.z);
-                    const v3 dpt = ref + mk((float)sx, (float)sy, (float)sz) * dx;
-                    const float weight = vget(w0, sx) * vget(w1, sy) * vget(w2, sz);
-                    velocity = velocity + cv * weight;
-                    grad = grad + outer(cv, dpt) * (weight * inv_d);
-                    vgd += weight * inv_d * dot(cv, dpt);
-                }
-            }
-
-            // ---- particle update (particle_update.rs:60-201, non-CPIC: Cdf = 0)
-            const float4* dr = reinterpret_cast<const float4*>(&P.def[pid]);
-            const float4 d0 = dr[0], d1 = dr[1], d2 = dr[2];
-            m3 F = mkm(mk(d0.x, d0.y, d0.z), mk(d1.x, d1.y, d1.z), mk(d2.x, d2.y, d2.z));
-            const float init_volume = d0.w, damping = d1.w;
-            const uint32_t mid = __float_as_uint(d2.w);
-            const Material& mat = P.materials[mid];
-            const uint32_t tag = mat.tag;
-
-            v3 v = velocity;
-            const float vl = length(v);
-            if (vl > dx / dt) v = ((v / vl) * dx) / dt;
-            v = v / (1.0f + damping * dt);
-            if (flags & PFLAG_FIXED) v = splat(0.f);
-            const v3 np_ = pt + v * dt;
-            const m3 A = grad;
-            if (tag != MODEL_FLUID) {
-                F = F + (A * dt) * F;
-            } else {
-                const float fd0 = F.c0.x;
-                float rate = vgd * dt / 3.0f;
-                rate = rclamp(rate, -0.1f, 0.1f);
-                const float nd = rclamp(fd0 + rate * fd0, 0.5f, 2.0f);
-                F = diag(splat(nd));
-            }
-            float st[4] = {0.f, 0.f, 0.f, 0.f};
-            if (mat.has_state) {
-                float4 s4 = P.pstate[pid];
-                st[0] = s4.x; st[1] = s4.y; st[2] = s4.z; st[3] = s4.w;
-            }
-            const m3 tau = model_update<NXM_FAST>(tag, mat.w, st, F, A);
-            m3 aff = A * mass - tau * (init_volume * inv_d * dt);
-            v3 new_pos = pt;
-            const bool nan = (np_.x != np_.x) || (np_.y != np_.y) || (np_.z != np_.z);
-            if (!nan && det(F) > 0.0f) {
-                new_pos = np_;
-            } else {
-                flags &= ~PFLAG_ENABLED;
-                v = splat(0.f);
-                F = mident();
-                aff = mzero();
-                mass = 0.f;
-            }
-            kr[0] = make_float4(new_pos.x, new_pos.y, new_pos.z, mass);
-            kr[1] = make_float4(v.x, v.y, v.z, __uint_as_float(flags));
-            kr[2] = make_float4(aff.c0.x, aff.c0.y, aff.c0.z, vgd);
-            kr[3] = make_float4(aff.c1.x, aff.c1.y, aff.c1.z, 0.f);
-            kr[4] = make_float4(aff.c2.x, aff.c2.y, aff.c2.z, 0.f);
-            float4* dw = reinterpret_cast<float4*>(&P.def[pid]);
-            dw[0] = make_float4(F.c0.x, F.c0.y, F.c0.z, init_volume);
-            dw[1] = make_float4(F.c1.x, F.c1.y, F.c1.z, damping);
-            dw[2] = make_float4(F.c2.x, F.c2.y, F.c2.z, d2.w);
-            if (mat.has_state) P.pstate[pid] = make_float4(st[0], st[1], st[2], st[3]);
-            // block key of the new position, for the next step's activation
-            const CellInfo nc = cell_info(dx, new_pos);
-            P.pcode[pid] = make_uint2(pack_key(nc.bx, nc.by, nc.bz), nc.ax | (nc.ay << 2) | (nc.az << 4));
+            const uint32_t pid = P.sorted[first + k];
+            const float4* kr = reinterpret_cast<const float4*>(&P.kin[pid]);
+            g2p_particle(P, prm, halo, pid, kr[0], kr[1]);
         }
         __syncthreads();
     }

@@ -15,34 +15,48 @@ __device__ __forceinline__ void set_status_f(Counters* c, uint32_t bit) { atomic
 // P2G (solver/p2g.rs:64-351 computes the same node sums in gather form).
 //
 // One CTA per active block (grid-stride).  The block's primary particles are
-// staged in shared memory in chunks of kP2gChunk: each staged record holds
-// q = m v + C (x_0 - x_p) (x_0 = stencil node (0,0,0)), m, C dx and the
-// three per-axis B-spline weight triples, so that the contribution to
-// stencil node s is w_x[s.x] w_y[s.y] w_z[s.z] (q + (C dx) s, m).  The chunk
-// is binned by associated cell (counting sort in shared memory); then each
-// warp takes one cell at a time with lane l < 27 owning stencil offset s(l):
-// the lanes read the cell's particles by broadcast and accumulate in
-// registers, and one shared atomic per lane and component adds the cell's
-// sum to the 6x6x6 node tile (the block plus the first two node layers of
-// its +1 neighbours).  The tile goes to global memory with one float4
-// atomic per non-empty node; nodes were zeroed by the sort.
-constexpr int kP2gThreads = 256;
+// staged in shared memory in chunks of kP2gChunk.  A staged record holds
+//   q = m v + C (x_0 - x_p)  (x_0 = stencil node (0,0,0)) and m,
+//   the three columns of C dx, each carrying one z weight w_z[k] alongside,
+//   the nine products w_x[i] w_y[j],
+// so the contribution to stencil node s is w_x[s.x] w_y[s.y] w_z[s.z]
+// (q + (C dx) s, m).  The chunk is binned by associated cell (counting sort
+// in shared memory).  Each warp then takes one cell at a time: lane l < 27
+// owns the stencil column (s.x, s.y) = ((l mod 9) mod 3, (l mod 9) / 3) for
+// particle group l / 9, so a pass reads three particles (three broadcast
+// addresses per load) and each lane accumulates its column's three nodes.  A
+// three-way shuffle exchange leaves lane l with the cell's full sum for node
+// (s.x, s.y, l / 9), which it adds to the warp's private 6x6x6 node tile
+// (the block plus the first two node layers of its +1 neighbours): the 27
+// lanes own distinct nodes and no other warp writes that tile, so no atomics.
+// At the end of the block the warp tiles are summed and each non-empty node
+// goes to global memory with one float4 atomic; nodes were zeroed by the sort.
+#ifndef NXM_P2G_WARPS
+#define NXM_P2G_WARPS 8
+#endif
 #ifndef NXM_P2G_CHUNK
-#define NXM_P2G_CHUNK 512
+#define NXM_P2G_CHUNK 256
 #endif
 #ifndef NXM_P2G_MIN_CTAS
 #define NXM_P2G_MIN_CTAS 3
 #endif
+constexpr int kP2gWarps = NXM_P2G_WARPS;
+constexpr int kP2gThreads = 32 * kP2gWarps;
 constexpr int kP2gChunk = NXM_P2G_CHUNK;  // particles staged per pass
-constexpr int kP2gRec = 24;  // floats per staged particle
-// record layout: [0..3] q.xyz, m | [4..12] (C dx) columns 0,1,2 | [13..15] w_x | [16..18] w_y | [19..21] w_z
-constexpr size_t kP2gSmem = (size_t)kP2gChunk * kP2gRec * 4 + 216 * 16 + (64 + 68) * 4 + kP2gChunk * (2 + 2 + 1);
+constexpr int kP2gRec = 28;  // floats per staged particle
+// record: [0..3] q.xyz, m | [4..7] (C dx).c0, w_z[0] | [8..11] (C dx).c1, w_z[1]
+//       | [12..15] (C dx).c2, w_z[2] | [16 + i + 3 j] w_x[i] w_y[j] | [25..27] unused
+constexpr size_t kP2gSmem = (size_t)kP2gWarps * 216 * 16 + (size_t)kP2gChunk * kP2gRec * 4 + (64 + 68) * 4 +
+                            (size_t)kP2gChunk * (2 + 2 + 1);
+static_assert(kP2gChunk <= 65536, "staged particle indices are 16-bit");
+
+__device__ __forceinline__ float4 f4add(float4 a, float4 b) { return make_float4(a.x + b.x, a.y + b.y, a.z + b.z, a.w + b.w); }
 
 __global__ void __launch_bounds__(kP2gThreads, NXM_P2G_MIN_CTAS) k_p2g(DevPtrs P) {
     extern __shared__ float4 p2g_smem[];
-    float* rec = reinterpret_cast<float*>(p2g_smem);
-    float* tile = rec + kP2gChunk * kP2gRec;  // 216 x (x, y, z, m)
-    int* cnt = reinterpret_cast<int*>(tile + 216 * 4);
+    float4* tiles = p2g_smem;  // kP2gWarps x 216 nodes of (x, y, z, m)
+    float* rec = reinterpret_cast<float*>(tiles + kP2gWarps * 216);
+    int* cnt = reinterpret_cast<int*>(rec + kP2gChunk * kP2gRec);
     int* start = cnt + 64;  // 65 used
     uint16_t* perm = reinterpret_cast<uint16_t*>(start + 68);
     uint16_t* prank = perm + kP2gChunk;
@@ -52,13 +66,21 @@ __global__ void __launch_bounds__(kP2gThreads, NXM_P2G_MIN_CTAS) k_p2g(DevPtrs P
     const float inv_dx = P.params->inv_dx;
     const uint32_t nb = P.counters->num_blocks;
     const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
-    const int sx = (int)(lane % 3u), sy = (int)((lane / 3u) % 3u), sz = (int)(lane / 9u);
+    // cell-phase roles; lanes 27..31 idle (zero weight, never write)
+    const bool worker = lane < 27u;
+    const uint32_t grp = worker ? lane / 9u : 0u;
+    const uint32_t sxy = worker ? lane % 9u : 0u;
+    const float fx = (float)(sxy % 3u), fy = (float)(sxy / 3u);
+    const uint32_t src1 = worker ? sxy + 9u * ((grp + 1u) % 3u) : lane;
+    const uint32_t src2 = worker ? sxy + 9u * ((grp + 2u) % 3u) : lane;
+    float4* tile = tiles + warp * 216u;
+
+    for (uint32_t t = tid; t < kP2gWarps * 216u; t += kP2gThreads) tiles[t] = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (tid < 64) cnt[tid] = 0;
+    __syncthreads();
     for (uint32_t b = blockIdx.x; b < nb; b += gridDim.x) {
         const uint32_t first = P.first[b], np = P.nprim[b];
         if (np == 0) continue;  // neighbour-only block: receives its sums from other CTAs
-        for (uint32_t t = tid; t < 216u * 4u; t += kP2gThreads) tile[t] = 0.f;
-        if (tid < 64) cnt[tid] = 0;
-        __syncthreads();
         const int4 vid = P.bvid[b];
         for (uint32_t base = 0; base < np; base += kP2gChunk) {
             const uint32_t m_chunk = min(np - base, (uint32_t)kP2gChunk);
@@ -84,11 +106,12 @@ __global__ void __launch_bounds__(kP2gThreads, NXM_P2G_MIN_CTAS) k_p2g(DevPtrs P
                 const v3 q = C * r + mk(vf.x, vf.y, vf.z) * m;
                 float4* rr = reinterpret_cast<float4*>(rec + k * kP2gRec);
                 rr[0] = make_float4(q.x, q.y, q.z, m);
-                rr[1] = make_float4(C.c0.x * dx, C.c0.y * dx, C.c0.z * dx, C.c1.x * dx);
-                rr[2] = make_float4(C.c1.y * dx, C.c1.z * dx, C.c2.x * dx, C.c2.y * dx);
-                rr[3] = make_float4(C.c2.z * dx, wx.x, wx.y, wx.z);
-                rr[4] = make_float4(wy.x, wy.y, wy.z, wz.x);
-                rr[5] = make_float4(wz.y, wz.z, 0.f, 0.f);
+                rr[1] = make_float4(C.c0.x * dx, C.c0.y * dx, C.c0.z * dx, wz.x);
+                rr[2] = make_float4(C.c1.x * dx, C.c1.y * dx, C.c1.z * dx, wz.y);
+                rr[3] = make_float4(C.c2.x * dx, C.c2.y * dx, C.c2.z * dx, wz.z);
+                rr[4] = make_float4(wx.x * wy.x, wx.y * wy.x, wx.z * wy.x, wx.x * wy.y);
+                rr[5] = make_float4(wx.y * wy.y, wx.z * wy.y, wx.x * wy.z, wx.y * wy.z);
+                rr[6] = make_float4(wx.z * wy.z, 0.f, 0.f, 0.f);
                 const uint32_t c = ci.ax + 4u * ci.ay + 16u * ci.az;
                 pcell[k] = (uint8_t)c;
                 prank[k] = (uint16_t)atomicAdd(&cnt[c], 1);
@@ -114,43 +137,62 @@ __global__ void __launch_bounds__(kP2gThreads, NXM_P2G_MIN_CTAS) k_p2g(DevPtrs P
                 if (c != 255u) perm[start[c] + prank[k]] = (uint16_t)k;
             }
             __syncthreads();
-            // 3. one warp per cell, lane = stencil offset
-            for (uint32_t c = warp; c < 64u; c += kP2gThreads / 32) {
+            if (tid < 64) cnt[tid] = 0;  // counts are consumed; ready for the next chunk
+            // 3. one warp per cell, three particles per pass
+            for (uint32_t c = warp; c < 64u; c += kP2gWarps) {
                 const int s0 = start[c], s1 = start[c + 1];
                 if (s0 == s1) continue;
-                float ax = 0.f, ay = 0.f, az = 0.f, am = 0.f;
-                for (int i = s0; i < s1; ++i) {
-                    const float* r = rec + (uint32_t)perm[i] * kP2gRec;
+                float4 a0 = make_float4(0.f, 0.f, 0.f, 0.f), a1 = a0, a2 = a0;  // s.z = 0, 1, 2
+                for (int i = s0; i < s1; i += 3) {
+                    const int j = i + (int)grp;
+                    const bool valid = worker && j < s1;
+                    const float* r = rec + (uint32_t)perm[valid ? j : s0] * kP2gRec;
                     const float4 qm = *reinterpret_cast<const float4*>(r);
-                    const float4 c4a = *reinterpret_cast<const float4*>(r + 4);
-                    const float4 c4b = *reinterpret_cast<const float4*>(r + 8);
-                    const float c22 = r[12];
-                    const float w = r[13 + sx] * r[16 + sy] * r[19 + sz];
-                    const float fx = (float)sx, fy = (float)sy, fz = (float)sz;
-                    const float vx = qm.x + c4a.x * fx + c4a.w * fy + c4b.z * fz;
-                    const float vy = qm.y + c4a.y * fx + c4b.x * fy + c4b.w * fz;
-                    const float vz = qm.z + c4a.z * fx + c4b.y * fy + c22 * fz;
-                    ax += w * vx;
-                    ay += w * vy;
-                    az += w * vz;
-                    am += w * qm.w;
+                    const float4 k0 = *reinterpret_cast<const float4*>(r + 4);
+                    const float4 k1 = *reinterpret_cast<const float4*>(r + 8);
+                    const float4 k2 = *reinterpret_cast<const float4*>(r + 12);
+                    const float wxy = valid ? r[16 + sxy] : 0.f;
+                    float bx = qm.x + k0.x * fx + k1.x * fy;
+                    float by = qm.y + k0.y * fx + k1.y * fy;
+                    float bz = qm.z + k0.z * fx + k1.z * fy;
+                    float w = wxy * k0.w;
+                    a0.x += w * bx; a0.y += w * by; a0.z += w * bz; a0.w += w * qm.w;
+                    bx += k2.x; by += k2.y; bz += k2.z;
+                    w = wxy * k1.w;
+                    a1.x += w * bx; a1.y += w * by; a1.z += w * bz; a1.w += w * qm.w;
+                    bx += k2.x; by += k2.y; bz += k2.z;
+                    w = wxy * k2.w;
+                    a2.x += w * bx; a2.y += w * by; a2.z += w * bz; a2.w += w * qm.w;
                 }
-                if (lane < 27u) {
+                // lane (sxy, g) collects node (sxy, s.z = g) from the three groups:
+                // from group g+1 its s.z = g sum, which that lane holds as (its g + 2) mod 3,
+                // from group g+2 likewise as (its g + 1) mod 3.
+                const float4 own = grp == 0u ? a0 : (grp == 1u ? a1 : a2);
+                const float4 out1 = grp == 0u ? a2 : (grp == 1u ? a0 : a1);
+                const float4 out2 = grp == 0u ? a1 : (grp == 1u ? a2 : a0);
+                float4 t;
+                t.x = own.x + __shfl_sync(0xFFFFFFFFu, out1.x, src1) + __shfl_sync(0xFFFFFFFFu, out2.x, src2);
+                t.y = own.y + __shfl_sync(0xFFFFFFFFu, out1.y, src1) + __shfl_sync(0xFFFFFFFFu, out2.y, src2);
+                t.z = own.z + __shfl_sync(0xFFFFFFFFu, out1.z, src1) + __shfl_sync(0xFFFFFFFFu, out2.z, src2);
+                t.w = own.w + __shfl_sync(0xFFFFFFFFu, out1.w, src1) + __shfl_sync(0xFFFFFFFFu, out2.w, src2);
+                if (worker) {
                     const uint32_t cx = c & 3u, cy = (c >> 2) & 3u, cz = c >> 4;
-                    const uint32_t node = (cx + sx) + 6u * (cy + sy) + 36u * (cz + sz);
-                    atomicAdd(&tile[node * 4 + 0], ax);
-                    atomicAdd(&tile[node * 4 + 1], ay);
-                    atomicAdd(&tile[node * 4 + 2], az);
-                    atomicAdd(&tile[node * 4 + 3], am);
+                    const uint32_t node = (cx + sxy % 3u) + 6u * (cy + sxy / 3u) + 36u * (cz + grp);
+                    tile[node] = f4add(tile[node], t);
                 }
             }
             __syncthreads();
-            if (tid < 64) cnt[tid] = 0;
-            __syncthreads();
         }
+        // 4. sum the warp tiles (clearing them) and flush the block's nodes
         for (uint32_t t = tid; t < 216u; t += kP2gThreads) {
-            const float a = tile[4 * t], bb = tile[4 * t + 1], cc = tile[4 * t + 2], m = tile[4 * t + 3];
-            if (a == 0.f && bb == 0.f && cc == 0.f && m == 0.f) continue;
+            float4 sum = tiles[t];
+            tiles[t] = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+            for (int w = 1; w < kP2gWarps; ++w) {
+                sum = f4add(sum, tiles[w * 216 + t]);
+                tiles[w * 216 + t] = make_float4(0.f, 0.f, 0.f, 0.f);
+            }
+            if (sum.x == 0.f && sum.y == 0.f && sum.z == 0.f && sum.w == 0.f) continue;
             const uint32_t tx = t % 6u, ty = (t / 6u) % 6u, tz = t / 36u;
             const uint32_t ox = tx >= 4u, oy = ty >= 4u, oz = tz >= 4u;
             const uint32_t oct = ox * 4u + oy * 2u + oz;
@@ -160,7 +202,7 @@ __global__ void __launch_bounds__(kP2gThreads, NXM_P2G_MIN_CTAS) k_p2g(DevPtrs P
                 continue;
             }
             const uint32_t node = blk * 64u + (tx - 4u * ox) + 4u * (ty - 4u * oy) + 16u * (tz - 4u * oz);
-            atomicAdd(&P.nodes[node], make_float4(a, bb, cc, m));
+            atomicAdd(&P.nodes[node], sum);
         }
         __syncthreads();
     }
