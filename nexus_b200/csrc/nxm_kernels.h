@@ -33,6 +33,14 @@ struct DevPtrs {
     uint32_t* phdr;          // per particle: primary header id
     uint32_t* scan_tmp;      // per block: offset inside its scan tile
     uint32_t* tile_sums;     // per scan tile of kScanTile blocks: its total
+    // G2P output.  In place: the *_out pointers equal the inputs and pid_in is
+    // null.  Reordering: sorted entry j is written to slot j of the *_out
+    // records, pid_out[j] = pid_in[its source slot] (pid = particle id).
+    PKin* kin_out;
+    PDef* def_out;
+    float4* pstate_out;
+    const uint32_t* pid_in;
+    uint32_t* pid_out;
 };
 
 constexpr uint32_t kScanTile = 1024;  // blocks per scan tile

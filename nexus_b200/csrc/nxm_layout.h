@@ -1,7 +1,9 @@
 // Memory layout of one MPM state in HBM (shared by the host library and the kernels).
 //
 // Particles are stored as two 16-byte-aligned records so that a particle
-// gathered through the sorted index costs whole 32-byte sectors:
+// gathered through the sorted index costs whole 32-byte sectors (in the fast
+// mode the records are kept in the previous step's sorted order, double
+// buffered, with the particle id of each slot alongside):
 //   PKin (80 B): x, mass | v, flags | C columns (c0.w = vel_grad_det)
 //   PDef (48 B): F columns | (f0.w = V0, f1.w = damping, f2.w = material id)
 // plus, for plastic models only, a float4 of model state words.
@@ -109,7 +111,9 @@ struct alignas(16) Counters {
     uint32_t sorted_len;    // total sorted ids, extras included
     uint32_t status;        // STATUS_* bits
     uint32_t codes_valid;   // 1 when pcode holds the block key of every particle's current position
-    uint32_t pad[2];
+    uint32_t unsorted;      // particles without a block this step, placed after the sorted ones
+                            // by the reordering G2P
+    uint32_t pad;
 };
 
 }  // namespace nxm

@@ -110,11 +110,15 @@ __global__ void k_sort_reset(DevPtrs P, uint32_t hash_cap) {
         P.counters->num_extra = 0;
         P.counters->num_blocks = 0;
         P.counters->sorted_len = 0;
+        P.counters->unsorted = 0;
     }
 }
 
 // sort.rs:104-121 gpu_touch_primary_blocks.  Block keys come from the cache
 // written by the previous step (or from the positions after an upload).
+// Each warp walks a contiguous range of particles, so consecutive passes
+// mostly see the block they inserted last: a pass whose lanes all carry the
+// key inserted by the previous pass skips the hash entirely.
 __global__ void __launch_bounds__(256) k_touch_primary(DevPtrs P) {
     const uint32_t n = P.params->n;
     const float dx = P.params->dx;
@@ -124,9 +128,12 @@ __global__ void __launch_bounds__(256) k_touch_primary(DevPtrs P) {
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
-    for (uint32_t base = warp * 32u; base < n; base += nwarps * 32u) {
+    const uint32_t per_warp = ((n + nwarps - 1) / nwarps + 31u) & ~31u;
+    const uint32_t lo = min(warp * per_warp, n), hi = min(lo + per_warp, n);
+    uint32_t known = NONE;  // a key this warp has already inserted
+    for (uint32_t base = lo; base < hi; base += 32u) {
         const uint32_t p = base + lane;
-        const bool active = p < n;
+        const bool active = p < hi;
         uint32_t key = NONE;
         if (active) {
             if (cached) {
@@ -138,9 +145,14 @@ __global__ void __launch_bounds__(256) k_touch_primary(DevPtrs P) {
                 P.pcode[p] = make_uint2(key, ci.ax | (ci.ay << 2) | (ci.az << 4));
             }
         }
-        uint32_t peers = __match_any_sync(0xFFFFFFFFu, key);
-        if (active && lane == (uint32_t)(__ffs(peers) - 1))
+        const uint32_t need = (active && key != known) ? key : NONE;
+        if (__all_sync(0xFFFFFFFFu, need == NONE)) continue;
+        uint32_t peers = __match_any_sync(0xFFFFFFFFu, need);
+        if (need != NONE && lane == (uint32_t)(__ffs(peers) - 1))
             hash_insert(P, key, key_x(key), key_y(key), key_z(key), true, 0, hmask, bcap);
+        // the last active lane's key is now in the table
+        const uint32_t last = min(31u, hi - 1u - base);
+        known = __shfl_sync(0xFFFFFFFFu, key, last);
     }
 }
 
@@ -195,9 +207,15 @@ __global__ void __launch_bounds__(256) k_count(DevPtrs P) {
         const uint32_t p = base + lane;
         uint32_t h0 = NONE;
         uint2 code = make_uint2(NONE, 0);
+        if (p < n) code = P.pcode[p];
+        {
+            // one probe per distinct block key in the warp
+            const uint32_t peers = __match_any_sync(0xFFFFFFFFu, p < n ? code.x : NONE);
+            const uint32_t leader = __ffs(peers) - 1;
+            if (p < n && lane == leader) h0 = hash_find(P, code.x, hmask);
+            h0 = __shfl_sync(0xFFFFFFFFu, h0, leader);
+        }
         if (p < n) {
-            code = P.pcode[p];
-            h0 = hash_find(P, code.x, hmask);
             P.phdr[p] = h0;
             if (h0 == NONE) set_status(P.counters, STATUS_MISSING_BLOCK);
         }
@@ -299,19 +317,27 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_apply(DevPtrs P) {
         uint32_t offset;
         cta_exclusive_scan(part, warp_tot, &offset);
         const uint32_t b0 = tile * kScanTile + threadIdx.x * kScanPer;
+        // all loads first: the stores below may alias them as far as the compiler knows
+        uint32_t cnt[kScanPer][NUM_BUCKETS], rel[kScanPer];
+#pragma unroll
+        for (uint32_t j = 0; j < kScanPer; ++j) {
+            const uint32_t b = b0 + j;
+            rel[j] = b < total ? P.scan_tmp[b] : 0u;
+#pragma unroll
+            for (int k = 0; k < NUM_BUCKETS; ++k) cnt[j][k] = b < total ? P.cursors[b * NUM_BUCKETS + k] : 0u;
+        }
 #pragma unroll
         for (uint32_t j = 0; j < kScanPer; ++j) {
             const uint32_t b = b0 + j;
             if (b >= total) break;
-            const uint32_t first = offset + P.scan_tmp[b];
+            const uint32_t first = offset + rel[j];
             uint32_t running = first;
             P.first[b] = first;
 #pragma unroll
             for (int k = 0; k < NUM_BUCKETS; ++k) {
                 if (k == NUM_PRIMARY_BUCKETS) P.nprim[b] = running - first;
-                const uint32_t c = P.cursors[b * NUM_BUCKETS + k];
                 P.cursors[b * NUM_BUCKETS + k] = running;
-                running += c;
+                running += cnt[j][k];
             }
             P.nwx[b] = running - first;
             if (b == total - 1) {

@@ -81,6 +81,33 @@ __global__ void k_pack_fields(const uint32_t* __restrict__ src, uint32_t stride_
     }
 }
 
+// Permuted storage (slot p holds particle pid[p]): scatter the fields by id.
+__global__ void k_pack_fields_perm(const uint32_t* __restrict__ src, uint32_t stride_words, uint32_t n,
+                                   const int* __restrict__ offsets, int nfields, const uint32_t* __restrict__ pid,
+                                   uint32_t* __restrict__ dst) {
+    const uint32_t total = n * (uint32_t)nfields;
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+        const uint32_t p = t / (uint32_t)nfields, f = t % (uint32_t)nfields;
+        dst[(size_t)pid[p] * nfields + f] = src[(size_t)p * stride_words + offsets[f]];
+    }
+}
+
+__global__ void k_iota(uint32_t* __restrict__ out, uint32_t first, uint32_t count) {
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < count; t += gridDim.x * blockDim.x) out[t] = first + t;
+}
+
+// Back to id order: record of slot p goes to slot pid[p] of the other buffers.
+__global__ void k_unpermute(const PKin* __restrict__ kin, const PDef* __restrict__ def,
+                            const float4* __restrict__ pstate, const uint32_t* __restrict__ pid, uint32_t n,
+                            PKin* __restrict__ kin_to, PDef* __restrict__ def_to, float4* __restrict__ pstate_to) {
+    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+        const uint32_t id = pid[p];
+        kin_to[id] = kin[p];
+        def_to[id] = def[p];
+        pstate_to[id] = pstate[p];
+    }
+}
+
 }  // namespace
 
 struct nxm_pipeline {
@@ -101,11 +128,22 @@ struct nxm_state {
     bool use_cpic = false;
     bool deterministic = false;
 
-    // particles
+    // particles.  Fast mode keeps the records in the previous step's sorted
+    // order: each step's G2P writes them to the *_alt buffers, which then
+    // become current (`parity` counts the swaps mod 2); pid[slot] is the
+    // particle id of a slot while `permuted`, otherwise slot == id.
     uint32_t n = 0, pcap = 0;
     PKin* kin = nullptr;
     PDef* def = nullptr;
     float4* pstate = nullptr;
+    PKin* kin_alt = nullptr;
+    PDef* def_alt = nullptr;
+    float4* pstate_alt = nullptr;
+    uint32_t* pid = nullptr;
+    uint32_t* pid_alt = nullptr;
+    bool permuted = false;
+    int parity = 0;
+    const uint32_t* sort_pid = nullptr;  // slot -> id map of the storage the last sort ran on (null: identity)
     uint2* pcode = nullptr;
     uint32_t* phdr = nullptr;
     uint32_t* sorted = nullptr;
@@ -140,9 +178,9 @@ struct nxm_state {
     Counters* h_counters = nullptr;  // pinned
     bool params_dirty = true;
 
-    // graph
-    cudaGraphExec_t graph = nullptr;
-    bool graph_valid = false;
+    // graphs (one per buffer parity)
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    bool graph_valid[2] = {false, false};
     int graph_kernels = 0;
     uint64_t launches = 0;
 
@@ -154,11 +192,26 @@ struct nxm_state {
 
 namespace {
 
+bool reorders(const nxm_state* s) { return !s->deterministic; }
+
 DevPtrs dev_ptrs(nxm_state* s) {
     DevPtrs P{};
     P.kin = s->kin;
     P.def = s->def;
     P.pstate = s->pstate;
+    if (reorders(s)) {
+        P.kin_out = s->kin_alt;
+        P.def_out = s->def_alt;
+        P.pstate_out = s->pstate_alt;
+        P.pid_in = s->pid;
+        P.pid_out = s->pid_alt;
+    } else {
+        P.kin_out = s->kin;
+        P.def_out = s->def;
+        P.pstate_out = s->pstate;
+        P.pid_in = nullptr;
+        P.pid_out = nullptr;
+    }
     P.materials = s->d_materials;
     P.colliders = s->d_colliders;
     P.tri = s->d_tri;
@@ -191,9 +244,46 @@ LaunchCfg launch_cfg(nxm_state* s) {
 }
 
 void invalidate_graph(nxm_state* s) {
-    if (s->graph) cudaGraphExecDestroy(s->graph);
-    s->graph = nullptr;
-    s->graph_valid = false;
+    for (int i = 0; i < 2; ++i) {
+        if (s->graph[i]) cudaGraphExecDestroy(s->graph[i]);
+        s->graph[i] = nullptr;
+        s->graph_valid[i] = false;
+    }
+}
+
+// The reordering G2P wrote the step's output to the *_alt buffers: make them current.
+void swap_buffers(nxm_state* s) {
+    std::swap(s->kin, s->kin_alt);
+    std::swap(s->def, s->def_alt);
+    std::swap(s->pstate, s->pstate_alt);
+    std::swap(s->pid, s->pid_alt);
+    s->parity ^= 1;
+}
+
+int grid_for_n(nxm_state* s, uint32_t n) {
+    int g = (int)std::min<uint32_t>((n + 255u) / 256u, (uint32_t)s->sm_count * 8u);
+    return g < 1 ? 1 : g;
+}
+
+// Brings permuted storage back to id order (before edits that address particles by id).
+int canonicalize(nxm_state* s) {
+    if (!s->permuted) return NXM_OK;
+    if (s->n) {
+        k_unpermute<<<grid_for_n(s, s->n), 256, 0, s->stream>>>(s->kin, s->def, s->pstate, s->pid, s->n, s->kin_alt,
+                                                                 s->def_alt, s->pstate_alt);
+        s->launches += 1;
+        NXM_TRY(cudaGetLastError());
+    }
+    std::swap(s->kin, s->kin_alt);
+    std::swap(s->def, s->def_alt);
+    std::swap(s->pstate, s->pstate_alt);
+    std::swap(s->pid, s->pid_alt);
+    s->parity ^= 1;
+    s->permuted = false;
+    NXM_TRY(cudaMemsetAsync(reinterpret_cast<char*>(s->d_counters) + offsetof(Counters, codes_valid), 0, 4,
+                            s->stream));
+    NXM_TRY(cudaStreamSynchronize(s->stream));
+    return NXM_OK;
 }
 
 int free_grid(nxm_state* s) {
@@ -223,24 +313,56 @@ int alloc_grid(nxm_state* s, uint32_t grid_capacity) {
     return NXM_OK;
 }
 
+// The particle arrays of a state (owned; freed on destruction unless released).
+struct ParticleBuffers {
+    PKin *kin = nullptr, *kin_alt = nullptr;
+    PDef *def = nullptr, *def_alt = nullptr;
+    float4 *pstate = nullptr, *pstate_alt = nullptr;
+    uint32_t *pid = nullptr, *pid_alt = nullptr, *phdr = nullptr, *sorted = nullptr;
+    uint2* pcode = nullptr;
+    cudaError_t alloc(uint32_t cap) {
+        cudaError_t e = cudaSuccess;
+        auto a = [&](auto** p, size_t count) {
+            if (e == cudaSuccess) e = dalloc(p, count);
+        };
+        a(&kin, cap); a(&def, cap); a(&pstate, cap);
+        a(&kin_alt, cap); a(&def_alt, cap); a(&pstate_alt, cap);
+        a(&pid, cap); a(&pid_alt, cap); a(&pcode, cap); a(&phdr, cap);
+        a(&sorted, (size_t)cap * 8);
+        return e;
+    }
+    void release() { *this = ParticleBuffers{}; }
+    ~ParticleBuffers() {
+        dfree(kin); dfree(def); dfree(pstate); dfree(kin_alt); dfree(def_alt); dfree(pstate_alt);
+        dfree(pid); dfree(pid_alt); dfree(pcode); dfree(phdr); dfree(sorted);
+    }
+};
+
+void free_particles(nxm_state* s) {
+    dfree(s->kin); dfree(s->def); dfree(s->pstate); dfree(s->kin_alt); dfree(s->def_alt); dfree(s->pstate_alt);
+    dfree(s->pid); dfree(s->pid_alt); dfree(s->pcode); dfree(s->phdr); dfree(s->sorted);
+}
+
 int reserve_particles(nxm_state* s, uint32_t need) {
     if (need <= s->pcap) return NXM_OK;
+    int rc = canonicalize(s);
+    if (rc) return rc;
     uint32_t cap = std::max<uint32_t>(need, s->pcap ? s->pcap * 2 : 1024);
-    PKin* kin; PDef* def; float4* pstate; uint2* pcode; uint32_t* phdr; uint32_t* sorted;
-    NXM_TRY(dalloc(&kin, cap));
-    NXM_TRY(dalloc(&def, cap));
-    NXM_TRY(dalloc(&pstate, cap));
-    NXM_TRY(dalloc(&pcode, cap));
-    NXM_TRY(dalloc(&phdr, cap));
-    NXM_TRY(dalloc(&sorted, (size_t)cap * 8));
+    ParticleBuffers t;
+    NXM_TRY(t.alloc(cap));
     if (s->n) {
-        NXM_TRY(cudaMemcpyAsync(kin, s->kin, sizeof(PKin) * s->n, cudaMemcpyDeviceToDevice, s->stream));
-        NXM_TRY(cudaMemcpyAsync(def, s->def, sizeof(PDef) * s->n, cudaMemcpyDeviceToDevice, s->stream));
-        NXM_TRY(cudaMemcpyAsync(pstate, s->pstate, sizeof(float4) * s->n, cudaMemcpyDeviceToDevice, s->stream));
+        NXM_TRY(cudaMemcpyAsync(t.kin, s->kin, sizeof(PKin) * s->n, cudaMemcpyDeviceToDevice, s->stream));
+        NXM_TRY(cudaMemcpyAsync(t.def, s->def, sizeof(PDef) * s->n, cudaMemcpyDeviceToDevice, s->stream));
+        NXM_TRY(cudaMemcpyAsync(t.pstate, s->pstate, sizeof(float4) * s->n, cudaMemcpyDeviceToDevice, s->stream));
     }
     NXM_TRY(cudaStreamSynchronize(s->stream));
-    dfree(s->kin); dfree(s->def); dfree(s->pstate); dfree(s->pcode); dfree(s->phdr); dfree(s->sorted);
-    s->kin = kin; s->def = def; s->pstate = pstate; s->pcode = pcode; s->phdr = phdr; s->sorted = sorted;
+    free_particles(s);
+    s->kin = t.kin; s->def = t.def; s->pstate = t.pstate;
+    s->kin_alt = t.kin_alt; s->def_alt = t.def_alt; s->pstate_alt = t.pstate_alt;
+    s->pid = t.pid; s->pid_alt = t.pid_alt;
+    s->pcode = t.pcode; s->phdr = t.phdr; s->sorted = t.sorted;
+    t.release();
+    s->sort_pid = nullptr;
     s->pcap = cap;
     invalidate_graph(s);
     s->params_dirty = true;
@@ -348,8 +470,12 @@ int ensure_ready(nxm_state* s) {
     return sync_params(s);
 }
 
+// Captures the step for the current buffer parity.
 int build_graph(nxm_state* s) {
-    invalidate_graph(s);
+    const int par = s->parity;
+    if (s->graph[par]) cudaGraphExecDestroy(s->graph[par]);
+    s->graph[par] = nullptr;
+    s->graph_valid[par] = false;
     cudaGraph_t g = nullptr;
     NXM_TRY(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
     int k = enqueue_step(s, s->stream, nullptr);
@@ -359,16 +485,36 @@ int build_graph(nxm_state* s) {
         if (g) cudaGraphDestroy(g);
         return NXM_E_CUDA;
     }
-    e = cudaGraphInstantiate(&s->graph, g, 0);
+    e = cudaGraphInstantiate(&s->graph[par], g, 0);
     cudaGraphDestroy(g);
     if (e != cudaSuccess) {
         (void)cudaGetLastError();
-        s->graph = nullptr;
+        s->graph[par] = nullptr;
         return NXM_E_CUDA;
     }
     s->graph_kernels = k;
-    s->graph_valid = true;
+    s->graph_valid[par] = true;
     return NXM_OK;
+}
+
+// Before a reordering step: slot == id unless the storage is already permuted.
+int prepare_reorder(nxm_state* s) {
+    if (!reorders(s) || s->permuted) return NXM_OK;
+    k_iota<<<grid_for_n(s, s->n), 256, 0, s->stream>>>(s->pid, 0u, s->n);
+    s->launches += 1;
+    NXM_TRY(cudaGetLastError());
+    return NXM_OK;
+}
+
+// After a step: the sorted ids refer to the slots the step started from.
+void finish_step(nxm_state* s) {
+    if (reorders(s)) {
+        s->sort_pid = s->pid;
+        swap_buffers(s);
+        s->permuted = true;
+    } else {
+        s->sort_pid = nullptr;
+    }
 }
 
 int pack_read(nxm_state* s, const void* records, uint32_t stride_bytes, const int* offsets, int nfields, void* out) {
@@ -384,8 +530,12 @@ int pack_read(nxm_state* s, const void* records, uint32_t stride_bytes, const in
     NXM_TRY(cudaMemcpyAsync(s->d_offsets, offsets, sizeof(int) * nfields, cudaMemcpyHostToDevice, s->stream));
     int grid = std::min<int>((int)((words + 255) / 256), s->sm_count * 8);
     if (grid < 1) grid = 1;
-    k_pack_fields<<<grid, 256, 0, s->stream>>>(reinterpret_cast<const uint32_t*>(records), stride_bytes / 4, s->n,
-                                                 s->d_offsets, nfields, s->d_pack);
+    if (s->permuted)
+        k_pack_fields_perm<<<grid, 256, 0, s->stream>>>(reinterpret_cast<const uint32_t*>(records), stride_bytes / 4,
+                                                          s->n, s->d_offsets, nfields, s->pid, s->d_pack);
+    else
+        k_pack_fields<<<grid, 256, 0, s->stream>>>(reinterpret_cast<const uint32_t*>(records), stride_bytes / 4, s->n,
+                                                     s->d_offsets, nfields, s->d_pack);
     s->launches += 1;
     NXM_TRY(cudaGetLastError());
     NXM_TRY(cudaMemcpyAsync(out, s->d_pack, words * 4, cudaMemcpyDeviceToHost, s->stream));
@@ -446,6 +596,11 @@ int upload_particles(nxm_state* s, const nxm_particles_soa* p, uint32_t count) {
     NXM_TRY(cudaMemcpyAsync(s->kin + s->n, hk.data(), sizeof(PKin) * count, cudaMemcpyHostToDevice, s->stream));
     NXM_TRY(cudaMemcpyAsync(s->def + s->n, hd.data(), sizeof(PDef) * count, cudaMemcpyHostToDevice, s->stream));
     NXM_TRY(cudaMemcpyAsync(s->pstate + s->n, hs.data(), sizeof(float4) * count, cudaMemcpyHostToDevice, s->stream));
+    if (s->permuted) {  // appended particles sit at slots == their ids
+        k_iota<<<grid_for_n(s, count), 256, 0, s->stream>>>(s->pid + s->n, s->n, count);
+        s->launches += 1;
+        NXM_TRY(cudaGetLastError());
+    }
     NXM_TRY(cudaStreamSynchronize(s->stream));
     s->n += count;
     s->params_dirty = true;
@@ -539,7 +694,7 @@ void nxm_state_destroy(nxm_state* s) {
     if (s->stream) cudaStreamSynchronize(s->stream);
     invalidate_graph(s);
     free_grid(s);
-    dfree(s->kin); dfree(s->def); dfree(s->pstate); dfree(s->pcode); dfree(s->phdr); dfree(s->sorted);
+    free_particles(s);
     dfree(s->d_materials); dfree(s->d_colliders); dfree(s->d_tri); dfree(s->d_params); dfree(s->d_counters);
     dfree(s->d_pack); dfree(s->d_offsets);
     if (s->h_counters) cudaFreeHost(s->h_counters);
@@ -641,6 +796,10 @@ int nxm_state_set_use_cpic(nxm_state* s, int enabled) {
 
 int nxm_state_set_deterministic(nxm_state* s, int enabled) {
     if (!s) return NXM_E_INVALID;
+    if (enabled) {  // the deterministic step works in place, in id order
+        int rc = canonicalize(s);
+        if (rc) return rc;
+    }
     if (s->deterministic != (enabled != 0)) invalidate_graph(s);
     s->deterministic = enabled != 0;
     return NXM_OK;
@@ -678,6 +837,9 @@ uint32_t nxm_particles_len(const nxm_state* s) { return s ? s->n : 0u; }
 int nxm_particles_swap_remove(nxm_state* s, const uint32_t* slots, uint32_t count, uint32_t* remaps,
                               uint32_t* num_remaps) {
     if (!s || (count && !slots)) return NXM_E_INVALID;
+    int rc = canonicalize(s);
+    if (rc) return rc;
+    s->sort_pid = nullptr;
     std::vector<uint32_t> t(slots, slots + count);
     std::sort(t.begin(), t.end(), [](uint32_t a, uint32_t b) { return a > b; });
     t.erase(std::unique(t.begin(), t.end()), t.end());
@@ -717,6 +879,9 @@ int nxm_particles_shift_remove(nxm_state* s, uint32_t start, uint32_t end) {
     if (!s || start > end || end > s->n) return NXM_E_INVALID;
     const uint32_t removed = end - start;
     if (removed == 0) return NXM_OK;
+    int rc = canonicalize(s);
+    if (rc) return rc;
+    s->sort_pid = nullptr;
     const uint32_t tail = s->n - end;
     if (tail) {
         PKin* tk; PDef* td; float4* ts;
@@ -747,11 +912,14 @@ int nxm_step(nxm_pipeline* pipeline, nxm_state* s, nxm_timestamps* ts) {
     int rc = ensure_ready(s);
     if (rc) return rc;
     if (s->n == 0) return NXM_OK;
+    rc = prepare_reorder(s);
+    if (rc) return rc;
     if (ts) {
         cudaEvent_t ev[5];
         for (auto& e : ev) NXM_TRY(cudaEventCreate(&e));
         int k = enqueue_step(s, s->stream, ev);
         s->launches += (uint64_t)k;
+        finish_step(s);
         cudaError_t e = cudaGetLastError();
         if (e == cudaSuccess) e = cudaEventSynchronize(ev[4]);
         if (e == cudaSuccess) {
@@ -764,12 +932,13 @@ int nxm_step(nxm_pipeline* pipeline, nxm_state* s, nxm_timestamps* ts) {
         for (auto& x : ev) cudaEventDestroy(x);
         return e == cudaSuccess ? NXM_OK : NXM_E_CUDA;
     }
-    if (!s->graph_valid) {
+    if (!s->graph_valid[s->parity]) {
         rc = build_graph(s);
         if (rc) return rc;
     }
-    NXM_TRY(cudaGraphLaunch(s->graph, s->stream));
+    NXM_TRY(cudaGraphLaunch(s->graph[s->parity], s->stream));
     s->launches += (uint64_t)s->graph_kernels;
+    finish_step(s);
     return NXM_OK;
 }
 
@@ -782,6 +951,7 @@ int nxm_debug_sort(nxm_pipeline* pipeline, nxm_state* s, int with_p2g) {
     LaunchCfg c = launch_cfg(s);
     fast::launch_sort(P, c, /*with_extras=*/true, /*canonical=*/s->deterministic, s->stream);
     s->launches += (uint64_t)sort_launches(s->deterministic);
+    s->sort_pid = s->permuted ? s->pid : nullptr;
     if (with_p2g) {
         if (s->deterministic) exact::launch_p2g_gather(P, c, s->stream);
         else fast::launch_p2g(P, c, s->stream);
@@ -934,7 +1104,14 @@ int nxm_grid_read_sorted_ids(nxm_state* s, uint32_t* out, uint32_t max_len) {
     len = std::min(len, std::min(max_len, s->pcap * 8u));
     if (len == 0) return NXM_OK;
     NXM_TRY(cudaMemcpyAsync(out, s->sorted, 4 * (size_t)len, cudaMemcpyDeviceToHost, s->stream));
+    std::vector<uint32_t> ids;
+    if (s->sort_pid) {  // the sort listed storage slots: report particle ids
+        ids.resize(s->n);
+        NXM_TRY(cudaMemcpyAsync(ids.data(), s->sort_pid, 4 * (size_t)s->n, cudaMemcpyDeviceToHost, s->stream));
+    }
     NXM_TRY(cudaStreamSynchronize(s->stream));
+    if (s->sort_pid)
+        for (uint32_t j = 0; j < len; ++j) out[j] = out[j] < s->n ? ids[out[j]] : out[j];
     return NXM_OK;
 }
 

@@ -128,12 +128,13 @@ __device__ __forceinline__ float4 halo_node(const DevPtrs& P, uint32_t b, uint32
 // g2p.rs:150-270 (non-CPIC) fused with particle_update.rs:60-201 for one
 // particle: gathers velocity and velocity gradient from the 6x6x6 halo of its
 // block (shared memory), then advects, updates F and the model, and writes the
-// particle back together with the block key of its new position.
+// particle (read from slot `src`, xm / vf = its first two kin words) to slot
+// `dst` of the output records, together with the block key of its new position.
 __device__ __forceinline__ void g2p_particle(const DevPtrs& P, const Params& prm, const float4* __restrict__ halo,
-                                             uint32_t pid, float4 xm, float4 vf) {
+                                             uint32_t src, uint32_t dst, float4 xm, float4 vf) {
     const float dx = prm.dx, dt = prm.dt;
     const float inv_d = 4.0f / (dx * dx);
-    float4* kr = reinterpret_cast<float4*>(&P.kin[pid]);
+    float4* kr = reinterpret_cast<float4*>(&P.kin_out[dst]);
     uint32_t flags = __float_as_uint(vf.w);
     const v3 pt = mk(xm.x, xm.y, xm.z);
     float mass = xm.w;
@@ -195,7 +196,7 @@ __device__ __forceinline__ void g2p_particle(const DevPtrs& P, const Params& prm
     }
 
     // ---- particle update (particle_update.rs:60-201, non-CPIC: Cdf = 0)
-    const float4* dr = reinterpret_cast<const float4*>(&P.def[pid]);
+    const float4* dr = reinterpret_cast<const float4*>(&P.def[src]);
     const float4 d0 = dr[0], d1 = dr[1], d2 = dr[2];
     m3 F = mkm(mk(d0.x, d0.y, d0.z), mk(d1.x, d1.y, d1.z), mk(d2.x, d2.y, d2.z));
     const float init_volume = d0.w, damping = d1.w;
@@ -221,7 +222,7 @@ __device__ __forceinline__ void g2p_particle(const DevPtrs& P, const Params& prm
     }
     float st[4] = {0.f, 0.f, 0.f, 0.f};
     if (mat.has_state) {
-        float4 s4 = P.pstate[pid];
+        float4 s4 = P.pstate[src];
         st[0] = s4.x; st[1] = s4.y; st[2] = s4.z; st[3] = s4.w;
     }
     const m3 tau = model_update<NXM_FAST>(tag, mat.w, st, F, A);
@@ -242,38 +243,102 @@ __device__ __forceinline__ void g2p_particle(const DevPtrs& P, const Params& prm
     kr[2] = make_float4(aff.c0.x, aff.c0.y, aff.c0.z, vgd);
     kr[3] = make_float4(aff.c1.x, aff.c1.y, aff.c1.z, 0.f);
     kr[4] = make_float4(aff.c2.x, aff.c2.y, aff.c2.z, 0.f);
-    float4* dw = reinterpret_cast<float4*>(&P.def[pid]);
+    float4* dw = reinterpret_cast<float4*>(&P.def_out[dst]);
     dw[0] = make_float4(F.c0.x, F.c0.y, F.c0.z, init_volume);
     dw[1] = make_float4(F.c1.x, F.c1.y, F.c1.z, damping);
     dw[2] = make_float4(F.c2.x, F.c2.y, F.c2.z, d2.w);
-    if (mat.has_state) P.pstate[pid] = make_float4(st[0], st[1], st[2], st[3]);
+    if (mat.has_state) P.pstate_out[dst] = make_float4(st[0], st[1], st[2], st[3]);
+    if (P.pid_in) P.pid_out[dst] = P.pid_in[src];
     // block key of the new position, for the next step's activation
     const CellInfo nc = cell_info(dx, new_pos);
-    P.pcode[pid] = make_uint2(pack_key(nc.bx, nc.by, nc.bz), nc.ax | (nc.ay << 2) | (nc.az << 4));
+    P.pcode[dst] = make_uint2(pack_key(nc.bx, nc.by, nc.bz), nc.ax | (nc.ay << 2) | (nc.az << 4));
 }
 
 #ifndef NXM_G2P_MIN_CTAS
 #define NXM_G2P_MIN_CTAS 4  // CTAs of 256 threads per SM the register budget is sized for
 #endif
 
-// One CTA per active block (grid-stride): the halo of the block and its +1
-// neighbours is staged in shared memory, then each thread gathers and
-// updates one of the block's primary particles.
+// One CTA per primary block (ids [0, num_primary); the other blocks hold no
+// particles), grid-stride: the halo of the block and its +1 neighbours is
+// staged in shared memory, then each thread gathers and updates one of the
+// block's primary particles.  The next block's header is loaded one block
+// ahead, and each thread's first particle is fetched alongside the halo so
+// that the two dependent load chains overlap.  When reordering, sorted entry
+// j = first + k goes to output slot j; particles the sort could not place
+// (their block was not created: capacity or hash overflow, reported in the
+// status word) are copied unchanged to the slots after the sorted ones.
 __global__ void __launch_bounds__(256, NXM_G2P_MIN_CTAS) k_g2p_update(DevPtrs P) {
     __shared__ float4 halo[216];
     const Params prm = *P.params;
-    const uint32_t nb = P.counters->num_blocks;
-    for (uint32_t b = blockIdx.x; b < nb; b += gridDim.x) {
-        const uint32_t first = P.first[b], np = P.nprim[b];
-        if (np == 0) continue;  // neighbour-only block: no primary particles to update
-        for (uint32_t t = threadIdx.x; t < 216u; t += blockDim.x) halo[t] = halo_node(P, b, t);
-        __syncthreads();
-        for (uint32_t k = threadIdx.x; k < np; k += blockDim.x) {
-            const uint32_t pid = P.sorted[first + k];
+    const uint32_t nbp = min(__ldcg(&P.counters->num_primary), __ldcg(&P.counters->num_blocks));
+    const uint32_t tid = threadIdx.x;
+    const uint32_t ht = tid < 216u ? tid : 0u;  // halo node of this thread
+    const uint32_t htx = ht % 6u, hty = (ht / 6u) % 6u, htz = ht / 36u;
+    const uint32_t hox = htx >= 4u, hoy = hty >= 4u, hoz = htz >= 4u;
+    const uint32_t hoct = hox * 4u + hoy * 2u + hoz;
+    const uint32_t hnode = (htx - 4u * hox) + 4u * (hty - 4u * hoy) + 16u * (htz - 4u * hoz);
+    uint32_t b = blockIdx.x;
+    uint32_t first = 0, np = 0;
+    if (b < nbp) {
+        first = __ldcg(&P.first[b]);
+        np = __ldcg(&P.nprim[b]);
+    }
+    while (b < nbp) {
+        const uint32_t bn = b + gridDim.x;
+        uint32_t nfirst = 0, nnp = 0;
+        if (bn < nbp) {
+            nfirst = __ldcg(&P.first[bn]);
+            nnp = __ldcg(&P.nprim[bn]);
+        }
+        const bool reorder = P.pid_in != nullptr;
+        uint32_t pid = tid < np ? __ldg(&P.sorted[first + tid]) : NONE;
+        const uint32_t hblk = (tid < 216u && hoct != 0u) ? __ldg(&P.nbh[b * NUM_NBH + hoct - 1u]) : b;
+        float4 xm = make_float4(0.f, 0.f, 0.f, 0.f), vf = xm;
+        if (pid != NONE) {
             const float4* kr = reinterpret_cast<const float4*>(&P.kin[pid]);
-            g2p_particle(P, prm, halo, pid, kr[0], kr[1]);
+            xm = kr[0];
+            vf = kr[1];
+        }
+        if (tid < 216u) {
+            float4 nd = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (hblk != NONE) nd = P.nodes[hblk * 64u + hnode];
+            halo[tid] = make_float4(nd.x, nd.y, nd.z, 0.f);
+        }
+        for (uint32_t t = tid + blockDim.x; t < 216u; t += blockDim.x) halo[t] = halo_node(P, b, t);
+        __syncthreads();
+        for (uint32_t k = tid; k < np; k += blockDim.x) {
+            if (k != tid) {
+                pid = P.sorted[first + k];
+                const float4* kr = reinterpret_cast<const float4*>(&P.kin[pid]);
+                xm = kr[0];
+                vf = kr[1];
+            }
+            g2p_particle(P, prm, halo, pid, reorder ? first + k : pid, xm, vf);
         }
         __syncthreads();
+        b = bn;
+        first = nfirst;
+        np = nnp;
+    }
+    if (P.pid_in) {
+        const uint32_t n = prm.n, sl = __ldcg(&P.counters->sorted_len);
+        for (uint32_t p = sl < n ? blockIdx.x * blockDim.x + tid : n; p < n; p += gridDim.x * blockDim.x) {
+            if (__ldcg(&P.phdr[p]) != NONE) continue;
+            const uint32_t dst = sl + atomicAdd(&P.counters->unsorted, 1u);
+            if (dst >= n) continue;  // not reached: exactly n - sl particles have no header
+            const float4* ks = reinterpret_cast<const float4*>(&P.kin[p]);
+            float4* kd = reinterpret_cast<float4*>(&P.kin_out[dst]);
+#pragma unroll
+            for (int w = 0; w < 5; ++w) kd[w] = ks[w];
+            const float4* ds = reinterpret_cast<const float4*>(&P.def[p]);
+            float4* dd = reinterpret_cast<float4*>(&P.def_out[dst]);
+#pragma unroll
+            for (int w = 0; w < 3; ++w) dd[w] = ds[w];
+            P.pstate_out[dst] = P.pstate[p];
+            P.pid_out[dst] = P.pid_in[p];
+            const CellInfo nc = cell_info(prm.dx, mk(ks[0].x, ks[0].y, ks[0].z));
+            P.pcode[dst] = make_uint2(pack_key(nc.bx, nc.by, nc.bz), nc.ax | (nc.ay << 2) | (nc.az << 4));
+        }
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) P.counters->codes_valid = 1u;
 }

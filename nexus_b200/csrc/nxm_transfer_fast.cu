@@ -52,7 +52,46 @@ static_assert(kP2gChunk <= 65536, "staged particle indices are 16-bit");
 
 __device__ __forceinline__ float4 f4add(float4 a, float4 b) { return make_float4(a.x + b.x, a.y + b.y, a.z + b.z, a.w + b.w); }
 
+// One staged particle's raw record (kin words 0..19) and a block header.
+struct P2gRaw {
+    float4 xm, vf, c0, c1, c2;
+};
+struct P2gHdr {
+    uint32_t first, np;
+};
+
+__device__ __forceinline__ P2gRaw p2g_load_raw(const DevPtrs& P, uint32_t pid) {
+    P2gRaw r;
+    if (pid == NONE) {
+        r.vf = make_float4(0.f, 0.f, 0.f, 0.f);  // flags 0: not staged
+        return r;
+    }
+    const float4* kr = reinterpret_cast<const float4*>(&P.kin[pid]);
+    r.xm = __ldg(kr);
+    r.vf = __ldg(kr + 1);
+    r.c0 = __ldg(kr + 2);
+    r.c1 = __ldg(kr + 3);
+    r.c2 = __ldg(kr + 4);
+    return r;
+}
+
+__device__ __forceinline__ P2gHdr p2g_load_hdr(const DevPtrs& P, uint32_t b, uint32_t nbp) {
+    P2gHdr h{0u, 0u};
+    if (b < nbp) {
+        h.first = __ldcg(&P.first[b]);
+        h.np = __ldcg(&P.nprim[b]);
+    }
+    return h;
+}
+
+// Work runs over the primary blocks only (ids [0, num_primary); the others
+// hold no particles).  Loads run ahead of use: the headers of the blocks two
+// grid strides ahead, the sorted id of the next chunk's particle right after
+// staging, and its 80-byte record at the start of the cell phase, so their
+// latency overlaps the current chunk's shared-memory work.
 __global__ void __launch_bounds__(kP2gThreads, NXM_P2G_MIN_CTAS) k_p2g(DevPtrs P) {
+    static_assert(kP2gChunk == kP2gThreads, "one staged particle per thread");
+    static_assert(kP2gThreads >= 216, "one flushed tile node per thread");
     extern __shared__ float4 p2g_smem[];
     float4* tiles = p2g_smem;  // kP2gWarps x 216 nodes of (x, y, z, m)
     float* rec = reinterpret_cast<float*>(tiles + kP2gWarps * 216);
@@ -64,7 +103,7 @@ __global__ void __launch_bounds__(kP2gThreads, NXM_P2G_MIN_CTAS) k_p2g(DevPtrs P
 
     const float dx = P.params->dx;
     const float inv_dx = P.params->inv_dx;
-    const uint32_t nb = P.counters->num_blocks;
+    const uint32_t nbp = min(__ldcg(&P.counters->num_primary), __ldcg(&P.counters->num_blocks));
     const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
     // cell-phase roles; lanes 27..31 idle (zero weight, never write)
     const bool worker = lane < 27u;
@@ -74,47 +113,63 @@ __global__ void __launch_bounds__(kP2gThreads, NXM_P2G_MIN_CTAS) k_p2g(DevPtrs P
     const uint32_t src1 = worker ? sxy + 9u * ((grp + 1u) % 3u) : lane;
     const uint32_t src2 = worker ? sxy + 9u * ((grp + 2u) % 3u) : lane;
     float4* tile = tiles + warp * 216u;
+    // flush role: tile node `tid` (tid < 216) of octant `foct`
+    const uint32_t ftx = tid % 6u, fty = (tid / 6u) % 6u, ftz = tid / 36u;
+    const uint32_t fox = ftx >= 4u, foy = fty >= 4u, foz = ftz >= 4u;
+    const uint32_t foct = fox * 4u + foy * 2u + foz;
+    const uint32_t fnode = (ftx - 4u * fox) + 4u * (fty - 4u * foy) + 16u * (ftz - 4u * foz);
 
+    uint32_t b = blockIdx.x;
+    if (b >= nbp) return;
+    const uint32_t stride = gridDim.x;
     for (uint32_t t = tid; t < kP2gWarps * 216u; t += kP2gThreads) tiles[t] = make_float4(0.f, 0.f, 0.f, 0.f);
     if (tid < 64) cnt[tid] = 0;
+    P2gHdr h = p2g_load_hdr(P, b, nbp);
+    P2gHdr hn = p2g_load_hdr(P, b + stride, nbp);
+    P2gHdr hnn = p2g_load_hdr(P, b + 2u * stride, nbp);
+    P2gRaw raw = p2g_load_raw(P, tid < h.np ? __ldg(&P.sorted[h.first + tid]) : NONE);
     __syncthreads();
-    for (uint32_t b = blockIdx.x; b < nb; b += gridDim.x) {
-        const uint32_t first = P.first[b], np = P.nprim[b];
-        if (np == 0) continue;  // neighbour-only block: receives its sums from other CTAs
+    for (;;) {
         const int4 vid = P.bvid[b];
-        for (uint32_t base = 0; base < np; base += kP2gChunk) {
-            const uint32_t m_chunk = min(np - base, (uint32_t)kP2gChunk);
-            // 1. stage and bin
-            for (uint32_t k = tid; k < m_chunk; k += kP2gThreads) {
-                const uint32_t pid = P.sorted[first + base + k];
-                const float4* kr = reinterpret_cast<const float4*>(&P.kin[pid]);
-                const float4 xm = __ldg(kr), vf = __ldg(kr + 1);
-                if (!(__float_as_uint(vf.w) & PFLAG_ENABLED)) {
+        const uint32_t fblk = (tid < 216u && foct != 0u) ? __ldg(&P.nbh[b * NUM_NBH + foct - 1u]) : b;
+        for (uint32_t base = 0; base < h.np; base += kP2gChunk) {
+            const uint32_t m_chunk = min(h.np - base, (uint32_t)kP2gChunk);
+            // 1. stage and bin this thread's particle (base + tid)
+            if (tid < m_chunk) {
+                const uint32_t k = tid;
+                if (!(__float_as_uint(raw.vf.w) & PFLAG_ENABLED)) {
                     pcell[k] = 255;
-                    continue;
+                } else {
+                    const v3 pt = mk(raw.xm.x, raw.xm.y, raw.xm.z);
+                    const float m = raw.xm.w;
+                    const CellInfo ci = cell_info(dx, pt);
+                    const v3 r = mk((float)(vid.x * 4 + (int)ci.ax), (float)(vid.y * 4 + (int)ci.ay),
+                                    (float)(vid.z * 4 + (int)ci.az)) * dx - pt;
+                    const v3 wx = kernel_eval_all(-r.x * inv_dx);
+                    const v3 wy = kernel_eval_all(-r.y * inv_dx);
+                    const v3 wz = kernel_eval_all(-r.z * inv_dx);
+                    const m3 C = mkm(mk(raw.c0.x, raw.c0.y, raw.c0.z), mk(raw.c1.x, raw.c1.y, raw.c1.z),
+                                     mk(raw.c2.x, raw.c2.y, raw.c2.z));
+                    const v3 q = C * r + mk(raw.vf.x, raw.vf.y, raw.vf.z) * m;
+                    float4* rr = reinterpret_cast<float4*>(rec + k * kP2gRec);
+                    rr[0] = make_float4(q.x, q.y, q.z, m);
+                    rr[1] = make_float4(C.c0.x * dx, C.c0.y * dx, C.c0.z * dx, wz.x);
+                    rr[2] = make_float4(C.c1.x * dx, C.c1.y * dx, C.c1.z * dx, wz.y);
+                    rr[3] = make_float4(C.c2.x * dx, C.c2.y * dx, C.c2.z * dx, wz.z);
+                    rr[4] = make_float4(wx.x * wy.x, wx.y * wy.x, wx.z * wy.x, wx.x * wy.y);
+                    rr[5] = make_float4(wx.y * wy.y, wx.z * wy.y, wx.x * wy.z, wx.y * wy.z);
+                    rr[6] = make_float4(wx.z * wy.z, 0.f, 0.f, 0.f);
+                    const uint32_t c = ci.ax + 4u * ci.ay + 16u * ci.az;
+                    pcell[k] = (uint8_t)c;
+                    prank[k] = (uint16_t)atomicAdd(&cnt[c], 1);
                 }
-                const float4 c0 = __ldg(kr + 2), c1 = __ldg(kr + 3), c2 = __ldg(kr + 4);
-                const v3 pt = mk(xm.x, xm.y, xm.z);
-                const float m = xm.w;
-                const CellInfo ci = cell_info(dx, pt);
-                const v3 r = mk((float)(vid.x * 4 + (int)ci.ax), (float)(vid.y * 4 + (int)ci.ay),
-                                (float)(vid.z * 4 + (int)ci.az)) * dx - pt;
-                const v3 wx = kernel_eval_all(-r.x * inv_dx);
-                const v3 wy = kernel_eval_all(-r.y * inv_dx);
-                const v3 wz = kernel_eval_all(-r.z * inv_dx);
-                const m3 C = mkm(mk(c0.x, c0.y, c0.z), mk(c1.x, c1.y, c1.z), mk(c2.x, c2.y, c2.z));
-                const v3 q = C * r + mk(vf.x, vf.y, vf.z) * m;
-                float4* rr = reinterpret_cast<float4*>(rec + k * kP2gRec);
-                rr[0] = make_float4(q.x, q.y, q.z, m);
-                rr[1] = make_float4(C.c0.x * dx, C.c0.y * dx, C.c0.z * dx, wz.x);
-                rr[2] = make_float4(C.c1.x * dx, C.c1.y * dx, C.c1.z * dx, wz.y);
-                rr[3] = make_float4(C.c2.x * dx, C.c2.y * dx, C.c2.z * dx, wz.z);
-                rr[4] = make_float4(wx.x * wy.x, wx.y * wy.x, wx.z * wy.x, wx.x * wy.y);
-                rr[5] = make_float4(wx.y * wy.y, wx.z * wy.y, wx.x * wy.z, wx.y * wy.z);
-                rr[6] = make_float4(wx.z * wy.z, 0.f, 0.f, 0.f);
-                const uint32_t c = ci.ax + 4u * ci.ay + 16u * ci.az;
-                pcell[k] = (uint8_t)c;
-                prank[k] = (uint16_t)atomicAdd(&cnt[c], 1);
+            }
+            // sorted id of this thread's particle in the next chunk (this block or the next one)
+            uint32_t pid_next = NONE;
+            if (base + kP2gChunk < h.np) {
+                if (base + kP2gChunk + tid < h.np) pid_next = __ldg(&P.sorted[h.first + base + kP2gChunk + tid]);
+            } else if (tid < hn.np) {
+                pid_next = __ldg(&P.sorted[hn.first + tid]);
             }
             __syncthreads();
             // 2. exclusive scan of the 64 cell counts
@@ -132,12 +187,13 @@ __global__ void __launch_bounds__(kP2gThreads, NXM_P2G_MIN_CTAS) k_p2g(DevPtrs P
                 if (lane == 31) start[64] = incl;
             }
             __syncthreads();
-            for (uint32_t k = tid; k < m_chunk; k += kP2gThreads) {
-                const uint32_t c = pcell[k];
-                if (c != 255u) perm[start[c] + prank[k]] = (uint16_t)k;
+            if (tid < m_chunk) {
+                const uint32_t c = pcell[tid];
+                if (c != 255u) perm[start[c] + prank[tid]] = (uint16_t)tid;
             }
             __syncthreads();
             if (tid < 64) cnt[tid] = 0;  // counts are consumed; ready for the next chunk
+            raw = p2g_load_raw(P, pid_next);
             // 3. one warp per cell, three particles per pass
             for (uint32_t c = warp; c < 64u; c += kP2gWarps) {
                 const int s0 = start[c], s1 = start[c + 1];
@@ -184,27 +240,25 @@ __global__ void __launch_bounds__(kP2gThreads, NXM_P2G_MIN_CTAS) k_p2g(DevPtrs P
             __syncthreads();
         }
         // 4. sum the warp tiles (clearing them) and flush the block's nodes
-        for (uint32_t t = tid; t < 216u; t += kP2gThreads) {
-            float4 sum = tiles[t];
-            tiles[t] = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (tid < 216u) {
+            float4 sum = tiles[tid];
+            tiles[tid] = make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
             for (int w = 1; w < kP2gWarps; ++w) {
-                sum = f4add(sum, tiles[w * 216 + t]);
-                tiles[w * 216 + t] = make_float4(0.f, 0.f, 0.f, 0.f);
+                sum = f4add(sum, tiles[w * 216 + tid]);
+                tiles[w * 216 + tid] = make_float4(0.f, 0.f, 0.f, 0.f);
             }
-            if (sum.x == 0.f && sum.y == 0.f && sum.z == 0.f && sum.w == 0.f) continue;
-            const uint32_t tx = t % 6u, ty = (t / 6u) % 6u, tz = t / 36u;
-            const uint32_t ox = tx >= 4u, oy = ty >= 4u, oz = tz >= 4u;
-            const uint32_t oct = ox * 4u + oy * 2u + oz;
-            const uint32_t blk = oct == 0 ? b : P.nbh[b * NUM_NBH + oct - 1u];
-            if (blk == NONE) {
-                set_status_f(P.counters, STATUS_MISSING_BLOCK);
-                continue;
+            if (sum.x != 0.f || sum.y != 0.f || sum.z != 0.f || sum.w != 0.f) {
+                if (fblk == NONE) set_status_f(P.counters, STATUS_MISSING_BLOCK);
+                else atomicAdd(&P.nodes[fblk * 64u + fnode], sum);
             }
-            const uint32_t node = blk * 64u + (tx - 4u * ox) + 4u * (ty - 4u * oy) + 16u * (tz - 4u * oz);
-            atomicAdd(&P.nodes[node], sum);
         }
         __syncthreads();
+        b += stride;
+        if (b >= nbp) break;
+        h = hn;
+        hn = hnn;
+        hnn = p2g_load_hdr(P, b + 2u * stride, nbp);
     }
 }
 

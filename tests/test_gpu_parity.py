@@ -177,6 +177,64 @@ def test_grid_capacity_overflow_is_reported(pipe):
         st.synchronize()
     assert e.value.code == NXM_E_CAPACITY
     assert st.status(clear=True) & 2
+    # no particle is lost or swapped: the ones without a block are carried over
+    # unchanged, the others moved by less than one cell (velocity clamp dx/dt)
+    got = st.read_positions()
+    assert np.isfinite(got).all()
+    assert np.abs(got - sc.particles.pos).max() <= sc.dx
+
+
+def test_sort_on_reordered_storage_matches_oracle(pipe):
+    """After fast steps the records sit in block order; the sort of that storage
+    reports particle ids and matches the oracle's sort of the same positions."""
+    import copy
+    from oracle.oracle import OracleScene
+    sc = scenes.mixed_materials(n_side=8)
+    st = state_from_scene(sc)
+    for _ in range(5):
+        pipe.step(st)
+    pos = st.read_positions()
+    pipe.debug_sort(st)
+    st.synchronize()
+    sc2 = copy.deepcopy(sc)
+    sc2.particles.pos[:] = pos
+    o = OracleScene(sc2)
+    o.sort()
+    errs = compare_sort(st.headers(), st.sorted_ids(), o.headers(), o.sorted_ids(), exact_order=False)
+    assert not errs, "\n".join(errs[:10])
+
+
+def test_edits_on_reordered_storage(pipe):
+    """swap_remove / shift_remove / append address particles by id also after
+    fast steps have left the records in block order."""
+    sc = scenes.mixed_materials(n_side=6)
+    st = state_from_scene(sc)
+    for _ in range(4):
+        pipe.step(st)
+    before = st.read_particles()
+    n = len(st)
+    remaps = st.swap_remove([5, n - 1, 17])
+    assert remaps == [(n - 2, 17), (n - 3, 5)]
+    after = st.read_particles()
+    idx = np.arange(n - 3)
+    idx[17], idx[5] = n - 2, n - 3
+    for k in ("pos", "vel", "aff", "def_grad", "mass", "model", "enabled"):
+        assert np.array_equal(after[k], before[k][idx]), k
+    st.shift_remove(10, 20)
+    shifted = st.read_particles()
+    keep = np.r_[0:10, 20:n - 3]
+    for k in ("pos", "def_grad", "model"):
+        assert np.array_equal(shifted[k], after[k][keep]), k
+    extra = scenes.elastic_cube(n_side=4).particles
+    m = len(st)
+    st.append(extra)
+    grown = st.read_particles()
+    assert np.array_equal(grown["pos"][:m], shifted["pos"]) and np.array_equal(grown["pos"][m:], extra.pos)
+    for _ in range(3):
+        pipe.step(st)
+    final = st.read_particles()
+    assert np.isfinite(final["pos"]).all()
+    assert np.abs(final["pos"][m:] - extra.pos).max() < 0.1
 
 
 def test_graph_replay_counts_kernels(pipe):
