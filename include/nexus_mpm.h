@@ -184,7 +184,10 @@ NXM_API int nxm_state_set_cell_width(nxm_state* state, float cell_width, uint32_
 
 /* MpmState::set_coupling (src_mpm/pipeline.rs:220-247) for one-way coupled
  * colliders given directly (at most 16).  `tri_vertices` holds 3 vertices
- * (9 floats) per triangle, in the local frame of the owning trimesh.  Unlike
+ * (9 floats) per triangle, in the local frame of the owning trimesh; a
+ * trimesh collider uses triangles [tri_first, tri_first + tri_count), for
+ * which the library builds a BVH and the feature pseudo-normals (the
+ * reference uploads both from its host mesh, rbd shapes/trimesh.rs).  Unlike
  * the reference, this does not switch CPIC on; see nxm_state_set_use_cpic. */
 NXM_API int nxm_state_set_colliders(nxm_state* state, const nxm_collider* colliders, uint32_t num_colliders,
                             const float* tri_vertices, uint32_t num_triangles);

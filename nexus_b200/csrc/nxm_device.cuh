@@ -27,6 +27,7 @@ struct m3 {
 __device__ __forceinline__ v3 mk(float x, float y, float z) { return v3{x, y, z}; }
 __device__ __forceinline__ v3 operator+(v3 a, v3 b) { return mk(a.x + b.x, a.y + b.y, a.z + b.z); }
 __device__ __forceinline__ v3 operator-(v3 a, v3 b) { return mk(a.x - b.x, a.y - b.y, a.z - b.z); }
+__device__ __forceinline__ v3 operator-(v3 a) { return mk(-a.x, -a.y, -a.z); }
 __device__ __forceinline__ v3 operator*(v3 a, float s) { return mk(a.x * s, a.y * s, a.z * s); }
 __device__ __forceinline__ v3 operator/(v3 a, float s) { return mk(a.x / s, a.y / s, a.z / s); }
 __device__ __forceinline__ float dot(v3 a, v3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
@@ -474,6 +475,95 @@ __device__ __forceinline__ Proj capsule_project_local(v3 a, v3 b, float radius, 
         r.point = pa + o * radius;
     }
     return r;
+}
+
+// Closest point on triangle (a, b, c) to p and the feature it lies on
+// (Ericson, Real-Time Collision Detection 5.1.5, Voronoi regions): feature 0
+// = vertex id 0..2, 1 = edge id 0 = ab, 1 = bc, 2 = ca, 2 = face.  The
+// reference projects with parry's triangle query (trimesh.rs:172); both give
+// the closest point, the feature numbering follows trimesh.rs:120-140.
+struct TriProj {
+    v3 point;
+    int feature, id;
+};
+__device__ __forceinline__ TriProj triangle_closest(v3 a, v3 b, v3 c, v3 p) {
+    TriProj r;
+    const v3 ab = b - a, ac = c - a, ap = p - a;
+    const float d1 = dot(ab, ap), d2 = dot(ac, ap);
+    if (d1 <= 0.f && d2 <= 0.f) { r.point = a; r.feature = 0; r.id = 0; return r; }
+    const v3 bp = p - b;
+    const float d3 = dot(ab, bp), d4 = dot(ac, bp);
+    if (d3 >= 0.f && d4 <= d3) { r.point = b; r.feature = 0; r.id = 1; return r; }
+    const float vc = d1 * d4 - d3 * d2;
+    if (vc <= 0.f && d1 >= 0.f && d3 <= 0.f) {
+        const float v = d1 / (d1 - d3);
+        r.point = a + ab * v; r.feature = 1; r.id = 0; return r;
+    }
+    const v3 cp = p - c;
+    const float d5 = dot(ab, cp), d6 = dot(ac, cp);
+    if (d6 >= 0.f && d5 <= d6) { r.point = c; r.feature = 0; r.id = 2; return r; }
+    const float vb = d5 * d2 - d1 * d6;
+    if (vb <= 0.f && d2 >= 0.f && d6 <= 0.f) {
+        const float w = d2 / (d2 - d6);
+        r.point = a + ac * w; r.feature = 1; r.id = 2; return r;
+    }
+    const float va = d3 * d6 - d5 * d4;
+    if (va <= 0.f && (d4 - d3) >= 0.f && (d5 - d6) >= 0.f) {
+        const float w = (d4 - d3) / ((d4 - d3) + (d5 - d6));
+        r.point = b + (c - b) * w; r.feature = 1; r.id = 1; return r;
+    }
+    const float denom = 1.0f / (va + vb + vc);
+    const float v = vb * denom, w = vc * denom;
+    r.point = a + (ab * v + ac * w);
+    r.feature = 2; r.id = 0;
+    return r;
+}
+
+// parry Aabb::distance_to_local_point(pt, solid = true).
+__device__ __forceinline__ float aabb_distance(const DevBvhNode& n, v3 p) {
+    const float dx = fmaxf(fmaxf(n.mn[0] - p.x, p.x - n.mx[0]), 0.f);
+    const float dy = fmaxf(fmaxf(n.mn[1] - p.y, p.y - n.mx[1]), 0.f);
+    const float dz = fmaxf(fmaxf(n.mn[2] - p.z, p.z - n.mx[2]), 0.f);
+    return sqrtf(dx * dx + dy * dy + dz * dz);
+}
+
+// trimesh.rs:155-207 project_local_point: closest triangle within max_dist
+// (the last one found wins ties, "dist <= best"), BVH traversal pruned by box
+// distance, then the inside test pn . (p - proj) <= 0 with the pseudo-normal
+// of the closest feature.  Returns false when no triangle is within max_dist.
+__device__ __forceinline__ bool trimesh_project_local(const DevTri* __restrict__ tris,
+                                                      const DevBvhNode* __restrict__ bvh, uint32_t first,
+                                                      uint32_t count, v3 pt, float max_dist, Proj& out) {
+    float best = max_dist;
+    TriProj bp;
+    bp.point = pt; bp.feature = 2; bp.id = 0;
+    uint32_t best_tri = NONE;
+    const uint32_t end = first + count;
+    uint32_t curr = first;
+    for (uint32_t it = 0; it < count && curr < end; ++it) {
+        const DevBvhNode n = bvh[curr];
+        if (n.entry & kBvhLeaf) {
+            const DevTri& t = tris[n.entry & ~kBvhLeaf];
+            const TriProj pr = triangle_closest(mk(t.v[0][0], t.v[0][1], t.v[0][2]), mk(t.v[1][0], t.v[1][1], t.v[1][2]),
+                                                mk(t.v[2][0], t.v[2][1], t.v[2][2]), pt);
+            const float d = length(pr.point - pt);
+            if (d <= best) {
+                best = d;
+                bp = pr;
+                best_tri = n.entry & ~kBvhLeaf;
+            }
+            curr = n.exit;
+        } else {
+            curr = aabb_distance(n, pt) <= best ? n.entry : n.exit;
+        }
+    }
+    if (best_tri == NONE) return false;
+    const DevTri& t = tris[best_tri];
+    const int k = bp.feature == 0 ? bp.id : (bp.feature == 1 ? 3 + bp.id : 6);
+    const v3 pn = mk(t.pn[k][0], t.pn[k][1], t.pn[k][2]);
+    out.point = bp.point;
+    out.inside = dot(pn, pt - bp.point) <= 0.f;
+    return true;
 }
 
 __device__ __forceinline__ v3 bc_project(uint32_t ty, float friction, v3 vel, v3 n) {

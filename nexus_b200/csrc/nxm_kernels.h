@@ -14,7 +14,8 @@ struct DevPtrs {
     float4* pstate;          // model state words (plastic models)
     const Material* materials;
     DevCollider* colliders;
-    const float4* tri;       // trimesh triangles: 3 float4 per triangle
+    const DevTri* tris;      // trimesh triangles of all trimesh colliders
+    const DevBvhNode* bvh;   // their BVHs
     const Params* params;
     Counters* counters;
     // hash map of block keys

@@ -84,9 +84,34 @@ struct alignas(16) DevCollider {
     float local_com[4];
     float com[4];   // world centre of mass (refreshed at the start of a step)
     uint32_t type, bc_type, tri_first, tri_count;
-    float bc_friction, pad[3];
+    float bc_friction;
+    uint32_t bvh_first, bvh_count;  // trimesh: its BVH nodes [bvh_first, bvh_first + bvh_count)
+    uint32_t pad;
 };
 static_assert(sizeof(DevCollider) == 176, "DevCollider layout");
+
+// One triangle of a trimesh collider (local frame of the mesh), with the
+// pseudo-normals of its features for the inside test (Baerentzen & Aanaes
+// 2005): pn[0..2] vertices a, b, c (angle-weighted), pn[3..5] edges ab, bc,
+// ca (sum of the unit normals of the faces sharing the edge), pn[6] face
+// (ab x ac, unnormalised).
+struct alignas(16) DevTri {
+    float v[3][4];
+    float pn[7][4];
+};
+static_assert(sizeof(DevTri) == 160, "DevTri layout");
+
+// Node of a stackless BVH in depth-first order.  Internal: `entry` = first
+// child, `exit` = the node after this subtree.  Leaf: `entry` = kBvhLeaf |
+// triangle index (into the state's triangle array).
+constexpr uint32_t kBvhLeaf = 0x80000000u;
+struct alignas(16) DevBvhNode {
+    float mn[3];
+    uint32_t entry;
+    float mx[3];
+    uint32_t exit;
+};
+static_assert(sizeof(DevBvhNode) == 32, "DevBvhNode layout");
 
 // Per-step parameters read by every kernel from device memory (so a captured
 // CUDA graph stays valid when they change).

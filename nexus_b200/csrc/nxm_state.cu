@@ -10,6 +10,8 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <map>
@@ -170,7 +172,8 @@ struct nxm_state {
     // colliders
     std::vector<DevCollider> colliders;
     DevCollider* d_colliders = nullptr;
-    float4* d_tri = nullptr;
+    DevTri* d_tris = nullptr;       // triangles of every trimesh collider (one copy per collider)
+    DevBvhNode* d_bvh = nullptr;    // their BVHs
 
     // control
     Params* d_params = nullptr;
@@ -214,7 +217,8 @@ DevPtrs dev_ptrs(nxm_state* s) {
     }
     P.materials = s->d_materials;
     P.colliders = s->d_colliders;
-    P.tri = s->d_tri;
+    P.tris = s->d_tris;
+    P.bvh = s->d_bvh;
     P.params = s->d_params;
     P.counters = s->d_counters;
     P.hkey = s->hkey;
@@ -607,6 +611,133 @@ int upload_particles(nxm_state* s, const nxm_particles_soa* p, uint32_t count) {
     return invalidate_codes(s);
 }
 
+// ---- trimesh colliders (host side) ------------------------------------------
+
+using VKey = std::array<uint32_t, 3>;  // vertex position, bit pattern
+
+VKey vkey(const float* v) { return VKey{f_bits(v[0]), f_bits(v[1]), f_bits(v[2])}; }
+
+// Triangle records with pseudo-normals for the triangles [first, first + count)
+// of `tri` (9 floats each), treated as one mesh: the pseudo-normal of a vertex
+// sums, over the mesh's non-degenerate triangles with a vertex at that exact
+// position, the unit face normal times the corner angle; that of an edge sums
+// the unit normals of the triangles sharing it (either orientation); that of
+// the face is ab x ac.  These are the pseudo-normals the reference uploads
+// per vertex and per triangle edge (rbd shapes/trimesh.rs:111-150).
+void trimesh_records(const float* tri, uint32_t first, uint32_t count, std::vector<DevTri>& out) {
+    std::map<VKey, std::array<double, 3>> vpn;
+    std::map<std::pair<VKey, VKey>, std::array<double, 3>> epn;
+    auto sub = [](const float* a, const float* b, double* r) {
+        for (int k = 0; k < 3; ++k) r[k] = (double)a[k] - (double)b[k];
+    };
+    auto ekey = [](const VKey& a, const VKey& b) { return a < b ? std::make_pair(a, b) : std::make_pair(b, a); };
+    for (uint32_t t = first; t < first + count; ++t) {
+        const float* q[3] = {tri + 9 * (size_t)t, tri + 9 * (size_t)t + 3, tri + 9 * (size_t)t + 6};
+        double u[3], w[3];
+        sub(q[1], q[0], u);
+        sub(q[2], q[0], w);
+        double fn[3] = {u[1] * w[2] - u[2] * w[1], u[2] * w[0] - u[0] * w[2], u[0] * w[1] - u[1] * w[0]};
+        const double fl = std::sqrt(fn[0] * fn[0] + fn[1] * fn[1] + fn[2] * fn[2]);
+        if (fl == 0.0) continue;
+        for (double& x : fn) x /= fl;
+        for (int k = 0; k < 3; ++k) {
+            double e0[3], e1[3];
+            sub(q[(k + 1) % 3], q[k], e0);
+            sub(q[(k + 2) % 3], q[k], e1);
+            const double l0 = std::sqrt(e0[0] * e0[0] + e0[1] * e0[1] + e0[2] * e0[2]);
+            const double l1 = std::sqrt(e1[0] * e1[0] + e1[1] * e1[1] + e1[2] * e1[2]);
+            double c = (e0[0] * e1[0] + e0[1] * e1[1] + e0[2] * e1[2]) / (l0 * l1);
+            c = std::min(1.0, std::max(-1.0, c));
+            const double ang = std::acos(c);
+            auto& a = vpn[vkey(q[k])];
+            for (int d = 0; d < 3; ++d) a[d] += fn[d] * ang;
+            auto& e = epn[ekey(vkey(q[k]), vkey(q[(k + 1) % 3]))];
+            for (int d = 0; d < 3; ++d) e[d] += fn[d];
+        }
+    }
+    for (uint32_t t = first; t < first + count; ++t) {
+        const float* q[3] = {tri + 9 * (size_t)t, tri + 9 * (size_t)t + 3, tri + 9 * (size_t)t + 6};
+        DevTri r{};
+        for (int k = 0; k < 3; ++k)
+            for (int d = 0; d < 3; ++d) r.v[k][d] = q[k][d];
+        for (int k = 0; k < 3; ++k) {
+            auto it = vpn.find(vkey(q[k]));
+            auto ie = epn.find(ekey(vkey(q[k]), vkey(q[(k + 1) % 3])));
+            for (int d = 0; d < 3; ++d) {
+                r.pn[k][d] = it == vpn.end() ? 0.f : (float)it->second[d];
+                r.pn[3 + k][d] = ie == epn.end() ? 0.f : (float)ie->second[d];
+            }
+        }
+        double u[3], w[3];
+        sub(q[1], q[0], u);
+        sub(q[2], q[0], w);
+        r.pn[6][0] = (float)(u[1] * w[2] - u[2] * w[1]);
+        r.pn[6][1] = (float)(u[2] * w[0] - u[0] * w[2]);
+        r.pn[6][2] = (float)(u[0] * w[1] - u[1] * w[0]);
+        out.push_back(r);
+    }
+}
+
+// Skip-link BVH over the records [base, base + count) of `tris`: median split
+// of the triangle centroids along the longest axis of their bounds, one
+// triangle per leaf, nodes in depth-first order starting at node index `node0`.
+struct BvhItem {
+    float mn[3], mx[3], c[3];
+    uint32_t tri;
+};
+uint32_t bvh_build(std::vector<BvhItem>& items, size_t lo, size_t hi, uint32_t node0, std::vector<DevBvhNode>& nodes) {
+    const uint32_t id = (uint32_t)nodes.size();
+    nodes.push_back(DevBvhNode{});
+    DevBvhNode n{};
+    float cmn[3], cmx[3];
+    for (int d = 0; d < 3; ++d) {
+        n.mn[d] = cmn[d] = 3.0e38f;
+        n.mx[d] = cmx[d] = -3.0e38f;
+    }
+    for (size_t i = lo; i < hi; ++i)
+        for (int d = 0; d < 3; ++d) {
+            n.mn[d] = std::min(n.mn[d], items[i].mn[d]);
+            n.mx[d] = std::max(n.mx[d], items[i].mx[d]);
+            cmn[d] = std::min(cmn[d], items[i].c[d]);
+            cmx[d] = std::max(cmx[d], items[i].c[d]);
+        }
+    if (hi - lo == 1) {
+        n.entry = kBvhLeaf | items[lo].tri;
+    } else {
+        int axis = 0;
+        for (int d = 1; d < 3; ++d)
+            if (cmx[d] - cmn[d] > cmx[axis] - cmn[axis]) axis = d;
+        const size_t mid = lo + (hi - lo) / 2;
+        std::nth_element(items.begin() + lo, items.begin() + mid, items.begin() + hi,
+                         [axis](const BvhItem& a, const BvhItem& b) { return a.c[axis] < b.c[axis]; });
+        n.entry = node0 + id + 1;
+        bvh_build(items, lo, mid, node0, nodes);
+        bvh_build(items, mid, hi, node0, nodes);
+    }
+    n.exit = node0 + (uint32_t)nodes.size();
+    nodes[id] = n;
+    return id;
+}
+
+void trimesh_bvh(const std::vector<DevTri>& tris, uint32_t base, uint32_t count, uint32_t node0,
+                 std::vector<DevBvhNode>& nodes) {
+    std::vector<BvhItem> items(count);
+    for (uint32_t i = 0; i < count; ++i) {
+        const DevTri& t = tris[base + i];
+        BvhItem& it = items[i];
+        for (int d = 0; d < 3; ++d) {
+            it.mn[d] = std::min(t.v[0][d], std::min(t.v[1][d], t.v[2][d]));
+            it.mx[d] = std::max(t.v[0][d], std::max(t.v[1][d], t.v[2][d]));
+            it.c[d] = (t.v[0][d] + t.v[1][d] + t.v[2][d]) / 3.0f;
+        }
+        it.tri = base + i;
+    }
+    std::vector<DevBvhNode> local;
+    local.reserve(2 * (size_t)count);
+    bvh_build(items, 0, count, node0, local);
+    nodes.insert(nodes.end(), local.begin(), local.end());
+}
+
 bool device_ok(int* dev, int* sms) {
     int count = 0;
     if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
@@ -695,7 +826,7 @@ void nxm_state_destroy(nxm_state* s) {
     invalidate_graph(s);
     free_grid(s);
     free_particles(s);
-    dfree(s->d_materials); dfree(s->d_colliders); dfree(s->d_tri); dfree(s->d_params); dfree(s->d_counters);
+    dfree(s->d_materials); dfree(s->d_colliders); dfree(s->d_tris); dfree(s->d_bvh); dfree(s->d_params); dfree(s->d_counters);
     dfree(s->d_pack); dfree(s->d_offsets);
     if (s->h_counters) cudaFreeHost(s->h_counters);
     if (s->stream) cudaStreamDestroy(s->stream);
@@ -751,18 +882,42 @@ int nxm_state_set_colliders(nxm_state* s, const nxm_collider* cols, uint32_t nco
         d.bc_friction = c.bc_friction;
         d.tri_first = c.tri_first;
         d.tri_count = c.tri_count;
-        if (d.type != SHAPE_BALL && d.type != SHAPE_CUBOID && d.type != SHAPE_CAPSULE) return NXM_E_UNSUPPORTED;
+        if (d.type != SHAPE_BALL && d.type != SHAPE_CUBOID && d.type != SHAPE_CAPSULE && d.type != SHAPE_TRIMESH)
+            return NXM_E_UNSUPPORTED;
+        if (d.type == SHAPE_TRIMESH &&
+            (!tri || c.tri_count == 0 || c.tri_first > ntri || c.tri_count > ntri - c.tri_first))
+            return NXM_E_INVALID;
     }
-    (void)tri;
-    (void)ntri;
+    // every trimesh gets its own triangle records and BVH
+    std::vector<DevTri> tris;
+    std::vector<DevBvhNode> bvh;
+    for (DevCollider& d : dc) {
+        if (d.type != SHAPE_TRIMESH) continue;
+        const uint32_t base = (uint32_t)tris.size();
+        trimesh_records(tri, d.tri_first, d.tri_count, tris);
+        d.bvh_first = (uint32_t)bvh.size();
+        trimesh_bvh(tris, base, d.tri_count, d.bvh_first, bvh);
+        d.bvh_count = (uint32_t)bvh.size() - d.bvh_first;
+    }
     NXM_TRY(cudaStreamSynchronize(s->stream));
     if (ncol)
         NXM_TRY(cudaMemcpyAsync(s->d_colliders, dc.data(), sizeof(DevCollider) * ncol, cudaMemcpyHostToDevice,
                                 s->stream));
+    const bool had_mesh = s->d_tris != nullptr;
+    dfree(s->d_tris);
+    dfree(s->d_bvh);
+    if (!tris.empty()) {
+        NXM_TRY(dalloc(&s->d_tris, tris.size()));
+        NXM_TRY(dalloc(&s->d_bvh, bvh.size()));
+        NXM_TRY(cudaMemcpyAsync(s->d_tris, tris.data(), sizeof(DevTri) * tris.size(), cudaMemcpyHostToDevice,
+                                s->stream));
+        NXM_TRY(cudaMemcpyAsync(s->d_bvh, bvh.data(), sizeof(DevBvhNode) * bvh.size(), cudaMemcpyHostToDevice,
+                                s->stream));
+    }
     NXM_TRY(cudaStreamSynchronize(s->stream));
     const bool had = !s->colliders.empty();
     s->colliders = dc;
-    if (had != !s->colliders.empty()) invalidate_graph(s);
+    if (had != !s->colliders.empty() || had_mesh || !tris.empty()) invalidate_graph(s);
     s->params_dirty = true;
     return NXM_OK;
 }

@@ -32,9 +32,12 @@ struct Collision {
     uint32_t closest;
 };
 
-// grid_update_collide.rs:30-99 collide() for analytic shapes (ball, cuboid,
-// capsule).  Trimesh colliders are rejected on the host for now.
-__device__ __forceinline__ Collision collide(const DevCollider* cols, uint32_t ncol, float dx, v3 point) {
+// grid_update_collide.rs:30-99 collide(): analytic shapes (ball, cuboid,
+// capsule) and triangle meshes (BVH query within 1.5 dx, as the reference's
+// project_local_point with max_dist; a mesh with no triangle that close is
+// skipped).
+__device__ __forceinline__ Collision collide(const DevPtrs& P, const DevCollider* cols, uint32_t ncol, float dx,
+                                             v3 point) {
     const float cap = dx * 1.5f;
     Collision col;
     col.normal = splat(0.f);
@@ -44,13 +47,20 @@ __device__ __forceinline__ Collision collide(const DevCollider* cols, uint32_t n
         const DevCollider& c = cols[i];
         quat q = quat{c.rot[0], c.rot[1], c.rot[2], c.rot[3]};
         v3 tra = mk(c.tra[0], c.tra[1], c.tra[2]);
-        v3 local = qrot(qconj(q), point - tra);
         Proj pr;
-        if (c.type == SHAPE_BALL) pr = ball_project_local(c.a[0], local);
-        else if (c.type == SHAPE_CUBOID) pr = cuboid_project_local(mk(c.a[0], c.a[1], c.a[2]), local);
-        else if (c.type == SHAPE_CAPSULE)
-            pr = capsule_project_local(mk(c.a[0], c.a[1], c.a[2]), mk(c.b[0], c.b[1], c.b[2]), c.b[3], local);
-        else { pr.point = local; pr.inside = false; }
+        if (c.type == SHAPE_TRIMESH) {
+            // pose.inverse() * point, as the inverse isometry applies it
+            const quat ci = qconj(q);
+            const v3 local = qrot(ci, point) + (-qrot(ci, tra));
+            if (!trimesh_project_local(P.tris, P.bvh, c.bvh_first, c.bvh_count, local, cap, pr)) continue;
+        } else {
+            v3 local = qrot(qconj(q), point - tra);
+            if (c.type == SHAPE_BALL) pr = ball_project_local(c.a[0], local);
+            else if (c.type == SHAPE_CUBOID) pr = cuboid_project_local(mk(c.a[0], c.a[1], c.a[2]), local);
+            else if (c.type == SHAPE_CAPSULE)
+                pr = capsule_project_local(mk(c.a[0], c.a[1], c.a[2]), mk(c.b[0], c.b[1], c.b[2]), c.b[3], local);
+            else { pr.point = local; pr.inside = false; }
+        }
         pr.point = qrot(q, pr.point) + tra;
         v3 dpt = pr.point - point;
         v3 ad = vabs(dpt);
@@ -93,7 +103,7 @@ __global__ void __launch_bounds__(256) k_grid_update(DevPtrs P) {
             int4 vid = P.bvid[b];
             v3 cell_pt = mk((float)(vid.x * 4 + (int)(k & 3u)), (float)(vid.y * 4 + (int)((k >> 2) & 3u)),
                             (float)(vid.z * 4 + (int)(k >> 4))) * dx;
-            Collision c = collide(scol, ncol, dx, cell_pt);
+            Collision c = collide(P, scol, ncol, dx, cell_pt);
             if (c.distance != MAX_FLT) {
                 const DevCollider& cc = scol[c.closest];
                 v3 bv = col_vel_at(cc, cell_pt);

@@ -22,7 +22,7 @@ from dataclasses import dataclass, field
 import numpy as np
 
 from .models import ParticleModel, BoundaryCondition
-from .particles import ParticleBatch, box_walls, collider_array
+from .particles import Collider, ParticleBatch, box_walls, collider_array
 
 _GOLDEN = np.uint64(0x9E3779B97F4A7C15)
 _M1 = np.uint64(0xBF58476D1CE4E5B9)
@@ -135,3 +135,36 @@ def mixed_materials(n_side: int = 12, seed: int = 7, dx: float = 1.0 / 64.0) -> 
     batch = ParticleBatch.concat(batches)
     cols = collider_array(box_walls(0.0, 1.0, BoundaryCondition.stick(), BoundaryCondition.separate(0.5)))
     return Scene("mixed_materials", dx, 1.0e-4, (0.0, 0.0, -9.81), batch, cols, 50, grid_capacity_for(batch.n))
+
+
+def height_field(n_vertices: int, seed: int, lo: float = 0.0, hi: float = 1.0, base: float = 0.05,
+                 amplitude: float = 0.02) -> np.ndarray:
+    """Triangles (ntri, 3, 3) of a square height field over [lo, hi]^2: an
+    n_vertices x n_vertices grid with heights base + U(0, amplitude), two
+    triangles per quad, counter-clockwise seen from +z (normals point up)."""
+    h = base + amplitude * uniform(seed, n_vertices * n_vertices)
+    xs = np.linspace(lo, hi, n_vertices)
+    v = np.stack(np.meshgrid(xs, xs, indexing="ij"), -1)  # [i, j] -> (x_i, y_j)
+    v = np.concatenate([v, h.reshape(n_vertices, n_vertices, 1)], -1).astype(np.float32)
+    a, b = v[:-1, :-1], v[1:, :-1]
+    c, d = v[1:, 1:], v[:-1, 1:]
+    t0 = np.stack([a, b, c], -2).reshape(-1, 3, 3)
+    t1 = np.stack([a, c, d], -2).reshape(-1, 3, 3)
+    return np.concatenate([t0, t1], 0)
+
+
+def trimesh_floor(n_side: int = 16, n_vertices: int = 21, seed: int = 11, steps: int = 100) -> Scene:
+    """A neo-Hookean cube (dx = 1/64) dropped onto a random height-field
+    trimesh floor (heights 0.05 + U(0, 0.02), as the coupling workload's
+    floor), inside five slip walls and a slip cuboid floor below the mesh."""
+    dx = 1.0 / 64.0
+    pos = lattice_block((0.35, 0.35, 0.085), (n_side, n_side, n_side), dx, seed)
+    model = ParticleModel.elastic_neo_hookean(1.0e5, 0.3)
+    batch = ParticleBatch.from_positions(pos, np.float32(dx) / np.float32(4.0), 1000.0, model)
+    batch.vel[:, 2] = -1.0
+    tri = height_field(n_vertices, seed + 1)
+    walls = box_walls(0.0, 1.0, BoundaryCondition.slip(), BoundaryCondition.slip())
+    mesh = Collider.trimesh(0, len(tri), (0.0, 0.0, 0.0), BoundaryCondition.separate(0.3))
+    cols = collider_array(walls + [mesh])
+    return Scene("trimesh_floor", dx, 1.0e-4, (0.0, 0.0, -9.81), batch, cols, steps, grid_capacity_for(batch.n),
+                 tri_vertices=tri.reshape(-1, 3))
