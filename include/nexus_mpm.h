@@ -298,6 +298,15 @@ NXM_API int nxm_sort_blocks_noalloc(const float* positions, uint32_t n, float ce
                                     int32_t* block_vids, uint32_t* block_ranges, uint32_t max_blocks,
                                     uint32_t* num_blocks, void* stream);
 
+/* WgTimestepBounds::compute_bounds (src_mpm/solver/timestep_bound.rs:24-46,
+ * kernel src_mpm_shaders/solver/timestep_bound.rs:59-115): the CFL bound on dt
+ * over the enabled particles, from each model's sound speed and the particle
+ * velocity plus its APIC term.  Enqueued on the state's stream and read back
+ * (synchronizes).  `*max_dt` = bits / 1e12 as the reference returns it;
+ * `bits` (nullable) receives the fixed-point value (dt * 1e12) as u32, or
+ * 0xFFFFFFFF when no particle is enabled. */
+NXM_API int nxm_state_estimate_timestep_bound(nxm_state* state, float* max_dt, uint32_t* bits);
+
 /* ---- synchronisation and status ------------------------------------------ */
 
 NXM_API int nxm_synchronize(nxm_state* state);

@@ -76,6 +76,8 @@ void launch_colliders_end(const DevPtrs& P, cudaStream_t s);
 
 namespace exact {
 void launch_p2g_gather(const DevPtrs& P, const LaunchCfg& c, cudaStream_t s);
+// Min over particles of the CFL bound into counters->dt_bound (reset by the caller).
+void launch_timestep_bound(const DevPtrs& P, const LaunchCfg& c, cudaStream_t s);
 void launch_grid_update(const DevPtrs& P, const LaunchCfg& c, cudaStream_t s);
 void launch_g2p_update(const DevPtrs& P, const LaunchCfg& c, cudaStream_t s);
 }  // namespace exact

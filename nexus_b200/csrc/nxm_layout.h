@@ -138,7 +138,7 @@ struct alignas(16) Counters {
     uint32_t codes_valid;   // 1 when pcode holds the block key of every particle's current position
     uint32_t unsorted;      // particles without a block this step, placed after the sorted ones
                             // by the reordering G2P
-    uint32_t pad;
+    uint32_t dt_bound;      // CFL bound, (dt * 1e12) as u32 (written by the timestep-bound query)
 };
 
 }  // namespace nxm

@@ -1117,6 +1117,25 @@ int nxm_debug_sort(nxm_pipeline* pipeline, nxm_state* s, int with_p2g) {
     return NXM_OK;
 }
 
+int nxm_state_estimate_timestep_bound(nxm_state* s, float* max_dt, uint32_t* bits) {
+    if (!s || !max_dt) return NXM_E_INVALID;
+    int rc = ensure_ready(s);
+    if (rc) return rc;
+    NXM_TRY(cudaMemsetAsync(reinterpret_cast<char*>(s->d_counters) + offsetof(Counters, dt_bound), 0xFF, 4,
+                            s->stream));
+    if (s->n) {
+        exact::launch_timestep_bound(dev_ptrs(s), launch_cfg(s), s->stream);
+        s->launches += 1;
+        NXM_TRY(cudaGetLastError());
+    }
+    NXM_TRY(cudaMemcpyAsync(s->h_counters, s->d_counters, sizeof(Counters), cudaMemcpyDeviceToHost, s->stream));
+    NXM_TRY(cudaStreamSynchronize(s->stream));
+    const uint32_t b = s->h_counters->dt_bound;
+    if (bits) *bits = b;
+    *max_dt = (float)b / 1.0e12f;
+    return NXM_OK;
+}
+
 int nxm_synchronize(nxm_state* s) {
     if (!s) return NXM_E_INVALID;
     NXM_TRY(cudaStreamSynchronize(s->stream));

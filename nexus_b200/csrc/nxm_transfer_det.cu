@@ -92,7 +92,79 @@ __global__ void __launch_bounds__(64) k_p2g_gather(DevPtrs P) {
     }
 }
 
+// CFL timestep bound (solver/timestep_bound.rs:59-115): per enabled
+// particle, the model's sound-speed bound (models/default.rs:268-343,
+// models/utils.rs:157-175) and the velocity + APIC bound, reduced with an
+// atomic min on the fixed-point value (dt * 1e12) as u32.  Built without
+// multiply-add contraction, so the value matches the f32 oracle's.
+__device__ __forceinline__ float sound_speed_bound(float alpha, float bulk, float shear, float density0,
+                                                   float def_grad_det, v3 vel, float cell_width) {
+    const float curr_density = density0 / fmaxf(def_grad_det, 1.0e-6f);
+    const float sound_speed = sqrtf((bulk + shear * 4.0f / 3.0f) / curr_density);
+    const float max_speed = fmaxf(length(vel), sound_speed);
+    return alpha * cell_width / max_speed;
+}
+// linear_elasticity.rs:58-80 / neo_hookean_elasticity.rs:43-65: words lambda, mu, cfl at w[o..o+3)
+__device__ __forceinline__ float elastic_bound(const float* w, int o, float hardening, float density0, float jdet,
+                                               v3 vel, float cw) {
+    const float bulk = w[o] + 2.0f * w[o + 1] / 3.0f;  // utils.rs:34-36
+    const float shear = w[o + 1];                      // utils.rs:28-30
+    return sound_speed_bound(w[o + 2], bulk * hardening, shear * hardening, density0, jdet, vel, cw);
+}
+
+__global__ void __launch_bounds__(256) k_timestep_bound(DevPtrs P) {
+    const uint32_t n = P.params->n;
+    const float cw = P.params->dx;
+    uint32_t best = 0xFFFFFFFFu;
+    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+        const float4* kr = reinterpret_cast<const float4*>(&P.kin[p]);
+        const float4 xm = kr[0], vf = kr[1];
+        if (!(__float_as_uint(vf.w) & PFLAG_ENABLED)) continue;
+        const float4 c0 = kr[2], c1 = kr[3], c2 = kr[4];
+        const float4* dr = reinterpret_cast<const float4*>(&P.def[p]);
+        const float4 d0 = dr[0], d1 = dr[1], d2 = dr[2];
+        const m3 F = mkm(mk(d0.x, d0.y, d0.z), mk(d1.x, d1.y, d1.z), mk(d2.x, d2.y, d2.z));
+        const Material& mat = P.materials[__float_as_uint(d2.w)];
+        const float* w = mat.w;
+        const float mass = xm.w;
+        const float density0 = mass / d0.w;
+        const float jdet = det(F);
+        const v3 vel = mk(vf.x, vf.y, vf.z);
+        float dt;
+        switch (mat.tag) {
+        case MODEL_ELASTIC_LINEAR:
+        case MODEL_ELASTIC_NEO_HOOKEAN: dt = elastic_bound(w, 0, 1.0f, density0, jdet, vel, cw); break;
+        case MODEL_SAND_LINEAR:
+        case MODEL_SAND_NEO_HOOKEAN: dt = elastic_bound(w, 10, 1.0f, density0, jdet, vel, cw); break;
+        case MODEL_FLUID:  // fluid.rs:88-108: bulk modulus * gamma, no shear
+            dt = sound_speed_bound(w[3], w[0] * w[1], 0.0f, density0, jdet, vel, cw);
+            break;
+        case MODEL_SNOW: {  // snow.rs:77-79: hardening from the particle's plastic det
+            const float hard = expf(w[3] * (1.0f - P.pstate[p].x));
+            dt = elastic_bound(w, 4, hard, density0, jdet, vel, cw);
+            break;
+        }
+        default: dt = 0.0f; break;
+        }
+        const v3 a0 = mk(c0.x, c0.y, c0.z), a1 = mk(c1.x, c1.y, c1.z), a2 = mk(c2.x, c2.y, c2.z);
+        const float na2 = dot(a0, a0) + dot(a1, a1) + dot(a2, a2);
+        const float d = (cw * cw) / 4.0f;
+        const float norm_b = d * sqrtf(na2) / mass;
+        const float apic_v = norm_b * 6.0f * sqrtf(3.0f) / cw;
+        const float v = length(vel) + apic_v;
+        dt = fminf(dt, cw / v);
+        best = min(best, __float2uint_rz(dt * 1.0e12f));  // saturating, NaN -> 0, as Rust `as u32`
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) best = min(best, __shfl_xor_sync(0xFFFFFFFFu, best, o));
+    if ((threadIdx.x & 31u) == 0 && best != 0xFFFFFFFFu) atomicMin(&P.counters->dt_bound, best);
+}
+
 }  // namespace
+
+void launch_timestep_bound(const DevPtrs& P, const LaunchCfg& c, cudaStream_t s) {
+    k_timestep_bound<<<c.sm_count * 4, 256, 0, s>>>(P);
+}
 
 void launch_p2g_gather(const DevPtrs& P, const LaunchCfg& c, cudaStream_t s) {
     k_p2g_gather<<<c.sm_count * 16, 64, 0, s>>>(P);

@@ -90,6 +90,7 @@ SIGNATURES = {
     "nxm_grid_read_sorted_ids": (C.c_int, [_vp, _u, C.c_uint32]),
     "nxm_grid_read_nodes": (C.c_int, [_vp, _f, C.c_uint32]),
     "nxm_debug_sort": (C.c_int, [_vp, _vp, C.c_int]),
+    "nxm_state_estimate_timestep_bound": (C.c_int, [_vp, _f, _u]),
     "nxm_synchronize": (C.c_int, [_vp]),
     "nxm_state_status": (C.c_int, [_vp, _u, C.c_int]),
     "nxm_error_string": (C.c_char_p, [C.c_int]),
@@ -281,6 +282,13 @@ class MpmState:
 
     def read_models(self) -> np.ndarray:
         return self._read("nxm_read_models", (len(self), 25), np.uint32, _u)
+
+    def estimate_timestep_bound(self) -> tuple[float, int]:
+        """``WgTimestepBounds::compute_bounds``: (max dt in seconds, fixed-point bits)."""
+        dt = np.zeros(1, np.float32)
+        bits = np.zeros(1, np.uint32)
+        _check(self.lib.nxm_state_estimate_timestep_bound(self.h, _p(dt, _f), _p(bits, _u)), "estimate_timestep_bound")
+        return float(dt[0]), int(bits[0])
 
     def read_particles(self) -> dict:
         return dict(pos=self.read_positions(), vel=self.read_velocities(), aff=self.read_affine(),

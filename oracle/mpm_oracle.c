@@ -1270,6 +1270,71 @@ int orc_run(scene_t *s, uint32_t steps) {
 /* Accessors for the parity tests                                            */
 /* ------------------------------------------------------------------------ */
 
+/* ------------------------------------------------------------------------ */
+/* CFL timestep bound: solver/timestep_bound.rs:59-115 (per particle, min),   */
+/* models/default.rs:268-343 (model sound speed), models/utils.rs:157-175.    */
+/* ------------------------------------------------------------------------ */
+
+/* utils.rs:157-175 ElasticitySoundSpeedTimestepBound::timestep_bound */
+static REAL sound_speed_bound(REAL alpha, REAL bulk, REAL shear, REAL density0, REAL def_grad_det, v3 vel,
+                              REAL cell_width) {
+    REAL curr_density = density0 / fmax(def_grad_det, (REAL)1.0e-6);
+    REAL sound_speed = sqrt((bulk + shear * (REAL)4.0 / (REAL)3.0) / curr_density);
+    REAL max_speed = fmax(vlen(vel), sound_speed);
+    return alpha * cell_width / max_speed;
+}
+
+/* linear_elasticity.rs:58-80 / neo_hookean_elasticity.rs:43-65 on words w[o..o+3) = lambda, mu, cfl */
+static REAL elastic_bound(const REAL *w, int o, REAL hardening, REAL density0, REAL jdet, v3 vel, REAL cw) {
+    REAL lambda = w[o], mu = w[o + 1], cfl = w[o + 2];
+    REAL bulk = lambda + (REAL)2.0 * mu / (REAL)3.0; /* utils.rs:34-36 */
+    REAL shear = mu;                                 /* utils.rs:28-30 */
+    return sound_speed_bound(cfl, bulk * hardening, shear * hardening, density0, jdet, vel, cw);
+}
+
+/* The bound in the reference's fixed-point form: (dt * 1e12) as u32, the
+ * minimum over enabled particles (0xFFFFFFFF when none). */
+uint32_t orc_timestep_bound_bits(const scene_t *s) {
+    uint32_t best = 0xFFFFFFFFu;
+    const REAL cw = s->dx;
+    for (uint32_t p = 0; p < s->n; ++p) {
+        if (s->enabled[p] == 0) continue;
+        const REAL *w = &s->words[(size_t)p * MODEL_WORDS];
+        REAL density0 = s->mass[p] / s->init_volume[p];
+        REAL jdet = mdet(s->F[p]);
+        v3 vel = s->vel[p];
+        REAL dt;
+        switch (s->tag[p]) {
+        case MODEL_ELASTIC_LINEAR:
+        case MODEL_ELASTIC_NEO_HOOKEAN: dt = elastic_bound(w, 0, (REAL)1.0, density0, jdet, vel, cw); break;
+        case MODEL_SAND_LINEAR:
+        case MODEL_SAND_NEO_HOOKEAN: dt = elastic_bound(w, 10, (REAL)1.0, density0, jdet, vel, cw); break;
+        case MODEL_FLUID: /* fluid.rs:88-108: bulk modulus * gamma, no shear; words k, gamma, mu, cfl, t */
+            dt = sound_speed_bound(w[3], w[0] * w[1], (REAL)0.0, density0, jdet, vel, cw);
+            break;
+        case MODEL_SNOW: { /* snow.rs:77-79 hardening = exp(h (1 - plastic_det)); elastic words 4..6 */
+            REAL hard = exp(w[3] * ((REAL)1.0 - w[0]));
+            dt = elastic_bound(w, 4, hard, density0, jdet, vel, cw);
+            break;
+        }
+        default: dt = (REAL)0.0; break;
+        }
+        m3 A = s->aff[p];
+        REAL na2 = vdot(A.c0, A.c0) + vdot(A.c1, A.c1) + vdot(A.c2, A.c2);
+        REAL d = (cw * cw) / (REAL)4.0;
+        REAL norm_b = d * sqrt(na2) / s->mass[p];
+        REAL apic_v = norm_b * (REAL)6.0 * sqrt((REAL)3.0) / cw;
+        REAL v = vlen(vel) + apic_v;
+        dt = fmin(dt, cw / v);
+        /* Rust `as u32`: truncation, saturating, NaN -> 0 */
+        REAL scaled = dt * (REAL)1.0e12;
+        uint32_t c = scaled != scaled ? 0u : (scaled >= (REAL)4294967295.0 ? 0xFFFFFFFFu
+                                                : (scaled <= 0 ? 0u : (uint32_t)scaled));
+        if (c < best) best = c;
+    }
+    return best;
+}
+
 uint32_t orc_num_blocks(const scene_t *s) { return s->num_blocks; }
 uint32_t orc_status(const scene_t *s) { return s->status; }
 uint32_t orc_capacity(const scene_t *s) { return s->capacity; }

@@ -58,7 +58,7 @@ def lib(precision: str = "f32"):
     L.orc_run.restype = C.c_int
     for name in ("orc_p2g", "orc_grid_update", "orc_g2p", "orc_particle_update"):
         getattr(L, name).argtypes = [C.c_void_p]
-    for name in ("orc_num_blocks", "orc_status", "orc_capacity", "orc_sorted_len"):
+    for name in ("orc_num_blocks", "orc_status", "orc_capacity", "orc_sorted_len", "orc_timestep_bound_bits"):
         getattr(L, name).argtypes = [C.c_void_p]
         getattr(L, name).restype = C.c_uint32
     L.orc_get_headers.argtypes = [C.c_void_p, _i]
@@ -143,6 +143,10 @@ class OracleScene:
     @property
     def num_blocks(self) -> int:
         return self.L.orc_num_blocks(self.h)
+
+    def timestep_bound_bits(self) -> int:
+        """CFL bound (solver/timestep_bound.rs:59-115) as (dt * 1e12) as u32."""
+        return int(self.L.orc_timestep_bound_bits(self.h))
 
     @property
     def status(self) -> int:

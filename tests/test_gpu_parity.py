@@ -156,6 +156,30 @@ def test_trimesh_floor_100_steps(pipe, deterministic):
     assert g["pos"][:, 2].min() > 0.05 - sc.dx
 
 
+@pytest.mark.parametrize("name", ["cube", "mixed", "sandwater"])
+def test_timestep_bound_matches_oracle(pipe, name):
+    """CFL bound: the same fixed-point value as the f32 oracle on the uploaded
+    state (random velocities and affine, so both terms matter), and within
+    rounding after steps in either mode (fast mode: on reordered storage)."""
+    from oracle.oracle import OracleScene
+    sc = _scene(name)
+    rng = np.random.default_rng(12)
+    sc.particles.vel[:] = (rng.standard_normal(sc.particles.vel.shape) * 2.0).astype(np.float32)
+    sc.particles.aff[:] = (rng.standard_normal(sc.particles.aff.shape) * 1e-3).astype(np.float32)
+    o = OracleScene(sc)
+    for deterministic in (False, True):
+        st = state_from_scene(sc, deterministic=deterministic)
+        dt, bits = st.estimate_timestep_bound()
+        assert bits == o.timestep_bound_bits()
+        assert dt == pytest.approx(bits / 1e12, rel=1e-6)
+        for _ in range(10):
+            pipe.step(st)
+        _, bits10 = st.estimate_timestep_bound()
+        o10 = OracleScene(sc)
+        o10.step(10)
+        assert bits10 == pytest.approx(o10.timestep_bound_bits(), rel=1e-5 if deterministic else 1e-3)
+
+
 def test_upload_readback_roundtrip(pipe):
     sc = scenes.mixed_materials(n_side=4)
     rng = np.random.default_rng(9)

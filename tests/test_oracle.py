@@ -272,3 +272,27 @@ def test_fp32_and_fp64_oracles_agree_on_elastic_cube(oracle_built):
     b.step(20)
     pa, pb = a.particles()["pos"], b.positions_f64()
     assert np.linalg.norm(pa - pb) / np.linalg.norm(pb) < 1e-6
+
+
+def test_timestep_bound_closed_form(oracle_built):
+    """CFL bound (solver/timestep_bound.rs:59-115): at rest with F = I and
+    C = 0 it is cfl * dx / sqrt((K + 4/3 G) / rho0) (utils.rs:157-175) for an
+    elastic solid and cfl * dx / sqrt(gamma K / rho0) for the Tait fluid; the
+    velocity term takes over once |v| exceeds the sound speed."""
+    from oracle.oracle import OracleScene
+    dx = 1.0 / 64.0
+    pos = scenes.lattice_block((0.4, 0.4, 0.4), (2, 2, 2), dx, 3)
+    for model, rho, speed in (
+            (ParticleModel.elastic_neo_hookean(1.0e5, 0.3), 1000.0, None),
+            (ParticleModel.water(1.0e5), 1000.0, math.sqrt(7.0 * 1.0e5 / 1000.0))):
+        batch = ParticleBatch.from_positions(pos, np.float32(dx / 4), rho, model)
+        sc = scenes.Scene("bound", dx, 1e-4, (0.0, 0.0, 0.0), batch, collider_array([]), 1, 64)
+        if speed is None:
+            lam, mu = lame_lambda_mu(1.0e5, 0.3)
+            speed = math.sqrt((lam + 2.0 * mu / 3.0 + 4.0 / 3.0 * mu) / rho)
+        want = 0.5 * dx / speed
+        got = OracleScene(sc).timestep_bound_bits() / 1e12
+        assert got == pytest.approx(want, rel=1e-5)
+        batch.vel[:] = (0.0, 0.0, 3.0 * speed)
+        got = OracleScene(sc).timestep_bound_bits() / 1e12
+        assert got == pytest.approx(min(0.5 * dx / (3.0 * speed), dx / (3.0 * speed)), rel=1e-5)
