@@ -298,6 +298,21 @@ NXM_API int nxm_sort_blocks_noalloc(const float* positions, uint32_t n, float ce
                                     int32_t* block_vids, uint32_t* block_ranges, uint32_t max_blocks,
                                     uint32_t* num_blocks, void* stream);
 
+/* ---- particle chunks (NexusState, src/state.rs:665-774) -------------------
+ * A chunk is a handle on a set of particles appended together (and later
+ * extended).  Removals swap-remove the chunk's slots (highest first) as
+ * GpuParticles::swap_remove does, moving the records on the device in one
+ * pass, and keep every particle's chunk ownership through the relocations. */
+NXM_API int nxm_chunk_add(nxm_state* state, const nxm_particle* particles, uint32_t count, uint32_t* chunk);
+NXM_API int nxm_chunk_extend(nxm_state* state, uint32_t chunk, const nxm_particle* particles, uint32_t count);
+NXM_API int nxm_chunk_remove(nxm_state* state, uint32_t chunk);
+/* Removes up to `count` of the chunk's particles (highest slots first); the
+ * chunk is kept even when emptied.  `removed` (nullable) receives the number. */
+NXM_API int nxm_chunk_remove_particles(nxm_state* state, uint32_t chunk, uint32_t count, uint32_t* removed);
+NXM_API int nxm_chunk_len(const nxm_state* state, uint32_t chunk, uint32_t* len);
+/* Owner chunk of each particle (0xFFFFFFFF: appended outside a chunk), len() entries. */
+NXM_API int nxm_chunk_of_particles(const nxm_state* state, uint32_t* out);
+
 /* WgTimestepBounds::compute_bounds (src_mpm/solver/timestep_bound.rs:24-46,
  * kernel src_mpm_shaders/solver/timestep_bound.rs:59-115): the CFL bound on dt
  * over the enabled particles, from each model's sound speed and the particle

@@ -94,6 +94,19 @@ __global__ void k_pack_fields_perm(const uint32_t* __restrict__ src, uint32_t st
     }
 }
 
+// Swap-removal data movement: record pairs[i].y moves to slot pairs[i].x.
+// Every source is at or above the new length and every destination below it,
+// so the moves are independent.
+__global__ void k_move_records(PKin* __restrict__ kin, PDef* __restrict__ def, float4* __restrict__ pstate,
+                               const uint2* __restrict__ pairs, uint32_t count) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+        const uint2 m = pairs[i];
+        kin[m.x] = kin[m.y];
+        def[m.x] = def[m.y];
+        pstate[m.x] = pstate[m.y];
+    }
+}
+
 __global__ void k_iota(uint32_t* __restrict__ out, uint32_t first, uint32_t count) {
     for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < count; t += gridDim.x * blockDim.x) out[t] = first + t;
 }
@@ -151,6 +164,11 @@ struct nxm_state {
     uint32_t* sorted = nullptr;
     std::vector<float> init_radius, phase, boundary_friction;
     std::vector<uint32_t> group_id;
+    // particle chunks (src/state.rs:665-774): owner chunk of each particle id
+    // (NONE for particles appended outside a chunk) and the live chunks' sizes
+    std::vector<uint32_t> slot2chunk;
+    std::map<uint32_t, uint32_t> chunks;
+    uint32_t next_chunk = 0;
 
     // materials (deduplicated model words)
     std::vector<Material> materials;
@@ -594,6 +612,7 @@ int upload_particles(nxm_state* s, const nxm_particles_soa* p, uint32_t count) {
         s->phase.push_back(p->phase ? p->phase[i] : 1.f);
         s->boundary_friction.push_back(p->boundary_friction ? p->boundary_friction[i] : 1.f);
         s->group_id.push_back(p->group_id ? p->group_id[i] : 0u);
+        s->slot2chunk.push_back(NONE);
     }
     rc = sync_materials(s);
     if (rc) return rc;
@@ -989,6 +1008,77 @@ int nxm_particles_append(nxm_state* s, const nxm_particle* particles, uint32_t c
 
 uint32_t nxm_particles_len(const nxm_state* s) { return s ? s->n : 0u; }
 
+// ---- particle chunks (NexusState, src/state.rs:665-774) ---------------------
+
+int nxm_chunk_add(nxm_state* s, const nxm_particle* particles, uint32_t count, uint32_t* chunk) {
+    if (!s || !chunk) return NXM_E_INVALID;
+    const uint32_t n0 = s->n;
+    int rc = nxm_particles_append(s, particles, count);
+    if (rc) return rc;
+    const uint32_t id = s->next_chunk++;
+    std::fill(s->slot2chunk.begin() + n0, s->slot2chunk.end(), id);
+    s->chunks[id] = count;
+    *chunk = id;
+    return NXM_OK;
+}
+
+int nxm_chunk_extend(nxm_state* s, uint32_t chunk, const nxm_particle* particles, uint32_t count) {
+    if (!s) return NXM_E_INVALID;
+    auto it = s->chunks.find(chunk);
+    if (it == s->chunks.end()) return NXM_E_INVALID;
+    const uint32_t n0 = s->n;
+    int rc = nxm_particles_append(s, particles, count);
+    if (rc) return rc;
+    std::fill(s->slot2chunk.begin() + n0, s->slot2chunk.end(), chunk);
+    it->second += count;
+    return NXM_OK;
+}
+
+// Slots of `chunk`, highest first, at most `limit`.
+static std::vector<uint32_t> chunk_slots_desc(const nxm_state* s, uint32_t chunk, size_t limit) {
+    std::vector<uint32_t> slots;
+    for (uint32_t i = s->n; i-- > 0 && slots.size() < limit;)
+        if (s->slot2chunk[i] == chunk) slots.push_back(i);
+    return slots;
+}
+
+int nxm_chunk_remove(nxm_state* s, uint32_t chunk) {
+    if (!s) return NXM_E_INVALID;
+    auto it = s->chunks.find(chunk);
+    if (it == s->chunks.end()) return NXM_E_INVALID;
+    std::vector<uint32_t> slots = chunk_slots_desc(s, chunk, s->n);
+    int rc = nxm_particles_swap_remove(s, slots.data(), (uint32_t)slots.size(), nullptr, nullptr);
+    if (rc) return rc;
+    s->chunks.erase(chunk);
+    return NXM_OK;
+}
+
+int nxm_chunk_remove_particles(nxm_state* s, uint32_t chunk, uint32_t count, uint32_t* removed) {
+    if (!s) return NXM_E_INVALID;
+    auto it = s->chunks.find(chunk);
+    if (it == s->chunks.end()) return NXM_E_INVALID;
+    std::vector<uint32_t> slots = chunk_slots_desc(s, chunk, count);
+    int rc = nxm_particles_swap_remove(s, slots.data(), (uint32_t)slots.size(), nullptr, nullptr);
+    if (rc) return rc;
+    it->second -= std::min<uint32_t>(it->second, (uint32_t)slots.size());
+    if (removed) *removed = (uint32_t)slots.size();
+    return NXM_OK;
+}
+
+int nxm_chunk_len(const nxm_state* s, uint32_t chunk, uint32_t* len) {
+    if (!s || !len) return NXM_E_INVALID;
+    auto it = s->chunks.find(chunk);
+    if (it == s->chunks.end()) return NXM_E_INVALID;
+    *len = it->second;
+    return NXM_OK;
+}
+
+int nxm_chunk_of_particles(const nxm_state* s, uint32_t* out) {
+    if (!s || (s->n && !out)) return NXM_E_INVALID;
+    std::copy(s->slot2chunk.begin(), s->slot2chunk.end(), out);
+    return NXM_OK;
+}
+
 int nxm_particles_swap_remove(nxm_state* s, const uint32_t* slots, uint32_t count, uint32_t* remaps,
                               uint32_t* num_remaps) {
     if (!s || (count && !slots)) return NXM_E_INVALID;
@@ -998,33 +1088,70 @@ int nxm_particles_swap_remove(nxm_state* s, const uint32_t* slots, uint32_t coun
     std::vector<uint32_t> t(slots, slots + count);
     std::sort(t.begin(), t.end(), [](uint32_t a, uint32_t b) { return a > b; });
     t.erase(std::unique(t.begin(), t.end()), t.end());
-    uint32_t nr = 0;
-    NXM_TRY(cudaStreamSynchronize(s->stream));
+    while (!t.empty() && t.front() >= s->n) t.erase(t.begin());  // out-of-range slots are ignored
+    if (t.empty()) {
+        if (num_remaps) *num_remaps = 0;
+        return NXM_OK;
+    }
+    const uint32_t n0 = s->n, n1 = n0 - (uint32_t)t.size();
+    // GpuParticles::swap_remove (src_mpm/solver/particle.rs:571-631): slots in
+    // descending order, each replaced by the current last particle; the remap
+    // list reports those moves in that order.
+    uint32_t nr = 0, n = n0;
     for (uint32_t slot : t) {
-        if (slot >= s->n) continue;
-        const uint32_t last = s->n - 1;
+        const uint32_t last = n - 1;
         if (slot != last) {
-            NXM_TRY(cudaMemcpyAsync(s->kin + slot, s->kin + last, sizeof(PKin), cudaMemcpyDeviceToDevice, s->stream));
-            NXM_TRY(cudaMemcpyAsync(s->def + slot, s->def + last, sizeof(PDef), cudaMemcpyDeviceToDevice, s->stream));
-            NXM_TRY(cudaMemcpyAsync(s->pstate + slot, s->pstate + last, sizeof(float4), cudaMemcpyDeviceToDevice,
-                                    s->stream));
             s->init_radius[slot] = s->init_radius[last];
             s->phase[slot] = s->phase[last];
             s->boundary_friction[slot] = s->boundary_friction[last];
             s->group_id[slot] = s->group_id[last];
+            s->slot2chunk[slot] = s->slot2chunk[last];
             if (remaps && nr < count) {
                 remaps[2 * nr] = last;
                 remaps[2 * nr + 1] = slot;
             }
             ++nr;
         }
-        s->init_radius.pop_back();
-        s->phase.pop_back();
-        s->boundary_friction.pop_back();
-        s->group_id.pop_back();
-        s->n -= 1;
+        --n;
     }
-    NXM_TRY(cudaStreamSynchronize(s->stream));
+    // The same result in one pass on the device: the i-th surviving particle
+    // at or above n1 (descending) lands in the i-th removed slot below n1
+    // (descending).  Sources are all >= n1 and destinations < n1.
+    std::vector<uint2> pairs;
+    {
+        std::vector<uint32_t> dst;  // removed slots below n1, descending
+        for (uint32_t slot : t)
+            if (slot < n1) dst.push_back(slot);
+        size_t k = 0;
+        auto removed = t.begin();  // descending
+        for (uint32_t src = n0; src-- > n1;) {
+            while (removed != t.end() && *removed > src) ++removed;
+            if (removed != t.end() && *removed == src) continue;  // removed itself
+            pairs.push_back(make_uint2(dst[k++], src));
+        }
+    }
+    if (!pairs.empty()) {
+        uint2* d_pairs = nullptr;
+        NXM_TRY(dalloc(&d_pairs, pairs.size()));
+        cudaError_t e = cudaMemcpyAsync(d_pairs, pairs.data(), sizeof(uint2) * pairs.size(), cudaMemcpyHostToDevice,
+                                        s->stream);
+        if (e == cudaSuccess) {
+            k_move_records<<<grid_for_n(s, (uint32_t)pairs.size()), 256, 0, s->stream>>>(s->kin, s->def, s->pstate,
+                                                                                        d_pairs,
+                                                                                        (uint32_t)pairs.size());
+            s->launches += 1;
+            e = cudaGetLastError();
+        }
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+        cudaFree(d_pairs);
+        NXM_TRY(e);
+    }
+    s->init_radius.resize(n1);
+    s->phase.resize(n1);
+    s->boundary_friction.resize(n1);
+    s->group_id.resize(n1);
+    s->slot2chunk.resize(n1);
+    s->n = n1;
     if (num_remaps) *num_remaps = nr;
     s->params_dirty = true;
     return invalidate_codes(s);
@@ -1057,6 +1184,7 @@ int nxm_particles_shift_remove(nxm_state* s, uint32_t start, uint32_t end) {
     erase(s->phase);
     erase(s->boundary_friction);
     erase(s->group_id);
+    erase(s->slot2chunk);
     s->n -= removed;
     s->params_dirty = true;
     return invalidate_codes(s);

@@ -14,7 +14,7 @@ import os
 
 import numpy as np
 
-from .particles import ParticleBatch, COLLIDER_DTYPE
+from .particles import ParticleBatch, COLLIDER_DTYPE, particle_records
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libnexus_mpm.so")
@@ -91,6 +91,12 @@ SIGNATURES = {
     "nxm_grid_read_nodes": (C.c_int, [_vp, _f, C.c_uint32]),
     "nxm_debug_sort": (C.c_int, [_vp, _vp, C.c_int]),
     "nxm_state_estimate_timestep_bound": (C.c_int, [_vp, _f, _u]),
+    "nxm_chunk_add": (C.c_int, [_vp, _vp, C.c_uint32, _u]),
+    "nxm_chunk_extend": (C.c_int, [_vp, C.c_uint32, _vp, C.c_uint32]),
+    "nxm_chunk_remove": (C.c_int, [_vp, C.c_uint32]),
+    "nxm_chunk_remove_particles": (C.c_int, [_vp, C.c_uint32, C.c_uint32, _u]),
+    "nxm_chunk_len": (C.c_int, [_vp, C.c_uint32, _u]),
+    "nxm_chunk_of_particles": (C.c_int, [_vp, _u]),
     "nxm_synchronize": (C.c_int, [_vp]),
     "nxm_state_status": (C.c_int, [_vp, _u, C.c_int]),
     "nxm_error_string": (C.c_char_p, [C.c_int]),
@@ -233,6 +239,35 @@ class MpmState:
             arr("boundary_friction", np.float32), arr("group_id", np.uint32), arr("enabled", np.uint32),
             arr("fixed", np.uint32), arr("model", np.uint32))
         _check(self.lib.nxm_particles_append_soa(self.h, C.byref(soa), batch.n), "append")
+
+    # -- particle chunks (NexusState, src/state.rs:665-774) ------------------------
+    def add_chunk(self, batch: ParticleBatch) -> int:
+        rec = particle_records(batch)
+        c = C.c_uint32()
+        _check(self.lib.nxm_chunk_add(self.h, rec.ctypes.data_as(C.c_void_p), batch.n, C.byref(c)), "chunk_add")
+        return c.value
+
+    def extend_chunk(self, chunk: int, batch: ParticleBatch):
+        rec = particle_records(batch)
+        _check(self.lib.nxm_chunk_extend(self.h, chunk, rec.ctypes.data_as(C.c_void_p), batch.n), "chunk_extend")
+
+    def remove_chunk(self, chunk: int):
+        _check(self.lib.nxm_chunk_remove(self.h, chunk), "chunk_remove")
+
+    def remove_particles_from_chunk(self, chunk: int, count: int) -> int:
+        r = C.c_uint32()
+        _check(self.lib.nxm_chunk_remove_particles(self.h, chunk, count, C.byref(r)), "chunk_remove_particles")
+        return r.value
+
+    def chunk_len(self, chunk: int) -> int:
+        r = C.c_uint32()
+        _check(self.lib.nxm_chunk_len(self.h, chunk, C.byref(r)), "chunk_len")
+        return r.value
+
+    def chunk_of_particles(self) -> np.ndarray:
+        out = np.zeros(max(len(self), 1), np.uint32)
+        _check(self.lib.nxm_chunk_of_particles(self.h, _p(out, _u)), "chunk_of_particles")
+        return out[:len(self)]
 
     def swap_remove(self, slots):
         s = np.ascontiguousarray(slots, np.uint32)

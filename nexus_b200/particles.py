@@ -110,6 +110,38 @@ COLLIDER_DTYPE = np.dtype([
 assert COLLIDER_DTYPE.itemsize == 128
 
 
+# nxm_particle (include/nexus_mpm.h), the reference's `Particle` fields.
+PARTICLE_DTYPE = np.dtype([
+    ("position", np.float32, 3), ("velocity", np.float32, 3), ("def_grad", np.float32, 9),
+    ("affine", np.float32, 9), ("force_dt", np.float32, 3), ("vel_grad_det", np.float32),
+    ("init_volume", np.float32), ("init_radius", np.float32), ("mass", np.float32), ("damping", np.float32),
+    ("phase", np.float32), ("boundary_friction", np.float32), ("group_id", np.uint32), ("enabled", np.uint32),
+    ("fixed", np.uint32), ("model", np.uint32, 25),
+])
+assert PARTICLE_DTYPE.itemsize == 248
+
+
+def particle_records(batch: "ParticleBatch") -> np.ndarray:
+    """The batch as an array of nxm_particle records."""
+    out = np.zeros(batch.n, dtype=PARTICLE_DTYPE)
+    out["position"] = batch.pos
+    out["velocity"] = batch.vel
+    out["def_grad"] = batch.def_grad.reshape(batch.n, 9)
+    out["affine"] = batch.aff.reshape(batch.n, 9)
+    out["vel_grad_det"] = batch.vel_grad_det
+    out["init_volume"] = batch.init_volume
+    out["init_radius"] = batch.init_radius
+    out["mass"] = batch.mass
+    out["damping"] = batch.damping
+    out["phase"] = batch.phase
+    out["boundary_friction"] = batch.boundary_friction
+    out["group_id"] = batch.group_id
+    out["enabled"] = batch.enabled
+    out["fixed"] = batch.fixed
+    out["model"] = batch.model
+    return out
+
+
 def _tag(ty: int) -> np.float32:
     return np.array([ty], dtype=np.uint32).view(np.float32)[0]
 

@@ -9,7 +9,7 @@ import numpy as np
 import pytest
 
 from nexus_b200 import build, mpm
-from nexus_b200.particles import COLLIDER_DTYPE
+from nexus_b200.particles import COLLIDER_DTYPE, PARTICLE_DTYPE
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 HEADER = os.path.join(ROOT, "include", "nexus_mpm.h")
@@ -61,6 +61,7 @@ int main(void) {{
     offs = list(map(int, b.split()))
     assert sizes[0] == COLLIDER_DTYPE.itemsize == 128
     assert sizes[1] == 100  # GpuParticleModel stride (models/default.rs:18)
+    assert sizes[2] == PARTICLE_DTYPE.itemsize
     assert sizes[3] == C.sizeof(mpm.ParticlesSoAC)
     assert sizes[4] == C.sizeof(mpm.SimulationParamsC) == 16
     assert sizes[5] == C.sizeof(mpm.CapacitiesC)

@@ -286,3 +286,41 @@ def test_graph_replay_counts_kernels(pipe):
         pipe.step(st)
     st.synchronize()
     assert st.kernel_launches() - before >= 3 * 10
+
+
+def test_particle_chunks(pipe):
+    """NexusState chunk management (src/state.rs:665-774): add / extend /
+    remove / remove_particles_from_chunk keep every particle's owner chunk and
+    record through the swap-removals, also after fast steps (reordered storage)."""
+    a = scenes.elastic_cube(n_side=6).particles
+    b = scenes.mixed_materials(n_side=5).particles
+    sc = scenes.elastic_cube(n_side=4)
+    st = MpmState(grid_size=4096, particles_capacity=64)
+    st.set_cell_width(sc.dx, 4096)
+    st.set_simulation_params(sc.gravity, sc.dt)
+    st.set_colliders(sc.colliders)
+    ca = st.add_chunk(a)
+    cb = st.add_chunk(b)
+    st.extend_chunk(ca, sc.particles)
+    assert st.chunk_len(ca) == a.n + sc.n and st.chunk_len(cb) == b.n
+    owner = st.chunk_of_particles()
+    assert (owner[:a.n] == ca).all() and (owner[a.n:a.n + b.n] == cb).all() and (owner[a.n + b.n:] == ca).all()
+    for _ in range(3):
+        pipe.step(st)
+    before = st.read_positions()
+    removed = st.remove_particles_from_chunk(cb, 40)
+    assert removed == 40 and st.chunk_len(cb) == b.n - 40
+    after = st.read_positions()
+    owner2 = st.chunk_of_particles()
+    assert (owner2 == cb).sum() == b.n - 40 and (owner2 == ca).sum() == a.n + sc.n
+    # every surviving record is one of the records before, at most once, with its owner
+    key = {tuple(p): o for p, o in zip(before.tolist(), owner.tolist())}
+    assert len(key) == len(before)
+    assert all(key[tuple(p)] == o for p, o in zip(after.tolist(), owner2.tolist()))
+    st.remove_chunk(ca)
+    assert len(st) == b.n - 40 and (st.chunk_of_particles() == cb).all()
+    with pytest.raises(NexusError):
+        st.chunk_len(ca)
+    pipe.step(st)
+    st.synchronize()
+    assert np.isfinite(st.read_positions()).all()
