@@ -295,6 +295,7 @@ def test_particle_chunks(pipe):
     a = scenes.elastic_cube(n_side=6).particles
     b = scenes.mixed_materials(n_side=5).particles
     sc = scenes.elastic_cube(n_side=4)
+    sc.particles.pos[:, 0] += np.float32(0.2)  # distinct from the n_side=6 cube's lattice (same seed)
     st = MpmState(grid_size=4096, particles_capacity=64)
     st.set_cell_width(sc.dx, 4096)
     st.set_simulation_params(sc.gravity, sc.dt)
