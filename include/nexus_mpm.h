@@ -298,6 +298,39 @@ NXM_API int nxm_sort_blocks_noalloc(const float* positions, uint32_t n, float ce
                                     int32_t* block_vids, uint32_t* block_ranges, uint32_t max_blocks,
                                     uint32_t* num_blocks, void* stream);
 
+/* ---- batched scenes ----------------------------------------------------------
+ * The batched form of the step: many independent scenes (same cell width,
+ * dt and gravity) advance together, each nxm_step being one launch sequence
+ * for all of them.  Scene s owns its own region of the block-key space (a
+ * cube of `scene_blocks` blocks per axis); its particles keep scene-local
+ * positions, so a scene steps exactly as it would alone, and its colliders
+ * act on its own grid nodes only.  No counterpart call in the reference,
+ * which steps one MpmState per pipeline call (src_mpm/pipeline.rs:385-526).
+ *
+ * Enable before adding any particle or collider (0 turns it off).  Particle
+ * blocks must stay within local block coordinates [1 - M, S - M - 3] with
+ * S = scene_blocks, M = S / 8 (a [0, 1]^3 scene fits S = 64 at dx = 1/128);
+ * nxm_scene_add refuses particles outside with NXM_E_INVALID. */
+NXM_API int nxm_state_enable_scenes(nxm_state* state, uint32_t scene_blocks);
+/* Scene slots available (0 when scenes are off). */
+NXM_API uint32_t nxm_scene_capacity(const nxm_state* state);
+/* Adds a scene: its particles (appended as one contiguous id range) and up to
+ * 16 colliders (triangles indexed within `tri_vertices`, as for
+ * nxm_state_set_colliders).  Returns NXM_E_CAPACITY when every slot is taken. */
+NXM_API int nxm_scene_add(nxm_state* state, const nxm_particle* particles, uint32_t count,
+                          const nxm_collider* colliders, uint32_t num_colliders, const float* tri_vertices,
+                          uint32_t num_triangles, uint32_t* scene);
+/* Removes scenes with their particles and colliders; the particle ids of the
+ * remaining scenes shift down, keeping their order. */
+NXM_API int nxm_scene_remove(nxm_state* state, const uint32_t* scenes, uint32_t count);
+/* The particle-id range [first, first + count) of a live scene. */
+NXM_API int nxm_scene_range(const nxm_state* state, uint32_t scene, uint32_t* first, uint32_t* count);
+/* Kinematic driving of collider `index` of a scene (as nxm_state_set_collider_velocity). */
+NXM_API int nxm_scene_set_collider_velocity(nxm_state* state, uint32_t scene, uint32_t index, const float linvel[3],
+                                            const float angvel[3]);
+/* Positions of particles [first, first + count) (3 floats each); synchronizes. */
+NXM_API int nxm_read_positions_range(nxm_state* state, uint32_t first, uint32_t count, float* out);
+
 /* ---- particle chunks (NexusState, src/state.rs:665-774) -------------------
  * A chunk is a handle on a set of particles appended together (and later
  * extended).  Removals swap-remove the chunk's slots (highest first) as

@@ -99,6 +99,34 @@ __device__ __forceinline__ uint32_t hash_key(uint32_t k) {
     return k;
 }
 
+// Batched scenes: block-key offset of a scene, and scene / offset of a block.
+__device__ __forceinline__ int floor_div(int a, int b) {
+    const int q = a / b;
+    return (a % b != 0 && (a < 0)) ? q - 1 : q;  // b > 0
+}
+__device__ __forceinline__ int3 scene_base_of(const Params& p, uint32_t sid) {
+    if (p.scene_blocks == 0) return make_int3(0, 0, 0);
+    const int S = (int)p.scene_blocks;
+    const int cx = (int)(sid % p.scene_cells[0]) + p.scene_cmin[0];
+    const int cy = (int)((sid / p.scene_cells[0]) % p.scene_cells[1]) + p.scene_cmin[1];
+    const int cz = (int)(sid / (p.scene_cells[0] * p.scene_cells[1])) + p.scene_cmin[2];
+    return make_int3(cx * S, cy * S, cz * S);
+}
+__device__ __forceinline__ int3 scene_base_of_block(const Params& p, int4 vid) {
+    if (p.scene_blocks == 0) return make_int3(0, 0, 0);
+    const int S = (int)p.scene_blocks, M = p.scene_margin;
+    return make_int3(floor_div(vid.x + M, S) * S, floor_div(vid.y + M, S) * S, floor_div(vid.z + M, S) * S);
+}
+// NONE for a block outside every scene cell (a particle that left its region).
+__device__ __forceinline__ uint32_t scene_of_block(const Params& p, int4 vid) {
+    const int S = (int)p.scene_blocks, M = p.scene_margin;
+    const uint32_t cx = (uint32_t)(floor_div(vid.x + M, S) - p.scene_cmin[0]);
+    const uint32_t cy = (uint32_t)(floor_div(vid.y + M, S) - p.scene_cmin[1]);
+    const uint32_t cz = (uint32_t)(floor_div(vid.z + M, S) - p.scene_cmin[2]);
+    if (cx >= p.scene_cells[0] || cy >= p.scene_cells[1] || cz >= p.scene_cells[2]) return NONE;
+    return cx + p.scene_cells[0] * (cy + p.scene_cells[1] * cz);
+}
+
 // assoc_cell = round(pt / dx) - 1, with an IEEE division as in the reference.
 __device__ __forceinline__ v3 assoc_cell_of(float dx, v3 pt) {
     return mk(roundf(__fdiv_rn(pt.x, dx)) - 1.0f, roundf(__fdiv_rn(pt.y, dx)) - 1.0f,

@@ -42,6 +42,10 @@ struct DevPtrs {
     float4* pstate_out;
     const uint32_t* pid_in;
     uint32_t* pid_out;
+    // batched scenes: scene of each particle id, and each scene's colliders
+    // [x, x + y) in `colliders`
+    const uint32_t* pscene;
+    const uint2* scene_cols;
 };
 
 constexpr uint32_t kScanTile = 1024;  // blocks per scan tile

@@ -126,7 +126,17 @@ struct alignas(16) Params {
     uint32_t hash_capacity;  // slots, power of two
     uint32_t sorted_capacity;
     uint32_t use_cpic;
+    // Batched scenes (scene_blocks != 0): scene s owns the block-key region of
+    // cell c(s) = (s mod cells[0], (s / cells[0]) mod cells[1], ...) + cmin, a
+    // cube of scene_blocks blocks per axis.  Its particles keep scene-local
+    // positions; a local block coordinate b in [-margin, scene_blocks - margin)
+    // has the key of b + c(s) * scene_blocks.
+    uint32_t scene_blocks;
+    int32_t scene_margin;
+    int32_t scene_cmin[3];
+    uint32_t scene_cells[3];
 };
+static_assert(sizeof(Params) == 80, "Params layout");
 
 // Device counters (reset each step by the sort).
 struct alignas(16) Counters {

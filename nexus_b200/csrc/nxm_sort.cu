@@ -141,7 +141,9 @@ __global__ void __launch_bounds__(256) k_touch_primary(DevPtrs P) {
             } else {
                 float4 xm = __ldg(reinterpret_cast<const float4*>(&P.kin[p]));
                 CellInfo ci = cell_info(dx, mk(xm.x, xm.y, xm.z));
-                key = pack_key(ci.bx, ci.by, ci.bz);
+                int3 o = make_int3(0, 0, 0);
+                if (P.params->scene_blocks) o = scene_base_of(*P.params, P.pscene[P.pid_in ? P.pid_in[p] : p]);
+                key = pack_key(ci.bx + o.x, ci.by + o.y, ci.bz + o.z);
                 P.pcode[p] = make_uint2(key, ci.ax | (ci.ay << 2) | (ci.az << 4));
             }
         }

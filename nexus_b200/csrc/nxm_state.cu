@@ -73,24 +73,151 @@ int model_state_words(uint32_t tag) {
     return 0;
 }
 
-// Packs selected 4-byte fields of per-particle records into a dense array.
-__global__ void k_pack_fields(const uint32_t* __restrict__ src, uint32_t stride_words, uint32_t n,
+// Packs selected 4-byte fields of the records of particles [first, first + n)
+// into a dense array.
+__global__ void k_pack_fields(const uint32_t* __restrict__ src, uint32_t stride_words, uint32_t first, uint32_t n,
                               const int* __restrict__ offsets, int nfields, uint32_t* __restrict__ dst) {
     const uint32_t total = n * (uint32_t)nfields;
     for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
-        const uint32_t p = t / (uint32_t)nfields, f = t % (uint32_t)nfields;
+        const uint32_t p = first + t / (uint32_t)nfields, f = t % (uint32_t)nfields;
         dst[t] = src[(size_t)p * stride_words + offsets[f]];
     }
 }
 
-// Permuted storage (slot p holds particle pid[p]): scatter the fields by id.
+// Permuted storage (slot p holds particle pid[p]): scatter the fields of the
+// particles with id in [first, first + count) by id (all n slots are scanned).
 __global__ void k_pack_fields_perm(const uint32_t* __restrict__ src, uint32_t stride_words, uint32_t n,
-                                   const int* __restrict__ offsets, int nfields, const uint32_t* __restrict__ pid,
-                                   uint32_t* __restrict__ dst) {
+                                   uint32_t first, uint32_t count, const int* __restrict__ offsets, int nfields,
+                                   const uint32_t* __restrict__ pid, uint32_t* __restrict__ dst) {
     const uint32_t total = n * (uint32_t)nfields;
     for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
         const uint32_t p = t / (uint32_t)nfields, f = t % (uint32_t)nfields;
-        dst[(size_t)pid[p] * nfields + f] = src[(size_t)p * stride_words + offsets[f]];
+        const uint32_t id = pid[p] - first;
+        if (id < count) dst[(size_t)id * nfields + f] = src[(size_t)p * stride_words + offsets[f]];
+    }
+}
+
+// ---- stable removal of particle-id ranges (compaction over storage slots) ----
+// `ranges` sorted and disjoint, `cum[i]` = total length of ranges before i.
+// Tiles of 1024 slots; 256 threads x 4 slots.
+__device__ __forceinline__ uint32_t range_of(uint32_t id, const uint2* __restrict__ ranges, uint32_t nr) {
+    uint32_t lo = 0, hi = nr;  // first range with start > id
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (ranges[mid].x <= id) lo = mid + 1; else hi = mid;
+    }
+    return lo;  // ranges[lo - 1] is the last one starting at or before id
+}
+__device__ __forceinline__ bool removed_id(uint32_t id, const uint2* __restrict__ ranges, uint32_t nr) {
+    const uint32_t r = range_of(id, ranges, nr);
+    return r > 0 && id < ranges[r - 1].y;
+}
+__device__ __forceinline__ uint32_t new_id_of(uint32_t id, const uint2* __restrict__ ranges,
+                                              const uint32_t* __restrict__ cum, uint32_t nr) {
+    const uint32_t r = range_of(id, ranges, nr);
+    return r == 0 ? id : id - cum[r - 1] - (ranges[r - 1].y - ranges[r - 1].x);  // id is past range r - 1
+}
+__device__ __forceinline__ uint32_t survivors4(uint32_t base, uint32_t n, const uint32_t* __restrict__ pid,
+                                              const uint2* __restrict__ ranges, uint32_t nr, bool keep[4]) {
+    uint32_t c = 0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const uint32_t p = base + k;
+        keep[k] = p < n && !removed_id(pid ? pid[p] : p, ranges, nr);
+        c += keep[k] ? 1u : 0u;
+    }
+    return c;
+}
+__device__ __forceinline__ uint32_t block_excl_scan256(uint32_t v, uint32_t* sh, uint32_t* total) {
+    const uint32_t lane = threadIdx.x & 31u, w = threadIdx.x >> 5;
+    uint32_t incl = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+        if (lane >= (uint32_t)o) incl += y;
+    }
+    if (lane == 31) sh[w] = incl;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t run = 0;
+        for (int i = 0; i < 8; ++i) {
+            const uint32_t t = sh[i];
+            sh[i] = run;
+            run += t;
+        }
+        sh[8] = run;
+    }
+    __syncthreads();
+    const uint32_t out = sh[w] + incl - v;
+    *total = sh[8];
+    __syncthreads();
+    return out;
+}
+__global__ void __launch_bounds__(256) k_rm_count(uint32_t n, const uint32_t* __restrict__ pid,
+                                                  const uint2* __restrict__ ranges, uint32_t nr,
+                                                  uint32_t* __restrict__ tiles) {
+    __shared__ uint32_t sh[9];
+    bool keep[4];
+    const uint32_t c = survivors4(blockIdx.x * 1024u + threadIdx.x * 4u, n, pid, ranges, nr, keep);
+    uint32_t total;
+    block_excl_scan256(c, sh, &total);
+    if (threadIdx.x == 0) tiles[blockIdx.x] = total;
+}
+__global__ void __launch_bounds__(1024) k_rm_scan(uint32_t* __restrict__ tiles, uint32_t ntiles) {
+    __shared__ uint32_t carry;
+    __shared__ uint32_t wsum[32];
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    for (uint32_t base = 0; base < ntiles; base += 1024u) {
+        const uint32_t i = base + threadIdx.x;
+        const uint32_t v = i < ntiles ? tiles[i] : 0u;
+        const uint32_t lane = threadIdx.x & 31u, w = threadIdx.x >> 5;
+        uint32_t incl = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+            if (lane >= (uint32_t)o) incl += y;
+        }
+        if (lane == 31) wsum[w] = incl;
+        __syncthreads();
+        if (w == 0) {
+            const uint32_t s = wsum[lane];
+            uint32_t si = s;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, si, o);
+                if (lane >= (uint32_t)o) si += y;
+            }
+            wsum[lane] = si - s;
+        }
+        __syncthreads();
+        if (i < ntiles) tiles[i] = carry + wsum[w] + incl - v;
+        __syncthreads();
+        if (threadIdx.x == 1023) carry += wsum[31] + incl;
+        __syncthreads();
+    }
+}
+__global__ void __launch_bounds__(256) k_rm_move(uint32_t n, const PKin* __restrict__ kin, const PDef* __restrict__ def,
+                                                 const float4* __restrict__ pstate, const uint32_t* __restrict__ pid,
+                                                 const uint2* __restrict__ ranges, const uint32_t* __restrict__ cum,
+                                                 uint32_t nr, const uint32_t* __restrict__ tiles,
+                                                 PKin* __restrict__ kin_to, PDef* __restrict__ def_to,
+                                                 float4* __restrict__ pstate_to, uint32_t* __restrict__ pid_to) {
+    __shared__ uint32_t sh[9];
+    bool keep[4];
+    const uint32_t base = blockIdx.x * 1024u + threadIdx.x * 4u;
+    const uint32_t c = survivors4(base, n, pid, ranges, nr, keep);
+    uint32_t total;
+    uint32_t dst = tiles[blockIdx.x] + block_excl_scan256(c, sh, &total);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        if (!keep[k]) continue;
+        const uint32_t p = base + k;
+        kin_to[dst] = kin[p];
+        def_to[dst] = def[p];
+        pstate_to[dst] = pstate[p];
+        if (pid) pid_to[dst] = new_id_of(pid[p], ranges, cum, nr);
+        ++dst;
     }
 }
 
@@ -190,6 +317,25 @@ struct nxm_state {
     // colliders
     std::vector<DevCollider> colliders;
     DevCollider* d_colliders = nullptr;
+    uint32_t col_cap = 0;
+
+    // batched scenes (scene_blocks != 0): scene slots on the block-key grid
+    // (see Params), each a contiguous range of particle ids with its own colliders
+    struct Scene {
+        bool live = false;
+        uint32_t first = 0, count = 0;
+        std::vector<nxm_collider> cols;
+        std::vector<float> tri;
+    };
+    uint32_t scene_blocks = 0;
+    int scene_margin = 0;
+    int scene_cmin[3] = {0, 0, 0};
+    uint32_t scene_cells[3] = {0, 0, 0};
+    std::vector<Scene> scenes;
+    std::vector<uint32_t> pscene;       // scene of each particle id
+    uint32_t* d_pscene = nullptr;
+    uint2* d_scene_cols = nullptr;      // per scene slot: its colliders in the table
+    uint32_t* d_tiles = nullptr;        // compaction scratch, one word per 1024 particles
     DevTri* d_tris = nullptr;       // triangles of every trimesh collider (one copy per collider)
     DevBvhNode* d_bvh = nullptr;    // their BVHs
 
@@ -235,6 +381,8 @@ DevPtrs dev_ptrs(nxm_state* s) {
     }
     P.materials = s->d_materials;
     P.colliders = s->d_colliders;
+    P.pscene = s->d_pscene;
+    P.scene_cols = s->d_scene_cols;
     P.tris = s->d_tris;
     P.bvh = s->d_bvh;
     P.params = s->d_params;
@@ -340,7 +488,8 @@ struct ParticleBuffers {
     PKin *kin = nullptr, *kin_alt = nullptr;
     PDef *def = nullptr, *def_alt = nullptr;
     float4 *pstate = nullptr, *pstate_alt = nullptr;
-    uint32_t *pid = nullptr, *pid_alt = nullptr, *phdr = nullptr, *sorted = nullptr;
+    uint32_t *pid = nullptr, *pid_alt = nullptr, *phdr = nullptr, *sorted = nullptr, *pscene = nullptr,
+             *tiles = nullptr;
     uint2* pcode = nullptr;
     cudaError_t alloc(uint32_t cap) {
         cudaError_t e = cudaSuccess;
@@ -351,18 +500,21 @@ struct ParticleBuffers {
         a(&kin_alt, cap); a(&def_alt, cap); a(&pstate_alt, cap);
         a(&pid, cap); a(&pid_alt, cap); a(&pcode, cap); a(&phdr, cap);
         a(&sorted, (size_t)cap * 8);
+        a(&pscene, cap);
+        a(&tiles, cap / 1024 + 2);
         return e;
     }
     void release() { *this = ParticleBuffers{}; }
     ~ParticleBuffers() {
         dfree(kin); dfree(def); dfree(pstate); dfree(kin_alt); dfree(def_alt); dfree(pstate_alt);
-        dfree(pid); dfree(pid_alt); dfree(pcode); dfree(phdr); dfree(sorted);
+        dfree(pid); dfree(pid_alt); dfree(pcode); dfree(phdr); dfree(sorted); dfree(pscene); dfree(tiles);
     }
 };
 
 void free_particles(nxm_state* s) {
     dfree(s->kin); dfree(s->def); dfree(s->pstate); dfree(s->kin_alt); dfree(s->def_alt); dfree(s->pstate_alt);
     dfree(s->pid); dfree(s->pid_alt); dfree(s->pcode); dfree(s->phdr); dfree(s->sorted);
+    dfree(s->d_pscene); dfree(s->d_tiles);
 }
 
 int reserve_particles(nxm_state* s, uint32_t need) {
@@ -383,7 +535,9 @@ int reserve_particles(nxm_state* s, uint32_t need) {
     s->kin_alt = t.kin_alt; s->def_alt = t.def_alt; s->pstate_alt = t.pstate_alt;
     s->pid = t.pid; s->pid_alt = t.pid_alt;
     s->pcode = t.pcode; s->phdr = t.phdr; s->sorted = t.sorted;
+    s->d_pscene = t.pscene; s->d_tiles = t.tiles;
     t.release();
+    if (s->n) NXM_TRY(cudaMemcpy(s->d_pscene, s->pscene.data(), 4 * (size_t)s->n, cudaMemcpyHostToDevice));
     s->sort_pid = nullptr;
     s->pcap = cap;
     invalidate_graph(s);
@@ -453,6 +607,12 @@ int sync_params(nxm_state* s) {
     p.hash_capacity = s->hash_cap;
     p.sorted_capacity = s->pcap * 8u;
     p.use_cpic = s->use_cpic ? 1u : 0u;
+    p.scene_blocks = s->scene_blocks;
+    p.scene_margin = s->scene_margin;
+    for (int k = 0; k < 3; ++k) {
+        p.scene_cmin[k] = s->scene_cmin[k];
+        p.scene_cells[k] = s->scene_cells[k];
+    }
     NXM_TRY(cudaMemcpyAsync(s->d_params, &p, sizeof(Params), cudaMemcpyHostToDevice, s->stream));
     NXM_TRY(cudaStreamSynchronize(s->stream));
     s->params_dirty = false;
@@ -539,10 +699,13 @@ void finish_step(nxm_state* s) {
     }
 }
 
-int pack_read(nxm_state* s, const void* records, uint32_t stride_bytes, const int* offsets, int nfields, void* out) {
+// Fields of particles [first, first + count) (ids), in id order, into `out`.
+int pack_read_range(nxm_state* s, const void* records, uint32_t stride_bytes, const int* offsets, int nfields,
+                    uint32_t first, uint32_t count, void* out) {
     if (!out) return NXM_E_INVALID;
-    if (s->n == 0) return NXM_OK;
-    const size_t words = (size_t)s->n * nfields;
+    if (first > s->n || count > s->n - first) return NXM_E_INVALID;
+    if (count == 0) return NXM_OK;
+    const size_t words = (size_t)count * nfields;
     if (words > s->pack_cap) {
         dfree(s->d_pack);
         NXM_TRY(dalloc(&s->d_pack, words));
@@ -550,19 +713,92 @@ int pack_read(nxm_state* s, const void* records, uint32_t stride_bytes, const in
     }
     if (!s->d_offsets) NXM_TRY(dalloc(&s->d_offsets, 32));
     NXM_TRY(cudaMemcpyAsync(s->d_offsets, offsets, sizeof(int) * nfields, cudaMemcpyHostToDevice, s->stream));
-    int grid = std::min<int>((int)((words + 255) / 256), s->sm_count * 8);
+    const size_t threads = (s->permuted ? (size_t)s->n : (size_t)count) * nfields;
+    int grid = (int)std::min<size_t>((threads + 255) / 256, (size_t)s->sm_count * 8);
     if (grid < 1) grid = 1;
     if (s->permuted)
         k_pack_fields_perm<<<grid, 256, 0, s->stream>>>(reinterpret_cast<const uint32_t*>(records), stride_bytes / 4,
-                                                          s->n, s->d_offsets, nfields, s->pid, s->d_pack);
+                                                          s->n, first, count, s->d_offsets, nfields, s->pid,
+                                                          s->d_pack);
     else
-        k_pack_fields<<<grid, 256, 0, s->stream>>>(reinterpret_cast<const uint32_t*>(records), stride_bytes / 4, s->n,
-                                                     s->d_offsets, nfields, s->d_pack);
+        k_pack_fields<<<grid, 256, 0, s->stream>>>(reinterpret_cast<const uint32_t*>(records), stride_bytes / 4, first,
+                                                     count, s->d_offsets, nfields, s->d_pack);
     s->launches += 1;
     NXM_TRY(cudaGetLastError());
     NXM_TRY(cudaMemcpyAsync(out, s->d_pack, words * 4, cudaMemcpyDeviceToHost, s->stream));
     NXM_TRY(cudaStreamSynchronize(s->stream));
     return NXM_OK;
+}
+
+int pack_read(nxm_state* s, const void* records, uint32_t stride_bytes, const int* offsets, int nfields, void* out) {
+    if (!out) return NXM_E_INVALID;
+    return pack_read_range(s, records, stride_bytes, offsets, nfields, 0, s->n, out);
+}
+
+// Removes the particles whose ids fall in `ranges` (sorted, disjoint), keeping
+// the others in their relative order (ids shift down), on canonical or
+// block-ordered storage alike: one compaction pass over the storage slots into
+// the other buffers, which then become current.  Host mirrors follow.
+int remove_id_ranges(nxm_state* s, std::vector<uint2> ranges) {
+    std::sort(ranges.begin(), ranges.end(), [](uint2 a, uint2 b) { return a.x < b.x; });
+    std::vector<uint2> rr;
+    for (uint2 r : ranges) {
+        r.y = std::min(r.y, s->n);
+        if (r.x >= r.y) continue;
+        if (!rr.empty() && r.x < rr.back().y) return NXM_E_INVALID;  // overlapping ranges
+        rr.push_back(r);
+    }
+    if (rr.empty()) return NXM_OK;
+    std::vector<uint32_t> cum(rr.size());
+    uint32_t removed = 0;
+    for (size_t i = 0; i < rr.size(); ++i) {
+        cum[i] = removed;
+        removed += rr[i].y - rr[i].x;
+    }
+    const uint32_t n0 = s->n, ntiles = (n0 + 1023u) / 1024u;
+    uint2* d_r = nullptr;
+    uint32_t* d_cum = nullptr;
+    cudaError_t e = dalloc(&d_r, rr.size());
+    if (e == cudaSuccess) e = dalloc(&d_cum, cum.size());
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_r, rr.data(), sizeof(uint2) * rr.size(), cudaMemcpyHostToDevice, s->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_cum, cum.data(), 4 * cum.size(), cudaMemcpyHostToDevice, s->stream);
+    const uint32_t* pid = s->permuted ? s->pid : nullptr;
+    const uint32_t nr = (uint32_t)rr.size();
+    if (e == cudaSuccess) {
+        k_rm_count<<<ntiles, 256, 0, s->stream>>>(n0, pid, d_r, nr, s->d_tiles);
+        k_rm_scan<<<1, 1024, 0, s->stream>>>(s->d_tiles, ntiles);
+        k_rm_move<<<ntiles, 256, 0, s->stream>>>(n0, s->kin, s->def, s->pstate, pid, d_r, d_cum, nr, s->d_tiles,
+                                                 s->kin_alt, s->def_alt, s->pstate_alt, s->pid_alt);
+        s->launches += 3;
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+    if (d_r) cudaFree(d_r);
+    if (d_cum) cudaFree(d_cum);
+    NXM_TRY(e);
+    swap_buffers(s);  // the compacted records (and, when permuted, their ids) are current
+    for (size_t i = rr.size(); i-- > 0;) {
+        auto erase = [&](auto& v) { v.erase(v.begin() + rr[i].x, v.begin() + rr[i].y); };
+        erase(s->init_radius);
+        erase(s->phase);
+        erase(s->boundary_friction);
+        erase(s->group_id);
+        erase(s->slot2chunk);
+        erase(s->pscene);
+    }
+    s->n = n0 - removed;
+    if (s->n) NXM_TRY(cudaMemcpy(s->d_pscene, s->pscene.data(), 4 * (size_t)s->n, cudaMemcpyHostToDevice));
+    for (auto& c : s->chunks) {  // recount chunk sizes
+        c.second = 0;
+    }
+    for (uint32_t o : s->slot2chunk)
+        if (o != NONE) {
+            auto it = s->chunks.find(o);
+            if (it != s->chunks.end()) ++it->second;
+        }
+    s->sort_pid = nullptr;
+    s->params_dirty = true;
+    return invalidate_codes(s);
 }
 
 int upload_particles(nxm_state* s, const nxm_particles_soa* p, uint32_t count) {
@@ -613,6 +849,7 @@ int upload_particles(nxm_state* s, const nxm_particles_soa* p, uint32_t count) {
         s->boundary_friction.push_back(p->boundary_friction ? p->boundary_friction[i] : 1.f);
         s->group_id.push_back(p->group_id ? p->group_id[i] : 0u);
         s->slot2chunk.push_back(NONE);
+        s->pscene.push_back(0u);
     }
     rc = sync_materials(s);
     if (rc) return rc;
@@ -757,6 +994,75 @@ void trimesh_bvh(const std::vector<DevTri>& tris, uint32_t base, uint32_t count,
     nodes.insert(nodes.end(), local.begin(), local.end());
 }
 
+// Device form of one nxm_collider (triangle indices shifted by `tri_offset`).
+int collider_from_abi(const nxm_collider& c, const float* tri, uint32_t ntri, uint32_t tri_offset, DevCollider& d) {
+    std::memset(&d, 0, sizeof(d));
+    std::memcpy(d.a, c.shape_a, 16);
+    std::memcpy(d.b, c.shape_b, 16);
+    std::memcpy(d.c, c.shape_c, 16);
+    std::memcpy(d.rot, c.rotation, 16);
+    std::memcpy(d.tra, c.translation, 12);
+    std::memcpy(d.linvel, c.linvel, 12);
+    std::memcpy(d.angvel, c.angvel, 12);
+    std::memcpy(d.local_com, c.local_com, 12);
+    d.type = f_bits(c.shape_a[3]);
+    d.bc_type = c.bc_type;
+    d.bc_friction = c.bc_friction;
+    d.tri_first = c.tri_first + tri_offset;
+    d.tri_count = c.tri_count;
+    if (d.type != SHAPE_BALL && d.type != SHAPE_CUBOID && d.type != SHAPE_CAPSULE && d.type != SHAPE_TRIMESH)
+        return NXM_E_UNSUPPORTED;
+    if (d.type == SHAPE_TRIMESH && (!tri || c.tri_count == 0 || c.tri_first > ntri || c.tri_count > ntri - c.tri_first))
+        return NXM_E_INVALID;
+    return NXM_OK;
+}
+
+// Uploads the collider table (every trimesh gets its own triangle records and
+// BVH, built from `tri`), growing the device table when needed.
+int install_colliders(nxm_state* s, std::vector<DevCollider> dc, const float* tri) {
+    std::vector<DevTri> tris;
+    std::vector<DevBvhNode> bvh;
+    for (DevCollider& d : dc) {
+        if (d.type != SHAPE_TRIMESH) continue;
+        const uint32_t base = (uint32_t)tris.size();
+        trimesh_records(tri, d.tri_first, d.tri_count, tris);
+        d.bvh_first = (uint32_t)bvh.size();
+        trimesh_bvh(tris, base, d.tri_count, d.bvh_first, bvh);
+        d.bvh_count = (uint32_t)bvh.size() - d.bvh_first;
+    }
+    NXM_TRY(cudaStreamSynchronize(s->stream));
+    bool realloc_graph = false;
+    if (dc.size() > s->col_cap) {
+        const uint32_t cap = std::max<uint32_t>((uint32_t)dc.size(), 2 * s->col_cap);
+        DevCollider* d = nullptr;
+        NXM_TRY(dalloc(&d, cap));
+        dfree(s->d_colliders);
+        s->d_colliders = d;
+        s->col_cap = cap;
+        realloc_graph = true;
+    }
+    if (!dc.empty())
+        NXM_TRY(cudaMemcpyAsync(s->d_colliders, dc.data(), sizeof(DevCollider) * dc.size(), cudaMemcpyHostToDevice,
+                                s->stream));
+    const bool had_mesh = s->d_tris != nullptr;
+    dfree(s->d_tris);
+    dfree(s->d_bvh);
+    if (!tris.empty()) {
+        NXM_TRY(dalloc(&s->d_tris, tris.size()));
+        NXM_TRY(dalloc(&s->d_bvh, bvh.size()));
+        NXM_TRY(cudaMemcpyAsync(s->d_tris, tris.data(), sizeof(DevTri) * tris.size(), cudaMemcpyHostToDevice,
+                                s->stream));
+        NXM_TRY(cudaMemcpyAsync(s->d_bvh, bvh.data(), sizeof(DevBvhNode) * bvh.size(), cudaMemcpyHostToDevice,
+                                s->stream));
+    }
+    NXM_TRY(cudaStreamSynchronize(s->stream));
+    const bool had = !s->colliders.empty();
+    s->colliders = dc;
+    if (realloc_graph || had != !s->colliders.empty() || had_mesh || !tris.empty()) invalidate_graph(s);
+    s->params_dirty = true;
+    return NXM_OK;
+}
+
 bool device_ok(int* dev, int* sms) {
     int count = 0;
     if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
@@ -826,6 +1132,7 @@ int nxm_state_create(const nxm_capacities* caps, nxm_state** out) {
     if (!rc && dalloc(&s->d_counters, 1) != cudaSuccess) rc = NXM_E_OOM;
     if (!rc && cudaMallocHost(reinterpret_cast<void**>(&s->h_counters), sizeof(Counters)) != cudaSuccess) rc = NXM_E_OOM;
     if (!rc && dalloc(&s->d_colliders, MAX_COLLIDERS) != cudaSuccess) rc = NXM_E_OOM;
+    s->col_cap = MAX_COLLIDERS;
     if (!rc && cudaMemsetAsync(s->d_counters, 0, sizeof(Counters), s->stream) != cudaSuccess) rc = NXM_E_CUDA;
     if (!rc) rc = alloc_grid(s, c.grid_size);
     if (!rc) rc = reserve_particles(s, std::max<uint32_t>(c.particles_capacity, 1));
@@ -845,7 +1152,7 @@ void nxm_state_destroy(nxm_state* s) {
     invalidate_graph(s);
     free_grid(s);
     free_particles(s);
-    dfree(s->d_materials); dfree(s->d_colliders); dfree(s->d_tris); dfree(s->d_bvh); dfree(s->d_params); dfree(s->d_counters);
+    dfree(s->d_materials); dfree(s->d_colliders); dfree(s->d_tris); dfree(s->d_bvh); dfree(s->d_scene_cols); dfree(s->d_params); dfree(s->d_counters);
     dfree(s->d_pack); dfree(s->d_offsets);
     if (s->h_counters) cudaFreeHost(s->h_counters);
     if (s->stream) cudaStreamDestroy(s->stream);
@@ -881,64 +1188,15 @@ int nxm_state_set_cell_width(nxm_state* s, float cell_width, uint32_t grid_capac
 
 int nxm_state_set_colliders(nxm_state* s, const nxm_collider* cols, uint32_t ncol, const float* tri, uint32_t ntri) {
     if (!s) return NXM_E_INVALID;
+    if (s->scene_blocks) return NXM_E_INVALID;  // batched scenes bring their own colliders
     if (ncol > (uint32_t)MAX_COLLIDERS) return NXM_E_INVALID;
     if (ncol && !cols) return NXM_E_INVALID;
     std::vector<DevCollider> dc(ncol);
     for (uint32_t i = 0; i < ncol; ++i) {
-        const nxm_collider& c = cols[i];
-        DevCollider& d = dc[i];
-        std::memset(&d, 0, sizeof(d));
-        std::memcpy(d.a, c.shape_a, 16);
-        std::memcpy(d.b, c.shape_b, 16);
-        std::memcpy(d.c, c.shape_c, 16);
-        std::memcpy(d.rot, c.rotation, 16);
-        std::memcpy(d.tra, c.translation, 12);
-        std::memcpy(d.linvel, c.linvel, 12);
-        std::memcpy(d.angvel, c.angvel, 12);
-        std::memcpy(d.local_com, c.local_com, 12);
-        d.type = f_bits(c.shape_a[3]);
-        d.bc_type = c.bc_type;
-        d.bc_friction = c.bc_friction;
-        d.tri_first = c.tri_first;
-        d.tri_count = c.tri_count;
-        if (d.type != SHAPE_BALL && d.type != SHAPE_CUBOID && d.type != SHAPE_CAPSULE && d.type != SHAPE_TRIMESH)
-            return NXM_E_UNSUPPORTED;
-        if (d.type == SHAPE_TRIMESH &&
-            (!tri || c.tri_count == 0 || c.tri_first > ntri || c.tri_count > ntri - c.tri_first))
-            return NXM_E_INVALID;
+        int rc = collider_from_abi(cols[i], tri, ntri, 0, dc[i]);
+        if (rc) return rc;
     }
-    // every trimesh gets its own triangle records and BVH
-    std::vector<DevTri> tris;
-    std::vector<DevBvhNode> bvh;
-    for (DevCollider& d : dc) {
-        if (d.type != SHAPE_TRIMESH) continue;
-        const uint32_t base = (uint32_t)tris.size();
-        trimesh_records(tri, d.tri_first, d.tri_count, tris);
-        d.bvh_first = (uint32_t)bvh.size();
-        trimesh_bvh(tris, base, d.tri_count, d.bvh_first, bvh);
-        d.bvh_count = (uint32_t)bvh.size() - d.bvh_first;
-    }
-    NXM_TRY(cudaStreamSynchronize(s->stream));
-    if (ncol)
-        NXM_TRY(cudaMemcpyAsync(s->d_colliders, dc.data(), sizeof(DevCollider) * ncol, cudaMemcpyHostToDevice,
-                                s->stream));
-    const bool had_mesh = s->d_tris != nullptr;
-    dfree(s->d_tris);
-    dfree(s->d_bvh);
-    if (!tris.empty()) {
-        NXM_TRY(dalloc(&s->d_tris, tris.size()));
-        NXM_TRY(dalloc(&s->d_bvh, bvh.size()));
-        NXM_TRY(cudaMemcpyAsync(s->d_tris, tris.data(), sizeof(DevTri) * tris.size(), cudaMemcpyHostToDevice,
-                                s->stream));
-        NXM_TRY(cudaMemcpyAsync(s->d_bvh, bvh.data(), sizeof(DevBvhNode) * bvh.size(), cudaMemcpyHostToDevice,
-                                s->stream));
-    }
-    NXM_TRY(cudaStreamSynchronize(s->stream));
-    const bool had = !s->colliders.empty();
-    s->colliders = dc;
-    if (had != !s->colliders.empty() || had_mesh || !tris.empty()) invalidate_graph(s);
-    s->params_dirty = true;
-    return NXM_OK;
+    return install_colliders(s, dc, tri);
 }
 
 int nxm_state_set_collider_velocity(nxm_state* s, uint32_t index, const float linvel[3], const float angvel[3]) {
@@ -1007,6 +1265,147 @@ int nxm_particles_append(nxm_state* s, const nxm_particle* particles, uint32_t c
 }
 
 uint32_t nxm_particles_len(const nxm_state* s) { return s ? s->n : 0u; }
+
+// ---- batched scenes ------------------------------------------------------------
+
+static int floor_div_i(int a, int b) { return a >= 0 ? a / b : -((-a + b - 1) / b); }
+
+int nxm_state_enable_scenes(nxm_state* s, uint32_t scene_blocks) {
+    if (!s || s->n != 0 || !s->colliders.empty()) return NXM_E_INVALID;
+    if (scene_blocks != 0 && (scene_blocks < 8 || scene_blocks > 512)) return NXM_E_INVALID;
+    dfree(s->d_scene_cols);
+    s->scenes.clear();
+    s->scene_blocks = scene_blocks;
+    if (scene_blocks) {
+        const int S = (int)scene_blocks, M = S / 8;
+        s->scene_margin = M;
+        // cells whose key region [c S - M, c S + S - M) lies inside the packed-key range
+        const int lo[3] = {-1023, -511, -1023}, hi[3] = {1024, 512, 1024};
+        size_t total = 1;
+        for (int k = 0; k < 3; ++k) {
+            const int cmin = -floor_div_i(-(lo[k] + M), S);  // ceil((lo + M) / S)
+            const int cmax = floor_div_i(hi[k] + 1 + M - S, S);
+            s->scene_cmin[k] = cmin;
+            s->scene_cells[k] = (uint32_t)std::max(0, cmax - cmin + 1);
+            total *= s->scene_cells[k];
+        }
+        s->scenes.assign(total, nxm_state::Scene{});
+        NXM_TRY(dalloc(&s->d_scene_cols, total));
+        NXM_TRY(cudaMemset(s->d_scene_cols, 0, sizeof(uint2) * total));
+    }
+    invalidate_graph(s);
+    s->params_dirty = true;
+    return NXM_OK;
+}
+
+uint32_t nxm_scene_capacity(const nxm_state* s) { return s ? (uint32_t)s->scenes.size() : 0u; }
+
+// Collider table of the live scenes, in scene-slot order, and each slot's range.
+static int rebuild_scene_colliders(nxm_state* s) {
+    std::vector<DevCollider> dc;
+    std::vector<float> tri;
+    std::vector<uint2> ranges(s->scenes.size(), make_uint2(0u, 0u));
+    for (size_t i = 0; i < s->scenes.size(); ++i) {
+        const nxm_state::Scene& sc = s->scenes[i];
+        if (!sc.live) continue;
+        const uint32_t toff = (uint32_t)(tri.size() / 9);
+        ranges[i] = make_uint2((uint32_t)dc.size(), (uint32_t)sc.cols.size());
+        for (const nxm_collider& c : sc.cols) {
+            DevCollider d;
+            int rc = collider_from_abi(c, sc.tri.data(), (uint32_t)(sc.tri.size() / 9), toff, d);
+            if (rc) return rc;
+            dc.push_back(d);
+        }
+        tri.insert(tri.end(), sc.tri.begin(), sc.tri.end());
+    }
+    NXM_TRY(cudaMemcpyAsync(s->d_scene_cols, ranges.data(), sizeof(uint2) * ranges.size(), cudaMemcpyHostToDevice,
+                            s->stream));
+    return install_colliders(s, dc, tri.data());
+}
+
+int nxm_scene_add(nxm_state* s, const nxm_particle* particles, uint32_t count, const nxm_collider* colliders,
+                  uint32_t num_colliders, const float* tri_vertices, uint32_t num_triangles, uint32_t* scene) {
+    if (!s || !scene || !s->scene_blocks || (count && !particles)) return NXM_E_INVALID;
+    if (num_colliders > (uint32_t)MAX_COLLIDERS || (num_colliders && !colliders)) return NXM_E_INVALID;
+    for (uint32_t i = 0; i < num_colliders; ++i) {
+        DevCollider d;
+        int rc = collider_from_abi(colliders[i], tri_vertices, num_triangles, 0, d);
+        if (rc) return rc;
+    }
+    // every particle's block (and its +1 neighbours) must stay inside the scene's key region
+    const float bw = 4.0f * s->dx;
+    const int M = s->scene_margin, S = (int)s->scene_blocks;
+    for (uint32_t i = 0; i < count; ++i)
+        for (int k = 0; k < 3; ++k) {
+            const float b = std::floor(particles[i].position[k] / bw);
+            if (!(b >= (float)(1 - M) && b <= (float)(S - M - 3))) return NXM_E_INVALID;
+        }
+    uint32_t slot = 0;
+    while (slot < s->scenes.size() && s->scenes[slot].live) ++slot;
+    if (slot == s->scenes.size()) return NXM_E_CAPACITY;
+    const uint32_t first = s->n;
+    int rc = nxm_particles_append(s, particles, count);
+    if (rc) return rc;
+    std::fill(s->pscene.begin() + first, s->pscene.end(), slot);
+    if (count)
+        NXM_TRY(cudaMemcpy(s->d_pscene + first, s->pscene.data() + first, 4 * (size_t)count, cudaMemcpyHostToDevice));
+    nxm_state::Scene& sc = s->scenes[slot];
+    sc.live = true;
+    sc.first = first;
+    sc.count = count;
+    sc.cols.assign(colliders, colliders + num_colliders);
+    sc.tri.assign(tri_vertices ? tri_vertices : nullptr,
+                  tri_vertices ? tri_vertices + 9 * (size_t)num_triangles : nullptr);
+    rc = rebuild_scene_colliders(s);
+    if (rc) return rc;
+    *scene = slot;
+    return NXM_OK;
+}
+
+int nxm_scene_remove(nxm_state* s, const uint32_t* scenes, uint32_t count) {
+    if (!s || (count && !scenes) || !s->scene_blocks) return NXM_E_INVALID;
+    std::vector<uint2> ranges;
+    std::vector<uint32_t> ids(scenes, scenes + count);
+    std::sort(ids.begin(), ids.end());
+    ids.erase(std::unique(ids.begin(), ids.end()), ids.end());
+    for (uint32_t id : ids)
+        if (id >= s->scenes.size() || !s->scenes[id].live) return NXM_E_INVALID;
+    for (uint32_t id : ids) ranges.push_back(make_uint2(s->scenes[id].first, s->scenes[id].first + s->scenes[id].count));
+    int rc = remove_id_ranges(s, ranges);
+    if (rc) return rc;
+    for (uint32_t id : ids) s->scenes[id] = nxm_state::Scene{};
+    for (nxm_state::Scene& sc : s->scenes) {  // ids after a removed range shift down by its length
+        if (!sc.live) continue;
+        uint32_t shift = 0;
+        for (uint2 r : ranges)
+            if (r.x < sc.first) shift += r.y - r.x;
+        sc.first -= shift;
+    }
+    return rebuild_scene_colliders(s);
+}
+
+int nxm_scene_range(const nxm_state* s, uint32_t scene, uint32_t* first, uint32_t* count) {
+    if (!s || !first || !count || scene >= s->scenes.size() || !s->scenes[scene].live) return NXM_E_INVALID;
+    *first = s->scenes[scene].first;
+    *count = s->scenes[scene].count;
+    return NXM_OK;
+}
+
+int nxm_scene_set_collider_velocity(nxm_state* s, uint32_t scene, uint32_t index, const float linvel[3],
+                                    const float angvel[3]) {
+    if (!s || scene >= s->scenes.size() || !s->scenes[scene].live || index >= s->scenes[scene].cols.size())
+        return NXM_E_INVALID;
+    uint32_t global = 0;
+    for (uint32_t i = 0; i < scene; ++i)
+        if (s->scenes[i].live) global += (uint32_t)s->scenes[i].cols.size();
+    return nxm_state_set_collider_velocity(s, global + index, linvel, angvel);
+}
+
+int nxm_read_positions_range(nxm_state* s, uint32_t first, uint32_t count, float* out) {
+    if (!s) return NXM_E_INVALID;
+    static const int off[3] = {0, 1, 2};
+    return pack_read_range(s, s->kin, sizeof(PKin), off, 3, first, count, out);
+}
 
 // ---- particle chunks (NexusState, src/state.rs:665-774) ---------------------
 
@@ -1159,35 +1558,8 @@ int nxm_particles_swap_remove(nxm_state* s, const uint32_t* slots, uint32_t coun
 
 int nxm_particles_shift_remove(nxm_state* s, uint32_t start, uint32_t end) {
     if (!s || start > end || end > s->n) return NXM_E_INVALID;
-    const uint32_t removed = end - start;
-    if (removed == 0) return NXM_OK;
-    int rc = canonicalize(s);
-    if (rc) return rc;
-    s->sort_pid = nullptr;
-    const uint32_t tail = s->n - end;
-    if (tail) {
-        PKin* tk; PDef* td; float4* ts;
-        NXM_TRY(dalloc(&tk, tail));
-        NXM_TRY(dalloc(&td, tail));
-        NXM_TRY(dalloc(&ts, tail));
-        NXM_TRY(cudaMemcpyAsync(tk, s->kin + end, sizeof(PKin) * tail, cudaMemcpyDeviceToDevice, s->stream));
-        NXM_TRY(cudaMemcpyAsync(td, s->def + end, sizeof(PDef) * tail, cudaMemcpyDeviceToDevice, s->stream));
-        NXM_TRY(cudaMemcpyAsync(ts, s->pstate + end, sizeof(float4) * tail, cudaMemcpyDeviceToDevice, s->stream));
-        NXM_TRY(cudaMemcpyAsync(s->kin + start, tk, sizeof(PKin) * tail, cudaMemcpyDeviceToDevice, s->stream));
-        NXM_TRY(cudaMemcpyAsync(s->def + start, td, sizeof(PDef) * tail, cudaMemcpyDeviceToDevice, s->stream));
-        NXM_TRY(cudaMemcpyAsync(s->pstate + start, ts, sizeof(float4) * tail, cudaMemcpyDeviceToDevice, s->stream));
-        NXM_TRY(cudaStreamSynchronize(s->stream));
-        cudaFree(tk); cudaFree(td); cudaFree(ts);
-    }
-    auto erase = [&](auto& v) { v.erase(v.begin() + start, v.begin() + end); };
-    erase(s->init_radius);
-    erase(s->phase);
-    erase(s->boundary_friction);
-    erase(s->group_id);
-    erase(s->slot2chunk);
-    s->n -= removed;
-    s->params_dirty = true;
-    return invalidate_codes(s);
+    if (start == end) return NXM_OK;
+    return remove_id_ranges(s, {make_uint2(start, end)});
 }
 
 int nxm_step(nxm_pipeline* pipeline, nxm_state* s, nxm_timestamps* ts) {

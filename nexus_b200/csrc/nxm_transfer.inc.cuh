@@ -84,9 +84,12 @@ __device__ __forceinline__ Collision collide(const DevPtrs& P, const DevCollider
 __global__ void __launch_bounds__(256) k_grid_update(DevPtrs P) {
     __shared__ DevCollider scol[MAX_COLLIDERS];
     const Params prm = *P.params;
-    const uint32_t ncol = prm.use_cpic ? 0u : min(prm.ncol, (uint32_t)MAX_COLLIDERS);
-    for (uint32_t i = threadIdx.x; i < ncol * (sizeof(DevCollider) / 4); i += blockDim.x)
-        reinterpret_cast<uint32_t*>(scol)[i] = reinterpret_cast<const uint32_t*>(P.colliders)[i];
+    // batched scenes: each block sees only its scene's colliders (global memory)
+    const bool scenes = prm.scene_blocks != 0;
+    const uint32_t ncol = prm.use_cpic ? 0u : (scenes ? prm.ncol : min(prm.ncol, (uint32_t)MAX_COLLIDERS));
+    if (!scenes)
+        for (uint32_t i = threadIdx.x; i < ncol * (sizeof(DevCollider) / 4); i += blockDim.x)
+            reinterpret_cast<uint32_t*>(scol)[i] = reinterpret_cast<const uint32_t*>(P.colliders)[i];
     __syncthreads();
     const float dx = prm.dx, dt = prm.dt;
     const v3 g = mk(prm.gravity[0], prm.gravity[1], prm.gravity[2]);
@@ -101,11 +104,21 @@ __global__ void __launch_bounds__(256) k_grid_update(DevPtrs P) {
         if (ncol > 0) {
             const uint32_t b = t >> 6, k = t & 63u;
             int4 vid = P.bvid[b];
+            const DevCollider* cols = scol;
+            uint32_t nc = ncol;
+            if (scenes) {
+                const uint32_t sid = scene_of_block(prm, vid);
+                const uint2 r = sid != NONE ? P.scene_cols[sid] : make_uint2(0u, 0u);
+                cols = P.colliders + r.x;
+                nc = r.y;
+                const int3 o = scene_base_of_block(prm, vid);  // scene-local node position
+                vid.x -= o.x; vid.y -= o.y; vid.z -= o.z;
+            }
             v3 cell_pt = mk((float)(vid.x * 4 + (int)(k & 3u)), (float)(vid.y * 4 + (int)((k >> 2) & 3u)),
                             (float)(vid.z * 4 + (int)(k >> 4))) * dx;
-            Collision c = collide(P, scol, ncol, dx, cell_pt);
+            Collision c = collide(P, cols, nc, dx, cell_pt);
             if (c.distance != MAX_FLT) {
-                const DevCollider& cc = scol[c.closest];
+                const DevCollider& cc = cols[c.closest];
                 v3 bv = col_vel_at(cc, cell_pt);
                 v3 delta = v - bv;
                 float nv = dot(delta, c.normal);
@@ -141,7 +154,7 @@ __device__ __forceinline__ float4 halo_node(const DevPtrs& P, uint32_t b, uint32
 // particle (read from slot `src`, xm / vf = its first two kin words) to slot
 // `dst` of the output records, together with the block key of its new position.
 __device__ __forceinline__ void g2p_particle(const DevPtrs& P, const Params& prm, const float4* __restrict__ halo,
-                                             uint32_t src, uint32_t dst, float4 xm, float4 vf) {
+                                             uint32_t src, uint32_t dst, float4 xm, float4 vf, int3 key_off) {
     const float dx = prm.dx, dt = prm.dt;
     const float inv_d = 4.0f / (dx * dx);
     float4* kr = reinterpret_cast<float4*>(&P.kin_out[dst]);
@@ -261,7 +274,8 @@ __device__ __forceinline__ void g2p_particle(const DevPtrs& P, const Params& prm
     if (P.pid_in) P.pid_out[dst] = P.pid_in[src];
     // block key of the new position, for the next step's activation
     const CellInfo nc = cell_info(dx, new_pos);
-    P.pcode[dst] = make_uint2(pack_key(nc.bx, nc.by, nc.bz), nc.ax | (nc.ay << 2) | (nc.az << 4));
+    P.pcode[dst] = make_uint2(pack_key(nc.bx + key_off.x, nc.by + key_off.y, nc.bz + key_off.z),
+                              nc.ax | (nc.ay << 2) | (nc.az << 4));
 }
 
 #ifndef NXM_G2P_MIN_CTAS
@@ -301,6 +315,7 @@ __global__ void __launch_bounds__(256, NXM_G2P_MIN_CTAS) k_g2p_update(DevPtrs P)
             nnp = __ldcg(&P.nprim[bn]);
         }
         const bool reorder = P.pid_in != nullptr;
+        const int3 key_off = prm.scene_blocks ? scene_base_of_block(prm, P.bvid[b]) : make_int3(0, 0, 0);
         uint32_t pid = tid < np ? __ldg(&P.sorted[first + tid]) : NONE;
         const uint32_t hblk = (tid < 216u && hoct != 0u) ? __ldg(&P.nbh[b * NUM_NBH + hoct - 1u]) : b;
         float4 xm = make_float4(0.f, 0.f, 0.f, 0.f), vf = xm;
@@ -323,7 +338,7 @@ __global__ void __launch_bounds__(256, NXM_G2P_MIN_CTAS) k_g2p_update(DevPtrs P)
                 xm = kr[0];
                 vf = kr[1];
             }
-            g2p_particle(P, prm, halo, pid, reorder ? first + k : pid, xm, vf);
+            g2p_particle(P, prm, halo, pid, reorder ? first + k : pid, xm, vf, key_off);
         }
         __syncthreads();
         b = bn;
@@ -347,7 +362,9 @@ __global__ void __launch_bounds__(256, NXM_G2P_MIN_CTAS) k_g2p_update(DevPtrs P)
             P.pstate_out[dst] = P.pstate[p];
             P.pid_out[dst] = P.pid_in[p];
             const CellInfo nc = cell_info(prm.dx, mk(ks[0].x, ks[0].y, ks[0].z));
-            P.pcode[dst] = make_uint2(pack_key(nc.bx, nc.by, nc.bz), nc.ax | (nc.ay << 2) | (nc.az << 4));
+            const int3 o = prm.scene_blocks ? scene_base_of(prm, P.pscene[P.pid_in[p]]) : make_int3(0, 0, 0);
+            P.pcode[dst] = make_uint2(pack_key(nc.bx + o.x, nc.by + o.y, nc.bz + o.z),
+                                      nc.ax | (nc.ay << 2) | (nc.az << 4));
         }
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) P.counters->codes_valid = 1u;

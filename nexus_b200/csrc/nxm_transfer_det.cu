@@ -24,7 +24,11 @@ __global__ void __launch_bounds__(64) k_p2g_gather(DevPtrs P) {
     const uint32_t tid = threadIdx.x;
     const int tx = (int)(tid & 3u), ty = (int)((tid >> 2) & 3u), tz = (int)(tid >> 4);
     for (uint32_t b = blockIdx.x; b < nb; b += gridDim.x) {
-        const int4 vid = P.bvid[b];
+        int4 vid = P.bvid[b];
+        {
+            const int3 o = scene_base_of_block(*P.params, vid);  // scene-local block coordinates
+            vid.x -= o.x; vid.y -= o.y; vid.z -= o.z;
+        }
         const v3 cell_pos = mk((float)(vid.x * 4 + tx), (float)(vid.y * 4 + ty), (float)(vid.z * 4 + tz)) * dx;
         const uint32_t first = P.first[b];
         const uint32_t num = P.nwx[b];

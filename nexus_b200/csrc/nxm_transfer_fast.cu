@@ -130,7 +130,11 @@ __global__ void __launch_bounds__(kP2gThreads, NXM_P2G_MIN_CTAS) k_p2g(DevPtrs P
     P2gRaw raw = p2g_load_raw(P, tid < h.np ? __ldg(&P.sorted[h.first + tid]) : NONE);
     __syncthreads();
     for (;;) {
-        const int4 vid = P.bvid[b];
+        int4 vid = P.bvid[b];
+        {
+            const int3 o = scene_base_of_block(*P.params, vid);  // scene-local block coordinates
+            vid.x -= o.x; vid.y -= o.y; vid.z -= o.z;
+        }
         const uint32_t fblk = (tid < 216u && foct != 0u) ? __ldg(&P.nbh[b * NUM_NBH + foct - 1u]) : b;
         for (uint32_t base = 0; base < h.np; base += kP2gChunk) {
             const uint32_t m_chunk = min(h.np - base, (uint32_t)kP2gChunk);
@@ -263,21 +267,26 @@ __global__ void __launch_bounds__(kP2gThreads, NXM_P2G_MIN_CTAS) k_p2g(DevPtrs P
 }
 
 // rigid_impulses.rs:167-185: world centre of mass from the current pose.
+__device__ __forceinline__ uint32_t collider_count(const Params& p) {
+    return p.scene_blocks ? p.ncol : min(p.ncol, (uint32_t)MAX_COLLIDERS);
+}
+
 __global__ void k_colliders_begin(DevPtrs P) {
-    const uint32_t i = threadIdx.x;
-    if (i >= P.params->ncol || i >= (uint32_t)MAX_COLLIDERS) return;
+    const uint32_t ncol = collider_count(*P.params);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < ncol; i += gridDim.x * blockDim.x) {
     DevCollider& c = P.colliders[i];
     quat q = quat{c.rot[0], c.rot[1], c.rot[2], c.rot[3]};
     v3 com = qrot(q, mk(c.local_com[0], c.local_com[1], c.local_com[2])) + mk(c.tra[0], c.tra[1], c.tra[2]);
     c.com[0] = com.x; c.com[1] = com.y; c.com[2] = com.z;
+    }
 }
 
 // dynamics/body.rs Velocity::integrate for one-way coupled bodies
 // (rigid_impulses.rs:66-140 with zero impulse and zero inverse mass).
 __global__ void k_colliders_end(DevPtrs P) {
-    const uint32_t i = threadIdx.x;
-    if (i >= P.params->ncol || i >= (uint32_t)MAX_COLLIDERS) return;
+    const uint32_t ncol = collider_count(*P.params);
     const float dt = P.params->dt;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < ncol; i += gridDim.x * blockDim.x) {
     DevCollider& c = P.colliders[i];
     quat q = quat{c.rot[0], c.rot[1], c.rot[2], c.rot[3]};
     v3 tra = mk(c.tra[0], c.tra[1], c.tra[2]);
@@ -302,6 +311,7 @@ __global__ void k_colliders_end(DevPtrs P) {
     float rl = 1.0f / sqrtf(nr.x * nr.x + nr.y * nr.y + nr.z * nr.z + nr.w * nr.w);
     c.rot[0] = nr.x * rl; c.rot[1] = nr.y * rl; c.rot[2] = nr.z * rl; c.rot[3] = nr.w * rl;
     c.tra[0] = nt.x; c.tra[1] = nt.y; c.tra[2] = nt.z;
+    }
 }
 
 }  // namespace
@@ -311,8 +321,8 @@ void launch_p2g(const DevPtrs& P, const LaunchCfg& c, cudaStream_t s) {
     k_p2g<<<c.sm_count * NXM_P2G_MIN_CTAS, kP2gThreads, kP2gSmem, s>>>(P);
 }
 
-void launch_colliders_begin(const DevPtrs& P, cudaStream_t s) { k_colliders_begin<<<1, 32, 0, s>>>(P); }
-void launch_colliders_end(const DevPtrs& P, cudaStream_t s) { k_colliders_end<<<1, 32, 0, s>>>(P); }
+void launch_colliders_begin(const DevPtrs& P, cudaStream_t s) { k_colliders_begin<<<8, 128, 0, s>>>(P); }
+void launch_colliders_end(const DevPtrs& P, cudaStream_t s) { k_colliders_end<<<8, 128, 0, s>>>(P); }
 
 }  // namespace fast
 }  // namespace nxm

@@ -91,6 +91,13 @@ SIGNATURES = {
     "nxm_grid_read_nodes": (C.c_int, [_vp, _f, C.c_uint32]),
     "nxm_debug_sort": (C.c_int, [_vp, _vp, C.c_int]),
     "nxm_state_estimate_timestep_bound": (C.c_int, [_vp, _f, _u]),
+    "nxm_state_enable_scenes": (C.c_int, [_vp, C.c_uint32]),
+    "nxm_scene_capacity": (C.c_uint32, [_vp]),
+    "nxm_scene_add": (C.c_int, [_vp, _vp, C.c_uint32, _vp, C.c_uint32, _f, C.c_uint32, _u]),
+    "nxm_scene_remove": (C.c_int, [_vp, _u, C.c_uint32]),
+    "nxm_scene_range": (C.c_int, [_vp, C.c_uint32, _u, _u]),
+    "nxm_scene_set_collider_velocity": (C.c_int, [_vp, C.c_uint32, C.c_uint32, _f, _f]),
+    "nxm_read_positions_range": (C.c_int, [_vp, C.c_uint32, C.c_uint32, _f]),
     "nxm_chunk_add": (C.c_int, [_vp, _vp, C.c_uint32, _u]),
     "nxm_chunk_extend": (C.c_int, [_vp, C.c_uint32, _vp, C.c_uint32]),
     "nxm_chunk_remove": (C.c_int, [_vp, C.c_uint32]),
@@ -240,6 +247,48 @@ class MpmState:
             arr("fixed", np.uint32), arr("model", np.uint32))
         _check(self.lib.nxm_particles_append_soa(self.h, C.byref(soa), batch.n), "append")
 
+    # -- batched scenes ------------------------------------------------------------------
+    def enable_scenes(self, scene_blocks: int):
+        _check(self.lib.nxm_state_enable_scenes(self.h, scene_blocks), "enable_scenes")
+
+    def scene_capacity(self) -> int:
+        return int(self.lib.nxm_scene_capacity(self.h))
+
+    def add_scene(self, batch: ParticleBatch, colliders=None, tri_vertices=None) -> int:
+        rec = particle_records(batch)
+        cols = np.ascontiguousarray(colliders if colliders is not None else np.zeros(0, COLLIDER_DTYPE),
+                                    dtype=COLLIDER_DTYPE)
+        tri = (np.zeros((0,), np.float32) if tri_vertices is None
+               else np.ascontiguousarray(tri_vertices, np.float32).reshape(-1))
+        sid = C.c_uint32()
+        _check(self.lib.nxm_scene_add(self.h, rec.ctypes.data_as(C.c_void_p), batch.n,
+                                      cols.ctypes.data_as(C.c_void_p), len(cols), _p(tri), tri.size // 9,
+                                      C.byref(sid)), "scene_add")
+        return sid.value
+
+    def remove_scenes(self, scenes):
+        ids = np.ascontiguousarray(list(scenes), np.uint32)
+        _check(self.lib.nxm_scene_remove(self.h, _p(ids, _u), len(ids)), "scene_remove")
+
+    def scene_range(self, scene: int) -> tuple[int, int]:
+        a, b = C.c_uint32(), C.c_uint32()
+        _check(self.lib.nxm_scene_range(self.h, scene, C.byref(a), C.byref(b)), "scene_range")
+        return a.value, b.value
+
+    def set_scene_collider_velocity(self, scene: int, index: int, linvel, angvel):
+        lv = np.asarray(linvel, np.float32)
+        av = np.asarray(angvel, np.float32)
+        _check(self.lib.nxm_scene_set_collider_velocity(self.h, scene, index, _p(lv), _p(av)),
+               "scene_set_collider_velocity")
+
+    def read_positions_range(self, first: int, count: int) -> np.ndarray:
+        out = np.zeros((max(count, 1), 3), np.float32)
+        _check(self.lib.nxm_read_positions_range(self.h, first, count, _p(out, _f)), "read_positions_range")
+        return out[:count]
+
+    def read_scene_positions(self, scene: int) -> np.ndarray:
+        return self.read_positions_range(*self.scene_range(scene))
+
     # -- particle chunks (NexusState, src/state.rs:665-774) ------------------------
     def add_chunk(self, batch: ParticleBatch) -> int:
         rec = particle_records(batch)
@@ -381,3 +430,24 @@ def state_from_scene(scene, deterministic: bool = False, grid_capacity: int | No
     st.set_deterministic(deterministic)
     st.append(scene.particles)
     return st
+
+
+def batched_state_from_scenes(scenes_, deterministic: bool = False, scene_blocks: int = 64,
+                              grid_capacity: int | None = None):
+    """One device state advancing several ``Scene``s together (same dx, dt and
+    gravity).  Returns the state and the scene slot of each input scene."""
+    s0 = scenes_[0]
+    for sc in scenes_:
+        if (sc.dx, sc.dt, tuple(sc.gravity)) != (s0.dx, s0.dt, tuple(s0.gravity)):
+            raise ValueError("batched scenes share dx, dt and gravity")
+    n = sum(sc.n for sc in scenes_)
+    cap = grid_capacity or sum(sc.grid_capacity for sc in scenes_)
+    st = MpmState(grid_size=cap, particles_capacity=n)
+    st.set_cell_width(s0.dx, cap)
+    st.set_simulation_params(s0.gravity, s0.dt)
+    st.set_deterministic(deterministic)
+    st.enable_scenes(scene_blocks)
+    slots = [st.add_scene(sc.particles, sc.colliders, sc.tri_vertices if sc.tri_vertices.size else None)
+             for sc in scenes_]
+    return st, slots
+

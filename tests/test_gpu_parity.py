@@ -325,3 +325,66 @@ def test_particle_chunks(pipe):
     pipe.step(st)
     st.synchronize()
     assert np.isfinite(st.read_positions()).all()
+
+
+def _batch_scenes():
+    a = scenes.elastic_cube(n_side=12, seed=21)
+    b = scenes.mixed_materials(n_side=6)
+    c = scenes.trimesh_floor(n_side=10)
+    return [a, b, c]
+
+
+def test_batched_scenes_step_as_alone(pipe):
+    """Several scenes in one state (one launch sequence per step): in
+    deterministic mode every scene's particles are bit-identical to the same
+    scene stepped alone, also after another scene is removed mid-run; in fast
+    mode each stays within the fast tolerance of its own oracle run."""
+    from nexus_b200.mpm import batched_state_from_scenes
+    from oracle.oracle import OracleScene
+    scs = _batch_scenes()
+    alone = []
+    for sc in scs:
+        st = state_from_scene(sc, deterministic=True)
+        for _ in range(30):
+            pipe.step(st)
+        alone.append(st.read_positions())
+    bst, slots = batched_state_from_scenes(scs, deterministic=True)
+    for _ in range(30):
+        pipe.step(bst)
+    for sc, sl, want in zip(scs, slots, alone):
+        got = bst.read_scene_positions(sl)
+        assert np.array_equal(got, want), (sc.name, np.abs(got - want).max())
+    # remove the middle scene; the others continue exactly as alone
+    bst.remove_scenes([slots[1]])
+    for i in (0, 2):
+        st = state_from_scene(scs[i], deterministic=True)
+        for _ in range(40):
+            pipe.step(st)
+        alone[i] = st.read_positions()
+    for _ in range(10):
+        pipe.step(bst)
+    for i in (0, 2):
+        assert np.array_equal(bst.read_scene_positions(slots[i]), alone[i]), scs[i].name
+    # fast mode (reordered storage, scatter P2G)
+    fst, fslots = batched_state_from_scenes(scs, deterministic=False)
+    for _ in range(30):
+        pipe.step(fst)
+    fst.synchronize()
+    for sc, sl in zip(scs, fslots):
+        o = OracleScene(sc)
+        o.step(30)
+        assert rel_l2(fst.read_scene_positions(sl), o.particles()["pos"]) < FAST_TOL, sc.name
+
+
+def test_batched_scene_limits(pipe):
+    from nexus_b200.mpm import batched_state_from_scenes, NXM_E_INVALID
+    scs = _batch_scenes()[:1]
+    st, _ = batched_state_from_scenes(scs)
+    assert st.scene_capacity() == 31 * 15 * 31
+    far = scenes.elastic_cube(n_side=4)
+    far.particles.pos[:, 0] += np.float32(10.0)  # beyond the scene's key region
+    with pytest.raises(NexusError) as e:
+        st.add_scene(far.particles)
+    assert e.value.code == NXM_E_INVALID
+    with pytest.raises(NexusError):
+        st.set_colliders(scs[0].colliders)  # colliders come per scene
