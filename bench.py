@@ -14,6 +14,13 @@ data path; value = particle-steps of all ranks / max time over ranks.
 
 ``--impl reference`` times the reference algorithm's CPU restatement (the
 oracle, OpenMP on all host cores) on the same scene; rank 0 only.
+
+The batched form is measured beside it (``batched`` in the JSON line): the
+256-scene mix (4k-128k particles per
+scene, neo-Hookean or sand, dx = 1/128) advanced in one state, one launch
+sequence per step for all scenes, against the same scenes stepped one by one
+(each alone in its own state), the plain per-scene loop.  With ``--gpus N``
+the scenes are sharded over the ranks (no collective on the data path).
 """
 from __future__ import annotations
 
@@ -139,13 +146,8 @@ def dist_setup():
 
 
 def all_max(x: float, world: int) -> float:
-    if world == 1:
-        return x
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    from nexus_b200.sharding import all_max as amax
+    return amax(x, world)
 
 
 def barrier(world: int):
@@ -243,6 +245,9 @@ def run_ours(args, world, rank, local):
 
     # end to end through the C ABI from pinned host buffers
     e2e = measure_e2e(scene, args, torch) if args.e2e else None
+    del st
+    batched = measure_batched(args, world, rank, torch) if args.batched_steps > 0 else None
+    serving = measure_serving(args, torch) if (args.serving_requests > 0 and world == 1) else None
 
     if rank != 0:
         return
@@ -269,8 +274,114 @@ def run_ours(args, world, rank, local):
         "e2e": e2e,
         "gpu_launches": launches,
         "cpu_baseline": cpu,
+        "batched": batched,
+        "serving": serving,
     }
     print(json.dumps(line), flush=True)
+
+
+def measure_batched(args, world, rank, torch):
+    """The batched mix on this rank's shard: one state, timed steps, then the
+    same scenes stepped one by one (plain loop) for the comparison."""
+    from nexus_b200 import scenes as S
+    from nexus_b200.mpm import MpmPipeline, batched_state_from_scenes, state_from_scene
+    from nexus_b200.sharding import shard_scenes, all_sum
+    mix = S.batched_mix(count=args.batched_scenes)
+    mine = [mix[i] for i in shard_scenes([sc.n for sc in mix], world)[rank]]
+    n = sum(sc.n for sc in mine)
+    pipe = MpmPipeline()
+    st, _ = batched_state_from_scenes(mine)
+    stream = torch.cuda.ExternalStream(st.cuda_stream())
+    for _ in range(max(3, args.warmup)):
+        pipe.step(st)
+    st.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier(world)
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    for _ in range(args.batched_steps):
+        pipe.step(st)
+    ev1.record(stream)
+    ev1.synchronize()
+    barrier(world)
+    ms = ev0.elapsed_time(ev1)
+    st.synchronize()
+    del st
+    max_ms = all_max(ms, world)
+    total = all_sum(float(n), world)
+    value = total * args.batched_steps / (max_ms / 1e3)
+    # plain loop: each scene alone, its own graph, one after the other
+    plain_ms = 0.0
+    for sc in mine:
+        one = state_from_scene(sc)
+        s1 = torch.cuda.ExternalStream(one.cuda_stream())
+        for _ in range(3):
+            pipe.step(one)
+        one.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(s1)
+        for _ in range(args.plain_steps):
+            pipe.step(one)
+        b.record(s1)
+        b.synchronize()
+        plain_ms += a.elapsed_time(b) / args.plain_steps
+        one.synchronize()
+        del one
+    plain_ms = all_max(plain_ms, world)
+    plain = total / (plain_ms / 1e3)
+    return {"workload": f"batched_mix_{len(mix)}", "scenes": len(mix), "particles": int(total),
+            "value": value, "unit": UNIT, "steps": args.batched_steps, "ms_per_step": max_ms / args.batched_steps,
+            "plain_scene_by_scene": {"value": plain, "unit": UNIT, "ms_per_step": plain_ms,
+                                     "how": f"each scene alone in its own state and graph, {args.plain_steps} "
+                                            f"timed steps after 3 warm-up, summed over scenes"},
+            "speedup_vs_plain": value / plain, "dx": mix[0].dx, "dt": mix[0].dt,
+            "parallelism": f"scene-sharded{world}" if world > 1 else "single"}
+
+
+def measure_serving(args, torch):
+    """Continuous batching of a Poisson request stream (mean 200 scenes/s):
+    aggregate particle-steps/s and p50/p99 arrival-to-completion latency,
+    beside a FIFO loop that runs each request alone (plain step) in arrival
+    order, whose latencies come from each scene's measured plain step time."""
+    from nexus_b200 import scenes as S
+    from nexus_b200.mpm import MpmPipeline, state_from_scene
+    from nexus_b200.serving import MpmServer, poisson_requests, latency_summary
+    reqs = poisson_requests(args.serving_requests, 200.0, 3000, S.serving_scene, (50, 2000))
+    srv = MpmServer(hbm_budget=150e9, particles_capacity=1 << 26, grid_capacity=1 << 22)
+    t0 = time.perf_counter()
+    results, rejected = srv.run(reqs)
+    wall = time.perf_counter() - t0
+    summ = latency_summary(results)
+    del srv
+    # FIFO plain loop: per-scene step time measured alone, then a virtual clock
+    pipe = MpmPipeline()
+    t_done, lat = 0.0, []
+    for r in sorted(reqs, key=lambda q: q.arrival):
+        one = state_from_scene(r.scene)
+        s1 = torch.cuda.ExternalStream(one.cuda_stream())
+        for _ in range(3):
+            pipe.step(one)
+        one.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(s1)
+        for _ in range(args.plain_steps):
+            pipe.step(one)
+        b.record(s1)
+        b.synchronize()
+        run_s = a.elapsed_time(b) / args.plain_steps / 1e3 * r.steps
+        one.synchronize()
+        del one
+        t_done = max(t_done, r.arrival) + run_s
+        lat.append(t_done - r.arrival)
+    work = sum(r.scene.n * r.steps for r in reqs)
+    return {"workload": "serving_poisson_200_per_s", "requests": len(reqs), "rejected": len(rejected),
+            "particles_per_request": "logU(2048, 524288)", "steps_per_request": "U{50..2000}",
+            "value": work / wall, "unit": UNIT, "wall_s": wall, "p50_s": summ["p50_s"], "p99_s": summ["p99_s"],
+            "plain_fifo": {"value": work / t_done, "unit": UNIT, "p50_s": float(np.percentile(lat, 50)),
+                           "p99_s": float(np.percentile(lat, 99)),
+                           "how": "each request alone in its own state, in arrival order; per-scene step time "
+                                  f"measured over {args.plain_steps} steps after 3 warm-up, times its budget"},
+            "note": f"{len(reqs)} requests of the 4000-request stream (same arrival rate and distributions)"}
 
 
 def measure_e2e(scene, args, torch):
@@ -329,6 +440,11 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=500)
     ap.add_argument("--no-e2e", dest="e2e", action="store_false")
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
+    ap.add_argument("--batched-steps", type=int, default=50,
+                    help="timed steps of the batched mix (0: skip it)")
+    ap.add_argument("--batched-scenes", type=int, default=256)
+    ap.add_argument("--plain-steps", type=int, default=10)
+    ap.add_argument("--serving-requests", type=int, default=200, help="0: skip the serving measurement")
     ap.add_argument("--traffic", type=float, default=None,
                     help="DRAM bytes per step from an ncu capture (see profiles/)")
     args = ap.parse_args()

@@ -19,6 +19,8 @@ from __future__ import annotations
 
 from dataclasses import dataclass, field
 
+import math
+
 import numpy as np
 
 from .models import ParticleModel, BoundaryCondition
@@ -168,3 +170,53 @@ def trimesh_floor(n_side: int = 16, n_vertices: int = 21, seed: int = 11, steps:
     cols = collider_array(walls + [mesh])
     return Scene("trimesh_floor", dx, 1.0e-4, (0.0, 0.0, -9.81), batch, cols, steps, grid_capacity_for(batch.n),
                  tri_vertices=tri.reshape(-1, 3))
+
+
+def random_box_scene(seed: int, dx: float, n_min: int, n_max: int, materials=("neo_hookean", "sand"),
+                     steps: int = 200, name: str = "box") -> Scene:
+    """One scene of the batched and serving workloads: a random axis-aligned
+    box of N ~ logU(n_min, n_max) particles, uniform random inside it, of one
+    material drawn uniformly from ``materials``: neo-Hookean solid (E ~
+    logU(1e4, 1e6), nu = 0.3, rho = 1000), Drucker-Prager sand (30 degrees,
+    E = 3.5e5, nu = 0.3, rho = 2700) or water (bulk modulus 1e5, rho = 1000).
+    Box sides start U(0.1, 0.4), are rescaled to the volume N (dx/2)^3 (8
+    particles per cell) and clamped to [0.1, 0.4]; the box sits at a random
+    place inside [4dx, 1 - 4dx]^3.  V0 = box volume / N, m = rho V0.  Six
+    slip walls bound [0, 1]^3; dt = 5e-5, gravity -z."""
+    u = uniform(seed, 16)
+    n = int(round(math.exp(math.log(n_min) + u[0] * (math.log(n_max) - math.log(n_min)))))
+    sides = 0.1 + 0.3 * u[1:4]
+    target = n * (dx / 2.0) ** 3
+    sides = np.clip(sides * (target / np.prod(sides)) ** (1.0 / 3.0), 0.1, 0.4)
+    lo = 4 * dx + u[4:7] * (1.0 - 8 * dx - sides)
+    pos = (lo + sides * uniform(seed, 3 * n, 16).reshape(n, 3)).astype(np.float32)
+    v0 = float(np.prod(sides)) / n
+    radius = np.float32(0.5 * v0 ** (1.0 / 3.0))
+    mat = materials[min(int(u[7] * len(materials)), len(materials) - 1)]
+    if mat == "neo_hookean":
+        e = math.exp(math.log(1.0e4) + u[8] * (math.log(1.0e6) - math.log(1.0e4)))
+        batch = ParticleBatch.from_positions(pos, radius, 1000.0, ParticleModel.elastic_neo_hookean(e, 0.3))
+    elif mat == "sand":
+        batch = ParticleBatch.from_positions(pos, radius, 2700.0,
+                                             ParticleModel.sand_with_friction_angle(3.5e5, 0.3, 30.0))
+    else:
+        batch = ParticleBatch.from_positions(pos, radius, 1000.0, ParticleModel.water(1.0e5))
+    cols = collider_array(box_walls(0.0, 1.0, BoundaryCondition.slip(), BoundaryCondition.slip()))
+    return Scene(name, dx, 5.0e-5, (0.0, 0.0, -9.81), batch, cols, steps, grid_capacity_for(batch.n))
+
+
+def batched_mix(count: int = 256, seed: int = 1000, dx: float = 1.0 / 128.0, steps: int = 200,
+                n_min: int = 4096, n_max: int = 131072) -> list:
+    """The batched workload: ``count`` independent scenes (seed + s for scene
+    s) from random_box_scene, neo-Hookean or sand half and half, 4k-128k
+    particles each, dx = 1/128, 200 steps."""
+    return [random_box_scene(seed + s, dx, n_min, n_max, ("neo_hookean", "sand"), steps, f"batched_{s}")
+            for s in range(count)]
+
+
+def serving_scene(i: int, seed: int = 3000) -> Scene:
+    """Request i of the serving workload: 2k-512k particles, elastic, sand or
+    water, dx = 1/128 or 1/256 (uniform)."""
+    u = uniform(seed + 7919 * (i + 1), 1)
+    dx = 1.0 / 128.0 if u[0] < 0.5 else 1.0 / 256.0
+    return random_box_scene(seed + i, dx, 2048, 524288, ("neo_hookean", "sand", "water"), name=f"serve_{i}")

@@ -1,0 +1,174 @@
+"""Serving form: continuous batching of independent MPM scenes on one GPU.
+
+Requests (a scene and a step budget) arrive over time.  A request is
+admitted as soon as it has arrived and its estimated HBM footprint fits the
+budget beside the scenes already running.  Every admitted scene then
+advances in the same batched state as all the others of its cell width, dt
+and gravity: one launch sequence per step for all of them (nxm_step on a
+state with batched scenes).  When a scene has taken its step budget, its
+particles are read back and the scene is removed, freeing memory for the next
+arrivals.  Scenes that arrive while others run start on the next step.
+
+Each scene steps exactly as it would alone (scene-local coordinates, its own
+block-key region and colliders), so a result does not depend on what else was
+in the mix or on when it was admitted.
+"""
+from __future__ import annotations
+
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from .mpm import MpmPipeline, MpmState
+from .scenes import Scene
+
+# Estimated device bytes per particle of a batched state: two copies of the
+# 144-byte particle record, sort scratch (block key 8, header 4, sorted ids
+# reserved 32), ids 8, scene index 4.
+BYTES_PER_PARTICLE = 2 * 144 + 8 + 4 + 32 + 8 + 4
+# Per grid block: 64 nodes of 16 bytes, header arrays, hash slots.
+BYTES_PER_BLOCK = 64 * 16 + 16 + 4 * 3 + 4 * 10 + 4 * 7 + 4 + 2 * 8
+
+
+@dataclass
+class Request:
+    rid: int
+    scene: Scene
+    steps: int
+    arrival: float  # seconds after the start of the run
+
+
+@dataclass
+class Result:
+    rid: int
+    n: int
+    steps: int
+    arrival: float
+    admitted: float
+    completed: float
+    positions: np.ndarray = field(repr=False)
+
+    @property
+    def latency(self) -> float:
+        return self.completed - self.arrival
+
+
+def footprint(scene: Scene) -> int:
+    """Estimated device bytes of a scene inside a batched state."""
+    return scene.n * BYTES_PER_PARTICLE + scene.grid_capacity * BYTES_PER_BLOCK
+
+
+class _Group:
+    """One batched state: the scenes sharing a cell width, dt and gravity."""
+
+    def __init__(self, key, particles_capacity: int, grid_capacity: int, scene_blocks: int, deterministic: bool):
+        dx, dt, gravity = key
+        self.state = MpmState(grid_size=grid_capacity, particles_capacity=particles_capacity)
+        self.state.set_cell_width(dx, grid_capacity)
+        self.state.set_simulation_params(gravity, dt)
+        self.state.set_deterministic(deterministic)
+        self.state.enable_scenes(scene_blocks)
+        self.active = {}  # slot -> [request, remaining steps, admitted time]
+        self.particles = 0
+        self.grid = 0
+
+
+class MpmServer:
+    """Request loop over batched states (one per cell width / dt / gravity)."""
+
+    def __init__(self, hbm_budget: float = 150e9, particles_capacity: int = 1 << 24,
+                 grid_capacity: int = 1 << 20, deterministic: bool = False, scene_blocks=None):
+        self.pipe = MpmPipeline()
+        self.budget = hbm_budget
+        self.particles_capacity = particles_capacity
+        self.grid_capacity = grid_capacity
+        self.deterministic = deterministic
+        self.scene_blocks = scene_blocks  # None: 64 blocks per scene axis at dx >= 1/128, else 128
+        self.groups = {}
+        self.in_use = 0
+        self.steps_taken = 0
+        self.particle_steps = 0
+
+    def _group(self, sc: Scene) -> _Group:
+        key = (float(sc.dx), float(sc.dt), tuple(float(g) for g in sc.gravity))
+        g = self.groups.get(key)
+        if g is None:
+            sb = self.scene_blocks or (64 if sc.dx >= 1.0 / 128.0 else 128)
+            g = self.groups[key] = _Group(key, self.particles_capacity, self.grid_capacity, sb, self.deterministic)
+        return g
+
+    def _fits(self, sc: Scene, g: _Group) -> bool:
+        return (self.in_use + footprint(sc) <= self.budget and g.particles + sc.n <= self.particles_capacity
+                and g.grid + sc.grid_capacity <= self.grid_capacity)
+
+    def run(self, requests, clock=time.perf_counter, idle_sleep: float = 1e-4):
+        """Serves ``requests`` (any order; by arrival) and returns the results by
+        request id, plus requests that can never fit (rejected)."""
+        pending = sorted(requests, key=lambda r: (r.arrival, r.rid))
+        results, rejected = {}, []
+        t0 = clock()
+        while pending or any(g.active for g in self.groups.values()):
+            now = clock() - t0
+            # admission, first come first served
+            while pending and pending[0].arrival <= now:
+                r = pending[0]
+                g = self._group(r.scene)
+                if footprint(r.scene) > self.budget or r.scene.n > self.particles_capacity:
+                    rejected.append(pending.pop(0))
+                    continue
+                if not self._fits(r.scene, g):
+                    break
+                pending.pop(0)
+                slot = g.state.add_scene(r.scene.particles, r.scene.colliders,
+                                         r.scene.tri_vertices if r.scene.tri_vertices.size else None)
+                g.active[slot] = [r, r.steps, clock() - t0]
+                g.particles += r.scene.n
+                g.grid += r.scene.grid_capacity
+                self.in_use += footprint(r.scene)
+            busy = [g for g in self.groups.values() if g.active]
+            if not busy:
+                if pending:
+                    time.sleep(min(idle_sleep, max(0.0, pending[0].arrival - (clock() - t0))))
+                continue
+            for g in busy:
+                self.pipe.step(g.state)
+                self.steps_taken += 1
+                self.particle_steps += g.particles
+            for g in busy:
+                done = []
+                for slot, rec in g.active.items():
+                    rec[1] -= 1
+                    if rec[1] == 0:
+                        done.append(slot)
+                for slot in done:
+                    r, _, admitted = g.active.pop(slot)
+                    pos = g.state.read_scene_positions(slot)  # waits for the scene's last step
+                    results[r.rid] = Result(r.rid, r.scene.n, r.steps, r.arrival, admitted, clock() - t0, pos)
+                if done:
+                    g.state.remove_scenes(done)
+                    g.particles = sum(rec[0].scene.n for rec in g.active.values())
+                    g.grid = sum(rec[0].scene.grid_capacity for rec in g.active.values())
+                    self.in_use = sum(footprint(rec[0].scene) for gg in self.groups.values()
+                                      for rec in gg.active.values())
+        return results, rejected
+
+
+def poisson_requests(count: int, rate: float, seed: int, make_scene, steps_range) -> list:
+    """``count`` requests with exponential inter-arrival times (mean 1/rate),
+    scene i = make_scene(i), steps uniform in steps_range (inclusive)."""
+    from .scenes import uniform
+    u = uniform(seed, 2 * count)
+    t, out = 0.0, []
+    lo, hi = steps_range
+    for i in range(count):
+        t += -np.log(max(1.0 - u[2 * i], 1e-300)) / rate
+        steps = lo + int(u[2 * i + 1] * (hi - lo + 1))
+        out.append(Request(i, make_scene(i), min(steps, hi), t))
+    return out
+
+
+def latency_summary(results) -> dict:
+    lat = np.array([r.latency for r in results.values()]) if results else np.zeros(0)
+    return {"completed": int(lat.size), "p50_s": float(np.percentile(lat, 50)) if lat.size else None,
+            "p99_s": float(np.percentile(lat, 99)) if lat.size else None}
