@@ -202,7 +202,12 @@ def random_box_scene(seed: int, dx: float, n_min: int, n_max: int, materials=("n
     else:
         batch = ParticleBatch.from_positions(pos, radius, 1000.0, ParticleModel.water(1.0e5))
     cols = collider_array(box_walls(0.0, 1.0, BoundaryCondition.slip(), BoundaryCondition.slip()))
-    return Scene(name, dx, 5.0e-5, (0.0, 0.0, -9.81), batch, cols, steps, grid_capacity_for(batch.n))
+    # blocks the box spans (plus a layer each side for neighbours and motion), twice over for slack
+    blocks = int(np.prod(np.ceil(sides / (4 * dx)) + 3))
+    cap = 1
+    while cap < 2 * blocks + 64:
+        cap <<= 1
+    return Scene(name, dx, 5.0e-5, (0.0, 0.0, -9.81), batch, cols, steps, max(cap, grid_capacity_for(batch.n)))
 
 
 def batched_mix(count: int = 256, seed: int = 1000, dx: float = 1.0 / 128.0, steps: int = 200,
