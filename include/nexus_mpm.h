@@ -94,7 +94,9 @@ typedef struct nxm_particle {
  * as nxm_particle; any pointer except position and model may be NULL to
  * take the Particle::new default: zero velocity/affine/force/vel_grad_det,
  * identity F, damping 0, phase 1, boundary_friction 1, group 0, enabled 1,
- * fixed 0; init_volume/mass are then required). */
+ * fixed 0; init_volume/mass are then required).  init_radius, phase,
+ * boundary_friction and group_id are part of the layout; the step does not
+ * read them and the library does not keep them. */
 typedef struct nxm_particles_soa {
     const float* position;        /* n*3 */
     const float* velocity;        /* n*3 */
@@ -310,14 +312,16 @@ NXM_API int nxm_sort_blocks_noalloc(const float* positions, uint32_t n, float ce
  * Enable before adding any particle or collider (0 turns it off).  Particle
  * blocks must stay within local block coordinates [1 - M, S - M - 3] with
  * S = scene_blocks, M = S / 8 (a [0, 1]^3 scene fits S = 64 at dx = 1/128);
- * nxm_scene_add refuses particles outside with NXM_E_INVALID. */
+ * nxm_scene_add refuses particles outside with NXM_E_INVALID.  In scene
+ * mode particles change only through the scene calls: the particle-level
+ * append / remove / chunk calls return NXM_E_INVALID. */
 NXM_API int nxm_state_enable_scenes(nxm_state* state, uint32_t scene_blocks);
 /* Scene slots available (0 when scenes are off). */
 NXM_API uint32_t nxm_scene_capacity(const nxm_state* state);
 /* Adds a scene: its particles (appended as one contiguous id range) and up to
  * 16 colliders (triangles indexed within `tri_vertices`, as for
  * nxm_state_set_colliders).  Returns NXM_E_CAPACITY when every slot is taken. */
-NXM_API int nxm_scene_add(nxm_state* state, const nxm_particle* particles, uint32_t count,
+NXM_API int nxm_scene_add(nxm_state* state, const nxm_particles_soa* particles, uint32_t count,
                           const nxm_collider* colliders, uint32_t num_colliders, const float* tri_vertices,
                           uint32_t num_triangles, uint32_t* scene);
 /* Removes scenes with their particles and colliders; the particle ids of the

@@ -221,6 +221,13 @@ __global__ void __launch_bounds__(256) k_rm_move(uint32_t n, const PKin* __restr
     }
 }
 
+// Id-indexed arrays follow a range removal: entry id goes to its new id.
+__global__ void k_rm_ids(uint32_t n, const uint32_t* __restrict__ src, const uint2* __restrict__ ranges,
+                         const uint32_t* __restrict__ cum, uint32_t nr, uint32_t* __restrict__ dst) {
+    for (uint32_t id = blockIdx.x * blockDim.x + threadIdx.x; id < n; id += gridDim.x * blockDim.x)
+        if (!removed_id(id, ranges, nr)) dst[new_id_of(id, ranges, cum, nr)] = src[id];
+}
+
 // Swap-removal data movement: record pairs[i].y moves to slot pairs[i].x.
 // Every source is at or above the new length and every destination below it,
 // so the moves are independent.
@@ -232,6 +239,10 @@ __global__ void k_move_records(PKin* __restrict__ kin, PDef* __restrict__ def, f
         def[m.x] = def[m.y];
         pstate[m.x] = pstate[m.y];
     }
+}
+
+__global__ void k_fill(uint32_t* __restrict__ out, uint32_t value, uint32_t count) {
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < count; t += gridDim.x * blockDim.x) out[t] = value;
 }
 
 __global__ void k_iota(uint32_t* __restrict__ out, uint32_t first, uint32_t count) {
@@ -289,11 +300,10 @@ struct nxm_state {
     uint2* pcode = nullptr;
     uint32_t* phdr = nullptr;
     uint32_t* sorted = nullptr;
-    std::vector<float> init_radius, phase, boundary_friction;
-    std::vector<uint32_t> group_id;
     // particle chunks (src/state.rs:665-774): owner chunk of each particle id
     // (NONE for particles appended outside a chunk) and the live chunks' sizes
-    std::vector<uint32_t> slot2chunk;
+    std::vector<uint32_t> slot2chunk;  // empty until the first chunk is created
+    bool chunks_used = false;
     std::map<uint32_t, uint32_t> chunks;
     uint32_t next_chunk = 0;
 
@@ -332,8 +342,8 @@ struct nxm_state {
     int scene_cmin[3] = {0, 0, 0};
     uint32_t scene_cells[3] = {0, 0, 0};
     std::vector<Scene> scenes;
-    std::vector<uint32_t> pscene;       // scene of each particle id
-    uint32_t* d_pscene = nullptr;
+    uint32_t* d_pscene = nullptr;       // scene of each particle id (device)
+    uint32_t* d_pscene_alt = nullptr;
     uint2* d_scene_cols = nullptr;      // per scene slot: its colliders in the table
     uint32_t* d_tiles = nullptr;        // compaction scratch, one word per 1024 particles
     DevTri* d_tris = nullptr;       // triangles of every trimesh collider (one copy per collider)
@@ -489,7 +499,7 @@ struct ParticleBuffers {
     PDef *def = nullptr, *def_alt = nullptr;
     float4 *pstate = nullptr, *pstate_alt = nullptr;
     uint32_t *pid = nullptr, *pid_alt = nullptr, *phdr = nullptr, *sorted = nullptr, *pscene = nullptr,
-             *tiles = nullptr;
+             *pscene_alt = nullptr, *tiles = nullptr;
     uint2* pcode = nullptr;
     cudaError_t alloc(uint32_t cap) {
         cudaError_t e = cudaSuccess;
@@ -501,20 +511,21 @@ struct ParticleBuffers {
         a(&pid, cap); a(&pid_alt, cap); a(&pcode, cap); a(&phdr, cap);
         a(&sorted, (size_t)cap * 8);
         a(&pscene, cap);
+        a(&pscene_alt, cap);
         a(&tiles, cap / 1024 + 2);
         return e;
     }
     void release() { *this = ParticleBuffers{}; }
     ~ParticleBuffers() {
         dfree(kin); dfree(def); dfree(pstate); dfree(kin_alt); dfree(def_alt); dfree(pstate_alt);
-        dfree(pid); dfree(pid_alt); dfree(pcode); dfree(phdr); dfree(sorted); dfree(pscene); dfree(tiles);
+        dfree(pid); dfree(pid_alt); dfree(pcode); dfree(phdr); dfree(sorted); dfree(pscene); dfree(pscene_alt); dfree(tiles);
     }
 };
 
 void free_particles(nxm_state* s) {
     dfree(s->kin); dfree(s->def); dfree(s->pstate); dfree(s->kin_alt); dfree(s->def_alt); dfree(s->pstate_alt);
     dfree(s->pid); dfree(s->pid_alt); dfree(s->pcode); dfree(s->phdr); dfree(s->sorted);
-    dfree(s->d_pscene); dfree(s->d_tiles);
+    dfree(s->d_pscene); dfree(s->d_pscene_alt); dfree(s->d_tiles);
 }
 
 int reserve_particles(nxm_state* s, uint32_t need) {
@@ -528,6 +539,7 @@ int reserve_particles(nxm_state* s, uint32_t need) {
         NXM_TRY(cudaMemcpyAsync(t.kin, s->kin, sizeof(PKin) * s->n, cudaMemcpyDeviceToDevice, s->stream));
         NXM_TRY(cudaMemcpyAsync(t.def, s->def, sizeof(PDef) * s->n, cudaMemcpyDeviceToDevice, s->stream));
         NXM_TRY(cudaMemcpyAsync(t.pstate, s->pstate, sizeof(float4) * s->n, cudaMemcpyDeviceToDevice, s->stream));
+        NXM_TRY(cudaMemcpyAsync(t.pscene, s->d_pscene, 4 * (size_t)s->n, cudaMemcpyDeviceToDevice, s->stream));
     }
     NXM_TRY(cudaStreamSynchronize(s->stream));
     free_particles(s);
@@ -535,9 +547,8 @@ int reserve_particles(nxm_state* s, uint32_t need) {
     s->kin_alt = t.kin_alt; s->def_alt = t.def_alt; s->pstate_alt = t.pstate_alt;
     s->pid = t.pid; s->pid_alt = t.pid_alt;
     s->pcode = t.pcode; s->phdr = t.phdr; s->sorted = t.sorted;
-    s->d_pscene = t.pscene; s->d_tiles = t.tiles;
+    s->d_pscene = t.pscene; s->d_pscene_alt = t.pscene_alt; s->d_tiles = t.tiles;
     t.release();
-    if (s->n) NXM_TRY(cudaMemcpy(s->d_pscene, s->pscene.data(), 4 * (size_t)s->n, cudaMemcpyHostToDevice));
     s->sort_pid = nullptr;
     s->pcap = cap;
     invalidate_graph(s);
@@ -770,6 +781,10 @@ int remove_id_ranges(nxm_state* s, std::vector<uint2> ranges) {
         k_rm_move<<<ntiles, 256, 0, s->stream>>>(n0, s->kin, s->def, s->pstate, pid, d_r, d_cum, nr, s->d_tiles,
                                                  s->kin_alt, s->def_alt, s->pstate_alt, s->pid_alt);
         s->launches += 3;
+        if (s->scene_blocks) {  // the per-id scene index follows the ids
+            k_rm_ids<<<grid_for_n(s, n0), 256, 0, s->stream>>>(n0, s->d_pscene, d_r, d_cum, nr, s->d_pscene_alt);
+            s->launches += 1;
+        }
         e = cudaGetLastError();
     }
     if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
@@ -777,25 +792,18 @@ int remove_id_ranges(nxm_state* s, std::vector<uint2> ranges) {
     if (d_cum) cudaFree(d_cum);
     NXM_TRY(e);
     swap_buffers(s);  // the compacted records (and, when permuted, their ids) are current
-    for (size_t i = rr.size(); i-- > 0;) {
-        auto erase = [&](auto& v) { v.erase(v.begin() + rr[i].x, v.begin() + rr[i].y); };
-        erase(s->init_radius);
-        erase(s->phase);
-        erase(s->boundary_friction);
-        erase(s->group_id);
-        erase(s->slot2chunk);
-        erase(s->pscene);
+    if (s->scene_blocks) std::swap(s->d_pscene, s->d_pscene_alt);
+    if (s->chunks_used) {
+        for (size_t i = rr.size(); i-- > 0;)
+            s->slot2chunk.erase(s->slot2chunk.begin() + rr[i].x, s->slot2chunk.begin() + rr[i].y);
+        for (auto& c : s->chunks) c.second = 0;  // recount chunk sizes
+        for (uint32_t o : s->slot2chunk)
+            if (o != NONE) {
+                auto it = s->chunks.find(o);
+                if (it != s->chunks.end()) ++it->second;
+            }
     }
     s->n = n0 - removed;
-    if (s->n) NXM_TRY(cudaMemcpy(s->d_pscene, s->pscene.data(), 4 * (size_t)s->n, cudaMemcpyHostToDevice));
-    for (auto& c : s->chunks) {  // recount chunk sizes
-        c.second = 0;
-    }
-    for (uint32_t o : s->slot2chunk)
-        if (o != NONE) {
-            auto it = s->chunks.find(o);
-            if (it != s->chunks.end()) ++it->second;
-        }
     s->sort_pid = nullptr;
     s->params_dirty = true;
     return invalidate_codes(s);
@@ -813,6 +821,7 @@ int upload_particles(nxm_state* s, const nxm_particles_soa* p, uint32_t count) {
     std::vector<PDef> hd(count);
     std::vector<float4> hs(count);
     static const float I9[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+    uint32_t last_mid = 0;
     for (uint32_t i = 0; i < count; ++i) {
         const float* x = p->position + 3 * (size_t)i;
         const float* v = p->velocity ? p->velocity + 3 * (size_t)i : nullptr;
@@ -832,7 +841,9 @@ int upload_particles(nxm_state* s, const nxm_particles_soa* p, uint32_t count) {
         k.vgd = p->vel_grad_det ? p->vel_grad_det[i] : 0.f;
         k.pad1 = 0.f; k.pad2 = 0.f;
         const nxm_particle_model& m = p->model[i];
-        const uint32_t mid = material_of(s, m);
+        // consecutive particles mostly share a model: look up only on a change
+        if (i == 0 || std::memcmp(&m, &p->model[i - 1], sizeof(m)) != 0) last_mid = material_of(s, m);
+        const uint32_t mid = last_mid;
         PDef& d = hd[i];
         d.f00 = F[0]; d.f10 = F[1]; d.f20 = F[2];
         d.f01 = F[3]; d.f11 = F[4]; d.f21 = F[5];
@@ -844,13 +855,12 @@ int upload_particles(nxm_state* s, const nxm_particles_soa* p, uint32_t count) {
         float st[4] = {0, 0, 0, 0};
         for (int w = 0; w < ns; ++w) st[w] = bits_f(m.data[w]);
         hs[i] = make_float4(st[0], st[1], st[2], st[3]);
-        s->init_radius.push_back(p->init_radius ? p->init_radius[i] : 0.f);
-        s->phase.push_back(p->phase ? p->phase[i] : 1.f);
-        s->boundary_friction.push_back(p->boundary_friction ? p->boundary_friction[i] : 1.f);
-        s->group_id.push_back(p->group_id ? p->group_id[i] : 0u);
-        s->slot2chunk.push_back(NONE);
-        s->pscene.push_back(0u);
     }
+    auto append = [count](auto& v, const auto* src, auto dflt) {
+        if (src) v.insert(v.end(), src, src + count);
+        else v.insert(v.end(), count, dflt);
+    };
+    if (s->chunks_used) s->slot2chunk.insert(s->slot2chunk.end(), count, NONE);
     rc = sync_materials(s);
     if (rc) return rc;
     NXM_TRY(cudaMemcpyAsync(s->kin + s->n, hk.data(), sizeof(PKin) * count, cudaMemcpyHostToDevice, s->stream));
@@ -1239,11 +1249,13 @@ int nxm_state_set_deterministic(nxm_state* s, int enabled) {
 
 int nxm_particles_append_soa(nxm_state* s, const nxm_particles_soa* p, uint32_t count) {
     if (!s) return NXM_E_INVALID;
+    if (s->scene_blocks) return NXM_E_INVALID;  // in scene mode particles change through the scene calls
     return upload_particles(s, p, count);
 }
 
 int nxm_particles_append(nxm_state* s, const nxm_particle* particles, uint32_t count) {
     if (!s || (count && !particles)) return NXM_E_INVALID;
+    if (s->scene_blocks) return NXM_E_INVALID;  // in scene mode particles change through the scene calls
     if (count == 0) return NXM_OK;
     std::vector<float> pos(3 * (size_t)count), vel(3 * (size_t)count), F(9 * (size_t)count), A(9 * (size_t)count);
     std::vector<float> vgd(count), v0(count), rad(count), mass(count), damp(count), phase(count), bf(count);
@@ -1323,9 +1335,9 @@ static int rebuild_scene_colliders(nxm_state* s) {
     return install_colliders(s, dc, tri.data());
 }
 
-int nxm_scene_add(nxm_state* s, const nxm_particle* particles, uint32_t count, const nxm_collider* colliders,
+int nxm_scene_add(nxm_state* s, const nxm_particles_soa* particles, uint32_t count, const nxm_collider* colliders,
                   uint32_t num_colliders, const float* tri_vertices, uint32_t num_triangles, uint32_t* scene) {
-    if (!s || !scene || !s->scene_blocks || (count && !particles)) return NXM_E_INVALID;
+    if (!s || !scene || !s->scene_blocks || (count && (!particles || !particles->position))) return NXM_E_INVALID;
     if (num_colliders > (uint32_t)MAX_COLLIDERS || (num_colliders && !colliders)) return NXM_E_INVALID;
     for (uint32_t i = 0; i < num_colliders; ++i) {
         DevCollider d;
@@ -1335,20 +1347,21 @@ int nxm_scene_add(nxm_state* s, const nxm_particle* particles, uint32_t count, c
     // every particle's block (and its +1 neighbours) must stay inside the scene's key region
     const float bw = 4.0f * s->dx;
     const int M = s->scene_margin, S = (int)s->scene_blocks;
-    for (uint32_t i = 0; i < count; ++i)
-        for (int k = 0; k < 3; ++k) {
-            const float b = std::floor(particles[i].position[k] / bw);
-            if (!(b >= (float)(1 - M) && b <= (float)(S - M - 3))) return NXM_E_INVALID;
-        }
+    for (size_t i = 0; i < 3 * (size_t)count; ++i) {
+        const float b = std::floor(particles->position[i] / bw);
+        if (!(b >= (float)(1 - M) && b <= (float)(S - M - 3))) return NXM_E_INVALID;
+    }
     uint32_t slot = 0;
     while (slot < s->scenes.size() && s->scenes[slot].live) ++slot;
     if (slot == s->scenes.size()) return NXM_E_CAPACITY;
     const uint32_t first = s->n;
-    int rc = nxm_particles_append(s, particles, count);
+    int rc = count ? upload_particles(s, particles, count) : NXM_OK;
     if (rc) return rc;
-    std::fill(s->pscene.begin() + first, s->pscene.end(), slot);
-    if (count)
-        NXM_TRY(cudaMemcpy(s->d_pscene + first, s->pscene.data() + first, 4 * (size_t)count, cudaMemcpyHostToDevice));
+    if (count) {
+        k_fill<<<grid_for_n(s, count), 256, 0, s->stream>>>(s->d_pscene + first, slot, count);
+        s->launches += 1;
+        NXM_TRY(cudaGetLastError());
+    }
     nxm_state::Scene& sc = s->scenes[slot];
     sc.live = true;
     sc.first = first;
@@ -1410,7 +1423,11 @@ int nxm_read_positions_range(nxm_state* s, uint32_t first, uint32_t count, float
 // ---- particle chunks (NexusState, src/state.rs:665-774) ---------------------
 
 int nxm_chunk_add(nxm_state* s, const nxm_particle* particles, uint32_t count, uint32_t* chunk) {
-    if (!s || !chunk) return NXM_E_INVALID;
+    if (!s || !chunk || s->scene_blocks) return NXM_E_INVALID;
+    if (!s->chunks_used) {
+        s->slot2chunk.assign(s->n, NONE);
+        s->chunks_used = true;
+    }
     const uint32_t n0 = s->n;
     int rc = nxm_particles_append(s, particles, count);
     if (rc) return rc;
@@ -1474,13 +1491,15 @@ int nxm_chunk_len(const nxm_state* s, uint32_t chunk, uint32_t* len) {
 
 int nxm_chunk_of_particles(const nxm_state* s, uint32_t* out) {
     if (!s || (s->n && !out)) return NXM_E_INVALID;
-    std::copy(s->slot2chunk.begin(), s->slot2chunk.end(), out);
+    if (!s->chunks_used) std::fill(out, out + s->n, NONE);
+    else std::copy(s->slot2chunk.begin(), s->slot2chunk.end(), out);
     return NXM_OK;
 }
 
 int nxm_particles_swap_remove(nxm_state* s, const uint32_t* slots, uint32_t count, uint32_t* remaps,
                               uint32_t* num_remaps) {
     if (!s || (count && !slots)) return NXM_E_INVALID;
+    if (s->scene_blocks) return NXM_E_INVALID;  // in scene mode particles change through the scene calls
     int rc = canonicalize(s);
     if (rc) return rc;
     s->sort_pid = nullptr;
@@ -1500,11 +1519,7 @@ int nxm_particles_swap_remove(nxm_state* s, const uint32_t* slots, uint32_t coun
     for (uint32_t slot : t) {
         const uint32_t last = n - 1;
         if (slot != last) {
-            s->init_radius[slot] = s->init_radius[last];
-            s->phase[slot] = s->phase[last];
-            s->boundary_friction[slot] = s->boundary_friction[last];
-            s->group_id[slot] = s->group_id[last];
-            s->slot2chunk[slot] = s->slot2chunk[last];
+            if (s->chunks_used) s->slot2chunk[slot] = s->slot2chunk[last];
             if (remaps && nr < count) {
                 remaps[2 * nr] = last;
                 remaps[2 * nr + 1] = slot;
@@ -1545,11 +1560,7 @@ int nxm_particles_swap_remove(nxm_state* s, const uint32_t* slots, uint32_t coun
         cudaFree(d_pairs);
         NXM_TRY(e);
     }
-    s->init_radius.resize(n1);
-    s->phase.resize(n1);
-    s->boundary_friction.resize(n1);
-    s->group_id.resize(n1);
-    s->slot2chunk.resize(n1);
+    if (s->chunks_used) s->slot2chunk.resize(n1);
     s->n = n1;
     if (num_remaps) *num_remaps = nr;
     s->params_dirty = true;
@@ -1558,6 +1569,7 @@ int nxm_particles_swap_remove(nxm_state* s, const uint32_t* slots, uint32_t coun
 
 int nxm_particles_shift_remove(nxm_state* s, uint32_t start, uint32_t end) {
     if (!s || start > end || end > s->n) return NXM_E_INVALID;
+    if (s->scene_blocks) return NXM_E_INVALID;  // in scene mode particles change through the scene calls
     if (start == end) return NXM_OK;
     return remove_id_ranges(s, {make_uint2(start, end)});
 }

@@ -93,7 +93,7 @@ SIGNATURES = {
     "nxm_state_estimate_timestep_bound": (C.c_int, [_vp, _f, _u]),
     "nxm_state_enable_scenes": (C.c_int, [_vp, C.c_uint32]),
     "nxm_scene_capacity": (C.c_uint32, [_vp]),
-    "nxm_scene_add": (C.c_int, [_vp, _vp, C.c_uint32, _vp, C.c_uint32, _f, C.c_uint32, _u]),
+    "nxm_scene_add": (C.c_int, [_vp, C.POINTER(ParticlesSoAC), C.c_uint32, _vp, C.c_uint32, _f, C.c_uint32, _u]),
     "nxm_scene_remove": (C.c_int, [_vp, _u, C.c_uint32]),
     "nxm_scene_range": (C.c_int, [_vp, C.c_uint32, _u, _u]),
     "nxm_scene_set_collider_velocity": (C.c_int, [_vp, C.c_uint32, C.c_uint32, _f, _f]),
@@ -230,21 +230,24 @@ class MpmState:
         _check(self.lib.nxm_state_set_deterministic(self.h, int(enabled)), "set_deterministic")
 
     # -- particles --------------------------------------------------------------
-    def append(self, batch: ParticleBatch):
-        """``GpuParticles::append`` (src_mpm/solver/particle.rs:533-565), bulk SoA form."""
-        keep = {}
-
+    @staticmethod
+    def _soa(batch: ParticleBatch, keep: dict):
         def arr(name, dtype):
             a = np.ascontiguousarray(getattr(batch, name), dtype=dtype)
             keep[name] = a
             return a.ctypes.data_as(C.c_void_p)
 
-        soa = ParticlesSoAC(
+        return ParticlesSoAC(
             arr("pos", np.float32), arr("vel", np.float32), arr("def_grad", np.float32), arr("aff", np.float32),
             arr("vel_grad_det", np.float32), arr("init_volume", np.float32), arr("init_radius", np.float32),
             arr("mass", np.float32), arr("damping", np.float32), arr("phase", np.float32),
             arr("boundary_friction", np.float32), arr("group_id", np.uint32), arr("enabled", np.uint32),
             arr("fixed", np.uint32), arr("model", np.uint32))
+
+    def append(self, batch: ParticleBatch):
+        """``GpuParticles::append`` (src_mpm/solver/particle.rs:533-565), bulk SoA form."""
+        keep = {}
+        soa = self._soa(batch, keep)
         _check(self.lib.nxm_particles_append_soa(self.h, C.byref(soa), batch.n), "append")
 
     # -- batched scenes ------------------------------------------------------------------
@@ -255,13 +258,14 @@ class MpmState:
         return int(self.lib.nxm_scene_capacity(self.h))
 
     def add_scene(self, batch: ParticleBatch, colliders=None, tri_vertices=None) -> int:
-        rec = particle_records(batch)
+        keep = {}
+        soa = self._soa(batch, keep)
         cols = np.ascontiguousarray(colliders if colliders is not None else np.zeros(0, COLLIDER_DTYPE),
                                     dtype=COLLIDER_DTYPE)
         tri = (np.zeros((0,), np.float32) if tri_vertices is None
                else np.ascontiguousarray(tri_vertices, np.float32).reshape(-1))
         sid = C.c_uint32()
-        _check(self.lib.nxm_scene_add(self.h, rec.ctypes.data_as(C.c_void_p), batch.n,
+        _check(self.lib.nxm_scene_add(self.h, C.byref(soa), batch.n,
                                       cols.ctypes.data_as(C.c_void_p), len(cols), _p(tri), tri.size // 9,
                                       C.byref(sid)), "scene_add")
         return sid.value

@@ -98,6 +98,12 @@ class MpmServer:
             g = self.groups[key] = _Group(key, self.particles_capacity, self.grid_capacity, sb, self.deterministic)
         return g
 
+    def prepare(self, scenes_):
+        """Creates the batched states the given scenes would use (device
+        allocation happens here rather than at a request's admission)."""
+        for sc in scenes_:
+            self._group(sc)
+
     def _fits(self, sc: Scene, g: _Group) -> bool:
         return (self.in_use + footprint(sc) <= self.budget and g.particles + sc.n <= self.particles_capacity
                 and g.grid + sc.grid_capacity <= self.grid_capacity)
