@@ -46,6 +46,10 @@ UNIT = "particle-steps/s"
 # read; Drucker-Prager state, 3 floats, read and written for sand).
 B_ALG_ELASTIC = 204
 B_ALG_SAND = 228
+# DRAM bytes read + written per step by the two transfer kernels (77 % of the
+# step) on the sand_water scene, from one ncu capture of the full scene
+# (k_p2g 182 MB + k_g2p_update 614 MB; the sort and grid kernels are not included).
+TRAFFIC_PER_STEP = 174.2e6 + 8.0e6 + 317.5e6 + 296.5e6
 
 
 def b_alg_per_particle(model_tags: np.ndarray) -> float:
@@ -446,8 +450,8 @@ def main():
     ap.add_argument("--batched-scenes", type=int, default=256)
     ap.add_argument("--plain-steps", type=int, default=10)
     ap.add_argument("--serving-requests", type=int, default=200, help="0: skip the serving measurement")
-    ap.add_argument("--traffic", type=float, default=None,
-                    help="DRAM bytes per step from an ncu capture (see profiles/)")
+    ap.add_argument("--traffic", type=float, default=TRAFFIC_PER_STEP,
+                    help="DRAM bytes per step from an ncu capture (profiles/k_p2g_k_g2p_update_sand_water_2M.md)")
     args = ap.parse_args()
     if args.impl == "reference":
         # CPU baseline arm: rank 0 alone runs it; other ranks exit without work.
