@@ -201,9 +201,18 @@ NXM_API int nxm_state_set_collider_velocity(nxm_state* state, uint32_t index, co
 /* Reads collider i's pose: quaternion x,y,z,w then translation (7 floats). */
 NXM_API int nxm_state_read_collider_pose(nxm_state* state, uint32_t index, float out[7]);
 
-/* MpmState::use_cpic (src_mpm/pipeline.rs:69).  CPIC coupling is not built
- * yet: enabling it returns NXM_E_UNSUPPORTED. */
+/* MpmState::use_cpic (src_mpm/pipeline.rs:69): CPIC coupling with the
+ * colliders (node and particle distance fields, compatible / incompatible
+ * P2G and G2P, penetration reprojection and penalty; two-way impulses off as
+ * in the reference build).  Built for analytic colliders (ball, cuboid,
+ * capsule): with a trimesh collider, enabling returns NXM_E_UNSUPPORTED (the
+ * reference samples rigid particles on meshes for it).  CPIC steps run the
+ * gather-form transfers with particles in id order. */
 NXM_API int nxm_state_set_use_cpic(nxm_state* state, int enabled);
+/* Particle Cdf (solver/particle.rs:35-50) of every particle: normal xyz,
+ * signed distance, rigid velocity xyz, affinity bits (u32 bits), 8 floats
+ * each; synchronizes. */
+NXM_API int nxm_read_cdf(nxm_state* state, float* out);
 
 /* Deterministic mode: canonical sort order (ascending id inside every sort
  * bucket) and the reference's atomic-free, gather-form P2G with its

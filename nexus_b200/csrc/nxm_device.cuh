@@ -594,6 +594,50 @@ __device__ __forceinline__ bool trimesh_project_local(const DevTri* __restrict__
     return true;
 }
 
+// CPIC affinity bits (grid/grid.rs:593-645): bit i = affinity to collider
+// i, bit 16 + i = on its inside; two sets agree if every common affinity has
+// the same sign.
+__device__ __forceinline__ bool aff_compatible(uint32_t a, uint32_t b) {
+    const uint32_t common = a & b & 0x0000FFFFu;
+    return ((a >> 16) & common) == ((b >> 16) & common);
+}
+
+// Inverse (into out) and determinant of a 4x4 matrix m[row][col] from its
+// 2x2 minors (Laplace expansion along the first two rows).
+__device__ __forceinline__ float inv4(const float (&m)[4][4], float (&out)[4][4]) {
+    const float s0 = m[0][0] * m[1][1] - m[1][0] * m[0][1];
+    const float s1 = m[0][0] * m[1][2] - m[1][0] * m[0][2];
+    const float s2 = m[0][0] * m[1][3] - m[1][0] * m[0][3];
+    const float s3 = m[0][1] * m[1][2] - m[1][1] * m[0][2];
+    const float s4 = m[0][1] * m[1][3] - m[1][1] * m[0][3];
+    const float s5 = m[0][2] * m[1][3] - m[1][2] * m[0][3];
+    const float c5 = m[2][2] * m[3][3] - m[3][2] * m[2][3];
+    const float c4 = m[2][1] * m[3][3] - m[3][1] * m[2][3];
+    const float c3 = m[2][1] * m[3][2] - m[3][1] * m[2][2];
+    const float c2 = m[2][0] * m[3][3] - m[3][0] * m[2][3];
+    const float c1 = m[2][0] * m[3][2] - m[3][0] * m[2][2];
+    const float c0 = m[2][0] * m[3][1] - m[3][0] * m[2][1];
+    const float det = s0 * c5 - s1 * c4 + s2 * c3 + s3 * c2 - s4 * c1 + s5 * c0;
+    const float id = 1.0f / det;
+    out[0][0] = (m[1][1] * c5 - m[1][2] * c4 + m[1][3] * c3) * id;
+    out[0][1] = (-m[0][1] * c5 + m[0][2] * c4 - m[0][3] * c3) * id;
+    out[0][2] = (m[3][1] * s5 - m[3][2] * s4 + m[3][3] * s3) * id;
+    out[0][3] = (-m[2][1] * s5 + m[2][2] * s4 - m[2][3] * s3) * id;
+    out[1][0] = (-m[1][0] * c5 + m[1][2] * c2 - m[1][3] * c1) * id;
+    out[1][1] = (m[0][0] * c5 - m[0][2] * c2 + m[0][3] * c1) * id;
+    out[1][2] = (-m[3][0] * s5 + m[3][2] * s2 - m[3][3] * s1) * id;
+    out[1][3] = (m[2][0] * s5 - m[2][2] * s2 + m[2][3] * s1) * id;
+    out[2][0] = (m[1][0] * c4 - m[1][1] * c2 + m[1][3] * c0) * id;
+    out[2][1] = (-m[0][0] * c4 + m[0][1] * c2 - m[0][3] * c0) * id;
+    out[2][2] = (m[3][0] * s4 - m[3][1] * s2 + m[3][3] * s0) * id;
+    out[2][3] = (-m[2][0] * s4 + m[2][1] * s2 - m[2][3] * s0) * id;
+    out[3][0] = (-m[1][0] * c3 + m[1][1] * c1 - m[1][2] * c0) * id;
+    out[3][1] = (m[0][0] * c3 - m[0][1] * c1 + m[0][2] * c0) * id;
+    out[3][2] = (-m[3][0] * s3 + m[3][1] * s1 - m[3][2] * s0) * id;
+    out[3][3] = (m[2][0] * s3 - m[2][1] * s1 + m[2][2] * s0) * id;
+    return det;
+}
+
 __device__ __forceinline__ v3 bc_project(uint32_t ty, float friction, v3 vel, v3 n) {
     if (ty == BC_STICK) return splat(0.f);
     if (ty == BC_SLIP) {

@@ -46,6 +46,13 @@ struct DevPtrs {
     // [x, x + y) in `colliders`
     const uint32_t* pscene;
     const uint2* scene_cols;
+    // CPIC (analytic colliders): node distance field (distance bits, affinity
+    // + sign bits, closest collider, unused), the nodes' incompatible
+    // momentum / velocity + mass, and per particle id 3 float4: normal +
+    // signed distance, rigid velocity + affinity bits, boundary friction.
+    uint4* ncdf;
+    float4* nodes_inc;
+    float4* pcdf;
 };
 
 constexpr uint32_t kScanTile = 1024;  // blocks per scan tile
@@ -82,6 +89,9 @@ namespace exact {
 void launch_p2g_gather(const DevPtrs& P, const LaunchCfg& c, cudaStream_t s);
 // Min over particles of the CFL bound into counters->dt_bound (reset by the caller).
 void launch_timestep_bound(const DevPtrs& P, const LaunchCfg& c, cudaStream_t s);
+// CPIC distance fields: per node (analytic colliders), then per particle.
+void launch_grid_update_cdf(const DevPtrs& P, const LaunchCfg& c, cudaStream_t s);
+void launch_g2p_cdf(const DevPtrs& P, const LaunchCfg& c, cudaStream_t s);
 void launch_grid_update(const DevPtrs& P, const LaunchCfg& c, cudaStream_t s);
 void launch_g2p_update(const DevPtrs& P, const LaunchCfg& c, cudaStream_t s);
 }  // namespace exact

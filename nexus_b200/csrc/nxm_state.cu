@@ -221,23 +221,30 @@ __global__ void __launch_bounds__(256) k_rm_move(uint32_t n, const PKin* __restr
     }
 }
 
-// Id-indexed arrays follow a range removal: entry id goes to its new id.
-__global__ void k_rm_ids(uint32_t n, const uint32_t* __restrict__ src, const uint2* __restrict__ ranges,
-                         const uint32_t* __restrict__ cum, uint32_t nr, uint32_t* __restrict__ dst) {
+// Id-indexed arrays (K elements per id) follow a range removal: entry id goes to its new id.
+template <class T, int K>
+__global__ void k_rm_ids(uint32_t n, const T* __restrict__ src, const uint2* __restrict__ ranges,
+                         const uint32_t* __restrict__ cum, uint32_t nr, T* __restrict__ dst) {
     for (uint32_t id = blockIdx.x * blockDim.x + threadIdx.x; id < n; id += gridDim.x * blockDim.x)
-        if (!removed_id(id, ranges, nr)) dst[new_id_of(id, ranges, cum, nr)] = src[id];
+        if (!removed_id(id, ranges, nr)) {
+            const uint32_t to = new_id_of(id, ranges, cum, nr);
+#pragma unroll
+            for (int k = 0; k < K; ++k) dst[(size_t)K * to + k] = src[(size_t)K * id + k];
+        }
 }
 
 // Swap-removal data movement: record pairs[i].y moves to slot pairs[i].x.
 // Every source is at or above the new length and every destination below it,
 // so the moves are independent.
 __global__ void k_move_records(PKin* __restrict__ kin, PDef* __restrict__ def, float4* __restrict__ pstate,
-                               const uint2* __restrict__ pairs, uint32_t count) {
+                               float4* __restrict__ pcdf, const uint2* __restrict__ pairs, uint32_t count) {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
         const uint2 m = pairs[i];
         kin[m.x] = kin[m.y];
         def[m.x] = def[m.y];
         pstate[m.x] = pstate[m.y];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) pcdf[3u * m.x + k] = pcdf[3u * m.y + k];
     }
 }
 
@@ -343,6 +350,10 @@ struct nxm_state {
     uint32_t scene_cells[3] = {0, 0, 0};
     std::vector<Scene> scenes;
     uint32_t* d_pscene = nullptr;       // scene of each particle id (device)
+    float4* d_pcdf = nullptr;           // CPIC particle fields, 3 float4 per particle id
+    float4* d_pcdf_alt = nullptr;
+    uint4* d_ncdf = nullptr;            // CPIC node distance fields (allocated with CPIC on)
+    float4* d_nodes_inc = nullptr;      // CPIC incompatible node fields
     uint32_t* d_pscene_alt = nullptr;
     uint2* d_scene_cols = nullptr;      // per scene slot: its colliders in the table
     uint32_t* d_tiles = nullptr;        // compaction scratch, one word per 1024 particles
@@ -369,7 +380,9 @@ struct nxm_state {
 
 namespace {
 
-bool reorders(const nxm_state* s) { return !s->deterministic; }
+// Fast mode keeps the records in block order; the deterministic and CPIC
+// steps work in place, in id order (CPIC's per-particle fields are id-indexed).
+bool reorders(const nxm_state* s) { return !s->deterministic && !s->use_cpic; }
 
 DevPtrs dev_ptrs(nxm_state* s) {
     DevPtrs P{};
@@ -392,6 +405,9 @@ DevPtrs dev_ptrs(nxm_state* s) {
     P.materials = s->d_materials;
     P.colliders = s->d_colliders;
     P.pscene = s->d_pscene;
+    P.ncdf = s->d_ncdf;
+    P.nodes_inc = s->d_nodes_inc;
+    P.pcdf = s->d_pcdf;
     P.scene_cols = s->d_scene_cols;
     P.tris = s->d_tris;
     P.bvh = s->d_bvh;
@@ -467,8 +483,19 @@ int canonicalize(nxm_state* s) {
 }
 
 int free_grid(nxm_state* s) {
+    dfree(s->d_ncdf); dfree(s->d_nodes_inc);
     dfree(s->hkey); dfree(s->hval); dfree(s->bvid); dfree(s->first); dfree(s->nprim); dfree(s->nwx);
     dfree(s->cursors); dfree(s->nbh); dfree(s->nodes); dfree(s->scan_tmp); dfree(s->tile_sums);
+    return NXM_OK;
+}
+
+// CPIC node fields, sized by the grid capacity.
+int alloc_cpic_grid(nxm_state* s) {
+    dfree(s->d_ncdf);
+    dfree(s->d_nodes_inc);
+    NXM_TRY(dalloc(&s->d_ncdf, (size_t)s->block_cap * 64));
+    NXM_TRY(dalloc(&s->d_nodes_inc, (size_t)s->block_cap * 64));
+    invalidate_graph(s);
     return NXM_OK;
 }
 
@@ -488,6 +515,10 @@ int alloc_grid(nxm_state* s, uint32_t grid_capacity) {
     NXM_TRY(dalloc(&s->scan_tmp, s->block_cap));
     NXM_TRY(dalloc(&s->tile_sums, s->block_cap / kScanTile + 2));
     NXM_TRY(cudaMemsetAsync(s->hkey, 0xFF, sizeof(uint32_t) * s->hash_cap, s->stream));
+    if (s->use_cpic) {
+        int rc = alloc_cpic_grid(s);
+        if (rc) return rc;
+    }
     invalidate_graph(s);
     s->params_dirty = true;
     return NXM_OK;
@@ -501,6 +532,7 @@ struct ParticleBuffers {
     uint32_t *pid = nullptr, *pid_alt = nullptr, *phdr = nullptr, *sorted = nullptr, *pscene = nullptr,
              *pscene_alt = nullptr, *tiles = nullptr;
     uint2* pcode = nullptr;
+    float4 *pcdf = nullptr, *pcdf_alt = nullptr;
     cudaError_t alloc(uint32_t cap) {
         cudaError_t e = cudaSuccess;
         auto a = [&](auto** p, size_t count) {
@@ -512,6 +544,8 @@ struct ParticleBuffers {
         a(&sorted, (size_t)cap * 8);
         a(&pscene, cap);
         a(&pscene_alt, cap);
+        a(&pcdf, 3 * (size_t)cap);
+        a(&pcdf_alt, 3 * (size_t)cap);
         a(&tiles, cap / 1024 + 2);
         return e;
     }
@@ -519,13 +553,14 @@ struct ParticleBuffers {
     ~ParticleBuffers() {
         dfree(kin); dfree(def); dfree(pstate); dfree(kin_alt); dfree(def_alt); dfree(pstate_alt);
         dfree(pid); dfree(pid_alt); dfree(pcode); dfree(phdr); dfree(sorted); dfree(pscene); dfree(pscene_alt); dfree(tiles);
+        dfree(pcdf); dfree(pcdf_alt);
     }
 };
 
 void free_particles(nxm_state* s) {
     dfree(s->kin); dfree(s->def); dfree(s->pstate); dfree(s->kin_alt); dfree(s->def_alt); dfree(s->pstate_alt);
     dfree(s->pid); dfree(s->pid_alt); dfree(s->pcode); dfree(s->phdr); dfree(s->sorted);
-    dfree(s->d_pscene); dfree(s->d_pscene_alt); dfree(s->d_tiles);
+    dfree(s->d_pscene); dfree(s->d_pscene_alt); dfree(s->d_tiles); dfree(s->d_pcdf); dfree(s->d_pcdf_alt);
 }
 
 int reserve_particles(nxm_state* s, uint32_t need) {
@@ -540,6 +575,7 @@ int reserve_particles(nxm_state* s, uint32_t need) {
         NXM_TRY(cudaMemcpyAsync(t.def, s->def, sizeof(PDef) * s->n, cudaMemcpyDeviceToDevice, s->stream));
         NXM_TRY(cudaMemcpyAsync(t.pstate, s->pstate, sizeof(float4) * s->n, cudaMemcpyDeviceToDevice, s->stream));
         NXM_TRY(cudaMemcpyAsync(t.pscene, s->d_pscene, 4 * (size_t)s->n, cudaMemcpyDeviceToDevice, s->stream));
+        NXM_TRY(cudaMemcpyAsync(t.pcdf, s->d_pcdf, 48 * (size_t)s->n, cudaMemcpyDeviceToDevice, s->stream));
     }
     NXM_TRY(cudaStreamSynchronize(s->stream));
     free_particles(s);
@@ -548,6 +584,7 @@ int reserve_particles(nxm_state* s, uint32_t need) {
     s->pid = t.pid; s->pid_alt = t.pid_alt;
     s->pcode = t.pcode; s->phdr = t.phdr; s->sorted = t.sorted;
     s->d_pscene = t.pscene; s->d_pscene_alt = t.pscene_alt; s->d_tiles = t.tiles;
+    s->d_pcdf = t.pcdf; s->d_pcdf_alt = t.pcdf_alt;
     t.release();
     s->sort_pid = nullptr;
     s->pcap = cap;
@@ -638,18 +675,25 @@ int enqueue_step(nxm_state* s, cudaStream_t st, cudaEvent_t* ev /* 5 events or n
     const bool has_col = !s->colliders.empty();
     if (ev) cudaEventRecord(ev[0], st);
     if (has_col) { fast::launch_colliders_begin(P, st); ++k; }
-    fast::launch_sort(P, c, /*with_extras=*/s->deterministic, /*canonical=*/s->deterministic, st);
+    // CPIC runs the reference's gather-form transfers, so it needs the sort's extras
+    const bool exact_path = s->deterministic || s->use_cpic;
+    fast::launch_sort(P, c, /*with_extras=*/exact_path, /*canonical=*/s->deterministic, st);
     k += sort_launches(s->deterministic);
+    if (s->use_cpic) {  // node and particle distance fields (pipeline.rs:433-460)
+        exact::launch_grid_update_cdf(P, c, st);
+        exact::launch_g2p_cdf(P, c, st);
+        k += 2;
+    }
     if (ev) cudaEventRecord(ev[1], st);
-    if (s->deterministic) exact::launch_p2g_gather(P, c, st);
+    if (exact_path) exact::launch_p2g_gather(P, c, st);
     else fast::launch_p2g(P, c, st);
     k += kP2gLaunches;
     if (ev) cudaEventRecord(ev[2], st);
-    if (s->deterministic) exact::launch_grid_update(P, c, st);
+    if (exact_path) exact::launch_grid_update(P, c, st);
     else fast::launch_grid_update(P, c, st);
     k += kGridLaunches;
     if (ev) cudaEventRecord(ev[3], st);
-    if (s->deterministic) exact::launch_g2p_update(P, c, st);
+    if (exact_path) exact::launch_g2p_update(P, c, st);
     else fast::launch_g2p_update(P, c, st);
     k += kG2pLaunches;
     if (has_col) { fast::launch_colliders_end(P, st); ++k; }
@@ -782,9 +826,12 @@ int remove_id_ranges(nxm_state* s, std::vector<uint2> ranges) {
                                                  s->kin_alt, s->def_alt, s->pstate_alt, s->pid_alt);
         s->launches += 3;
         if (s->scene_blocks) {  // the per-id scene index follows the ids
-            k_rm_ids<<<grid_for_n(s, n0), 256, 0, s->stream>>>(n0, s->d_pscene, d_r, d_cum, nr, s->d_pscene_alt);
+            k_rm_ids<uint32_t, 1><<<grid_for_n(s, n0), 256, 0, s->stream>>>(n0, s->d_pscene, d_r, d_cum, nr,
+                                                                             s->d_pscene_alt);
             s->launches += 1;
         }
+        k_rm_ids<float4, 3><<<grid_for_n(s, n0), 256, 0, s->stream>>>(n0, s->d_pcdf, d_r, d_cum, nr, s->d_pcdf_alt);
+        s->launches += 1;
         e = cudaGetLastError();
     }
     if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
@@ -793,6 +840,7 @@ int remove_id_ranges(nxm_state* s, std::vector<uint2> ranges) {
     NXM_TRY(e);
     swap_buffers(s);  // the compacted records (and, when permuted, their ids) are current
     if (s->scene_blocks) std::swap(s->d_pscene, s->d_pscene_alt);
+    std::swap(s->d_pcdf, s->d_pcdf_alt);
     if (s->chunks_used) {
         for (size_t i = rr.size(); i-- > 0;)
             s->slot2chunk.erase(s->slot2chunk.begin() + rr[i].x, s->slot2chunk.begin() + rr[i].y);
@@ -866,6 +914,12 @@ int upload_particles(nxm_state* s, const nxm_particles_soa* p, uint32_t count) {
     NXM_TRY(cudaMemcpyAsync(s->kin + s->n, hk.data(), sizeof(PKin) * count, cudaMemcpyHostToDevice, s->stream));
     NXM_TRY(cudaMemcpyAsync(s->def + s->n, hd.data(), sizeof(PDef) * count, cudaMemcpyHostToDevice, s->stream));
     NXM_TRY(cudaMemcpyAsync(s->pstate + s->n, hs.data(), sizeof(float4) * count, cudaMemcpyHostToDevice, s->stream));
+    {  // CPIC fields start empty; boundary friction (default 1) scales the colliders' friction there
+        std::vector<float4> hc(3 * (size_t)count, make_float4(0.f, 0.f, 0.f, 0.f));
+        for (uint32_t i = 0; i < count; ++i) hc[3 * (size_t)i + 2].x = p->boundary_friction ? p->boundary_friction[i] : 1.f;
+        NXM_TRY(cudaMemcpyAsync(s->d_pcdf + 3 * (size_t)s->n, hc.data(), sizeof(float4) * hc.size(),
+                                cudaMemcpyHostToDevice, s->stream));
+    }
     if (s->permuted) {  // appended particles sit at slots == their ids
         k_iota<<<grid_for_n(s, count), 256, 0, s->stream>>>(s->pid + s->n, s->n, count);
         s->launches += 1;
@@ -1205,6 +1259,7 @@ int nxm_state_set_colliders(nxm_state* s, const nxm_collider* cols, uint32_t nco
     for (uint32_t i = 0; i < ncol; ++i) {
         int rc = collider_from_abi(cols[i], tri, ntri, 0, dc[i]);
         if (rc) return rc;
+        if (s->use_cpic && dc[i].type == SHAPE_TRIMESH) return NXM_E_UNSUPPORTED;
     }
     return install_colliders(s, dc, tri);
 }
@@ -1230,10 +1285,25 @@ int nxm_state_read_collider_pose(nxm_state* s, uint32_t index, float out[7]) {
 
 int nxm_state_set_use_cpic(nxm_state* s, int enabled) {
     if (!s) return NXM_E_INVALID;
-    if (enabled) return NXM_E_UNSUPPORTED;
-    s->use_cpic = false;
+    if (enabled) {
+        for (const DevCollider& c : s->colliders)
+            if (c.type == SHAPE_TRIMESH) return NXM_E_UNSUPPORTED;  // trimesh CPIC needs rigid particles
+        int rc = canonicalize(s);  // CPIC steps in place, in id order
+        if (rc) return rc;
+        rc = alloc_cpic_grid(s);
+        if (rc) return rc;
+    }
+    if (s->use_cpic != (enabled != 0)) invalidate_graph(s);
+    s->use_cpic = enabled != 0;
     s->params_dirty = true;
     return NXM_OK;
+}
+
+int nxm_read_cdf(nxm_state* s, float* out) {
+    if (!s) return NXM_E_INVALID;
+    static const int off[8] = {0, 1, 2, 3, 4, 5, 6, 7};
+    if (s->permuted) return NXM_E_INVALID;  // the fields are id-indexed; CPIC keeps id order
+    return pack_read(s, s->d_pcdf, 48, off, 8, out);
 }
 
 int nxm_state_set_deterministic(nxm_state* s, int enabled) {
@@ -1551,7 +1621,7 @@ int nxm_particles_swap_remove(nxm_state* s, const uint32_t* slots, uint32_t coun
                                         s->stream);
         if (e == cudaSuccess) {
             k_move_records<<<grid_for_n(s, (uint32_t)pairs.size()), 256, 0, s->stream>>>(s->kin, s->def, s->pstate,
-                                                                                        d_pairs,
+                                                                                        s->d_pcdf, d_pairs,
                                                                                         (uint32_t)pairs.size());
             s->launches += 1;
             e = cudaGetLastError();

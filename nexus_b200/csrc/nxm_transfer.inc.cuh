@@ -11,6 +11,9 @@
 #ifndef NXM_FAST
 #error "define NXM_FAST (true: fast build, false: reference operation order)"
 #endif
+#ifndef NXM_CPIC
+#define NXM_CPIC 0  // 1: also build the CPIC branches (deterministic-build kernels only)
+#endif
 
 namespace nxm {
 namespace NXM_NS {
@@ -132,8 +135,27 @@ __global__ void __launch_bounds__(256) k_grid_update(DevPtrs P) {
             }
         }
         P.nodes[t] = make_float4(v.x, v.y, v.z, mass);
+#if NXM_CPIC
+        if (prm.use_cpic) {  // grid_update.rs:55-66: the incompatible field gets the same update
+            const float4 ni = P.nodes_inc[t];
+            const float mi = ni.w;
+            const float inv_mi = mi > 0.f ? 1.0f / mi : 0.0f;
+            v3 vi = (mk(ni.x, ni.y, ni.z) + g * (mi * dt)) * inv_mi;
+            vi = vclamp(vi, -lim, lim);
+            P.nodes_inc[t] = make_float4(vi.x, vi.y, vi.z, mi);
+        }
+#endif
     }
 }
+
+// CPIC context of one block for G2P: the incompatible velocities and node
+// distance fields of its 6x6x6 halo, and the colliders it sees.
+struct CpicCtx {
+    const float4* halo_inc;
+    const uint2* halo_cdf;  // affinity bits, closest collider
+    const DevCollider* cols;
+    uint32_t ncols;
+};
 
 // Velocity of shared-halo node t (t = x + 6 y + 36 z, x, y, z in [0, 6)) of
 // block b: node (x mod 4, ...) of the block itself or of one of its +1
@@ -154,7 +176,8 @@ __device__ __forceinline__ float4 halo_node(const DevPtrs& P, uint32_t b, uint32
 // particle (read from slot `src`, xm / vf = its first two kin words) to slot
 // `dst` of the output records, together with the block key of its new position.
 __device__ __forceinline__ void g2p_particle(const DevPtrs& P, const Params& prm, const float4* __restrict__ halo,
-                                             uint32_t src, uint32_t dst, float4 xm, float4 vf, int3 key_off) {
+                                             uint32_t src, uint32_t dst, float4 xm, float4 vf, int3 key_off,
+                                             const CpicCtx& cx) {
     const float dx = prm.dx, dt = prm.dt;
     const float inv_d = 4.0f / (dx * dx);
     float4* kr = reinterpret_cast<float4*>(&P.kin_out[dst]);
@@ -162,6 +185,22 @@ __device__ __forceinline__ void g2p_particle(const DevPtrs& P, const Params& prm
     const v3 pt = mk(xm.x, xm.y, xm.z);
     float mass = xm.w;
 
+#if NXM_CPIC
+    // particle Cdf (normal, signed distance, affinity) from this step's g2p_cdf pass
+    const bool cpic = prm.use_cpic != 0;
+    float4 crec0 = make_float4(0.f, 0.f, 0.f, 0.f), crec1 = crec0;
+    float bfric = 1.0f;
+    if (cpic) {
+        crec0 = P.pcdf[3u * src];
+        crec1 = P.pcdf[3u * src + 1u];
+        bfric = P.pcdf[3u * src + 2u].x;
+    }
+    const uint32_t paff = __float_as_uint(crec1.w);
+    const v3 pnormal = mk(crec0.x, crec0.y, crec0.z);
+    v3 rigid_vel = splat(0.f);
+#else
+    (void)cx;
+#endif
     // ---- G2P (g2p.rs:150-270)
     v3 velocity = splat(0.f);
     m3 grad = mzero();
@@ -208,15 +247,41 @@ __device__ __forceinline__ void g2p_particle(const DevPtrs& P, const Params& prm
         for (int i = 0; i < 27; ++i) {
             int sx, sy, sz;
             nbh_shift(i, sx, sy, sz);
-            const float4 h = halo[packed + (uint32_t)(sx + 6 * sy + 36 * sz)];
-            const v3 cv = mk(h.x, h.y, h.z);
+            const uint32_t hid = packed + (uint32_t)(sx + 6 * sy + 36 * sz);
+            const float4 h = halo[hid];
+            v3 cv = mk(h.x, h.y, h.z);
             const v3 dpt = ref + mk((float)sx, (float)sy, (float)sz) * dx;
+#if NXM_CPIC
+            if (cpic) {
+                // g2p.rs:206-235: an incompatible node gives its second velocity,
+                // projected by its closest body's boundary condition
+                const uint2 nc = cx.halo_cdf[hid];
+                if (!aff_compatible(paff, nc.x)) {
+                    const float4 hi = cx.halo_inc[hid];
+                    cv = mk(hi.x, hi.y, hi.z);
+                    if (nc.y != NONE) {
+                        const DevCollider& c = cx.cols[nc.y];
+                        const v3 cell_center = dpt + pt;
+                        const v3 bv = col_vel_at(c, cell_center);
+                        cv = bv + bc_project(c.bc_type, c.bc_friction * bfric, cv - bv, pnormal);
+                    }
+                }
+            }
+#endif
             const float weight = vget(w0, sx) * vget(w1, sy) * vget(w2, sz);
             velocity = velocity + cv * weight;
             grad = grad + outer(cv, dpt) * (weight * inv_d);
             vgd += weight * inv_d * dot(cv, dpt);
         }
+#if NXM_CPIC
+        if (cpic)  // g2p.rs:248-262: velocity of every body the particle has affinity with
+            for (uint32_t ic = 0; ic < 16u && ic < cx.ncols; ++ic)
+                if (paff & (1u << ic)) rigid_vel = rigid_vel + col_vel_at(cx.cols[ic], pt);
+#endif
     }
+#if NXM_CPIC
+    if (cpic) P.pcdf[3u * src + 1u] = make_float4(rigid_vel.x, rigid_vel.y, rigid_vel.z, crec1.w);
+#endif
 
     // ---- particle update (particle_update.rs:60-201, non-CPIC: Cdf = 0)
     const float4* dr = reinterpret_cast<const float4*>(&P.def[src]);
@@ -228,11 +293,21 @@ __device__ __forceinline__ void g2p_particle(const DevPtrs& P, const Params& prm
     const uint32_t tag = mat.tag;
 
     v3 v = velocity;
+#if NXM_CPIC
+    // particle_update.rs:98-102: reproject a penetrating particle
+    if (cpic && crec0.w < -0.05f * dx) v = rigid_vel + bc_project(BC_SLIP, 0.0f, v - rigid_vel, pnormal);
+#endif
     const float vl = length(v);
     if (vl > dx / dt) v = ((v / vl) * dx) / dt;
     v = v / (1.0f + damping * dt);
     if (flags & PFLAG_FIXED) v = splat(0.f);
     const v3 np_ = pt + v * dt;
+#if NXM_CPIC
+    if (cpic && crec0.w < -0.05f * dx) {  // particle_update.rs:132-136 penalty, PENALTY_COEFF = 1e3
+        const float corrected = fmaxf(crec0.w, -0.3f * dx);
+        v = v + pnormal * (dt * -corrected * 1.0e3f);
+    }
+#endif
     const m3 A = grad;
     if (tag != MODEL_FLUID) {
         F = F + (A * dt) * F;
@@ -293,6 +368,10 @@ __device__ __forceinline__ void g2p_particle(const DevPtrs& P, const Params& prm
 // status word) are copied unchanged to the slots after the sorted ones.
 __global__ void __launch_bounds__(256, NXM_G2P_MIN_CTAS) k_g2p_update(DevPtrs P) {
     __shared__ float4 halo[216];
+#if NXM_CPIC
+    __shared__ float4 halo_inc[216];
+    __shared__ uint2 halo_cdf[216];
+#endif
     const Params prm = *P.params;
     const uint32_t nbp = min(__ldcg(&P.counters->num_primary), __ldcg(&P.counters->num_blocks));
     const uint32_t tid = threadIdx.x;
@@ -330,6 +409,31 @@ __global__ void __launch_bounds__(256, NXM_G2P_MIN_CTAS) k_g2p_update(DevPtrs P)
             halo[tid] = make_float4(nd.x, nd.y, nd.z, 0.f);
         }
         for (uint32_t t = tid + blockDim.x; t < 216u; t += blockDim.x) halo[t] = halo_node(P, b, t);
+        CpicCtx cx{nullptr, nullptr, P.colliders, 0u};
+#if NXM_CPIC
+        if (prm.use_cpic) {
+            for (uint32_t t = tid; t < 216u; t += blockDim.x) {
+                const uint32_t tx = t % 6u, ty = (t / 6u) % 6u, tz = t / 36u;
+                const uint32_t ox = tx >= 4u, oy = ty >= 4u, oz = tz >= 4u;
+                const uint32_t oct = ox * 4u + oy * 2u + oz;
+                const uint32_t blk = oct == 0 ? b : P.nbh[b * NUM_NBH + oct - 1u];
+                const uint32_t node = (tx - 4u * ox) + 4u * (ty - 4u * oy) + 16u * (tz - 4u * oz);
+                halo_inc[t] = blk == NONE ? make_float4(0.f, 0.f, 0.f, 0.f) : P.nodes_inc[blk * 64u + node];
+                const uint4 nc = blk == NONE ? make_uint4(0u, 0u, NONE, 0u) : P.ncdf[blk * 64u + node];
+                halo_cdf[t] = make_uint2(nc.y, nc.z);
+            }
+            cx.halo_inc = halo_inc;
+            cx.halo_cdf = halo_cdf;
+            if (prm.scene_blocks) {
+                const uint32_t sid = scene_of_block(prm, P.bvid[b]);
+                const uint2 r = sid != NONE ? P.scene_cols[sid] : make_uint2(0u, 0u);
+                cx.cols = P.colliders + r.x;
+                cx.ncols = min(r.y, (uint32_t)MAX_COLLIDERS);
+            } else {
+                cx.ncols = min(prm.ncol, (uint32_t)MAX_COLLIDERS);
+            }
+        }
+#endif
         __syncthreads();
         for (uint32_t k = tid; k < np; k += blockDim.x) {
             if (k != tid) {
@@ -338,7 +442,7 @@ __global__ void __launch_bounds__(256, NXM_G2P_MIN_CTAS) k_g2p_update(DevPtrs P)
                 xm = kr[0];
                 vf = kr[1];
             }
-            g2p_particle(P, prm, halo, pid, reorder ? first + k : pid, xm, vf, key_off);
+            g2p_particle(P, prm, halo, pid, reorder ? first + k : pid, xm, vf, key_off, cx);
         }
         __syncthreads();
         b = bn;

@@ -6,6 +6,7 @@
 // operation (up to the last bits of logf/expf/sinf).
 #define NXM_NS exact
 #define NXM_FAST false
+#define NXM_CPIC 1
 #include "nxm_transfer.inc.cuh"
 
 namespace nxm {
@@ -18,6 +19,8 @@ __global__ void __launch_bounds__(64) k_p2g_gather(DevPtrs P) {
     __shared__ float smx[64], smy[64], smz[64], smass[64];
     __shared__ float saff[9][64];
     __shared__ int szkey[64];
+    __shared__ uint32_t safn[64];  // particle affinity bits (CPIC)
+    const bool cpic = P.params->use_cpic != 0;
     const float dx = P.params->dx;
     const float inv_cell_width = 1.0f / dx;
     const uint32_t nb = P.counters->num_blocks;
@@ -35,8 +38,9 @@ __global__ void __launch_bounds__(64) k_p2g_gather(DevPtrs P) {
         const uint32_t last = first + num;
         const uint32_t primaries_end = first + P.nprim[b];
         const uint32_t nchunks = (num + 63u) / 64u;
-        v3 acc_mv = splat(0.f);
-        float acc_mass = 0.f;
+        v3 acc_mv = splat(0.f), acc_mvi = splat(0.f);
+        float acc_mass = 0.f, acc_massi = 0.f;
+        const uint32_t node_aff = cpic ? P.ncdf[b * 64u + tid].y : 0u;
         for (uint32_t chunk = 0; chunk < nchunks; ++chunk) {
             const uint32_t chunk_base = first + chunk * 64u;
             __syncthreads();
@@ -49,6 +53,7 @@ __global__ void __launch_bounds__(64) k_p2g_gather(DevPtrs P) {
                 const v3 ac = assoc_cell_of(dx, pt);
                 int zk = f2i_sat(ac.z) - vid.z * 4;
                 szkey[tid] = zk < -2 ? -2 : zk;
+                safn[tid] = cpic ? __float_as_uint(P.pcdf[3u * pid + 1u].w) : 0u;
                 if (__float_as_uint(vf.w) & PFLAG_ENABLED) {
                     const float4 c0 = kr[2], c1 = kr[3], c2 = kr[4];
                     const float m = xm.w;
@@ -86,12 +91,19 @@ __global__ void __launch_bounds__(64) k_p2g_gather(DevPtrs P) {
                                      mk(saff[6][p], saff[7][p], saff[8][p]));
                     const v3 vel_contribution = (A * dpt + mk(smx[p], smy[p], smz[p])) * weight;
                     const float mass_contribution = smass[p] * weight;
-                    acc_mv = acc_mv + vel_contribution;
-                    acc_mass += mass_contribution;
+                    // p2g.rs:268-305: an incompatible particle feeds the node's second field
+                    if (cpic && !aff_compatible(safn[p], node_aff)) {
+                        acc_mvi = acc_mvi + vel_contribution;
+                        acc_massi += mass_contribution;
+                    } else {
+                        acc_mv = acc_mv + vel_contribution;
+                        acc_mass += mass_contribution;
+                    }
                 }
             }
         }
         P.nodes[b * 64u + tid] = make_float4(acc_mv.x, acc_mv.y, acc_mv.z, acc_mass);
+        if (cpic) P.nodes_inc[b * 64u + tid] = make_float4(acc_mvi.x, acc_mvi.y, acc_mvi.z, acc_massi);
         __syncthreads();
     }
 }
@@ -164,7 +176,182 @@ __global__ void __launch_bounds__(256) k_timestep_bound(DevPtrs P) {
     if ((threadIdx.x & 31u) == 0 && best != 0xFFFFFFFFu) atomicMin(&P.counters->dt_bound, best);
 }
 
+// ---- CPIC distance fields (analytic colliders) ------------------------------
+
+// Colliders a block sees: all (at most 16), or its scene's in batched mode.
+__device__ __forceinline__ const DevCollider* block_colliders(const DevPtrs& P, const Params& prm, int4 vid,
+                                                             uint32_t* n) {
+    if (prm.scene_blocks) {
+        const uint32_t sid = scene_of_block(prm, vid);
+        const uint2 r = sid != NONE ? P.scene_cols[sid] : make_uint2(0u, 0u);
+        *n = min(r.y, (uint32_t)MAX_COLLIDERS);
+        return P.colliders + r.x;
+    }
+    *n = min(prm.ncol, (uint32_t)MAX_COLLIDERS);
+    return P.colliders;
+}
+
+// solver/grid_update_cdf.rs:18-58: per node, every ball / cuboid / capsule
+// within 1.5 dx (or containing the node) sets its affinity bit (and its sign
+// bit when inside); the closest by unsigned distance is kept.  Trimeshes
+// reach the reference's node field through rigid particles (p2g_cdf.rs),
+// not built here: the host refuses CPIC with a trimesh collider.
+__global__ void __launch_bounds__(256) k_grid_update_cdf(DevPtrs P) {
+    const Params prm = *P.params;
+    const float dx = prm.dx, cap = dx * 1.5f;
+    const uint32_t total = P.counters->num_blocks * 64u;
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+        const uint32_t b = t >> 6, k = t & 63u;
+        int4 vid = P.bvid[b];
+        uint32_t ncol;
+        const DevCollider* cols = block_colliders(P, prm, vid, &ncol);
+        const int3 o = scene_base_of_block(prm, vid);
+        vid.x -= o.x; vid.y -= o.y; vid.z -= o.z;
+        const v3 point = mk((float)(vid.x * 4 + (int)(k & 3u)), (float)(vid.y * 4 + (int)((k >> 2) & 3u)),
+                            (float)(vid.z * 4 + (int)(k >> 4))) * dx;
+        float dist = MAX_FLT;
+        uint32_t aff = 0u, closest = NONE;
+        for (uint32_t i = 0; i < ncol; ++i) {
+            const DevCollider& c = cols[i];
+            if (c.type == SHAPE_TRIMESH) continue;
+            const quat q = quat{c.rot[0], c.rot[1], c.rot[2], c.rot[3]};
+            const v3 tra = mk(c.tra[0], c.tra[1], c.tra[2]);
+            const v3 local = qrot(qconj(q), point - tra);
+            Proj pr;
+            if (c.type == SHAPE_BALL) pr = ball_project_local(c.a[0], local);
+            else if (c.type == SHAPE_CUBOID) pr = cuboid_project_local(mk(c.a[0], c.a[1], c.a[2]), local);
+            else if (c.type == SHAPE_CAPSULE)
+                pr = capsule_project_local(mk(c.a[0], c.a[1], c.a[2]), mk(c.b[0], c.b[1], c.b[2]), c.b[3], local);
+            else { pr.point = local; pr.inside = false; }
+            pr.point = qrot(q, pr.point) + tra;
+            const v3 dpt = pr.point - point;
+            const v3 ad = vabs(dpt);
+            if (pr.inside || (ad.x <= cap && ad.y <= cap && ad.z <= cap)) {
+                const float d = length(dpt);
+                if (d < dist) {
+                    closest = i;
+                    dist = d;
+                }
+                aff |= (pr.inside ? 0x00010001u : 0x00000001u) << i;
+            }
+        }
+        P.ncdf[t] = make_uint4(__float_as_uint(dist), aff, closest, 0u);
+    }
+}
+
+// solver/g2p_cdf.rs:150-290: per primary particle, its affinity (the node
+// bits; sign bits remembered from the previous step, or for a new affinity
+// the sign of the weighted node distances) and an MLS fit distance = n . dpt
+// + d over the nodes sharing an affinity with it (normal = n / |n|, signed
+// distance = d); a singular fit (determinant <= 1e-8) zeroes the record.
+// One CTA per primary block, the 6x6x6 node field in shared memory.
+__global__ void __launch_bounds__(128) k_g2p_cdf(DevPtrs P) {
+    __shared__ uint4 halo[216];
+    const Params prm = *P.params;
+    const float dx = prm.dx;
+    const uint32_t nbp = min(__ldcg(&P.counters->num_primary), __ldcg(&P.counters->num_blocks));
+    for (uint32_t b = blockIdx.x; b < nbp; b += gridDim.x) {
+        for (uint32_t t = threadIdx.x; t < 216u; t += blockDim.x) {
+            const uint32_t tx = t % 6u, ty = (t / 6u) % 6u, tz = t / 36u;
+            const uint32_t ox = tx >= 4u, oy = ty >= 4u, oz = tz >= 4u;
+            const uint32_t oct = ox * 4u + oy * 2u + oz;
+            const uint32_t blk = oct == 0 ? b : P.nbh[b * NUM_NBH + oct - 1u];
+            halo[t] = blk == NONE ? make_uint4(__float_as_uint(MAX_FLT), 0u, NONE, 0u)
+                                  : P.ncdf[blk * 64u + (tx - 4u * ox) + 4u * (ty - 4u * oy) + 16u * (tz - 4u * oz)];
+        }
+        __syncthreads();
+        const uint32_t first = P.first[b], np = P.nprim[b];
+        for (uint32_t k = threadIdx.x; k < np; k += blockDim.x) {
+            const uint32_t pid = P.sorted[first + k];
+            float4* rec = &P.pcdf[3u * pid];
+            const uint32_t prev = __float_as_uint(rec[1].w);
+            const float4 xm = reinterpret_cast<const float4*>(&P.kin[pid])[0];
+            const v3 pt = mk(xm.x, xm.y, xm.z);
+            const v3 ref = assoc_cell_of(dx, pt) * dx - pt;
+            const v3 w0 = kernel_eval_all(-ref.x / dx), w1 = kernel_eval_all(-ref.y / dx),
+                     w2 = kernel_eval_all(-ref.z / dx);
+            const CellInfo ci = cell_info(dx, pt);
+            const uint32_t packed = ci.ax + 6u * ci.ay + 36u * ci.az;
+            uint32_t pa = 0u;
+            float sums[16];
+#pragma unroll
+            for (int ic = 0; ic < 16; ++ic) sums[ic] = 0.f;
+            for (int i = 0; i < 27; ++i) {
+                int sx, sy, sz;
+                nbh_shift(i, sx, sy, sz);
+                const uint4 nd = halo[packed + (uint32_t)(sx + 6 * sy + 36 * sz)];
+                pa |= nd.y & 0x0000FFFFu;
+                const float weight = vget(w0, sx) * vget(w1, sy) * vget(w2, sz);
+                const float ndist = __uint_as_float(nd.x);
+#pragma unroll
+                for (int ic = 0; ic < 16; ++ic) {
+                    const float compatible = (nd.y & (1u << ic)) ? 1.0f : 0.0f;
+                    const float sign = ((nd.y >> 16) & (1u << ic)) ? -1.0f : 1.0f;
+                    sums[ic] += compatible * weight * sign * ndist;
+                }
+            }
+#pragma unroll
+            for (int ic = 0; ic < 16; ++ic) {
+                if (!(prev & (1u << ic))) {
+                    if (sums[ic] < 0.f) pa |= 0x00010000u << ic;
+                } else {
+                    pa |= prev & (0x00010000u << ic);
+                }
+            }
+            float q[4][4], u[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+            for (int r = 0; r < 4; ++r)
+#pragma unroll
+                for (int c = 0; c < 4; ++c) q[r][c] = 0.f;
+            for (int i = 0; i < 27; ++i) {
+                int sx, sy, sz;
+                nbh_shift(i, sx, sy, sz);
+                const uint4 nd = halo[packed + (uint32_t)(sx + 6 * sy + 36 * sz)];
+                const v3 dpt = ref + mk((float)sx, (float)sy, (float)sz) * dx;
+                const float weight = vget(w0, sx) * vget(w1, sy) * vget(w2, sz);
+                const uint32_t combined = nd.y & pa & 0x0000FFFFu;
+                const uint32_t sdiff = ((nd.y >> 16) ^ (pa >> 16)) & combined;
+                const float pv[4] = {dpt.x, dpt.y, dpt.z, 1.0f};
+                if (combined != 0u) {
+                    const float ndist = __uint_as_float(nd.x);
+                    const float dd = sdiff == 0u ? ndist : -ndist;
+#pragma unroll
+                    for (int r = 0; r < 4; ++r)
+#pragma unroll
+                        for (int c = 0; c < 4; ++c) q[r][c] += pv[r] * pv[c] * weight;
+#pragma unroll
+                    for (int r = 0; r < 4; ++r) u[r] += pv[r] * (weight * dd);
+                }
+            }
+            float qi[4][4];
+            const float dt4 = inv4(q, qi);
+            if (dt4 > 1.0e-8f) {
+                float r4[4];
+#pragma unroll
+                for (int i = 0; i < 4; ++i) r4[i] = qi[i][0] * u[0] + qi[i][1] * u[1] + qi[i][2] * u[2] + qi[i][3] * u[3];
+                const v3 nv = mk(r4[0], r4[1], r4[2]);
+                const float len = length(nv);
+                const v3 n = len > 1.0e-6f ? nv / len : splat(0.f);
+                rec[0] = make_float4(n.x, n.y, n.z, r4[3]);
+                rec[1] = make_float4(0.f, 0.f, 0.f, __uint_as_float(pa));
+            } else {
+                rec[0] = make_float4(0.f, 0.f, 0.f, 0.f);
+                rec[1] = make_float4(0.f, 0.f, 0.f, __uint_as_float(0u));
+            }
+        }
+        __syncthreads();
+    }
+}
+
 }  // namespace
+
+void launch_grid_update_cdf(const DevPtrs& P, const LaunchCfg& c, cudaStream_t s) {
+    k_grid_update_cdf<<<c.sm_count * 8, 256, 0, s>>>(P);
+}
+
+void launch_g2p_cdf(const DevPtrs& P, const LaunchCfg& c, cudaStream_t s) {
+    k_g2p_cdf<<<c.sm_count * 4, 128, 0, s>>>(P);
+}
 
 void launch_timestep_bound(const DevPtrs& P, const LaunchCfg& c, cudaStream_t s) {
     k_timestep_bound<<<c.sm_count * 4, 256, 0, s>>>(P);

@@ -91,6 +91,7 @@ SIGNATURES = {
     "nxm_grid_read_nodes": (C.c_int, [_vp, _f, C.c_uint32]),
     "nxm_debug_sort": (C.c_int, [_vp, _vp, C.c_int]),
     "nxm_state_estimate_timestep_bound": (C.c_int, [_vp, _f, _u]),
+    "nxm_read_cdf": (C.c_int, [_vp, _f]),
     "nxm_state_enable_scenes": (C.c_int, [_vp, C.c_uint32]),
     "nxm_scene_capacity": (C.c_uint32, [_vp]),
     "nxm_scene_add": (C.c_int, [_vp, C.POINTER(ParticlesSoAC), C.c_uint32, _vp, C.c_uint32, _f, C.c_uint32, _u]),
@@ -371,6 +372,14 @@ class MpmState:
     def read_models(self) -> np.ndarray:
         return self._read("nxm_read_models", (len(self), 25), np.uint32, _u)
 
+    def read_cdf(self) -> dict:
+        """CPIC particle fields: normal, signed distance, rigid velocity, affinity bits."""
+        out = np.zeros((max(len(self), 1), 8), np.float32)
+        _check(self.lib.nxm_read_cdf(self.h, _p(out, _f)), "read_cdf")
+        out = out[:len(self)]
+        return dict(normal=out[:, :3], signed_distance=out[:, 3], rigid_vel=out[:, 4:7],
+                    affinity=out[:, 7].copy().view(np.uint32))
+
     def estimate_timestep_bound(self) -> tuple[float, int]:
         """``WgTimestepBounds::compute_bounds``: (max dt in seconds, fixed-point bits)."""
         dt = np.zeros(1, np.float32)
@@ -425,13 +434,16 @@ class MpmState:
         return int(self.lib.nxm_state_cuda_stream(self.h) or 0)
 
 
-def state_from_scene(scene, deterministic: bool = False, grid_capacity: int | None = None) -> MpmState:
+def state_from_scene(scene, deterministic: bool = False, grid_capacity: int | None = None,
+                     use_cpic: bool = False) -> MpmState:
     """Builds a device state for a ``nexus_b200.scenes.Scene``."""
     st = MpmState(grid_size=grid_capacity or scene.grid_capacity, particles_capacity=scene.n)
     st.set_cell_width(scene.dx, grid_capacity or scene.grid_capacity)
     st.set_simulation_params(scene.gravity, scene.dt)
     st.set_colliders(scene.colliders, scene.tri_vertices if scene.tri_vertices.size else None)
     st.set_deterministic(deterministic)
+    if use_cpic:
+        st.set_use_cpic(True)
     st.append(scene.particles)
     return st
 

@@ -225,3 +225,27 @@ def serving_scene(i: int, seed: int = 3000) -> Scene:
     u = uniform(seed + 7919 * (i + 1), 1)
     dx = 1.0 / 128.0 if u[0] < 0.5 else 1.0 / 256.0
     return random_box_scene(seed + i, dx, 2048, 524288, ("neo_hookean", "sand", "water"), name=f"serve_{i}")
+
+
+def cpic_drop(n_side: int = 12, seed: int = 17, steps: int = 100) -> Scene:
+    """Colliders close to the particles from the first step, at the scale of
+    the reference's CPIC scenes (cell width 0.5, a 32-unit domain: the
+    particle distance-field fit keeps only nodes with a 4x4 moment
+    determinant above 1e-8, which meter-sized cells pass): a neo-Hookean
+    cube and a sand block falling at 10 m/s onto the slip floor, the cube
+    also onto a ball moving along x at 2 m/s (the cube starts 0.4 above it,
+    the sand 0.9 above the floor), inside five slip walls."""
+    L, dx = 32.0, 0.5
+    cube = ParticleBatch.from_positions(lattice_block((0.30 * L, 0.30 * L, 2.4), (n_side, n_side, n_side), dx, seed),
+                                        np.float32(dx) / np.float32(4.0), 1000.0,
+                                        ParticleModel.elastic_neo_hookean(1.0e5, 0.3))
+    sand = ParticleBatch.from_positions(lattice_block((0.62 * L, 0.30 * L, 0.9), (n_side, n_side, n_side // 2), dx,
+                                                      seed, 3 * n_side ** 3),
+                                        np.float32(dx) / np.float32(4.0), 2700.0,
+                                        ParticleModel.sand_with_friction_angle(3.5e5, 0.3, 30.0))
+    batch = ParticleBatch.concat([cube, sand])
+    batch.vel[:, 2] = -10.0
+    ball = Collider.ball(2.0, (0.40 * L, 0.40 * L, 0.0), BoundaryCondition.separate(0.2))
+    ball.linvel = (2.0, 0.0, 0.0)
+    cols = collider_array(box_walls(0.0, L, BoundaryCondition.slip(), BoundaryCondition.slip(), thickness=2.0) + [ball])
+    return Scene("cpic_drop", dx, 1.0e-3, (0.0, 0.0, -9.81), batch, cols, steps, grid_capacity_for(batch.n))

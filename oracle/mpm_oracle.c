@@ -203,12 +203,16 @@ typedef struct {
     uint32_t nbh[NUM_NBH];
 } header_t;
 
-/* grid.rs:401-421 Node (the non-CPIC fields used on this path). */
+/* grid.rs:401-421 Node, with the NodeCdf of grid.rs:367-375 (distance,
+ * affinity + sign bits, closest collider). */
 typedef struct {
     v3 mv;
     REAL mass;
     v3 mv_incompat;
     REAL mass_incompat;
+    REAL cdf_distance;
+    uint32_t cdf_aff;
+    uint32_t cdf_closest;
 } node_t;
 
 /* ------------------------------------------------------------------------ */
@@ -626,6 +630,11 @@ typedef struct {
     REAL *vgd, *mass, *init_volume, *damping;
     uint32_t *enabled, *fixed, *tag;
     REAL *words; /* n * 24 */
+    REAL *bfric; /* boundary_friction */
+    /* particle Cdf (solver/particle.rs:35-50): normal, signed distance, rigid velocity, affinity bits */
+    v3 *cdf_normal, *cdf_rigid_vel;
+    REAL *cdf_sd;
+    uint32_t *cdf_aff;
     /* params */
     v3 gravity;
     REAL dt;
@@ -668,6 +677,12 @@ scene_t *orc_create(uint32_t n, double dx, uint32_t grid_capacity) {
     s->init_volume = xcalloc(n, sizeof(REAL));
     s->damping = xcalloc(n, sizeof(REAL));
     s->enabled = xcalloc(n, sizeof(uint32_t));
+    s->bfric = xcalloc(n, sizeof(REAL));
+    for (uint32_t i = 0; i < n; ++i) s->bfric[i] = (REAL)1.0;
+    s->cdf_normal = xcalloc(n, sizeof(v3));
+    s->cdf_rigid_vel = xcalloc(n, sizeof(v3));
+    s->cdf_sd = xcalloc(n, sizeof(REAL));
+    s->cdf_aff = xcalloc(n, sizeof(uint32_t));
     s->fixed = xcalloc(n, sizeof(uint32_t));
     s->tag = xcalloc(n, sizeof(uint32_t));
     s->words = xcalloc((size_t)n * MODEL_WORDS, sizeof(REAL));
@@ -687,6 +702,7 @@ void orc_destroy(scene_t *s) {
     if (!s) return;
     free(s->pos); free(s->vel); free(s->aff); free(s->F); free(s->vgd); free(s->mass);
     free(s->init_volume); free(s->damping); free(s->enabled); free(s->fixed); free(s->tag);
+    free(s->bfric); free(s->cdf_normal); free(s->cdf_rigid_vel); free(s->cdf_sd); free(s->cdf_aff);
     free(s->words); free(s->hstate); free(s->hvalue); free(s->howner); free(s->hdr);
     free(s->nodes); free(s->sorted); free(s->scan); free(s->col); free(s->tri);
     free(s);
@@ -719,6 +735,23 @@ void orc_set_particles(scene_t *s, const float *pos, const float *vel, const flo
         s->fixed[i] = fixed[i];
         s->tag[i] = model[25 * (size_t)i];
         for (int k = 0; k < MODEL_WORDS; ++k) s->words[(size_t)i * MODEL_WORDS + k] = bits2f(model[25 * (size_t)i + 1 + k]);
+    }
+}
+
+void orc_set_boundary_friction(scene_t *s, const float *bf) {
+    for (uint32_t i = 0; i < s->n; ++i) s->bfric[i] = bf[i];
+}
+
+static float f2bitsf(uint32_t u) { float f; memcpy(&f, &u, 4); return f; }
+
+/* Particle Cdf: normal xyz, signed distance, rigid velocity xyz, affinity bits (as float bits). */
+void orc_get_cdf(const scene_t *s, float *out8) {
+    for (uint32_t i = 0; i < s->n; ++i) {
+        float *o = out8 + 8 * (size_t)i;
+        o[0] = (float)s->cdf_normal[i].x; o[1] = (float)s->cdf_normal[i].y; o[2] = (float)s->cdf_normal[i].z;
+        o[3] = (float)s->cdf_sd[i];
+        o[4] = (float)s->cdf_rigid_vel[i].x; o[5] = (float)s->cdf_rigid_vel[i].y; o[6] = (float)s->cdf_rigid_vel[i].z;
+        o[7] = f2bitsf(s->cdf_aff[i]);
     }
 }
 
@@ -941,7 +974,19 @@ int orc_sort(scene_t *s) {
 }
 
 /* ------------------------------------------------------------------------ */
-/* P2G (gather form): solver/p2g.rs:64-351 with USE_CPIC = false             */
+/* CPIC affinity bits (grid/grid.rs:593-645)                                 */
+/* ------------------------------------------------------------------------ */
+
+#define AFF_MASK 0x0000FFFFu
+#define AFF_SIGN_SHIFT 16
+static inline int aff_compatible(uint32_t a, uint32_t b) {
+    uint32_t common = a & b & AFF_MASK;
+    return ((a >> AFF_SIGN_SHIFT) & common) == ((b >> AFF_SIGN_SHIFT) & common);
+}
+
+/* ------------------------------------------------------------------------ */
+/* P2G (gather form): solver/p2g.rs:64-351 (USE_CPIC: compatible and         */
+/* incompatible sums, two-way impulses off as TWO_WAYS_COUPLING_ENABLED)     */
 /* ------------------------------------------------------------------------ */
 
 void orc_p2g(scene_t *s) {
@@ -961,16 +1006,21 @@ void orc_p2g(scene_t *s) {
         v3 acc_mv[64];
         REAL acc_m[64];
         for (int t = 0; t < 64; ++t) { acc_mv[t] = V(0, 0, 0); acc_m[t] = 0; }
+        v3 acc_mvi[64];
+        REAL acc_mi[64];
+        for (int t = 0; t < 64; ++t) { acc_mvi[t] = V(0, 0, 0); acc_mi[t] = 0; }
         v3 spos[64], smom[64];
         REAL smass[64];
         m3 saff[64];
         int32_t szkey[64];
+        uint32_t safn[64];
         for (uint32_t chunk = 0; chunk < nchunks; ++chunk) {
             uint32_t base = first + chunk * 64;
             uint32_t clen = (last - base) < 64 ? (last - base) : 64;
             for (uint32_t k = 0; k < clen; ++k) {
                 uint32_t pid = s->sorted[base + k];
                 v3 pt = s->pos[pid];
+                safn[k] = s->cdf_aff[pid];
                 v3 ac = assoc_cell_of(dx, pt);
                 int32_t zk = r_to_i32(ac.z) - vid.z * 4;
                 szkey[k] = zk < -2 ? -2 : zk;
@@ -998,14 +1048,21 @@ void orc_p2g(scene_t *s) {
                     for (int tx = 0; tx < 4; ++tx) {
                         int t = tx + 4 * ty + 16 * tz;
                         v3 cell_pos = vmul(V((REAL)(vid.x * 4 + tx), (REAL)(vid.y * 4 + ty), (REAL)(vid.z * 4 + tz)), dx);
+                        const uint32_t node_aff = s->nodes[(size_t)bi * 64 + t].cdf_aff;
                         for (uint32_t p = 0; p < clen; ++p) {
                             v3 dpt = vsub(cell_pos, spos[p]);
                             REAL w = kernel_eval(dpt.x * inv_dx) * kernel_eval(dpt.y * inv_dx) * kernel_eval(dpt.z * inv_dx);
                             if (w != 0) {
                                 v3 vc = vmul(vadd(mv(saff[p], dpt), smom[p]), w);
                                 REAL mc = smass[p] * w;
-                                acc_mv[t] = vadd(acc_mv[t], vc);
-                                acc_m[t] += mc;
+                                /* p2g.rs:268-305: an incompatible particle feeds the node's second field */
+                                if (s->use_cpic && !aff_compatible(safn[p], node_aff)) {
+                                    acc_mvi[t] = vadd(acc_mvi[t], vc);
+                                    acc_mi[t] += mc;
+                                } else {
+                                    acc_mv[t] = vadd(acc_mv[t], vc);
+                                    acc_m[t] += mc;
+                                }
                             }
                         }
                     }
@@ -1015,8 +1072,8 @@ void orc_p2g(scene_t *s) {
             node_t *nd = &s->nodes[(size_t)bi * 64 + t];
             nd->mv = acc_mv[t];
             nd->mass = acc_m[t];
-            nd->mv_incompat = V(0, 0, 0);
-            nd->mass_incompat = 0;
+            nd->mv_incompat = acc_mvi[t];
+            nd->mass_incompat = acc_mi[t];
         }
     }
 }
@@ -1127,6 +1184,14 @@ static inline v3 halo_vel(const scene_t *s, const uint32_t octant_hdr[8], int sx
     return s->nodes[(size_t)h * 64 + lx + 4 * ly + 16 * lz].mv;
 }
 
+static inline const node_t *halo_node(const scene_t *s, const uint32_t octant_hdr[8], int sx, int sy, int sz) {
+    int ox = sx >= 4, oy = sy >= 4, oz = sz >= 4;
+    uint32_t h = octant_hdr[ox * 4 + oy * 2 + oz];
+    if (h == NONE_U32) return NULL;
+    int lx = sx - 4 * ox, ly = sy - 4 * oy, lz = sz - 4 * oz;
+    return &s->nodes[(size_t)h * 64 + lx + 4 * ly + 16 * lz];
+}
+
 void orc_g2p(scene_t *s) {
     const REAL dx = s->dx;
     const REAL inv_d = (REAL)4.0 / (dx * dx);
@@ -1151,11 +1216,35 @@ void orc_g2p(scene_t *s) {
                     int sx = NBH_SHIFTS[i][0], sy = NBH_SHIFTS[i][1], sz = NBH_SHIFTS[i][2];
                     v3 cv = halo_vel(s, oct, (int)a[0] + sx, (int)a[1] + sy, (int)a[2] + sz);
                     v3 dpt = vadd(ref, vmul(V((REAL)sx, (REAL)sy, (REAL)sz), dx));
+                    if (s->use_cpic) {
+                        /* g2p.rs:206-235: an incompatible node gives its second velocity,
+                         * projected by the closest body's boundary condition */
+                        const node_t *nd = halo_node(s, oct, (int)a[0] + sx, (int)a[1] + sy, (int)a[2] + sz);
+                        uint32_t naff = nd ? nd->cdf_aff : 0u, nclosest = nd ? nd->cdf_closest : NONE_U32;
+                        if (!aff_compatible(s->cdf_aff[pid], naff)) {
+                            cv = nd ? nd->mv_incompat : V(0, 0, 0);
+                            if (nclosest != NONE_U32) {
+                                const collider_t *c = &s->col[nclosest];
+                                v3 cell_center = vadd(dpt, pt);
+                                v3 bv = velocity_at_point(c, cell_center);
+                                cv = vadd(bv, bc_project(c->bc_type, c->bc_friction * s->bfric[pid], vsub(cv, bv),
+                                                         s->cdf_normal[pid]));
+                            }
+                        }
+                    }
                     REAL weight = vget(w[0], sx) * vget(w[1], sy) * vget(w[2], sz);
                     velocity = vadd(velocity, vmul(cv, weight));
                     grad = madd(grad, mscale(mouter(cv, dpt), weight * inv_d));
                     vgd += weight * inv_d * vdot(cv, dpt);
                 }
+            }
+            if (s->use_cpic) {
+                /* g2p.rs:248-262: rigid velocity of every collider the particle has affinity with */
+                v3 rv = V(0, 0, 0);
+                if (s->enabled[pid] != 0)
+                    for (uint32_t ic = 0; ic < 16 && ic < s->ncol; ++ic)
+                        if (s->cdf_aff[pid] & (1u << ic)) rv = vadd(rv, velocity_at_point(&s->col[ic], s->pos[pid]));
+                s->cdf_rigid_vel[pid] = rv;
             }
             s->aff[pid] = grad;
             s->vgd[pid] = vgd;
@@ -1179,13 +1268,22 @@ void orc_particle_update(scene_t *s) {
         v3 v = s->vel[p];
         m3 F = s->F[p];
         v3 pos = s->pos[p];
-        /* non-CPIC: the particle Cdf stays zero, so the penetration
-         * reprojection (:98-102) and penalty (:132-136) never trigger. */
+        /* particle_update.rs:98-102: reproject a penetrating particle (the Cdf is
+         * zero without CPIC, so this and the penalty below never trigger then) */
+        const REAL sd = s->cdf_sd[p];
+        if (sd < (REAL)-0.05 * dx) {
+            v3 rv = s->cdf_rigid_vel[p];
+            v = vadd(rv, bc_project(BC_SLIP, (REAL)0.0, vsub(v, rv), s->cdf_normal[p]));
+        }
         REAL vl = vlen(v);
         if (vl > dx / dt) v = vdiv(vmul(vdiv(v, vl), dx), dt);
         v = vdiv(v, (REAL)1.0 + s->damping[p] * dt);
         if (s->fixed[p] != 0) v = V(0, 0, 0);
         v3 np = vadd(pos, vmul(v, dt));
+        if (sd < (REAL)-0.05 * dx) { /* particle_update.rs:132-136 penalty impulse, PENALTY_COEFF = 1e3 */
+            REAL corrected = fmax(sd, (REAL)-0.3 * dx);
+            v = vadd(v, vmul(s->cdf_normal[p], dt * -corrected * (REAL)1.0e3));
+        }
         m3 A = s->aff[p];
         if (!fluid) {
             F = madd(F, mm(mscale(A, dt), F));
@@ -1249,10 +1347,189 @@ static void update_world_com(scene_t *s) {
     for (uint32_t i = 0; i < s->ncol; ++i) s->col[i].com = pose_apply(s->col[i].pose, s->col[i].local_com);
 }
 
-/* src_mpm/pipeline.rs:385-526 MpmPipeline::step (non-CPIC path). */
+/* ------------------------------------------------------------------------ */
+/* CPIC CDF passes for analytic colliders                                    */
+/* ------------------------------------------------------------------------ */
+
+/* solver/grid_update_cdf.rs:18-58 collide(): per node, every ball / cuboid /
+ * capsule within 1.5 dx (or containing it) sets its affinity bit (and sign
+ * bit when inside); the closest one by unsigned distance is kept.  Triangle
+ * meshes reach the node CDF through rigid particles (p2g_cdf.rs), which this
+ * restatement does not cover. */
+void orc_grid_update_cdf(scene_t *s) {
+    const REAL dx = s->dx, cap = s->dx * (REAL)1.5;
+    const int64_t nb = (int64_t)s->num_blocks;
+#pragma omp parallel for schedule(static)
+    for (int64_t bi = 0; bi < nb; ++bi) {
+        const i3 vid = s->hdr[bi].vid;
+        for (int t = 0; t < 64; ++t) {
+            v3 point = vmul(V((REAL)(vid.x * 4 + (t & 3)), (REAL)(vid.y * 4 + ((t >> 2) & 3)), (REAL)(vid.z * 4 + (t >> 4))), dx);
+            REAL dist = MAX_FLT;
+            uint32_t affb = 0, closest = NONE_U32;
+            for (uint32_t i = 0; i < s->ncol && i < 16; ++i) {
+                const collider_t *c = &s->col[i];
+                if (c->type == SHAPE_TRIMESH) continue;
+                v3 local = pose_inv_apply(c->pose, point);
+                proj_t pr;
+                if (c->type == SHAPE_BALL) pr = ball_project_local(c->a[0], local);
+                else if (c->type == SHAPE_CUBOID) pr = cuboid_project_local(V(c->a[0], c->a[1], c->a[2]), local);
+                else if (c->type == SHAPE_CAPSULE)
+                    pr = capsule_project_local(V(c->a[0], c->a[1], c->a[2]), V(c->b[0], c->b[1], c->b[2]), c->b[3], local);
+                else { pr.point = local; pr.inside = 0; }
+                pr.point = pose_apply(c->pose, pr.point);
+                v3 dpt = vsub(pr.point, point);
+                v3 ad = vabs(dpt);
+                int within = ad.x <= cap && ad.y <= cap && ad.z <= cap;
+                if (pr.inside || within) {
+                    REAL d = vlen(dpt);
+                    if (d < dist) { closest = i; dist = d; }
+                    affb |= (pr.inside ? 0x00010001u : 0x00000001u) << i;
+                }
+            }
+            node_t *nd = &s->nodes[(size_t)bi * 64 + t];
+            nd->cdf_distance = dist;
+            nd->cdf_aff = affb;
+            nd->cdf_closest = closest;
+        }
+    }
+}
+
+/* Inverse and determinant of a 4x4 matrix m[row][col] from its 2x2 minors
+ * (Laplace expansion along the first two rows). */
+static REAL inv4(const REAL m[4][4], REAL out[4][4]) {
+    REAL s0 = m[0][0] * m[1][1] - m[1][0] * m[0][1];
+    REAL s1 = m[0][0] * m[1][2] - m[1][0] * m[0][2];
+    REAL s2 = m[0][0] * m[1][3] - m[1][0] * m[0][3];
+    REAL s3 = m[0][1] * m[1][2] - m[1][1] * m[0][2];
+    REAL s4 = m[0][1] * m[1][3] - m[1][1] * m[0][3];
+    REAL s5 = m[0][2] * m[1][3] - m[1][2] * m[0][3];
+    REAL c5 = m[2][2] * m[3][3] - m[3][2] * m[2][3];
+    REAL c4 = m[2][1] * m[3][3] - m[3][1] * m[2][3];
+    REAL c3 = m[2][1] * m[3][2] - m[3][1] * m[2][2];
+    REAL c2 = m[2][0] * m[3][3] - m[3][0] * m[2][3];
+    REAL c1 = m[2][0] * m[3][2] - m[3][0] * m[2][2];
+    REAL c0 = m[2][0] * m[3][1] - m[3][0] * m[2][1];
+    REAL det = s0 * c5 - s1 * c4 + s2 * c3 + s3 * c2 - s4 * c1 + s5 * c0;
+    REAL id = (REAL)1.0 / det;
+    out[0][0] = (m[1][1] * c5 - m[1][2] * c4 + m[1][3] * c3) * id;
+    out[0][1] = (-m[0][1] * c5 + m[0][2] * c4 - m[0][3] * c3) * id;
+    out[0][2] = (m[3][1] * s5 - m[3][2] * s4 + m[3][3] * s3) * id;
+    out[0][3] = (-m[2][1] * s5 + m[2][2] * s4 - m[2][3] * s3) * id;
+    out[1][0] = (-m[1][0] * c5 + m[1][2] * c2 - m[1][3] * c1) * id;
+    out[1][1] = (m[0][0] * c5 - m[0][2] * c2 + m[0][3] * c1) * id;
+    out[1][2] = (-m[3][0] * s5 + m[3][2] * s2 - m[3][3] * s1) * id;
+    out[1][3] = (m[2][0] * s5 - m[2][2] * s2 + m[2][3] * s1) * id;
+    out[2][0] = (m[1][0] * c4 - m[1][1] * c2 + m[1][3] * c0) * id;
+    out[2][1] = (-m[0][0] * c4 + m[0][1] * c2 - m[0][3] * c0) * id;
+    out[2][2] = (m[3][0] * s4 - m[3][1] * s2 + m[3][3] * s0) * id;
+    out[2][3] = (-m[2][0] * s4 + m[2][1] * s2 - m[2][3] * s0) * id;
+    out[3][0] = (-m[1][0] * c3 + m[1][1] * c1 - m[1][2] * c0) * id;
+    out[3][1] = (m[0][0] * c3 - m[0][1] * c1 + m[0][2] * c0) * id;
+    out[3][2] = (-m[3][0] * s3 + m[3][1] * s1 - m[3][2] * s0) * id;
+    out[3][3] = (m[2][0] * s3 - m[2][1] * s1 + m[2][2] * s0) * id;
+    return det;
+}
+
+double orc_inv4(const double *m16, double *out16) {
+    REAL m[4][4], o[4][4];
+    for (int i = 0; i < 16; ++i) m[i / 4][i % 4] = (REAL)m16[i];
+    REAL d = inv4(m, o);
+    for (int i = 0; i < 16; ++i) out16[i] = (double)o[i / 4][i % 4];
+    return (double)d;
+}
+
+/* solver/g2p_cdf.rs:150-290 particle_g2p: the particle's affinity (the node
+ * bits, with sign bits remembered from the previous step or, for a new
+ * affinity, from the sign of the weighted node distances) and an MLS fit
+ * of the signed distance field, distance = n . dpt + d, over the nodes that
+ * share an affinity with it: normal = n / |n|, signed distance = d. */
+void orc_g2p_cdf(scene_t *s) {
+    const REAL dx = s->dx;
+    const int64_t nb = (int64_t)s->num_blocks;
+#pragma omp parallel for schedule(dynamic, 4)
+    for (int64_t bi = 0; bi < nb; ++bi) {
+        const header_t *h = &s->hdr[bi];
+        uint32_t oct[8];
+        for (int o = 0; o < 8; ++o) oct[o] = find_header(s, i3add(h->vid, ASSOC_SHIFT[o]));
+        for (uint32_t k = h->first_particle; k < h->first_particle + h->num_particles; ++k) {
+            uint32_t pid = s->sorted[k];
+            const uint32_t prev = s->cdf_aff[pid];
+            v3 pt = s->pos[pid];
+            v3 ref = vsub(vmul(assoc_cell_of(dx, pt), dx), pt);
+            v3 w[3] = {kernel_eval_all(-ref.x / dx), kernel_eval_all(-ref.y / dx), kernel_eval_all(-ref.z / dx)};
+            uint32_t a[3];
+            assoc_in_block(dx, pt, a);
+            uint32_t pa = 0;
+            REAL sums[16];
+            for (int ic = 0; ic < 16; ++ic) sums[ic] = 0;
+            for (int i = 0; i < 27; ++i) {
+                int sx = NBH_SHIFTS[i][0], sy = NBH_SHIFTS[i][1], sz = NBH_SHIFTS[i][2];
+                const node_t *nd = halo_node(s, oct, (int)a[0] + sx, (int)a[1] + sy, (int)a[2] + sz);
+                uint32_t naff = nd ? nd->cdf_aff : 0u;
+                REAL ndist = nd ? nd->cdf_distance : MAX_FLT;
+                pa |= naff & AFF_MASK;
+                REAL weight = vget(w[0], sx) * vget(w[1], sy) * vget(w[2], sz);
+                for (int ic = 0; ic < 16; ++ic) {
+                    REAL compatible = (naff & (1u << ic)) ? (REAL)1.0 : (REAL)0.0;
+                    REAL sign = ((naff >> AFF_SIGN_SHIFT) & (1u << ic)) ? (REAL)-1.0 : (REAL)1.0;
+                    sums[ic] += compatible * weight * sign * ndist;
+                }
+            }
+            for (int ic = 0; ic < 16; ++ic) {
+                if (!(prev & (1u << ic))) {
+                    if (sums[ic] < 0) pa |= 0x00010000u << ic;
+                } else {
+                    pa |= prev & (0x00010000u << ic);
+                }
+            }
+            REAL q[4][4] = {{0}}, u[4] = {0, 0, 0, 0};
+            for (int i = 0; i < 27; ++i) {
+                int sx = NBH_SHIFTS[i][0], sy = NBH_SHIFTS[i][1], sz = NBH_SHIFTS[i][2];
+                const node_t *nd = halo_node(s, oct, (int)a[0] + sx, (int)a[1] + sy, (int)a[2] + sz);
+                uint32_t naff = nd ? nd->cdf_aff : 0u;
+                REAL ndist = nd ? nd->cdf_distance : MAX_FLT;
+                v3 dpt = vadd(ref, vmul(V((REAL)sx, (REAL)sy, (REAL)sz), dx));
+                REAL weight = vget(w[0], sx) * vget(w[1], sy) * vget(w[2], sz);
+                uint32_t combined = naff & pa & AFF_MASK;
+                uint32_t sdiff = ((naff >> AFF_SIGN_SHIFT) ^ (pa >> AFF_SIGN_SHIFT)) & combined;
+                REAL pv[4] = {dpt.x, dpt.y, dpt.z, (REAL)1.0};
+                if (combined != 0) {
+                    REAL dd = sdiff == 0 ? ndist : -ndist;
+                    for (int r = 0; r < 4; ++r)
+                        for (int c = 0; c < 4; ++c) q[r][c] += pv[r] * pv[c] * weight;
+                    for (int r = 0; r < 4; ++r) u[r] += pv[r] * (weight * dd);
+                }
+            }
+            REAL qi[4][4];
+            REAL det = inv4(q, qi);
+            if (det > (REAL)1.0e-8) {
+                REAL r[4];
+                for (int i = 0; i < 4; ++i) r[i] = qi[i][0] * u[0] + qi[i][1] * u[1] + qi[i][2] * u[2] + qi[i][3] * u[3];
+                v3 nv = V(r[0], r[1], r[2]);
+                REAL len = vlen(nv);
+                s->cdf_normal[pid] = len > (REAL)1.0e-6 ? vdiv(nv, len) : V(0, 0, 0);
+                s->cdf_sd[pid] = r[3];
+                s->cdf_rigid_vel[pid] = V(0, 0, 0);
+                s->cdf_aff[pid] = pa;
+            } else {
+                s->cdf_normal[pid] = V(0, 0, 0);
+                s->cdf_sd[pid] = 0;
+                s->cdf_rigid_vel[pid] = V(0, 0, 0);
+                s->cdf_aff[pid] = 0;
+            }
+        }
+    }
+}
+
+/* src_mpm/pipeline.rs:385-526 MpmPipeline::step; with CPIC, the node and
+ * particle CDF passes run between the sort and P2G. */
 int orc_step(scene_t *s) {
     update_world_com(s);
     orc_sort(s);
+    if (s->use_cpic) {
+        orc_grid_update_cdf(s);
+        orc_g2p_cdf(s);
+    }
     orc_p2g(s);
     orc_grid_update(s);
     orc_g2p(s);

@@ -56,7 +56,12 @@ def lib(precision: str = "f32"):
         getattr(L, name).restype = C.c_int
     L.orc_run.argtypes = [C.c_void_p, C.c_uint32]
     L.orc_run.restype = C.c_int
-    for name in ("orc_p2g", "orc_grid_update", "orc_g2p", "orc_particle_update"):
+    L.orc_set_boundary_friction.argtypes = [C.c_void_p, _f]
+    L.orc_get_cdf.argtypes = [C.c_void_p, _f]
+    L.orc_inv4.argtypes = [_d, _d]
+    L.orc_inv4.restype = C.c_double
+    for name in ("orc_p2g", "orc_grid_update", "orc_g2p", "orc_particle_update", "orc_grid_update_cdf",
+                 "orc_g2p_cdf"):
         getattr(L, name).argtypes = [C.c_void_p]
     for name in ("orc_num_blocks", "orc_status", "orc_capacity", "orc_sorted_len", "orc_timestep_bound_bits"):
         getattr(L, name).argtypes = [C.c_void_p]
@@ -111,6 +116,21 @@ class OracleScene:
                 (p.pos, p.vel, p.aff, p.def_grad, p.vel_grad_det, p.mass, p.init_volume, p.damping)]
         ints = [np.ascontiguousarray(a, dtype=np.uint32) for a in (p.enabled, p.fixed, p.model)]
         self.L.orc_set_particles(self.h, *[_ptr(a, _f) for a in arrs], *[_ptr(a, _u) for a in ints])
+        bf = np.ascontiguousarray(p.boundary_friction, dtype=np.float32)
+        self.L.orc_set_boundary_friction(self.h, _ptr(bf, _f))
+
+    def cdf(self) -> dict:
+        """Particle Cdf (CPIC): normal, signed distance, rigid velocity, affinity bits."""
+        out = np.zeros((self.n, 8), np.float32)
+        self.L.orc_get_cdf(self.h, _ptr(out, _f))
+        return dict(normal=out[:, :3], signed_distance=out[:, 3], rigid_vel=out[:, 4:7],
+                    affinity=out[:, 7].copy().view(np.uint32))
+
+    def grid_update_cdf(self):
+        self.L.orc_grid_update_cdf(self.h)
+
+    def g2p_cdf(self):
+        self.L.orc_g2p_cdf(self.h)
 
     def set_colliders(self, colliders, tri_vertices=None):
         cols = np.ascontiguousarray(colliders)
@@ -242,6 +262,14 @@ def bc_project(ty, friction, vel, n, precision="f32") -> np.ndarray:
     out = np.zeros(3, np.float32)
     lib(precision).orc_bc_project(ty, friction, _ptr(v, _f), _ptr(nn, _f), _ptr(out, _f))
     return out
+
+
+def inv4(m, precision="f64"):
+    """(inverse, determinant) of a 4x4 matrix by the oracle's 2x2-minor expansion."""
+    a = np.ascontiguousarray(m, np.float64).reshape(16)
+    out = np.zeros(16, np.float64)
+    det = lib(precision).orc_inv4(_ptr(a, _d), _ptr(out, _d))
+    return out.reshape(4, 4), det
 
 
 def prefix_sum(values) -> np.ndarray:

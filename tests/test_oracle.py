@@ -296,3 +296,34 @@ def test_timestep_bound_closed_form(oracle_built):
         batch.vel[:] = (0.0, 0.0, 3.0 * speed)
         got = OracleScene(sc).timestep_bound_bits() / 1e12
         assert got == pytest.approx(min(0.5 * dx / (3.0 * speed), dx / (3.0 * speed)), rel=1e-5)
+
+
+def test_inv4_matches_numpy(oracle_built):
+    from oracle.oracle import inv4
+    rng = np.random.default_rng(3)
+    for _ in range(5):
+        m = rng.standard_normal((4, 4))
+        inv, det = inv4(m)
+        assert np.allclose(inv, np.linalg.inv(m), atol=1e-10)
+        assert det == pytest.approx(np.linalg.det(m), rel=1e-10)
+
+
+def test_cpic_keeps_particles_at_the_colliders(oracle_built):
+    """CPIC (analytic colliders): particles near the floor and the moving ball
+    take affinities, come closer to the surfaces than the grid-projection band
+    of the non-CPIC path (1.5 dx), stay outside the ball to a fraction of a
+    cell, and none is lost to an inverted F, where the non-CPIC run loses some."""
+    from oracle.oracle import OracleScene
+    sc = scenes.cpic_drop()
+    runs = {}
+    for cpic in (False, True):
+        o = OracleScene(sc)
+        o.set_use_cpic(cpic)
+        o.step(100)
+        runs[cpic] = (o.particles(), o.cdf())
+    p, c = runs[True]
+    ball = np.array([12.8 + 2.0 * 0.1, 12.8, 0.0])
+    assert p["enabled"].all() and not runs[False][0]["enabled"].all()
+    assert (c["affinity"] != 0).sum() > 100
+    assert p["pos"][:, 2].min() < 0.5 * 1.5 * sc.dx < runs[False][0]["pos"][:, 2].min()
+    assert np.linalg.norm(p["pos"] - ball, axis=1).min() > 2.0 - 0.5 * sc.dx
