@@ -55,7 +55,7 @@ struct DevPtrs {
     float4* pcdf;
 };
 
-constexpr uint32_t kScanTile = 1024;  // blocks per scan tile
+constexpr uint32_t kScanTile = 256;  // blocks per scan tile (one per thread of a scan CTA)
 
 struct LaunchCfg {
     int sm_count;

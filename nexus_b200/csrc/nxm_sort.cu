@@ -89,6 +89,26 @@ __device__ __forceinline__ uint32_t warp_agg_add(uint32_t key, uint32_t* addr) {
     return base + rank;
 }
 
+// Warp-aggregated atomicAdd without a result (fire-and-forget).
+__device__ __forceinline__ void warp_agg_red(uint32_t key, uint32_t* addr) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t peers = __match_any_sync(0xFFFFFFFFu, key);
+    if (key != NONE && lane == (uint32_t)(__ffs(peers) - 1)) atomicAdd(addr, (uint32_t)__popc(peers));
+}
+
+// The contiguous particle range [lo, hi) of this warp (a multiple of 32 long):
+// with particles stored in block order, a warp's consecutive passes mostly see
+// the same block, which lets the passes below skip repeated hash work.
+__device__ __forceinline__ void warp_range(uint32_t n, uint32_t& lo, uint32_t& hi) {
+    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+    const uint32_t per_warp = ((n + nwarps - 1) / nwarps + 31u) & ~31u;
+    lo = min(warp * per_warp, n);
+    hi = min(lo + per_warp, n);
+}
+
+constexpr int kSortBatch = 4;  // passes of 32 particles whose loads are issued together
+
 __device__ __forceinline__ bool spills(uint32_t ax, uint32_t ay, uint32_t az, int sx, int sy, int sz) {
     // sort.rs:320-329, EXTRA_PARTICLE_MIN_SHIFT = 2
     return (sx == 0 || ax >= 2) && (sy == 0 || ay >= 2) && (sz == 0 || az >= 2);
@@ -126,35 +146,44 @@ __global__ void __launch_bounds__(256) k_touch_primary(DevPtrs P) {
     const uint32_t bcap = P.params->block_capacity;
     const bool cached = P.counters->codes_valid != 0;
     const uint32_t lane = threadIdx.x & 31u;
-    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
-    const uint32_t per_warp = ((n + nwarps - 1) / nwarps + 31u) & ~31u;
-    const uint32_t lo = min(warp * per_warp, n), hi = min(lo + per_warp, n);
+    uint32_t lo, hi;
+    warp_range(n, lo, hi);
     uint32_t known = NONE;  // a key this warp has already inserted
-    for (uint32_t base = lo; base < hi; base += 32u) {
-        const uint32_t p = base + lane;
-        const bool active = p < hi;
-        uint32_t key = NONE;
-        if (active) {
-            if (cached) {
-                key = __ldg(&P.pcode[p].x);
-            } else {
-                float4 xm = __ldg(reinterpret_cast<const float4*>(&P.kin[p]));
-                CellInfo ci = cell_info(dx, mk(xm.x, xm.y, xm.z));
-                int3 o = make_int3(0, 0, 0);
-                if (P.params->scene_blocks) o = scene_base_of(*P.params, P.pscene[P.pid_in ? P.pid_in[p] : p]);
-                key = pack_key(ci.bx + o.x, ci.by + o.y, ci.bz + o.z);
-                P.pcode[p] = make_uint2(key, ci.ax | (ci.ay << 2) | (ci.az << 4));
+    for (uint32_t base = lo; base < hi; base += 32u * kSortBatch) {
+        uint32_t keys[kSortBatch];
+#pragma unroll
+        for (int j = 0; j < kSortBatch; ++j) {
+            const uint32_t p = base + 32u * j + lane;
+            uint32_t key = NONE;
+            if (p < hi) {
+                if (cached) {
+                    key = __ldg(&P.pcode[p].x);
+                } else {
+                    float4 xm = __ldg(reinterpret_cast<const float4*>(&P.kin[p]));
+                    CellInfo ci = cell_info(dx, mk(xm.x, xm.y, xm.z));
+                    int3 o = make_int3(0, 0, 0);
+                    if (P.params->scene_blocks) o = scene_base_of(*P.params, P.pscene[P.pid_in ? P.pid_in[p] : p]);
+                    key = pack_key(ci.bx + o.x, ci.by + o.y, ci.bz + o.z);
+                    P.pcode[p] = make_uint2(key, ci.ax | (ci.ay << 2) | (ci.az << 4));
+                }
             }
+            keys[j] = key;
         }
-        const uint32_t need = (active && key != known) ? key : NONE;
-        if (__all_sync(0xFFFFFFFFu, need == NONE)) continue;
-        uint32_t peers = __match_any_sync(0xFFFFFFFFu, need);
-        if (need != NONE && lane == (uint32_t)(__ffs(peers) - 1))
-            hash_insert(P, key, key_x(key), key_y(key), key_z(key), true, 0, hmask, bcap);
-        // the last active lane's key is now in the table
-        const uint32_t last = min(31u, hi - 1u - base);
-        known = __shfl_sync(0xFFFFFFFFu, key, last);
+#pragma unroll
+        for (int j = 0; j < kSortBatch; ++j) {
+            const uint32_t b32 = base + 32u * j;
+            if (b32 >= hi) break;
+            const bool active = b32 + lane < hi;
+            const uint32_t key = keys[j];
+            const uint32_t need = (active && key != known) ? key : NONE;
+            if (!__all_sync(0xFFFFFFFFu, need == NONE)) {
+                const uint32_t peers = __match_any_sync(0xFFFFFFFFu, need);
+                if (need != NONE && lane == (uint32_t)(__ffs(peers) - 1))
+                    hash_insert(P, key, key_x(key), key_y(key), key_z(key), true, 0, hmask, bcap);
+            }
+            // the last active lane's key is now in the table
+            known = __shfl_sync(0xFFFFFFFFu, key, min(31u, hi - 1u - b32));
+        }
     }
 }
 
@@ -203,39 +232,57 @@ __global__ void __launch_bounds__(256) k_count(DevPtrs P) {
     const uint32_t n = P.params->n;
     const uint32_t hmask = P.params->hash_capacity - 1;
     const uint32_t lane = threadIdx.x & 31u;
-    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
-    for (uint32_t base = warp * 32u; base < n; base += nwarps * 32u) {
-        const uint32_t p = base + lane;
-        uint32_t h0 = NONE;
-        uint2 code = make_uint2(NONE, 0);
-        if (p < n) code = P.pcode[p];
-        {
-            // one probe per distinct block key in the warp
-            const uint32_t peers = __match_any_sync(0xFFFFFFFFu, p < n ? code.x : NONE);
-            const uint32_t leader = __ffs(peers) - 1;
-            if (p < n && lane == leader) h0 = hash_find(P, code.x, hmask);
-            h0 = __shfl_sync(0xFFFFFFFFu, h0, leader);
+    uint32_t lo, hi;
+    warp_range(n, lo, hi);
+    uint32_t known_key = NONE, known_h0 = NONE;  // the last key this warp looked up
+    for (uint32_t base = lo; base < hi; base += 32u * kSortBatch) {
+        uint2 codes[kSortBatch];
+#pragma unroll
+        for (int j = 0; j < kSortBatch; ++j) {
+            const uint32_t p = base + 32u * j + lane;
+            codes[j] = p < hi ? P.pcode[p] : make_uint2(NONE, 0u);
         }
-        if (p < n) {
-            P.phdr[p] = h0;
-            if (h0 == NONE) set_status(P.counters, STATUS_MISSING_BLOCK);
-        }
-        const uint32_t ax = code.y & 3u, ay = (code.y >> 2) & 3u, az = (code.y >> 4) & 3u;
-        uint32_t key = (h0 != NONE) ? h0 * 16u + az : NONE;
-        warp_agg_add(key, key != NONE ? &P.cursors[h0 * NUM_BUCKETS + az] : nullptr);
-        if (!kExtras) continue;
-        for (int i = 1; i < 8; ++i) {
-            int sx, sy, sz;
-            assoc_shift(i, sx, sy, sz);
-            uint32_t hi = NONE, e = 0;
-            if (h0 != NONE && spills(ax, ay, az, sx, sy, sz)) {
-                hi = P.nbh[h0 * NUM_NBH + (i - 1)];
-                if (hi == NONE) set_status(P.counters, STATUS_MISSING_BLOCK);
-                e = extra_bucket(az, sz);
+#pragma unroll
+        for (int j = 0; j < kSortBatch; ++j) {
+            const uint32_t b32 = base + 32u * j;
+            if (b32 >= hi) break;
+            const uint32_t p = b32 + lane;
+            const bool active = p < hi;
+            const uint2 code = codes[j];
+            const uint32_t key = active ? code.x : NONE;
+            uint32_t h0;
+            if (__all_sync(0xFFFFFFFFu, !active || key == known_key)) {
+                h0 = active ? known_h0 : NONE;
+            } else {  // one probe per distinct block key in the warp
+                const uint32_t peers = __match_any_sync(0xFFFFFFFFu, key);
+                const uint32_t leader = __ffs(peers) - 1;
+                uint32_t h = NONE;
+                if (active && lane == leader) h = hash_find(P, key, hmask);
+                h0 = __shfl_sync(0xFFFFFFFFu, h, leader);
             }
-            uint32_t k2 = (hi != NONE) ? hi * 16u + e : NONE;
-            warp_agg_add(k2, k2 != NONE ? &P.cursors[hi * NUM_BUCKETS + e] : nullptr);
+            const uint32_t last = min(31u, hi - 1u - b32);
+            known_key = __shfl_sync(0xFFFFFFFFu, key, last);
+            known_h0 = __shfl_sync(0xFFFFFFFFu, h0, last);
+            if (active) {
+                P.phdr[p] = h0;
+                if (h0 == NONE) set_status(P.counters, STATUS_MISSING_BLOCK);
+            }
+            const uint32_t ax = code.y & 3u, ay = (code.y >> 2) & 3u, az = (code.y >> 4) & 3u;
+            const uint32_t bkey = (h0 != NONE) ? h0 * 16u + az : NONE;
+            warp_agg_red(bkey, bkey != NONE ? &P.cursors[h0 * NUM_BUCKETS + az] : nullptr);
+            if (!kExtras) continue;
+            for (int i = 1; i < 8; ++i) {
+                int sx, sy, sz;
+                assoc_shift(i, sx, sy, sz);
+                uint32_t hn = NONE, e = 0;
+                if (h0 != NONE && spills(ax, ay, az, sx, sy, sz)) {
+                    hn = P.nbh[h0 * NUM_NBH + (i - 1)];
+                    if (hn == NONE) set_status(P.counters, STATUS_MISSING_BLOCK);
+                    e = extra_bucket(az, sz);
+                }
+                const uint32_t k2 = (hn != NONE) ? hn * 16u + e : NONE;
+                warp_agg_red(k2, k2 != NONE ? &P.cursors[hn * NUM_BUCKETS + e] : nullptr);
+            }
         }
     }
 }
@@ -356,32 +403,49 @@ __global__ void __launch_bounds__(256) k_finalize(DevPtrs P) {
     const uint32_t n = P.params->n;
     const uint32_t scap = P.params->sorted_capacity;
     const uint32_t lane = threadIdx.x & 31u;
-    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
-    for (uint32_t base = warp * 32u; base < n; base += nwarps * 32u) {
-        const uint32_t p = base + lane;
-        uint32_t h0 = NONE;
-        uint32_t code = 0;
-        if (p < n) {
-            h0 = P.phdr[p];
-            code = P.pcode[p].y;
+    const uint32_t lt_mask = (1u << lane) - 1u;
+    uint32_t lo, hi;
+    warp_range(n, lo, hi);
+    for (uint32_t base = lo; base < hi; base += 32u * kSortBatch) {
+        uint32_t h0[kSortBatch], code[kSortBatch];
+#pragma unroll
+        for (int j = 0; j < kSortBatch; ++j) {
+            const uint32_t p = base + 32u * j + lane;
+            h0[j] = p < hi ? P.phdr[p] : NONE;
+            code[j] = p < hi ? P.pcode[p].y : 0u;
         }
-        const uint32_t ax = code & 3u, ay = (code >> 2) & 3u, az = (code >> 4) & 3u;
-        uint32_t key = (h0 != NONE) ? h0 * 16u + az : NONE;
-        uint32_t slot = warp_agg_add(key, key != NONE ? &P.cursors[h0 * NUM_BUCKETS + az] : nullptr);
-        if (key != NONE && slot < scap) P.sorted[slot] = p;
-        if (!kExtras) continue;
-        for (int i = 1; i < 8; ++i) {
-            int sx, sy, sz;
-            assoc_shift(i, sx, sy, sz);
-            uint32_t hi = NONE, e = 0;
-            if (h0 != NONE && spills(ax, ay, az, sx, sy, sz)) {
-                hi = P.nbh[h0 * NUM_NBH + (i - 1)];
-                e = extra_bucket(az, sz);
+        // the bucket atomics of all passes in flight together, then the scatter
+        uint32_t key[kSortBatch], leader[kSortBatch], rank[kSortBatch], got[kSortBatch];
+#pragma unroll
+        for (int j = 0; j < kSortBatch; ++j) {
+            const uint32_t az = (code[j] >> 4) & 3u;
+            key[j] = (h0[j] != NONE) ? h0[j] * 16u + az : NONE;
+            const uint32_t peers = __match_any_sync(0xFFFFFFFFu, key[j]);
+            leader[j] = __ffs(peers) - 1;
+            rank[j] = __popc(peers & lt_mask);
+            got[j] = 0u;
+            if (key[j] != NONE && lane == leader[j])
+                got[j] = atomicAdd(&P.cursors[h0[j] * NUM_BUCKETS + az], (uint32_t)__popc(peers));
+        }
+#pragma unroll
+        for (int j = 0; j < kSortBatch; ++j) {
+            const uint32_t p = base + 32u * j + lane;
+            const uint32_t slot = __shfl_sync(0xFFFFFFFFu, got[j], leader[j]) + rank[j];
+            if (key[j] != NONE && slot < scap) P.sorted[slot] = p;
+            if (!kExtras) continue;
+            const uint32_t ax = code[j] & 3u, ay = (code[j] >> 2) & 3u, az = (code[j] >> 4) & 3u;
+            for (int i = 1; i < 8; ++i) {
+                int sx, sy, sz;
+                assoc_shift(i, sx, sy, sz);
+                uint32_t hn = NONE, e = 0;
+                if (h0[j] != NONE && spills(ax, ay, az, sx, sy, sz)) {
+                    hn = P.nbh[h0[j] * NUM_NBH + (i - 1)];
+                    e = extra_bucket(az, sz);
+                }
+                const uint32_t k2 = (hn != NONE) ? hn * 16u + e : NONE;
+                const uint32_t s2 = warp_agg_add(k2, k2 != NONE ? &P.cursors[hn * NUM_BUCKETS + e] : nullptr);
+                if (k2 != NONE && s2 < scap) P.sorted[s2] = p;
             }
-            uint32_t k2 = (hi != NONE) ? hi * 16u + e : NONE;
-            uint32_t s2 = warp_agg_add(k2, k2 != NONE ? &P.cursors[hi * NUM_BUCKETS + e] : nullptr);
-            if (k2 != NONE && s2 < scap) P.sorted[s2] = p;
         }
     }
 }

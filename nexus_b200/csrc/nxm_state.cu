@@ -904,10 +904,6 @@ int upload_particles(nxm_state* s, const nxm_particles_soa* p, uint32_t count) {
         for (int w = 0; w < ns; ++w) st[w] = bits_f(m.data[w]);
         hs[i] = make_float4(st[0], st[1], st[2], st[3]);
     }
-    auto append = [count](auto& v, const auto* src, auto dflt) {
-        if (src) v.insert(v.end(), src, src + count);
-        else v.insert(v.end(), count, dflt);
-    };
     if (s->chunks_used) s->slot2chunk.insert(s->slot2chunk.end(), count, NONE);
     rc = sync_materials(s);
     if (rc) return rc;

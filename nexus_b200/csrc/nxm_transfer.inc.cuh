@@ -308,6 +308,17 @@ __device__ __forceinline__ void g2p_particle(const DevPtrs& P, const Params& prm
         v = v + pnormal * (dt * -corrected * 1.0e3f);
     }
 #endif
+    // The new position, velocity and block key follow from the gather alone:
+    // written ahead of the constitutive update (fewer values live across it);
+    // a particle that the check after it disables is rewritten there.
+    const bool nan = (np_.x != np_.x) || (np_.y != np_.y) || (np_.z != np_.z);
+    kr[0] = make_float4(np_.x, np_.y, np_.z, mass);
+    kr[1] = make_float4(v.x, v.y, v.z, __uint_as_float(flags));
+    {
+        const CellInfo nc = cell_info(dx, np_);
+        P.pcode[dst] = make_uint2(pack_key(nc.bx + key_off.x, nc.by + key_off.y, nc.bz + key_off.z),
+                                  nc.ax | (nc.ay << 2) | (nc.az << 4));
+    }
     const m3 A = grad;
     if (tag != MODEL_FLUID) {
         F = F + (A * dt) * F;
@@ -325,19 +336,16 @@ __device__ __forceinline__ void g2p_particle(const DevPtrs& P, const Params& prm
     }
     const m3 tau = model_update<NXM_FAST>(tag, mat.w, st, F, A);
     m3 aff = A * mass - tau * (init_volume * inv_d * dt);
-    v3 new_pos = pt;
-    const bool nan = (np_.x != np_.x) || (np_.y != np_.y) || (np_.z != np_.z);
-    if (!nan && det(F) > 0.0f) {
-        new_pos = np_;
-    } else {
+    if (nan || !(det(F) > 0.0f)) {  // disabled: rewrite what was written ahead
         flags &= ~PFLAG_ENABLED;
-        v = splat(0.f);
         F = mident();
         aff = mzero();
-        mass = 0.f;
+        kr[0] = make_float4(pt.x, pt.y, pt.z, 0.f);
+        kr[1] = make_float4(0.f, 0.f, 0.f, __uint_as_float(flags));
+        const CellInfo oc = cell_info(dx, pt);
+        P.pcode[dst] = make_uint2(pack_key(oc.bx + key_off.x, oc.by + key_off.y, oc.bz + key_off.z),
+                                  oc.ax | (oc.ay << 2) | (oc.az << 4));
     }
-    kr[0] = make_float4(new_pos.x, new_pos.y, new_pos.z, mass);
-    kr[1] = make_float4(v.x, v.y, v.z, __uint_as_float(flags));
     kr[2] = make_float4(aff.c0.x, aff.c0.y, aff.c0.z, vgd);
     kr[3] = make_float4(aff.c1.x, aff.c1.y, aff.c1.z, 0.f);
     kr[4] = make_float4(aff.c2.x, aff.c2.y, aff.c2.z, 0.f);
@@ -347,10 +355,6 @@ __device__ __forceinline__ void g2p_particle(const DevPtrs& P, const Params& prm
     dw[2] = make_float4(F.c2.x, F.c2.y, F.c2.z, d2.w);
     if (mat.has_state) P.pstate_out[dst] = make_float4(st[0], st[1], st[2], st[3]);
     if (P.pid_in) P.pid_out[dst] = P.pid_in[src];
-    // block key of the new position, for the next step's activation
-    const CellInfo nc = cell_info(dx, new_pos);
-    P.pcode[dst] = make_uint2(pack_key(nc.bx + key_off.x, nc.by + key_off.y, nc.bz + key_off.z),
-                              nc.ax | (nc.ay << 2) | (nc.az << 4));
 }
 
 #ifndef NXM_G2P_MIN_CTAS
