@@ -209,7 +209,8 @@ __device__ __forceinline__ void g2p_particle(const DevPtrs& P, const Params& prm
         // Same sums, factored: with dpt_i = ref + s_i dx,
         //   grad = inv_d (v (x) ref + dx [Sx Sy Sz]),  S_a = sum_i w_i v_i s_i,a
         //   vgd  = inv_d (v . ref + dx (Sx.x + Sy.y + Sz.z))
-        // so each node costs one weight product and 3 + (s != 0) FMAs.
+        // so each node costs one weight product and (1 + nonzero s) FMA pairs:
+        // the x, y components accumulate as packed f32x2 (FFMA2), z on its own.
         const float inv_dx = prm.inv_dx;
         const v3 ref = assoc_cell_of(dx, pt) * dx - pt;
         const v3 wx = kernel_eval_all(-ref.x * inv_dx);
@@ -217,7 +218,8 @@ __device__ __forceinline__ void g2p_particle(const DevPtrs& P, const Params& prm
         const v3 wz = kernel_eval_all(-ref.z * inv_dx);
         const CellInfo ci = cell_info(dx, pt);
         const uint32_t packed = ci.ax + 6u * ci.ay + 36u * ci.az;
-        v3 sxv = splat(0.f), syv = splat(0.f), szv = splat(0.f);
+        float2 vxy = make_float2(0.f, 0.f), sxxy = vxy, syxy = vxy, szxy = vxy;
+        float vz = 0.f, sxz = 0.f, syz = 0.f, szz = 0.f;
 #pragma unroll
         for (int sz = 0; sz < 3; ++sz) {
 #pragma unroll
@@ -226,14 +228,30 @@ __device__ __forceinline__ void g2p_particle(const DevPtrs& P, const Params& prm
 #pragma unroll
                 for (int sx = 0; sx < 3; ++sx) {
                     const float4 h = halo[packed + (uint32_t)(sx + 6 * sy + 36 * sz)];
-                    const v3 wc = mk(h.x, h.y, h.z) * (vget(wx, sx) * wyz);
-                    velocity = velocity + wc;
-                    if (sx) sxv = sxv + wc * (float)sx;
-                    if (sy) syv = syv + wc * (float)sy;
-                    if (sz) szv = szv + wc * (float)sz;
+                    const float2 hxy = make_float2(h.x, h.y);
+                    const float w = vget(wx, sx) * wyz;
+                    vxy = __ffma2_rn(make_float2(w, w), hxy, vxy);
+                    vz = fmaf(w, h.z, vz);
+                    if (sx) {
+                        const float ws = w * (float)sx;
+                        sxxy = __ffma2_rn(make_float2(ws, ws), hxy, sxxy);
+                        sxz = fmaf(ws, h.z, sxz);
+                    }
+                    if (sy) {
+                        const float ws = w * (float)sy;
+                        syxy = __ffma2_rn(make_float2(ws, ws), hxy, syxy);
+                        syz = fmaf(ws, h.z, syz);
+                    }
+                    if (sz) {
+                        const float ws = w * (float)sz;
+                        szxy = __ffma2_rn(make_float2(ws, ws), hxy, szxy);
+                        szz = fmaf(ws, h.z, szz);
+                    }
                 }
             }
         }
+        velocity = mk(vxy.x, vxy.y, vz);
+        const v3 sxv = mk(sxxy.x, sxxy.y, sxz), syv = mk(syxy.x, syxy.y, syz), szv = mk(szxy.x, szxy.y, szz);
         grad = (outer(velocity, ref) + mkm(sxv, syv, szv) * dx) * inv_d;
         vgd = (dot(velocity, ref) + dx * (sxv.x + syv.y + szv.z)) * inv_d;
     } else if (flags & PFLAG_ENABLED) {
