@@ -252,6 +252,7 @@ def run_ours(args, world, rank, local):
     del st
     batched = measure_batched(args, world, rank, torch) if args.batched_steps > 0 else None
     serving = measure_serving(args, torch) if (args.serving_requests > 0 and world == 1) else None
+    coupled = measure_coupled(args, torch) if (args.coupled_steps > 0 and world == 1) else None
 
     if rank != 0:
         return
@@ -280,6 +281,7 @@ def run_ours(args, world, rank, local):
         "cpu_baseline": cpu,
         "batched": batched,
         "serving": serving,
+        "coupled": coupled,
     }
     print(json.dumps(line), flush=True)
 
@@ -340,6 +342,66 @@ def measure_batched(args, world, rank, torch):
                                             f"timed steps after 3 warm-up, summed over scenes"},
             "speedup_vs_plain": value / plain, "dx": mix[0].dx, "dt": mix[0].dt,
             "parallelism": f"scene-sharded{world}" if world > 1 else "single"}
+
+
+def measure_coupled(args, torch):
+    """The coupled batched mix (configs[3]: 64 sand scenes, each with eight
+    kinematic bodies on seeded trajectories driven every step and a
+    20,000-triangle height-field floor) in one state, against the same scenes
+    stepped one by one with the same driving."""
+    from nexus_b200 import scenes as S
+    from nexus_b200.mpm import (MpmPipeline, batched_state_from_scenes, batched_collider_offsets,
+                                drive_kinematics, state_from_scene)
+    mix = S.coupled_mix(count=args.coupled_scenes)
+    n = sum(sc.n for sc in mix)
+    pipe = MpmPipeline()
+    st, slots = batched_state_from_scenes(mix)
+    offs = batched_collider_offsets(mix, slots)
+    dt = mix[0].dt
+    stream = torch.cuda.ExternalStream(st.cuda_stream())
+    step = 0
+    for _ in range(3):
+        drive_kinematics(st, mix, offs, step * dt)
+        pipe.step(st)
+        step += 1
+    st.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.coupled_steps):
+        drive_kinematics(st, mix, offs, step * dt)
+        pipe.step(st)
+        step += 1
+    ev1.record(stream)
+    ev1.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    st.synchronize()
+    del st
+    plain_ms = 0.0
+    for sc in mix:
+        one = state_from_scene(sc)
+        s1 = torch.cuda.ExternalStream(one.cuda_stream())
+        for k in range(3):
+            drive_kinematics(one, [sc], [0], k * dt)
+            pipe.step(one)
+        one.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(s1)
+        for k in range(args.plain_steps):
+            drive_kinematics(one, [sc], [0], (3 + k) * dt)
+            pipe.step(one)
+        b.record(s1)
+        b.synchronize()
+        plain_ms += a.elapsed_time(b) / args.plain_steps
+        one.synchronize()
+        del one
+    value = n * args.coupled_steps / (ms / 1e3)
+    plain = n / (plain_ms / 1e3)
+    return {"workload": f"coupled_mix_{len(mix)}", "scenes": len(mix), "particles": n,
+            "colliders_per_scene": int(len(mix[0].colliders)), "triangles_per_scene": int(len(mix[0].tri_vertices) // 3),
+            "value": value, "unit": UNIT, "steps": args.coupled_steps, "ms_per_step": ms / args.coupled_steps,
+            "plain_scene_by_scene": {"value": plain, "unit": UNIT, "ms_per_step": plain_ms},
+            "speedup_vs_plain": value / plain, "dx": mix[0].dx, "dt": dt,
+            "how": "timed steps include writing every kinematic body's velocity (one stream-ordered call per step)"}
 
 
 def measure_serving(args, torch):
@@ -450,6 +512,8 @@ def main():
     ap.add_argument("--batched-scenes", type=int, default=256)
     ap.add_argument("--plain-steps", type=int, default=10)
     ap.add_argument("--serving-requests", type=int, default=200, help="0: skip the serving measurement")
+    ap.add_argument("--coupled-steps", type=int, default=50, help="timed steps of the coupled mix (0: skip it)")
+    ap.add_argument("--coupled-scenes", type=int, default=64)
     ap.add_argument("--traffic", type=float, default=TRAFFIC_PER_STEP,
                     help="DRAM bytes per step from an ncu capture (profiles/k_p2g_k_g2p_update_sand_water_2M.md)")
     args = ap.parse_args()

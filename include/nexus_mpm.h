@@ -198,6 +198,13 @@ NXM_API int nxm_state_set_colliders(nxm_state* state, const nxm_collider* collid
  * d(pose)/dt each step; the step integrates the pose from it). */
 NXM_API int nxm_state_set_collider_velocity(nxm_state* state, uint32_t index, const float linvel[3], const float angvel[3]);
 
+/* Kinematic driving of colliders [first, first + count) at once: 6 floats
+ * each (linear then angular velocity).  Ordered on the state's stream before
+ * the next step, without a host synchronisation (the source array may be
+ * reused as soon as the call returns).  No reference counterpart: the
+ * reference writes body velocities one buffer at a time. */
+NXM_API int nxm_state_set_collider_velocities(nxm_state* state, uint32_t first, uint32_t count, const float* vel6);
+
 /* Reads collider i's pose: quaternion x,y,z,w then translation (7 floats). */
 NXM_API int nxm_state_read_collider_pose(nxm_state* state, uint32_t index, float out[7]);
 

@@ -248,6 +248,17 @@ __global__ void k_move_records(PKin* __restrict__ kin, PDef* __restrict__ def, f
     }
 }
 
+// Kinematic driving of many colliders: vel6[i] = linvel xyz, angvel xyz of collider first + i.
+__global__ void k_set_velocities(DevCollider* __restrict__ cols, const float* __restrict__ vel6, uint32_t first,
+                                 uint32_t count) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+        DevCollider& c = cols[first + i];
+        const float* v = vel6 + 6 * (size_t)i;
+        c.linvel[0] = v[0]; c.linvel[1] = v[1]; c.linvel[2] = v[2];
+        c.angvel[0] = v[3]; c.angvel[1] = v[4]; c.angvel[2] = v[5];
+    }
+}
+
 __global__ void k_fill(uint32_t* __restrict__ out, uint32_t value, uint32_t count) {
     for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < count; t += gridDim.x * blockDim.x) out[t] = value;
 }
@@ -335,6 +346,8 @@ struct nxm_state {
     std::vector<DevCollider> colliders;
     DevCollider* d_colliders = nullptr;
     uint32_t col_cap = 0;
+    float* d_vel6 = nullptr;  // staging of bulk collider velocities
+    size_t vel_cap = 0;
 
     // batched scenes (scene_blocks != 0): scene slots on the block-key grid
     // (see Params), each a contiguous range of particle ids with its own colliders
@@ -1212,7 +1225,7 @@ void nxm_state_destroy(nxm_state* s) {
     invalidate_graph(s);
     free_grid(s);
     free_particles(s);
-    dfree(s->d_materials); dfree(s->d_colliders); dfree(s->d_tris); dfree(s->d_bvh); dfree(s->d_scene_cols); dfree(s->d_params); dfree(s->d_counters);
+    dfree(s->d_materials); dfree(s->d_colliders); dfree(s->d_tris); dfree(s->d_bvh); dfree(s->d_scene_cols); dfree(s->d_vel6); dfree(s->d_params); dfree(s->d_counters);
     dfree(s->d_pack); dfree(s->d_offsets);
     if (s->h_counters) cudaFreeHost(s->h_counters);
     if (s->stream) cudaStreamDestroy(s->stream);
@@ -1266,6 +1279,25 @@ int nxm_state_set_collider_velocity(nxm_state* s, uint32_t index, const float li
     char* base = reinterpret_cast<char*>(s->d_colliders + index);
     NXM_TRY(cudaMemcpyAsync(base + offsetof(DevCollider, linvel), buf, 32, cudaMemcpyHostToDevice, s->stream));
     NXM_TRY(cudaStreamSynchronize(s->stream));
+    return NXM_OK;
+}
+
+int nxm_state_set_collider_velocities(nxm_state* s, uint32_t first, uint32_t count, const float* vel6) {
+    if (!s || (count && !vel6) || first > s->colliders.size() || count > s->colliders.size() - first)
+        return NXM_E_INVALID;
+    if (count == 0) return NXM_OK;
+    const size_t need = 6 * (size_t)count;
+    if (need > s->vel_cap) {
+        NXM_TRY(cudaStreamSynchronize(s->stream));  // the old staging buffer may still be read
+        dfree(s->d_vel6);
+        NXM_TRY(dalloc(&s->d_vel6, need));
+        s->vel_cap = need;
+    }
+    // pageable source: the copy has taken the data when the call returns
+    NXM_TRY(cudaMemcpyAsync(s->d_vel6, vel6, 4 * need, cudaMemcpyHostToDevice, s->stream));
+    k_set_velocities<<<(count + 127) / 128, 128, 0, s->stream>>>(s->d_colliders, s->d_vel6, first, count);
+    s->launches += 1;
+    NXM_TRY(cudaGetLastError());
     return NXM_OK;
 }
 

@@ -92,6 +92,7 @@ SIGNATURES = {
     "nxm_debug_sort": (C.c_int, [_vp, _vp, C.c_int]),
     "nxm_state_estimate_timestep_bound": (C.c_int, [_vp, _f, _u]),
     "nxm_read_cdf": (C.c_int, [_vp, _f]),
+    "nxm_state_set_collider_velocities": (C.c_int, [_vp, C.c_uint32, C.c_uint32, _f]),
     "nxm_state_enable_scenes": (C.c_int, [_vp, C.c_uint32]),
     "nxm_scene_capacity": (C.c_uint32, [_vp]),
     "nxm_scene_add": (C.c_int, [_vp, C.POINTER(ParticlesSoAC), C.c_uint32, _vp, C.c_uint32, _f, C.c_uint32, _u]),
@@ -223,6 +224,12 @@ class MpmState:
         out = np.zeros(7, np.float32)
         _check(self.lib.nxm_state_read_collider_pose(self.h, index, _p(out)), "read_collider_pose")
         return out
+
+    def set_collider_velocities(self, first: int, vel6):
+        """Linear + angular velocity (n, 6) of colliders first.. first + n, stream-ordered."""
+        v = np.ascontiguousarray(vel6, np.float32).reshape(-1, 6)
+        _check(self.lib.nxm_state_set_collider_velocities(self.h, first, len(v), _p(v, _f)),
+               "set_collider_velocities")
 
     def set_use_cpic(self, enabled: bool):
         _check(self.lib.nxm_state_set_use_cpic(self.h, int(enabled)), "set_use_cpic")
@@ -466,4 +473,26 @@ def batched_state_from_scenes(scenes_, deterministic: bool = False, scene_blocks
     slots = [st.add_scene(sc.particles, sc.colliders, sc.tri_vertices if sc.tri_vertices.size else None)
              for sc in scenes_]
     return st, slots
+
+
+def batched_collider_offsets(scenes_, slots) -> list:
+    """Index of each scene's first collider in a batched state's collider table
+    (the live scenes' colliders in scene-slot order), for kinematic driving."""
+    off, acc = {}, 0
+    for i in sorted(range(len(slots)), key=lambda k: slots[k]):
+        off[i] = acc
+        acc += len(scenes_[i].colliders)
+    return [off[i] for i in range(len(scenes_))]
+
+
+def drive_kinematics(state: MpmState, scenes_, offsets, t: float):
+    """Writes every kinematic body's velocity at time t (one stream-ordered call)."""
+    from .scenes import kinematic_velocities
+    total = max([o + len(sc.colliders) for o, sc in zip(offsets, scenes_)] + [0])
+    vel = np.zeros((total, 6), np.float32)
+    for o, sc in zip(offsets, scenes_):
+        idx, v = kinematic_velocities(sc, t)
+        vel[o + idx] = v
+    if total:
+        state.set_collider_velocities(0, vel)
 

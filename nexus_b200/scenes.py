@@ -58,6 +58,9 @@ class Scene:
     steps: int
     grid_capacity: int
     tri_vertices: np.ndarray = field(default_factory=lambda: np.zeros((0, 3), np.float32))
+    # kinematic bodies: rows (collider index, p0 xyz, v0 xyz, a xyz, omega, phi) of
+    # p(t) = p0 + v0 t + a sin(omega t + phi)
+    kinematics: np.ndarray = field(default_factory=lambda: np.zeros((0, 12), np.float64))
 
     @property
     def n(self) -> int:
@@ -249,3 +252,65 @@ def cpic_drop(n_side: int = 12, seed: int = 17, steps: int = 100) -> Scene:
     ball.linvel = (2.0, 0.0, 0.0)
     cols = collider_array(box_walls(0.0, L, BoundaryCondition.slip(), BoundaryCondition.slip(), thickness=2.0) + [ball])
     return Scene("cpic_drop", dx, 1.0e-3, (0.0, 0.0, -9.81), batch, cols, steps, grid_capacity_for(batch.n))
+
+
+def kinematic_velocities(scene: Scene, t: float) -> tuple[np.ndarray, np.ndarray]:
+    """(collider indices, (k, 6) linear + angular velocity) of the scene's
+    kinematic bodies at time t: dp/dt = v0 + a omega cos(omega t + phi)."""
+    k = scene.kinematics
+    if k.size == 0:
+        return np.zeros(0, np.int64), np.zeros((0, 6), np.float32)
+    om, ph = k[:, 10:11], k[:, 11:12]
+    v = k[:, 4:7] + k[:, 7:10] * om * np.cos(om * t + ph)
+    out = np.zeros((len(k), 6), np.float32)
+    out[:, :3] = v
+    return k[:, 0].astype(np.int64), out
+
+
+def coupled_scene(s: int, seed: int = 2000, dx: float = 1.0 / 128.0, n_min: int = 32768, n_max: int = 262144,
+                  floor_vertices: int = 101, steps: int = 300) -> Scene:
+    """Scene s of the coupled workload: a random box of N ~ logU(n_min, n_max)
+    Drucker-Prager sand particles (as the batched workload, placed above the
+    floor), eight kinematic bodies (cuboid, ball or capsule, size U(0.05,
+    0.2)) moving along p(t) = p0 + v0 t + a sin(omega t + phi) with seeded
+    parameters, a height-field trimesh floor (floor_vertices^2 vertices,
+    heights 0.05 + U(0, 0.02)), and six slip walls bounding [0, 1]^3."""
+    sd = seed + s
+    box = random_box_scene(sd, dx, n_min, n_max, ("sand",), steps, f"coupled_{s}")
+    pos = box.particles.pos
+    lift = max(0.0, 0.09 - float(pos[:, 2].min()))  # the box starts above the floor mesh
+    top = float(pos[:, 2].max()) + lift
+    pos[:, 2] += np.float32(lift - max(0.0, top - (1.0 - 4 * dx)))
+    u = uniform(sd + 7777, 8 * 16)
+    cols = box_walls(0.0, 1.0, BoundaryCondition.slip(), BoundaryCondition.slip())
+    kin = []
+    for b in range(8):
+        r = u[16 * b:16 * (b + 1)]
+        size = 0.05 + 0.15 * r[0]
+        p0 = np.array([0.2 + 0.6 * r[1], 0.2 + 0.6 * r[2], 0.2 + 0.4 * r[3]])
+        v0 = -0.2 + 0.4 * r[4:7]
+        a = 0.1 * r[7:10]
+        om, ph = 1.0 + 9.0 * r[10], 2.0 * math.pi * r[11]
+        start = tuple(p0 + a * math.sin(ph))
+        bc = BoundaryCondition.separate(0.3)
+        kind = int(r[12] * 3)
+        if kind == 0:
+            c = Collider.cuboid((size / 2, size / 2, size / 2), start, bc)
+        elif kind == 1:
+            c = Collider.ball(size / 2, start, bc)
+        else:
+            c = Collider.capsule((0.0, 0.0, -size / 2), (0.0, 0.0, size / 2), size / 4, start, bc)
+        kin.append([len(cols), *p0, *v0, *a, om, ph])
+        cols.append(c)
+    tri = height_field(floor_vertices, sd + 1)
+    cols.append(Collider.trimesh(0, len(tri), (0.0, 0.0, 0.0), BoundaryCondition.separate(0.3)))
+    box.colliders = collider_array(cols)
+    box.tri_vertices = tri.reshape(-1, 3)
+    box.kinematics = np.asarray(kin, np.float64)
+    return box
+
+
+def coupled_mix(count: int = 64, seed: int = 2000, steps: int = 300, **kw) -> list:
+    """The coupled batched workload: coupled_scene(s) for s in [0, count)."""
+    return [coupled_scene(s, seed, steps=steps, **kw) for s in range(count)]
+
