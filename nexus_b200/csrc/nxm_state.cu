@@ -259,6 +259,15 @@ __global__ void k_set_velocities(DevCollider* __restrict__ cols, const float* __
     }
 }
 
+// Fresh CPIC records: empty distance field, the particle's boundary friction (1 if none given).
+__global__ void k_init_pcdf(float4* __restrict__ pcdf, const float* __restrict__ bfric, uint32_t count) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+        pcdf[3 * (size_t)i] = make_float4(0.f, 0.f, 0.f, 0.f);
+        pcdf[3 * (size_t)i + 1] = make_float4(0.f, 0.f, 0.f, 0.f);
+        pcdf[3 * (size_t)i + 2] = make_float4(bfric ? bfric[i] : 1.0f, 0.f, 0.f, 0.f);
+    }
+}
+
 __global__ void k_fill(uint32_t* __restrict__ out, uint32_t value, uint32_t count) {
     for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < count; t += gridDim.x * blockDim.x) out[t] = value;
 }
@@ -924,10 +933,21 @@ int upload_particles(nxm_state* s, const nxm_particles_soa* p, uint32_t count) {
     NXM_TRY(cudaMemcpyAsync(s->def + s->n, hd.data(), sizeof(PDef) * count, cudaMemcpyHostToDevice, s->stream));
     NXM_TRY(cudaMemcpyAsync(s->pstate + s->n, hs.data(), sizeof(float4) * count, cudaMemcpyHostToDevice, s->stream));
     {  // CPIC fields start empty; boundary friction (default 1) scales the colliders' friction there
-        std::vector<float4> hc(3 * (size_t)count, make_float4(0.f, 0.f, 0.f, 0.f));
-        for (uint32_t i = 0; i < count; ++i) hc[3 * (size_t)i + 2].x = p->boundary_friction ? p->boundary_friction[i] : 1.f;
-        NXM_TRY(cudaMemcpyAsync(s->d_pcdf + 3 * (size_t)s->n, hc.data(), sizeof(float4) * hc.size(),
-                                cudaMemcpyHostToDevice, s->stream));
+        const float* bf = nullptr;
+        if (p->boundary_friction) {
+            if (count > s->pack_cap) {
+                NXM_TRY(cudaStreamSynchronize(s->stream));
+                dfree(s->d_pack);
+                NXM_TRY(dalloc(&s->d_pack, count));
+                s->pack_cap = count;
+            }
+            NXM_TRY(cudaMemcpyAsync(s->d_pack, p->boundary_friction, 4 * (size_t)count, cudaMemcpyHostToDevice,
+                                    s->stream));
+            bf = reinterpret_cast<const float*>(s->d_pack);
+        }
+        k_init_pcdf<<<grid_for_n(s, count), 256, 0, s->stream>>>(s->d_pcdf + 3 * (size_t)s->n, bf, count);
+        s->launches += 1;
+        NXM_TRY(cudaGetLastError());
     }
     if (s->permuted) {  // appended particles sit at slots == their ids
         k_iota<<<grid_for_n(s, count), 256, 0, s->stream>>>(s->pid + s->n, s->n, count);
