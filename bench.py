@@ -490,7 +490,8 @@ def measure_e2e(scene, args, torch):
     dt = time.perf_counter() - t0
     upload = sum(a.nbytes for a in batch.__dict__.values())
     return {"value": p.n * steps / dt, "unit": UNIT, "steps": steps,
-            "h2d_bytes_per_step": int(upload / steps + 32), "d2h_bytes_per_step": int(p.n * 12 / steps + 32),
+            # per step: a 32-byte collider velocity write, a 48-byte counters read (status)
+            "h2d_bytes_per_step": int(upload / steps + 32), "d2h_bytes_per_step": int(p.n * 12 / steps + 48),
             "how": "host wall clock: state create + SoA upload from pinned memory + per step (collider velocity "
                    "H2D, step, status D2H) + final positions D2H"}
 

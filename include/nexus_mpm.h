@@ -211,11 +211,24 @@ NXM_API int nxm_state_read_collider_pose(nxm_state* state, uint32_t index, float
 /* MpmState::use_cpic (src_mpm/pipeline.rs:69): CPIC coupling with the
  * colliders (node and particle distance fields, compatible / incompatible
  * P2G and G2P, penetration reprojection and penalty; two-way impulses off as
- * in the reference build).  Built for analytic colliders (ball, cuboid,
- * capsule): with a trimesh collider, enabling returns NXM_E_UNSUPPORTED (the
- * reference samples rigid particles on meshes for it).  CPIC steps run the
+ * in the reference build).  Analytic colliders (ball, cuboid, capsule) enter
+ * the node field directly (solver/grid_update_cdf.rs); trimesh colliders
+ * through rigid particles sampled on their surface at the cell width
+ * (sampling/sample_trimesh.rs, resampled when the colliders or the cell width
+ * change), moved with the collider pose each step, sorted into the blocks
+ * and projected on the nodes (solver/rigid_particle_update.rs,
+ * grid/sort.rs:165-249 and 493-667, solver/p2g_cdf.rs).  Trimesh CPIC is not
+ * available in batched-scene mode (NXM_E_UNSUPPORTED).  CPIC steps run the
  * gather-form transfers with particles in id order. */
 NXM_API int nxm_state_set_use_cpic(nxm_state* state, int enabled);
+/* Number of CPIC rigid particles (GpuRigidParticles::len,
+ * src_mpm/solver/particle.rs:351-354); 0 without CPIC or trimesh colliders. */
+NXM_API int nxm_state_num_rigid_particles(const nxm_state* state, uint32_t* count);
+/* The CPIC rigid particles in sampling order: local position xyz, owning
+ * collider (u32 bits), triangle index inside that collider's range (u32
+ * bits), 5 floats each (the reference's sample_points + sample_ids,
+ * sampling/sample_trimesh.rs:33-56). */
+NXM_API int nxm_read_rigid_particles(nxm_state* state, float* out);
 /* Particle Cdf (solver/particle.rs:35-50) of every particle: normal xyz,
  * signed distance, rigid velocity xyz, affinity bits (u32 bits), 8 floats
  * each; synchronizes. */

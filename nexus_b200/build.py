@@ -21,7 +21,7 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler",
           "--expt-relaxed-constexpr", f"-I{INCLUDE}", f"-I{CSRC}"]
 
 UNITS = {
-    "nxm_state.cu": [],
+    "nxm_state.cu": ["-Xcompiler", "-ffp-contract=off"],  # f32 trimesh sampling, operation by operation
     "nxm_sort.cu": [],
     "nxm_transfer_fast.cu": [],
     "nxm_transfer_det.cu": ["--fmad=false"],

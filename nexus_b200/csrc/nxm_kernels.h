@@ -53,6 +53,17 @@ struct DevPtrs {
     uint4* ncdf;
     float4* nodes_inc;
     float4* pcdf;
+    // CPIC rigid particles of the trimesh colliders: local and world
+    // position (w = packed triangle / collider word), block-activation flag,
+    // per block the count (then the placement cursor) and first entry of the
+    // block-sorted list (own block plus extras).
+    uint32_t nrp;
+    const float4* rp_local;
+    float4* rp_world;
+    uint8_t* rp_need;
+    uint32_t* rp_count;
+    uint32_t* rp_first;
+    uint32_t* rp_sorted;
 };
 
 constexpr uint32_t kScanTile = 256;  // blocks per scan tile (one per thread of a scan CTA)
@@ -77,7 +88,11 @@ namespace fast {
 // blocks its stencil reaches (the reference's full sorted-id layout, used by
 // the gather-form P2G); the scatter P2G needs the primaries only.
 // `canonical`: order each bucket by ascending particle id.
-void launch_sort(const DevPtrs& P, const LaunchCfg& c, bool with_extras, bool canonical, cudaStream_t s);
+// `rigid`: also activate the blocks of the CPIC rigid particles and sort them
+// by block (P.nrp > 0; their world positions already written).
+void launch_sort(const DevPtrs& P, const LaunchCfg& c, bool with_extras, bool canonical, cudaStream_t s,
+                 bool rigid = false);
+constexpr int kRigidSortLaunches = 5;
 void launch_p2g(const DevPtrs& P, const LaunchCfg& c, cudaStream_t s);
 void launch_grid_update(const DevPtrs& P, const LaunchCfg& c, cudaStream_t s);
 void launch_g2p_update(const DevPtrs& P, const LaunchCfg& c, cudaStream_t s);
@@ -92,6 +107,10 @@ void launch_timestep_bound(const DevPtrs& P, const LaunchCfg& c, cudaStream_t s)
 // CPIC distance fields: per node (analytic colliders), then per particle.
 void launch_grid_update_cdf(const DevPtrs& P, const LaunchCfg& c, cudaStream_t s);
 void launch_g2p_cdf(const DevPtrs& P, const LaunchCfg& c, cudaStream_t s);
+// CPIC rigid particles: world positions from the collider poses, and the
+// triangle projections merged into the node distance field.
+void launch_rigid_transform(const DevPtrs& P, const LaunchCfg& c, cudaStream_t s);
+void launch_p2g_cdf(const DevPtrs& P, const LaunchCfg& c, cudaStream_t s);
 void launch_grid_update(const DevPtrs& P, const LaunchCfg& c, cudaStream_t s);
 void launch_g2p_update(const DevPtrs& P, const LaunchCfg& c, cudaStream_t s);
 }  // namespace exact

@@ -149,6 +149,15 @@ struct alignas(16) Counters {
     uint32_t unsorted;      // particles without a block this step, placed after the sorted ones
                             // by the reordering G2P
     uint32_t dt_bound;      // CFL bound, (dt * 1e12) as u32 (written by the timestep-bound query)
+    uint32_t rigid_len;     // CPIC: entries of the block-sorted rigid-particle list
+    uint32_t pad[3];
 };
+static_assert(sizeof(Counters) == 48, "Counters layout");
+
+// CPIC rigid particle (a surface sample of a trimesh collider): position and
+// a packed word, triangle index into the state's triangle array in the low
+// kRigidTriBits bits, owning collider above them.
+constexpr uint32_t kRigidTriBits = 28;
+constexpr uint32_t kRigidTriMask = (1u << kRigidTriBits) - 1u;
 
 }  // namespace nxm

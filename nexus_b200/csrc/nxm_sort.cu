@@ -131,6 +131,7 @@ __global__ void k_sort_reset(DevPtrs P, uint32_t hash_cap) {
         P.counters->num_blocks = 0;
         P.counters->sorted_len = 0;
         P.counters->unsorted = 0;
+        P.counters->rigid_len = 0;
     }
 }
 
@@ -222,6 +223,8 @@ __global__ void __launch_bounds__(256) k_block_prep(DevPtrs P) {
             P.nbh[b * NUM_NBH + k] = hash_find(P, pack_key(v.x + sx, v.y + sy, v.z + sz), hmask);
         } else if (k < NUM_NBH + NUM_BUCKETS) {
             P.cursors[b * NUM_BUCKETS + (k - NUM_NBH)] = 0;
+        } else if (k == 63u && P.rp_count) {
+            P.rp_count[b] = 0;
         }
     }
 }
@@ -554,10 +557,130 @@ void launch_sort_positions(const DevPtrs& P, const LaunchCfg& c, const float4* p
 }
 
 
+// ---------------------------------------------------------------------------
+// CPIC rigid particles (src_mpm/grid/grid.rs:95-121, sort.rs:165-249, 493-667).
+// ---------------------------------------------------------------------------
+
+namespace {
+
+__device__ __forceinline__ CellInfo rigid_cell(const DevPtrs& P, uint32_t i, float dx) {
+    const float4 w = P.rp_world[i];
+    return cell_info(dx, mk(w.x, w.y, w.z));
+}
+
+// sort.rs:200-249 gpu_mark_rigid_particles_needing_block: a rigid particle
+// needs its own block when that block is missing while one of its +1
+// neighbours exists (without it the particle could not be listed there).
+// Runs on the hash as the particle passes left it, before any insertion.
+__global__ void __launch_bounds__(256) k_rigid_mark(DevPtrs P) {
+    const uint32_t hmask = P.params->hash_capacity - 1;
+    const float dx = P.params->dx;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < P.nrp; i += gridDim.x * blockDim.x) {
+        const CellInfo ci = rigid_cell(P, i, dx);
+        int k = 0;
+        for (; k < 8; ++k) {
+            int sx, sy, sz;
+            assoc_shift(k, sx, sy, sz);
+            if (hash_find(P, pack_key(ci.bx + sx, ci.by + sy, ci.bz + sz), hmask) != NONE) break;
+        }
+        P.rp_need[i] = (k > 0 && k < 8) ? 1u : 0u;
+    }
+}
+
+// sort.rs:165-198 gpu_touch_rigid_particle_blocks: the marked particles'
+// blocks join the neighbour-pass blocks (ids after the primaries).
+__global__ void __launch_bounds__(256) k_rigid_touch(DevPtrs P) {
+    const uint32_t hmask = P.params->hash_capacity - 1;
+    const uint32_t bcap = P.params->block_capacity;
+    const uint32_t nprim = min(__ldcg(&P.counters->num_primary), bcap);
+    const float dx = P.params->dx;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < P.nrp; i += gridDim.x * blockDim.x) {
+        if (!P.rp_need[i]) continue;
+        const CellInfo ci = rigid_cell(P, i, dx);
+        hash_insert(P, pack_key(ci.bx, ci.by, ci.bz), ci.bx, ci.by, ci.bz, false, nprim, hmask, bcap);
+    }
+}
+
+// The blocks a rigid particle is listed in: its own block (NONE if missing:
+// the particle is skipped) and each existing +1 neighbour its 3-cell range
+// reaches (sort.rs:509-553).  Returns how many; out[0] is the own block.
+__device__ __forceinline__ int rigid_blocks(const DevPtrs& P, uint32_t i, float dx, uint32_t hmask, uint32_t out[8]) {
+    const CellInfo ci = rigid_cell(P, i, dx);
+    const uint32_t h0 = hash_find(P, pack_key(ci.bx, ci.by, ci.bz), hmask);
+    if (h0 == NONE) return 0;
+    int n = 0;
+    out[n++] = h0;
+    for (int k = 1; k < 8; ++k) {
+        int sx, sy, sz;
+        assoc_shift(k, sx, sy, sz);
+        if (!spills(ci.ax, ci.ay, ci.az, sx, sy, sz)) continue;
+        const uint32_t hb = P.nbh[h0 * NUM_NBH + k - 1];
+        if (hb != NONE) out[n++] = hb;
+    }
+    return n;
+}
+
+// sort.rs:493-556 gpu_update_block_rigid_particle_count.
+__global__ void __launch_bounds__(256) k_rigid_count(DevPtrs P) {
+    const uint32_t hmask = P.params->hash_capacity - 1;
+    const float dx = P.params->dx;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < P.nrp; i += gridDim.x * blockDim.x) {
+        uint32_t hb[8];
+        const int n = rigid_blocks(P, i, dx, hmask, hb);
+        for (int k = 0; k < n; ++k) atomicAdd(&P.rp_count[hb[k]], 1u);
+    }
+}
+
+// Each block with rigid entries takes a contiguous range of the list (the
+// reference lays the ranges out by a prefix sum, sort.rs:558-600; p2g_cdf
+// reads one block's range, so the order of the ranges is free): one atomic
+// per warp on the list length, a warp scan for the lanes' offsets.  The
+// count becomes the placement cursor.
+__global__ void __launch_bounds__(256) k_rigid_alloc(DevPtrs P) {
+    const uint32_t nb = __ldcg(&P.counters->num_blocks);
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < nb; base += stride) {
+        const uint32_t b = base + lane;
+        const uint32_t cnt = b < nb ? P.rp_count[b] : 0u;
+        uint32_t incl = cnt;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t v = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+            if (lane >= (uint32_t)o) incl += v;
+        }
+        const uint32_t total = __shfl_sync(0xFFFFFFFFu, incl, 31);
+        uint32_t start = 0;
+        if (lane == 31u && total) start = atomicAdd(&P.counters->rigid_len, total);
+        start = __shfl_sync(0xFFFFFFFFu, start, 31);
+        if (b < nb) {
+            P.rp_first[b] = start + incl - cnt;
+            P.rp_count[b] = 0;
+        }
+    }
+}
+
+// sort.rs:602-667 gpu_finalize_rigid_particles_sort: the same block set as
+// the count pass, so every claimed slot stays inside its block's range.
+__global__ void __launch_bounds__(256) k_rigid_finalize(DevPtrs P) {
+    const uint32_t hmask = P.params->hash_capacity - 1;
+    const float dx = P.params->dx;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < P.nrp; i += gridDim.x * blockDim.x) {
+        uint32_t hb[8];
+        const int n = rigid_blocks(P, i, dx, hmask, hb);
+        for (int k = 0; k < n; ++k) {
+            const uint32_t slot = atomicAdd(&P.rp_count[hb[k]], 1u);
+            P.rp_sorted[P.rp_first[hb[k]] + slot] = i;
+        }
+    }
+}
+
+}  // namespace
 
 namespace fast {
 
-void launch_sort(const DevPtrs& P, const LaunchCfg& c, bool with_extras, bool canonical, cudaStream_t s) {
+void launch_sort(const DevPtrs& P, const LaunchCfg& c, bool with_extras, bool canonical, cudaStream_t s,
+                 bool rigid) {
     const int g = grid_for(c.sm_count, 8);
     int reset_grid = (int)((c.hash_capacity + 255u) / 256u);
     if (reset_grid > g) reset_grid = g;
@@ -565,6 +688,10 @@ void launch_sort(const DevPtrs& P, const LaunchCfg& c, bool with_extras, bool ca
     k_sort_reset<<<reset_grid, 256, 0, s>>>(P, c.hash_capacity);
     k_touch_primary<<<g, 256, 0, s>>>(P);
     k_touch_nbh<<<g, 256, 0, s>>>(P);
+    if (rigid) {
+        k_rigid_mark<<<g, 256, 0, s>>>(P);
+        k_rigid_touch<<<g, 256, 0, s>>>(P);
+    }
     k_block_prep<<<g, 256, 0, s>>>(P);
     if (with_extras) k_count<true><<<g, 256, 0, s>>>(P);
     else k_count<false><<<g, 256, 0, s>>>(P);
@@ -573,6 +700,11 @@ void launch_sort(const DevPtrs& P, const LaunchCfg& c, bool with_extras, bool ca
     if (with_extras) k_finalize<true><<<g, 256, 0, s>>>(P);
     else k_finalize<false><<<g, 256, 0, s>>>(P);
     if (canonical) k_sort_segments<<<grid_for(c.sm_count, 4), 256, 0, s>>>(P);
+    if (rigid) {
+        k_rigid_count<<<g, 256, 0, s>>>(P);
+        k_rigid_alloc<<<g, 256, 0, s>>>(P);
+        k_rigid_finalize<<<g, 256, 0, s>>>(P);
+    }
 }
 
 }  // namespace fast

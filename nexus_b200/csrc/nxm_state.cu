@@ -16,6 +16,7 @@
 #include <cstring>
 #include <map>
 #include <new>
+#include <set>
 #include <vector>
 
 #include "../../include/nexus_mpm.h"
@@ -381,6 +382,21 @@ struct nxm_state {
     uint32_t* d_tiles = nullptr;        // compaction scratch, one word per 1024 particles
     DevTri* d_tris = nullptr;       // triangles of every trimesh collider (one copy per collider)
     DevBvhNode* d_bvh = nullptr;    // their BVHs
+    std::vector<DevTri> tris_host;  // host copy of d_tris
+    std::vector<uint32_t> tri_base; // per collider: its first record in d_tris (trimesh only)
+
+    // CPIC rigid particles: surface samples of the trimesh colliders
+    // (local position + packed triangle / collider word), their world
+    // positions, activation flags and block-sorted list; per block counts
+    // and first entries (sized by the grid capacity, with the CPIC node fields)
+    uint32_t nrp = 0;
+    std::vector<float4> rp_host;
+    float4* d_rp_local = nullptr;
+    float4* d_rp_world = nullptr;
+    uint8_t* d_rp_need = nullptr;
+    uint32_t* d_rp_sorted = nullptr;
+    uint32_t* d_rp_count = nullptr;
+    uint32_t* d_rp_first = nullptr;
 
     // control
     Params* d_params = nullptr;
@@ -433,6 +449,15 @@ DevPtrs dev_ptrs(nxm_state* s) {
     P.scene_cols = s->d_scene_cols;
     P.tris = s->d_tris;
     P.bvh = s->d_bvh;
+    if (s->use_cpic && s->nrp) {
+        P.nrp = s->nrp;
+        P.rp_local = s->d_rp_local;
+        P.rp_world = s->d_rp_world;
+        P.rp_need = s->d_rp_need;
+        P.rp_sorted = s->d_rp_sorted;
+        P.rp_count = s->d_rp_count;
+        P.rp_first = s->d_rp_first;
+    }
     P.params = s->d_params;
     P.counters = s->d_counters;
     P.hkey = s->hkey;
@@ -505,7 +530,7 @@ int canonicalize(nxm_state* s) {
 }
 
 int free_grid(nxm_state* s) {
-    dfree(s->d_ncdf); dfree(s->d_nodes_inc);
+    dfree(s->d_ncdf); dfree(s->d_nodes_inc); dfree(s->d_rp_count); dfree(s->d_rp_first);
     dfree(s->hkey); dfree(s->hval); dfree(s->bvid); dfree(s->first); dfree(s->nprim); dfree(s->nwx);
     dfree(s->cursors); dfree(s->nbh); dfree(s->nodes); dfree(s->scan_tmp); dfree(s->tile_sums);
     return NXM_OK;
@@ -515,8 +540,12 @@ int free_grid(nxm_state* s) {
 int alloc_cpic_grid(nxm_state* s) {
     dfree(s->d_ncdf);
     dfree(s->d_nodes_inc);
+    dfree(s->d_rp_count);
+    dfree(s->d_rp_first);
     NXM_TRY(dalloc(&s->d_ncdf, (size_t)s->block_cap * 64));
     NXM_TRY(dalloc(&s->d_nodes_inc, (size_t)s->block_cap * 64));
+    NXM_TRY(dalloc(&s->d_rp_count, s->block_cap));
+    NXM_TRY(dalloc(&s->d_rp_first, s->block_cap));
     invalidate_graph(s);
     return NXM_OK;
 }
@@ -699,10 +728,13 @@ int enqueue_step(nxm_state* s, cudaStream_t st, cudaEvent_t* ev /* 5 events or n
     if (has_col) { fast::launch_colliders_begin(P, st); ++k; }
     // CPIC runs the reference's gather-form transfers, so it needs the sort's extras
     const bool exact_path = s->deterministic || s->use_cpic;
-    fast::launch_sort(P, c, /*with_extras=*/exact_path, /*canonical=*/s->deterministic, st);
-    k += sort_launches(s->deterministic);
+    const bool rigid = P.nrp > 0;  // CPIC with trimesh colliders
+    if (rigid) { exact::launch_rigid_transform(P, c, st); ++k; }  // pipeline.rs:393-405
+    fast::launch_sort(P, c, /*with_extras=*/exact_path, /*canonical=*/s->deterministic, st, rigid);
+    k += sort_launches(s->deterministic) + (rigid ? fast::kRigidSortLaunches : 0);
     if (s->use_cpic) {  // node and particle distance fields (pipeline.rs:433-460)
         exact::launch_grid_update_cdf(P, c, st);
+        if (rigid) { exact::launch_p2g_cdf(P, c, st); ++k; }
         exact::launch_g2p_cdf(P, c, st);
         k += 2;
     }
@@ -1087,6 +1119,108 @@ void trimesh_bvh(const std::vector<DevTri>& tris, uint32_t base, uint32_t count,
     nodes.insert(nodes.end(), local.begin(), local.end());
 }
 
+// ---- CPIC rigid particles (host side) ------------------------------------------
+//
+// src_mpm/sampling/sample_trimesh.rs:66-231 sample_mesh, in f32 operation by
+// operation (this file is built with -ffp-contract=off): per triangle, rows
+// perpendicular to its longest edge every step / sqrt(2) with points every
+// step / sqrt(2) along each row (none on the edges), then each edge not seen
+// before (vertices identified by their position bits) sampled every
+// step / sqrt(2) from its first vertex (excluded).  The sampling step is the
+// cell width (solver/particle.rs:296-349).
+
+constexpr float kSampleEps = 1.0e-5f;
+
+struct F3 {
+    float x, y, z;
+};
+static inline F3 f3sub(F3 a, F3 b) { return F3{a.x - b.x, a.y - b.y, a.z - b.z}; }
+static inline F3 f3add(F3 a, F3 b) { return F3{a.x + b.x, a.y + b.y, a.z + b.z}; }
+static inline F3 f3mul(F3 a, float s) { return F3{a.x * s, a.y * s, a.z * s}; }
+static inline F3 f3div(F3 a, float s) { return F3{a.x / s, a.y / s, a.z / s}; }
+static inline float f3dot(F3 a, F3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+static inline float f3len(F3 a) { return std::sqrt(f3dot(a, a)); }
+// Rust `f32 as u32`: saturating, NaN -> 0.
+static inline uint32_t count_of(float f) {
+    return !(f > 0.0f) ? 0u : (f >= 4294967295.0f ? 0xFFFFFFFFu : (uint32_t)f);
+}
+
+struct RigidSample {
+    F3 p;
+    uint32_t tri;  // index into the state's triangle records
+};
+
+void sample_edge(F3 a, F3 b, float step, uint32_t tri, std::vector<RigidSample>& out) {
+    const F3 ab = f3sub(b, a);
+    const float len = f3len(ab);
+    if (!(len > kSampleEps)) return;
+    const F3 dir = f3div(ab, len);
+    const float spacing = step / std::sqrt(2.0f);
+    const uint32_t n = count_of(std::ceil(len / spacing));
+    for (uint32_t i = 1; i < n; ++i) out.push_back(RigidSample{f3add(a, f3mul(dir, spacing * (float)i)), tri});
+}
+
+void sample_triangle(F3 a, F3 b, F3 c, float step, uint32_t tri, std::vector<RigidSample>& out) {
+    const float d_ab = f3len(f3sub(b, a)), d_bc = f3len(f3sub(c, b)), d_ca = f3len(f3sub(a, c));
+    const float mx = std::fmax(std::fmax(d_ab, d_bc), d_ca);
+    if (mx == d_bc) {
+        const F3 t = a; a = b; b = c; c = t;
+    } else if (mx == d_ca) {
+        const F3 t = a; a = c; c = b; b = t;
+    }
+    const F3 ac = f3sub(c, a), base = f3sub(b, a);
+    const float base_length = f3len(base);
+    const F3 base_dir = f3div(base, base_length);
+    const float spacing = step / std::sqrt(2.0f);
+    const float base_steps = std::ceil(base_length / spacing);
+    const F3 base_step = f3mul(base_dir, spacing);
+    const float ac_off = f3dot(ac, base_dir);
+    const float bc_off = base_length - ac_off;
+    if (ac_off < kSampleEps || bc_off < kSampleEps || base_length < kSampleEps) return;
+    const F3 height = f3sub(ac, f3mul(base_dir, ac_off));
+    const float height_length = f3len(height);
+    const F3 height_dir = f3div(height, height_length);
+    const float tan_a = height_length / ac_off, tan_b = height_length / bc_off;
+    const uint32_t nb = count_of(base_steps);
+    for (uint32_t i = 1; i < nb; ++i) {
+        const F3 bp = f3add(a, f3mul(base_step, (float)i));
+        const float h_ac = tan_a * f3len(f3sub(a, bp));
+        const float h_bc = tan_b * f3len(f3sub(b, bp));
+        const float hl = std::fmin(h_ac, h_bc);
+        const uint32_t nh = count_of(std::ceil(hl / spacing));
+        const F3 hstep = f3mul(height_dir, spacing);
+        for (uint32_t j = 1; j < nh; ++j) {
+            const F3 pp = f3add(bp, f3mul(hstep, (float)j));
+            if (!std::isfinite(pp.x) || !std::isfinite(pp.y) || !std::isfinite(pp.z)) continue;
+            out.push_back(RigidSample{pp, tri});
+        }
+    }
+}
+
+// Samples of the triangle records [base, base + count) (one mesh).
+void sample_mesh(const std::vector<DevTri>& tris, uint32_t base, uint32_t count, float step,
+                 std::vector<RigidSample>& out) {
+    std::map<VKey, uint32_t> vid;
+    std::set<std::pair<uint32_t, uint32_t>> seen;
+    auto id_of = [&vid](const float* v) {
+        auto it = vid.emplace(vkey(v), (uint32_t)vid.size());
+        return it.first->second;
+    };
+    auto first_visit = [&seen](uint32_t a, uint32_t b) {
+        return seen.insert(a < b ? std::make_pair(a, b) : std::make_pair(b, a)).second;
+    };
+    for (uint32_t t = base; t < base + count; ++t) {
+        const DevTri& r = tris[t];
+        const F3 q[3] = {F3{r.v[0][0], r.v[0][1], r.v[0][2]}, F3{r.v[1][0], r.v[1][1], r.v[1][2]},
+                         F3{r.v[2][0], r.v[2][1], r.v[2][2]}};
+        const uint32_t i0 = id_of(r.v[0]), i1 = id_of(r.v[1]), i2 = id_of(r.v[2]);
+        sample_triangle(q[0], q[1], q[2], step, t, out);
+        if (first_visit(i0, i1)) sample_edge(q[0], q[1], step, t, out);
+        if (first_visit(i1, i2)) sample_edge(q[1], q[2], step, t, out);
+        if (first_visit(i2, i0)) sample_edge(q[2], q[0], step, t, out);
+    }
+}
+
 // Device form of one nxm_collider (triangle indices shifted by `tri_offset`).
 int collider_from_abi(const nxm_collider& c, const float* tri, uint32_t ntri, uint32_t tri_offset, DevCollider& d) {
     std::memset(&d, 0, sizeof(d));
@@ -1112,12 +1246,20 @@ int collider_from_abi(const nxm_collider& c, const float* tri, uint32_t ntri, ui
 
 // Uploads the collider table (every trimesh gets its own triangle records and
 // BVH, built from `tri`), growing the device table when needed.
+int rebuild_rigid_particles(nxm_state* s);
+
 int install_colliders(nxm_state* s, std::vector<DevCollider> dc, const float* tri) {
     std::vector<DevTri> tris;
     std::vector<DevBvhNode> bvh;
-    for (DevCollider& d : dc) {
+    std::vector<uint32_t> tri_base(dc.size(), 0u);
+    if (s->use_cpic && s->scene_blocks)
+        for (const DevCollider& d : dc)
+            if (d.type == SHAPE_TRIMESH) return NXM_E_UNSUPPORTED;  // rigid particles of one scene only
+    for (size_t i = 0; i < dc.size(); ++i) {
+        DevCollider& d = dc[i];
         if (d.type != SHAPE_TRIMESH) continue;
         const uint32_t base = (uint32_t)tris.size();
+        tri_base[i] = base;
         trimesh_records(tri, d.tri_first, d.tri_count, tris);
         d.bvh_first = (uint32_t)bvh.size();
         trimesh_bvh(tris, base, d.tri_count, d.bvh_first, bvh);
@@ -1151,8 +1293,48 @@ int install_colliders(nxm_state* s, std::vector<DevCollider> dc, const float* tr
     NXM_TRY(cudaStreamSynchronize(s->stream));
     const bool had = !s->colliders.empty();
     s->colliders = dc;
-    if (realloc_graph || had != !s->colliders.empty() || had_mesh || !tris.empty()) invalidate_graph(s);
+    s->tris_host = std::move(tris);
+    s->tri_base = std::move(tri_base);
+    if (realloc_graph || had != !s->colliders.empty() || had_mesh || !s->tris_host.empty()) invalidate_graph(s);
     s->params_dirty = true;
+    return rebuild_rigid_particles(s);
+}
+
+// (Re)samples the CPIC rigid particles of the trimesh colliders (none
+// without CPIC), as the reference does when the coupling is set
+// (src_mpm/pipeline.rs:211-245).
+int rebuild_rigid_particles(nxm_state* s) {
+    NXM_TRY(cudaStreamSynchronize(s->stream));
+    dfree(s->d_rp_local); dfree(s->d_rp_world); dfree(s->d_rp_need); dfree(s->d_rp_sorted);
+    const bool had = s->nrp != 0;
+    s->nrp = 0;
+    s->rp_host.clear();
+    if (s->use_cpic) {
+        if (s->tris_host.size() > kRigidTriMask) return NXM_E_INVALID;
+        std::vector<RigidSample> smp;
+        for (size_t i = 0; i < s->colliders.size(); ++i) {
+            const DevCollider& d = s->colliders[i];
+            if (d.type != SHAPE_TRIMESH) continue;
+            const size_t before = smp.size();
+            sample_mesh(s->tris_host, s->tri_base[i], d.tri_count, s->dx, smp);
+            for (size_t k = before; k < smp.size(); ++k) {
+                const RigidSample& r = smp[k];
+                s->rp_host.push_back(make_float4(r.p.x, r.p.y, r.p.z, bits_f(r.tri | ((uint32_t)i << kRigidTriBits))));
+            }
+        }
+        if (s->rp_host.size() > (size_t)UINT32_MAX / 8) return NXM_E_INVALID;
+        s->nrp = (uint32_t)s->rp_host.size();
+    }
+    if (s->nrp) {
+        NXM_TRY(dalloc(&s->d_rp_local, s->nrp));
+        NXM_TRY(dalloc(&s->d_rp_world, s->nrp));
+        NXM_TRY(dalloc(&s->d_rp_need, s->nrp));
+        NXM_TRY(dalloc(&s->d_rp_sorted, 8 * (size_t)s->nrp));
+        NXM_TRY(cudaMemcpyAsync(s->d_rp_local, s->rp_host.data(), sizeof(float4) * s->nrp, cudaMemcpyHostToDevice,
+                                s->stream));
+        NXM_TRY(cudaStreamSynchronize(s->stream));
+    }
+    if (had || s->nrp) invalidate_graph(s);
     return NXM_OK;
 }
 
@@ -1247,6 +1429,7 @@ void nxm_state_destroy(nxm_state* s) {
     free_particles(s);
     dfree(s->d_materials); dfree(s->d_colliders); dfree(s->d_tris); dfree(s->d_bvh); dfree(s->d_scene_cols); dfree(s->d_vel6); dfree(s->d_params); dfree(s->d_counters);
     dfree(s->d_pack); dfree(s->d_offsets);
+    dfree(s->d_rp_local); dfree(s->d_rp_world); dfree(s->d_rp_need); dfree(s->d_rp_sorted);
     if (s->h_counters) cudaFreeHost(s->h_counters);
     if (s->stream) cudaStreamDestroy(s->stream);
     delete s;
@@ -1274,6 +1457,8 @@ int nxm_state_set_cell_width(nxm_state* s, float cell_width, uint32_t grid_capac
     s->dx = cell_width;
     int rc = alloc_grid(s, grid_capacity);
     if (rc) return rc;
+    rc = rebuild_rigid_particles(s);  // sampled at the cell width
+    if (rc) return rc;
     NXM_TRY(cudaStreamSynchronize(s->stream));
     s->params_dirty = true;
     return invalidate_codes(s);
@@ -1288,7 +1473,6 @@ int nxm_state_set_colliders(nxm_state* s, const nxm_collider* cols, uint32_t nco
     for (uint32_t i = 0; i < ncol; ++i) {
         int rc = collider_from_abi(cols[i], tri, ntri, 0, dc[i]);
         if (rc) return rc;
-        if (s->use_cpic && dc[i].type == SHAPE_TRIMESH) return NXM_E_UNSUPPORTED;
     }
     return install_colliders(s, dc, tri);
 }
@@ -1334,8 +1518,9 @@ int nxm_state_read_collider_pose(nxm_state* s, uint32_t index, float out[7]) {
 int nxm_state_set_use_cpic(nxm_state* s, int enabled) {
     if (!s) return NXM_E_INVALID;
     if (enabled) {
-        for (const DevCollider& c : s->colliders)
-            if (c.type == SHAPE_TRIMESH) return NXM_E_UNSUPPORTED;  // trimesh CPIC needs rigid particles
+        if (s->scene_blocks)
+            for (const DevCollider& c : s->colliders)
+                if (c.type == SHAPE_TRIMESH) return NXM_E_UNSUPPORTED;  // rigid particles of one scene only
         int rc = canonicalize(s);  // CPIC steps in place, in id order
         if (rc) return rc;
         rc = alloc_cpic_grid(s);
@@ -1344,6 +1529,26 @@ int nxm_state_set_use_cpic(nxm_state* s, int enabled) {
     if (s->use_cpic != (enabled != 0)) invalidate_graph(s);
     s->use_cpic = enabled != 0;
     s->params_dirty = true;
+    return rebuild_rigid_particles(s);
+}
+
+int nxm_state_num_rigid_particles(const nxm_state* s, uint32_t* count) {
+    if (!s || !count) return NXM_E_INVALID;
+    *count = s->nrp;
+    return NXM_OK;
+}
+
+int nxm_read_rigid_particles(nxm_state* s, float* out) {
+    if (!s || (s->nrp && !out)) return NXM_E_INVALID;
+    for (uint32_t i = 0; i < s->nrp; ++i) {
+        const float4& r = s->rp_host[i];
+        const uint32_t word = f_bits(r.w);
+        const uint32_t col = word >> kRigidTriBits;
+        float* o = out + 5 * (size_t)i;
+        o[0] = r.x; o[1] = r.y; o[2] = r.z;
+        o[3] = bits_f(col);
+        o[4] = bits_f((word & kRigidTriMask) - s->tri_base[col]);
+    }
     return NXM_OK;
 }
 

@@ -176,7 +176,7 @@ __global__ void __launch_bounds__(256) k_timestep_bound(DevPtrs P) {
     if ((threadIdx.x & 31u) == 0 && best != 0xFFFFFFFFu) atomicMin(&P.counters->dt_bound, best);
 }
 
-// ---- CPIC distance fields (analytic colliders) ------------------------------
+// ---- CPIC distance fields -----------------------------------------------------
 
 // Colliders a block sees: all (at most 16), or its scene's in batched mode.
 __device__ __forceinline__ const DevCollider* block_colliders(const DevPtrs& P, const Params& prm, int4 vid,
@@ -194,8 +194,7 @@ __device__ __forceinline__ const DevCollider* block_colliders(const DevPtrs& P, 
 // solver/grid_update_cdf.rs:18-58: per node, every ball / cuboid / capsule
 // within 1.5 dx (or containing the node) sets its affinity bit (and its sign
 // bit when inside); the closest by unsigned distance is kept.  Trimeshes
-// reach the reference's node field through rigid particles (p2g_cdf.rs),
-// not built here: the host refuses CPIC with a trimesh collider.
+// reach the node field through their rigid particles (k_p2g_cdf).
 __global__ void __launch_bounds__(256) k_grid_update_cdf(DevPtrs P) {
     const Params prm = *P.params;
     const float dx = prm.dx, cap = dx * 1.5f;
@@ -236,6 +235,105 @@ __global__ void __launch_bounds__(256) k_grid_update_cdf(DevPtrs P) {
             }
         }
         P.ncdf[t] = make_uint4(__float_as_uint(dist), aff, closest, 0u);
+    }
+}
+
+// Collider pose as glam's Pose3 (rotation quaternion, translation).
+__device__ __forceinline__ v3 pose_apply(const DevCollider& c, v3 p) {
+    return qrot(quat{c.rot[0], c.rot[1], c.rot[2], c.rot[3]}, p) + mk(c.tra[0], c.tra[1], c.tra[2]);
+}
+
+// rigid_particle_update.rs:9-31 gpu_transform_sample_points: world position
+// of every rigid particle from its collider's pose at the start of the step.
+__global__ void __launch_bounds__(256) k_rigid_transform(DevPtrs P) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < P.nrp; i += gridDim.x * blockDim.x) {
+        const float4 l = P.rp_local[i];
+        const DevCollider& c = P.colliders[__float_as_uint(l.w) >> kRigidTriBits];
+        const v3 w = pose_apply(c, mk(l.x, l.y, l.z));
+        P.rp_world[i] = make_float4(w.x, w.y, w.z, l.w);
+    }
+}
+
+// solver/p2g_cdf.rs:52-259 gpu_p2g_cdf: one CTA of 64 threads (one per node)
+// per active block with rigid entries.  Chunks of 64 listed rigid particles
+// are staged in shared memory: their triangle in world space (the local
+// vertices times the collider pose, rigid_particle_update.rs:33-54), their
+// associated cell round(x / dx) - 1 and collider.  A node within the 3-cell
+// range of an entry projects on its triangle; a projection inside the face
+// sets the collider's affinity bit (and the sign bit for a node behind the
+// face).  The reference keeps the first strictly closer entry in list order;
+// the list order here comes from atomics, so the rigid candidates reduce to
+// the lowest (distance, collider) pair, which is what the reference's
+// ascending-id order gives, and only a strictly closer one replaces the
+// analytic colliders' result.
+__global__ void __launch_bounds__(64) k_p2g_cdf(DevPtrs P) {
+    __shared__ float4 sa[64], sb[64], sc[64];
+    __shared__ int4 sassoc[64];  // associated cell, collider
+    const float dx = P.params->dx;
+    const uint32_t nb = __ldcg(&P.counters->num_blocks);
+    const uint32_t tid = threadIdx.x;
+    for (uint32_t b = blockIdx.x; b < nb; b += gridDim.x) {
+        const uint32_t num = P.rp_count[b];
+        if (num == 0) continue;
+        const uint32_t first = P.rp_first[b];
+        const int4 vid = P.bvid[b];
+        const int cx = vid.x * 4 + (int)(tid & 3u), cy = vid.y * 4 + (int)((tid >> 2) & 3u),
+                  cz = vid.z * 4 + (int)(tid >> 4);
+        const v3 cell_pos = mk((float)cx, (float)cy, (float)cz) * dx;
+        const uint4 nc = P.ncdf[b * 64u + tid];
+        uint32_t aff = nc.y;
+        float rbest = MAX_FLT;
+        uint32_t rcol = NONE;
+        for (uint32_t chunk = 0; chunk < num; chunk += 64u) {
+            __syncthreads();
+            if (chunk + tid < num) {
+                const uint32_t id = P.rp_sorted[first + chunk + tid];
+                const float4 w = P.rp_world[id];
+                const uint32_t word = __float_as_uint(w.w);
+                const uint32_t col = word >> kRigidTriBits;
+                const DevCollider& c = P.colliders[col];
+                const DevTri& t = P.tris[word & kRigidTriMask];
+                const v3 a = pose_apply(c, mk(t.v[0][0], t.v[0][1], t.v[0][2]));
+                const v3 bb = pose_apply(c, mk(t.v[1][0], t.v[1][1], t.v[1][2]));
+                const v3 cc = pose_apply(c, mk(t.v[2][0], t.v[2][1], t.v[2][2]));
+                sa[tid] = make_float4(a.x, a.y, a.z, 0.f);
+                sb[tid] = make_float4(bb.x, bb.y, bb.z, 0.f);
+                sc[tid] = make_float4(cc.x, cc.y, cc.z, 0.f);
+                const v3 ac = assoc_cell_of(dx, mk(w.x, w.y, w.z));
+                sassoc[tid] = make_int4(f2i_sat(ac.x), f2i_sat(ac.y), f2i_sat(ac.z), (int)col);
+            }
+            __syncthreads();
+            const uint32_t len = min(64u, num - chunk);
+            for (uint32_t p = 0; p < len; ++p) {
+                const int4 as = sassoc[p];
+                const int sx = cx - as.x, sy = cy - as.y, sz = cz - as.z;
+                if (sx < 0 || sx > 2 || sy < 0 || sy > 2 || sz < 0 || sz > 2) continue;
+                const float4 fa = sa[p], fb = sb[p], fc = sc[p];
+                const v3 a = mk(fa.x, fa.y, fa.z), bb = mk(fb.x, fb.y, fb.z), cc = mk(fc.x, fc.y, fc.z);
+                const v3 ap = cell_pos - a, bp = cell_pos - bb, cp = cell_pos - cc;
+                const v3 ab = bb - a, acv = cc - a, bc = cc - bb;
+                const v3 n = cross(ab, acv);
+                const float nl = length(n);
+                if (nl != 0.f && dot(cross(ab, n), ap) <= 0.f && dot(cross(bc, n), bp) <= 0.f &&
+                    dot(cross(acv, n), cp) >= 0.f) {
+                    const float sd = dot(n, ap) / nl;
+                    const float d = fabsf(sd);
+                    const uint32_t col = (uint32_t)as.w;
+                    aff |= (sd < 0.f ? 0x00010001u : 0x00000001u) << col;
+                    if (d < rbest || (d == rbest && col < rcol)) {
+                        rbest = d;
+                        rcol = col;
+                    }
+                }
+            }
+        }
+        float dist = __uint_as_float(nc.x);
+        uint32_t closest = nc.z;
+        if (rbest < dist) {
+            dist = rbest;
+            closest = rcol;
+        }
+        P.ncdf[b * 64u + tid] = make_uint4(__float_as_uint(dist), aff, closest, 0u);
     }
 }
 
@@ -351,6 +449,14 @@ void launch_grid_update_cdf(const DevPtrs& P, const LaunchCfg& c, cudaStream_t s
 
 void launch_g2p_cdf(const DevPtrs& P, const LaunchCfg& c, cudaStream_t s) {
     k_g2p_cdf<<<c.sm_count * 4, 128, 0, s>>>(P);
+}
+
+void launch_rigid_transform(const DevPtrs& P, const LaunchCfg& c, cudaStream_t s) {
+    k_rigid_transform<<<c.sm_count * 4, 256, 0, s>>>(P);
+}
+
+void launch_p2g_cdf(const DevPtrs& P, const LaunchCfg& c, cudaStream_t s) {
+    k_p2g_cdf<<<c.sm_count * 16, 64, 0, s>>>(P);
 }
 
 void launch_timestep_bound(const DevPtrs& P, const LaunchCfg& c, cudaStream_t s) {

@@ -92,6 +92,8 @@ SIGNATURES = {
     "nxm_debug_sort": (C.c_int, [_vp, _vp, C.c_int]),
     "nxm_state_estimate_timestep_bound": (C.c_int, [_vp, _f, _u]),
     "nxm_read_cdf": (C.c_int, [_vp, _f]),
+    "nxm_state_num_rigid_particles": (C.c_int, [_vp, _u]),
+    "nxm_read_rigid_particles": (C.c_int, [_vp, _f]),
     "nxm_state_set_collider_velocities": (C.c_int, [_vp, C.c_uint32, C.c_uint32, _f]),
     "nxm_state_enable_scenes": (C.c_int, [_vp, C.c_uint32]),
     "nxm_scene_capacity": (C.c_uint32, [_vp]),
@@ -386,6 +388,22 @@ class MpmState:
         out = out[:len(self)]
         return dict(normal=out[:, :3], signed_distance=out[:, 3], rigid_vel=out[:, 4:7],
                     affinity=out[:, 7].copy().view(np.uint32))
+
+    def num_rigid_particles(self) -> int:
+        """``GpuRigidParticles::len``: CPIC surface samples of the trimesh colliders."""
+        n = np.zeros(1, np.uint32)
+        _check(self.lib.nxm_state_num_rigid_particles(self.h, _p(n, _u)), "num_rigid_particles")
+        return int(n[0])
+
+    def read_rigid_particles(self) -> dict:
+        """CPIC rigid particles in sampling order: local position, collider,
+        triangle index inside the collider's triangle range."""
+        n = self.num_rigid_particles()
+        out = np.zeros((max(n, 1), 5), np.float32)
+        _check(self.lib.nxm_read_rigid_particles(self.h, _p(out, _f)), "read_rigid_particles")
+        out = out[:n]
+        return dict(local=out[:, :3], collider=out[:, 3].copy().view(np.uint32),
+                    triangle=out[:, 4].copy().view(np.uint32))
 
     def estimate_timestep_bound(self) -> tuple[float, int]:
         """``WgTimestepBounds::compute_bounds``: (max dt in seconds, fixed-point bits)."""

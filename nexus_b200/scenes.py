@@ -254,6 +254,51 @@ def cpic_drop(n_side: int = 12, seed: int = 17, steps: int = 100) -> Scene:
     return Scene("cpic_drop", dx, 1.0e-3, (0.0, 0.0, -9.81), batch, cols, steps, grid_capacity_for(batch.n))
 
 
+def box_mesh(half: float) -> np.ndarray:
+    """Triangles (12, 3, 3) of the closed box [-half, half]^3, counter-clockwise
+    seen from outside."""
+    h = float(half)
+    corner = lambda i: (h if i & 1 else -h, h if i & 2 else -h, h if i & 4 else -h)
+    quads = [(0, 2, 3, 1), (4, 5, 7, 6), (0, 1, 5, 4), (2, 6, 7, 3), (0, 4, 6, 2), (1, 3, 7, 5)]
+    tri = []
+    for a, b, c, d in quads:
+        tri += [[corner(a), corner(b), corner(c)], [corner(a), corner(c), corner(d)]]
+    return np.asarray(tri, np.float32)
+
+
+def cpic_trimesh(n_side: int = 10, seed: int = 23, steps: int = 100) -> Scene:
+    """CPIC with trimesh colliders at the scale of the reference's CPIC scenes
+    (cell width 0.5, a 32-unit domain): a height-field floor mesh (17 x 17
+    vertices over the domain, heights 1 + U(0, 0.5)) under a neo-Hookean
+    cube and a sand block falling at 10 m/s from 0.6 above its highest
+    point, and a closed box mesh (half-size 1.5) beside the sand moving
+    along -x at 5 m/s while spinning about z at 2 rad/s; five slip cuboid
+    walls (analytic colliders) around the domain."""
+    L, dx = 32.0, 0.5
+    floor = height_field(17, seed + 1, 0.0, L, base=1.0, amplitude=0.5)
+    box = box_mesh(1.5)
+    tri = np.concatenate([floor, box], 0)
+    cube = ParticleBatch.from_positions(lattice_block((0.30 * L, 0.30 * L, 2.1), (n_side, n_side, n_side), dx, seed),
+                                        np.float32(dx) / np.float32(4.0), 1000.0,
+                                        ParticleModel.elastic_neo_hookean(1.0e5, 0.3))
+    sand = ParticleBatch.from_positions(lattice_block((0.60 * L, 0.55 * L, 2.1), (n_side, n_side, n_side // 2), dx,
+                                                      seed, 3 * n_side ** 3),
+                                        np.float32(dx) / np.float32(4.0), 2700.0,
+                                        ParticleModel.sand_with_friction_angle(3.5e5, 0.3, 30.0))
+    batch = ParticleBatch.concat([cube, sand])
+    batch.vel[:, 2] = -10.0
+    sand_hi_x = 0.60 * L + n_side * dx / 2
+    mesh_floor = Collider.trimesh(0, len(floor), (0.0, 0.0, 0.0), BoundaryCondition.separate(0.3))
+    mesh_box = Collider.trimesh(len(floor), len(box), (sand_hi_x + 1.8, 0.55 * L + 1.25, 2.9),
+                                BoundaryCondition.slip())
+    mesh_box.linvel = (-5.0, 0.0, 0.0)
+    mesh_box.angvel = (0.0, 0.0, 2.0)
+    walls = box_walls(0.0, L, BoundaryCondition.slip(), BoundaryCondition.slip(), thickness=2.0)[:-1]
+    cols = collider_array(walls + [mesh_floor, mesh_box])
+    return Scene("cpic_trimesh", dx, 1.0e-3, (0.0, 0.0, -9.81), batch, cols, steps, 4096,
+                 tri_vertices=tri.reshape(-1, 3))
+
+
 def kinematic_velocities(scene: Scene, t: float) -> tuple[np.ndarray, np.ndarray]:
     """(collider indices, (k, 6) linear + angular velocity) of the scene's
     kinematic bodies at time t: dp/dt = v0 + a omega cos(omega t + phi)."""

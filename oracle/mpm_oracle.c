@@ -201,6 +201,8 @@ typedef struct {
     uint32_t num_particles_with_extras;
     uint32_t cursors[NUM_BUCKETS];
     uint32_t nbh[NUM_NBH];
+    uint32_t first_rigid;     /* CPIC: the block's range of the sorted rigid-particle list */
+    uint32_t num_rigid;
 } header_t;
 
 /* grid.rs:401-421 Node, with the NodeCdf of grid.rs:367-375 (distance,
@@ -653,6 +655,16 @@ typedef struct {
     collider_t *col;
     v3 *tri; /* 3 vertices per triangle, local frame of the owning trimesh */
     uint32_t ntri;
+    /* CPIC rigid particles: surface samples of the trimesh colliders
+     * (solver/particle.rs:296-349), local and world positions, owning
+     * collider and triangle (index into `tri`), the block-activation flag
+     * and the block-sorted list with extras. */
+    uint32_t nrp;
+    int rp_dirty;
+    v3 *rp_local, *rp_world;
+    uint32_t *rp_col, *rp_tri;
+    uint8_t *rp_need;
+    uint32_t *rp_sorted;
     /* diagnostics */
     uint32_t status;
 } scene_t;
@@ -705,6 +717,7 @@ void orc_destroy(scene_t *s) {
     free(s->bfric); free(s->cdf_normal); free(s->cdf_rigid_vel); free(s->cdf_sd); free(s->cdf_aff);
     free(s->words); free(s->hstate); free(s->hvalue); free(s->howner); free(s->hdr);
     free(s->nodes); free(s->sorted); free(s->scan); free(s->col); free(s->tri);
+    free(s->rp_local); free(s->rp_world); free(s->rp_col); free(s->rp_tri); free(s->rp_need); free(s->rp_sorted);
     free(s);
 }
 
@@ -785,7 +798,7 @@ void orc_set_params(scene_t *s, const float *gravity, float dt) {
     s->dt = dt;
 }
 
-void orc_set_use_cpic(scene_t *s, int on) { s->use_cpic = on; }
+void orc_set_use_cpic(scene_t *s, int on) { s->use_cpic = on; s->rp_dirty = 1; }
 
 /* Collider table.  Per collider, 32 floats:
  *   [0..4)  shape a, [4..8) shape b, [8..12) shape c      (Shape, shape.rs:29-73)
@@ -820,6 +833,7 @@ void orc_set_colliders(scene_t *s, uint32_t ncol, const float *desc, uint32_t nt
     }
     for (uint32_t t = 0; t < ntri * 3; ++t)
         s->tri[t] = V(tri_vertices[3 * t], tri_vertices[3 * t + 1], tri_vertices[3 * t + 2]);
+    s->rp_dirty = 1;
 }
 
 void orc_set_collider_velocity(scene_t *s, uint32_t i, const float *lin, const float *ang) {
@@ -834,6 +848,200 @@ void orc_get_collider_pose(const scene_t *s, uint32_t i, float *out7) {
     out7[0] = (float)c->pose.rot.x; out7[1] = (float)c->pose.rot.y; out7[2] = (float)c->pose.rot.z;
     out7[3] = (float)c->pose.rot.w; out7[4] = (float)c->pose.tra.x; out7[5] = (float)c->pose.tra.y;
     out7[6] = (float)c->pose.tra.z;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Rigid particles of trimesh colliders (CPIC):                              */
+/* src_mpm/sampling/sample_trimesh.rs, in f32 as the reference samples       */
+/* ------------------------------------------------------------------------ */
+
+#define SAMPLE_EPS 1.0e-5f  /* sample_trimesh.rs:12 */
+
+typedef struct { float x, y, z; } f3;
+static inline f3 F3(float x, float y, float z) { f3 r = {x, y, z}; return r; }
+static inline f3 fsub(f3 a, f3 b) { return F3(a.x - b.x, a.y - b.y, a.z - b.z); }
+static inline f3 fadd(f3 a, f3 b) { return F3(a.x + b.x, a.y + b.y, a.z + b.z); }
+static inline f3 fmulv(f3 a, float s) { return F3(a.x * s, a.y * s, a.z * s); }
+static inline f3 fdivv(f3 a, float s) { return F3(a.x / s, a.y / s, a.z / s); }
+static inline float fdot3(f3 a, f3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+static inline float flen3(f3 a) { return sqrtf(fdot3(a, a)); }
+/* Rust `f32 as u32` / `as usize` for the step counts: saturating, NaN -> 0. */
+static inline uint32_t f_to_count(float f) { return !(f > 0.0f) ? 0u : (f >= 4294967295.0f ? 0xFFFFFFFFu : (uint32_t)f); }
+
+typedef struct { f3 *pt; uint32_t *tri; uint32_t len, cap; } samples_t;
+static void samples_push(samples_t *b, f3 p, uint32_t tri) {
+    if (b->len == b->cap) {
+        b->cap = b->cap ? 2 * b->cap : 1024;
+        b->pt = realloc(b->pt, sizeof(f3) * b->cap);
+        b->tri = realloc(b->tri, sizeof(uint32_t) * b->cap);
+    }
+    b->pt[b->len] = p;
+    b->tri[b->len++] = tri;
+}
+
+/* sample_trimesh.rs:116-138 sample_edge: points every xy_spacing/sqrt(2)
+ * from a (excluded) toward b. */
+static void sample_edge(f3 a, f3 b, float xy_spacing, uint32_t tri, samples_t *out) {
+    f3 ab = fsub(b, a);
+    float len = flen3(ab);
+    if (len > SAMPLE_EPS) {
+        f3 dir = fdivv(ab, len);
+        float spacing = xy_spacing / sqrtf(2.0f);
+        uint32_t nsteps = f_to_count(ceilf(len / spacing));
+        for (uint32_t i = 1; i < nsteps; ++i) samples_push(out, fadd(a, fmulv(dir, spacing * (float)i)), tri);
+    }
+}
+
+/* sample_trimesh.rs:140-231 sample_triangle: the longest edge is the base;
+ * rows perpendicular to it every spacing, points along each row every
+ * spacing, none on the base, the row ends or the vertices. */
+static void sample_triangle(f3 a, f3 b, f3 c, float xy_spacing, uint32_t tri, samples_t *out) {
+    float d_ab = flen3(fsub(b, a)), d_bc = flen3(fsub(c, b)), d_ca = flen3(fsub(a, c));
+    float mx = fmaxf(fmaxf(d_ab, d_bc), d_ca);
+    if (mx == d_bc) { f3 t = a; a = b; b = c; c = t; }
+    else if (mx == d_ca) { f3 t = a; a = c; c = b; b = t; }
+    f3 ac = fsub(c, a), base = fsub(b, a);
+    float base_length = flen3(base);
+    f3 base_dir = fdivv(base, base_length);
+    float spacing = xy_spacing / sqrtf(2.0f);
+    float base_steps = ceilf(base_length / spacing);
+    f3 base_step = fmulv(base_dir, spacing);
+    float ac_off = fdot3(ac, base_dir);
+    float bc_off = base_length - ac_off;
+    if (ac_off < SAMPLE_EPS || bc_off < SAMPLE_EPS || base_length < SAMPLE_EPS) return;
+    f3 height = fsub(ac, fmulv(base_dir, ac_off));
+    float height_length = flen3(height);
+    f3 height_dir = fdivv(height, height_length);
+    float tan_a = height_length / ac_off, tan_b = height_length / bc_off;
+    uint32_t nb = f_to_count(base_steps);
+    for (uint32_t i = 1; i < nb; ++i) {
+        f3 bp = fadd(a, fmulv(base_step, (float)i));
+        float h_ac = tan_a * flen3(fsub(a, bp));
+        float h_bc = tan_b * flen3(fsub(b, bp));
+        float hl = fminf(h_ac, h_bc);
+        uint32_t nh = f_to_count(ceilf(hl / spacing));
+        f3 hstep = fmulv(height_dir, spacing);
+        for (uint32_t j = 1; j < nh; ++j) {
+            f3 pp = fadd(bp, fmulv(hstep, (float)j));
+            if (!isfinite(pp.x) || !isfinite(pp.y) || !isfinite(pp.z)) continue;
+            samples_push(out, pp, tri);
+        }
+    }
+}
+
+/* Vertex identity of a triangle soup: equal position bits = one vertex (the
+ * reference's meshes are indexed; a soup carries the index as the position). */
+typedef struct { uint32_t *key; uint32_t *id; uint32_t mask, count; } vtab_t;
+static uint32_t mix3(uint32_t a, uint32_t b, uint32_t c) {
+    uint32_t h = hash_key(a) ^ 0x9E3779B9u;
+    h = hash_key(h ^ b) + 0x7F4A7C15u;
+    return hash_key(h ^ c);
+}
+static uint32_t vtab_id(vtab_t *t, f3 p) {
+    uint32_t k0, k1, k2;
+    memcpy(&k0, &p.x, 4); memcpy(&k1, &p.y, 4); memcpy(&k2, &p.z, 4);
+    uint32_t slot = mix3(k0, k1, k2) & t->mask;
+    for (;;) {
+        uint32_t *k = t->key + 3 * (size_t)slot;
+        if (t->id[slot] == NONE_U32) {
+            k[0] = k0; k[1] = k1; k[2] = k2;
+            t->id[slot] = t->count++;
+            return t->id[slot];
+        }
+        if (k[0] == k0 && k[1] == k1 && k[2] == k2) return t->id[slot];
+        slot = (slot + 1) & t->mask;
+    }
+}
+typedef struct { uint64_t *key; uint32_t mask; } etab_t;
+/* sample_trimesh.rs:73-81: true the first time an (unordered) edge is seen. */
+static int etab_insert(etab_t *t, uint32_t a, uint32_t b) {
+    if (b > a) { uint32_t x = a; a = b; b = x; }
+    uint64_t key = ((uint64_t)a << 32) | b;
+    uint32_t slot = mix3(a, b, 0x51u) & t->mask;
+    for (;;) {
+        if (t->key[slot] == UINT64_MAX) { t->key[slot] = key; return 1; }
+        if (t->key[slot] == key) return 0;
+        slot = (slot + 1) & t->mask;
+    }
+}
+
+/* sample_trimesh.rs:66-114 sample_mesh for every trimesh collider in
+ * collider order (solver/particle.rs:305-346), sampling step = cell width. */
+static void build_rigid_particles(scene_t *s) {
+    free(s->rp_local); free(s->rp_world); free(s->rp_col); free(s->rp_tri); free(s->rp_need); free(s->rp_sorted);
+    s->rp_local = s->rp_world = NULL;
+    s->rp_col = s->rp_tri = s->rp_sorted = NULL;
+    s->rp_need = NULL;
+    s->nrp = 0;
+    s->rp_dirty = 0;
+    if (!s->use_cpic) return;
+    samples_t all = {0};
+    uint32_t *cols = NULL;
+    size_t cols_cap = 0;
+    const float step = (float)s->dx;
+    for (uint32_t ci = 0; ci < s->ncol; ++ci) {
+        const collider_t *c = &s->col[ci];
+        if (c->type != SHAPE_TRIMESH) continue;
+        uint32_t cap = 16;
+        while (cap < 6 * c->tri_count + 16) cap <<= 1;
+        vtab_t vt = {malloc(sizeof(uint32_t) * 3 * (size_t)cap), malloc(sizeof(uint32_t) * cap), cap - 1, 0};
+        etab_t et = {malloc(sizeof(uint64_t) * cap), cap - 1};
+        for (uint32_t i = 0; i < cap; ++i) { vt.id[i] = NONE_U32; et.key[i] = UINT64_MAX; }
+        const uint32_t before = all.len;
+        for (uint32_t t = c->tri_first; t < c->tri_first + c->tri_count; ++t) {
+            f3 q[3];
+            uint32_t vid[3];
+            for (int k = 0; k < 3; ++k) {
+                v3 v = s->tri[3 * (size_t)t + k];
+                q[k] = F3((float)v.x, (float)v.y, (float)v.z);
+                vid[k] = vtab_id(&vt, q[k]);
+            }
+            sample_triangle(q[0], q[1], q[2], step, t, &all);
+            if (etab_insert(&et, vid[0], vid[1])) sample_edge(q[0], q[1], step, t, &all);
+            if (etab_insert(&et, vid[1], vid[2])) sample_edge(q[1], q[2], step, t, &all);
+            if (etab_insert(&et, vid[2], vid[0])) sample_edge(q[2], q[0], step, t, &all);
+        }
+        free(vt.key); free(vt.id); free(et.key);
+        if (all.len > cols_cap) {
+            cols_cap = all.cap;
+            cols = realloc(cols, sizeof(uint32_t) * cols_cap);
+        }
+        for (uint32_t i = before; i < all.len; ++i) cols[i] = ci;
+    }
+    s->nrp = all.len;
+    s->rp_local = xcalloc(s->nrp, sizeof(v3));
+    s->rp_world = xcalloc(s->nrp, sizeof(v3));
+    s->rp_col = xcalloc(s->nrp, sizeof(uint32_t));
+    s->rp_tri = xcalloc(s->nrp, sizeof(uint32_t));
+    s->rp_need = xcalloc(s->nrp, 1);
+    s->rp_sorted = xcalloc((size_t)s->nrp * 8, sizeof(uint32_t));
+    for (uint32_t i = 0; i < s->nrp; ++i) {
+        s->rp_local[i] = V(all.pt[i].x, all.pt[i].y, all.pt[i].z);
+        s->rp_col[i] = cols[i];
+        s->rp_tri[i] = all.tri[i];
+    }
+    free(all.pt); free(all.tri); free(cols);
+}
+
+uint32_t orc_num_rigid(scene_t *s) {
+    if (s->rp_dirty) build_rigid_particles(s);
+    return s->nrp;
+}
+/* Per rigid particle 5 floats: local position, collider (u32 bits), triangle
+ * index inside its collider's range (u32 bits). */
+void orc_get_rigid(scene_t *s, float *out5) {
+    if (s->rp_dirty) build_rigid_particles(s);
+    for (uint32_t i = 0; i < s->nrp; ++i) {
+        float *o = out5 + 5 * (size_t)i;
+        o[0] = (float)s->rp_local[i].x; o[1] = (float)s->rp_local[i].y; o[2] = (float)s->rp_local[i].z;
+        o[3] = f2bitsf(s->rp_col[i]);
+        o[4] = f2bitsf(s->rp_tri[i] - s->col[s->rp_col[i]].tri_first);
+    }
+}
+
+/* rigid_particle_update.rs:9-31 gpu_transform_sample_points. */
+static void transform_rigid_particles(scene_t *s) {
+    for (uint32_t i = 0; i < s->nrp; ++i) s->rp_world[i] = pose_apply(s->col[s->rp_col[i]].pose, s->rp_local[i]);
 }
 
 /* ------------------------------------------------------------------------ */
@@ -894,6 +1102,41 @@ static inline int spills(const uint32_t assoc[3], i3 bshift) {
     return (bshift.x == 0 || assoc[0] >= 2) && (bshift.y == 0 || assoc[1] >= 2) && (bshift.z == 0 || assoc[2] >= 2);
 }
 
+/* sort.rs:493-667: rigid particles per block (their own block, plus each
+ * +1 neighbour their 3-cell range reaches when it exists; a particle whose
+ * own block is missing is skipped), exclusive scan, placement in ascending
+ * particle order. */
+static void rigid_sort(scene_t *s) {
+    const REAL dx = s->dx;
+    for (int pass = 0; pass < 2; ++pass) {
+        if (pass == 1) {
+            uint32_t run = 0;
+            for (uint32_t b = 0; b < s->num_blocks; ++b) {
+                s->hdr[b].first_rigid = run;
+                run += s->hdr[b].num_rigid;
+                s->hdr[b].num_rigid = 0;
+            }
+        } else {
+            for (uint32_t b = 0; b < s->num_blocks; ++b) s->hdr[b].num_rigid = 0;
+        }
+        for (uint32_t p = 0; p < s->nrp; ++p) {
+            uint32_t h0 = find_header(s, block_of_point(dx, s->rp_world[p]));
+            if (h0 == NONE_U32) continue;
+            uint32_t assoc[3];
+            assoc_in_block(dx, s->rp_world[p], assoc);
+            uint32_t hs[8], nh = 0;
+            hs[nh++] = h0;
+            for (int i = 1; i < 8; ++i)
+                if (spills(assoc, ASSOC_SHIFT[i]) && s->hdr[h0].nbh[i - 1] != NONE_U32) hs[nh++] = s->hdr[h0].nbh[i - 1];
+            for (uint32_t k = 0; k < nh; ++k) {
+                header_t *h = &s->hdr[hs[k]];
+                if (pass == 1) s->rp_sorted[h->first_rigid + h->num_rigid] = p;
+                h->num_rigid += 1;
+            }
+        }
+    }
+}
+
 int orc_sort(scene_t *s) {
     const REAL dx = s->dx;
     /* grid.rs:660-685 reset_hmap */
@@ -906,6 +1149,20 @@ int orc_sort(scene_t *s) {
     for (uint32_t b = 0; b < nbase; ++b) {
         i3 vid = s->hdr[b].vid;
         for (int i = 1; i < 8; ++i) mark_active(s, i3add(vid, ASSOC_SHIFT[i]));
+    }
+    /* grid.rs:95-121: CPIC rigid particles whose own block is missing while
+     * one of its +1 neighbours exists get their own block (sort.rs:200-249
+     * marks them all first, sort.rs:165-198 then inserts). */
+    if (s->use_cpic && s->nrp) {
+        for (uint32_t p = 0; p < s->nrp; ++p) {
+            i3 b0 = block_of_point(dx, s->rp_world[p]);
+            int i = 0;
+            for (; i < 8; ++i)
+                if (find_header(s, i3add(b0, ASSOC_SHIFT[i])) != NONE_U32) break;
+            s->rp_need[p] = (uint8_t)(i > 0 && i < 8);
+        }
+        for (uint32_t p = 0; p < s->nrp; ++p)
+            if (s->rp_need[p]) mark_active(s, block_of_point(dx, s->rp_world[p]));
     }
     /* sort.rs:261-279 update_nbh_block_ids */
     for (uint32_t b = 0; b < s->num_blocks; ++b)
@@ -970,6 +1227,7 @@ int orc_sort(scene_t *s) {
             }
         }
     }
+    if (s->use_cpic && s->nrp) rigid_sort(s);
     return (int)s->status;
 }
 
@@ -1354,8 +1612,7 @@ static void update_world_com(scene_t *s) {
 /* solver/grid_update_cdf.rs:18-58 collide(): per node, every ball / cuboid /
  * capsule within 1.5 dx (or containing it) sets its affinity bit (and sign
  * bit when inside); the closest one by unsigned distance is kept.  Triangle
- * meshes reach the node CDF through rigid particles (p2g_cdf.rs), which this
- * restatement does not cover. */
+ * meshes reach the node CDF through rigid particles (orc_p2g_cdf). */
 void orc_grid_update_cdf(scene_t *s) {
     const REAL dx = s->dx, cap = s->dx * (REAL)1.5;
     const int64_t nb = (int64_t)s->num_blocks;
@@ -1390,6 +1647,53 @@ void orc_grid_update_cdf(scene_t *s) {
             nd->cdf_distance = dist;
             nd->cdf_aff = affb;
             nd->cdf_closest = closest;
+        }
+    }
+}
+
+/* solver/p2g_cdf.rs:52-259 gpu_p2g_cdf: every rigid particle listed in a
+ * block projects the node positions of the block within its 3-cell range
+ * (associated cell round(x / dx) - 1 to + 2) on its triangle (world
+ * vertices = pose * local vertices, rigid_particle_update.rs:33-54); a
+ * projection inside the face sets the collider's affinity bit (and the sign
+ * bit for a node behind the face) and may lower the node distance (strict
+ * <, list order = ascending particle order). */
+void orc_p2g_cdf(scene_t *s) {
+    const REAL dx = s->dx;
+    const int64_t nb = (int64_t)s->num_blocks;
+#pragma omp parallel for schedule(dynamic, 4)
+    for (int64_t bi = 0; bi < nb; ++bi) {
+        const header_t *h = &s->hdr[bi];
+        if (h->num_rigid == 0) continue;
+        const i3 vid = h->vid;
+        for (int t = 0; t < 64; ++t) {
+            const i3 cell = {vid.x * 4 + (t & 3), vid.y * 4 + ((t >> 2) & 3), vid.z * 4 + (t >> 4)};
+            const v3 cell_pos = vmul(V((REAL)cell.x, (REAL)cell.y, (REAL)cell.z), dx);
+            node_t *nd = &s->nodes[(size_t)bi * 64 + t];
+            for (uint32_t k = 0; k < h->num_rigid; ++k) {
+                const uint32_t p = s->rp_sorted[h->first_rigid + k];
+                const v3 ac = assoc_cell_of(dx, s->rp_world[p]);
+                const int32_t sx = cell.x - r_to_i32(ac.x), sy = cell.y - r_to_i32(ac.y), sz = cell.z - r_to_i32(ac.z);
+                if (sx < 0 || sx > 2 || sy < 0 || sy > 2 || sz < 0 || sz > 2) continue;
+                const uint32_t cid = s->rp_col[p];
+                const collider_t *c = &s->col[cid];
+                const v3 *tv = &s->tri[3 * (size_t)s->rp_tri[p]];
+                const v3 a = pose_apply(c->pose, tv[0]), b = pose_apply(c->pose, tv[1]), cc = pose_apply(c->pose, tv[2]);
+                const v3 ap = vsub(cell_pos, a), bp = vsub(cell_pos, b), cp = vsub(cell_pos, cc);
+                const v3 ab = vsub(b, a), acv = vsub(cc, a), bc = vsub(cc, b);
+                const v3 n = vcross(ab, acv);
+                const REAL nl = vlen(n);
+                if (nl != 0 && vdot(vcross(ab, n), ap) <= 0 && vdot(vcross(bc, n), bp) <= 0 &&
+                    vdot(vcross(acv, n), cp) >= 0) {
+                    const REAL sd = vdot(n, ap) / nl;
+                    const REAL d = fabs(sd);
+                    nd->cdf_aff |= (sd < 0 ? 0x00010001u : 0x00000001u) << cid;
+                    if (d < nd->cdf_distance) {
+                        nd->cdf_distance = d;
+                        nd->cdf_closest = cid;
+                    }
+                }
+            }
         }
     }
 }
@@ -1525,9 +1829,14 @@ void orc_g2p_cdf(scene_t *s) {
  * particle CDF passes run between the sort and P2G. */
 int orc_step(scene_t *s) {
     update_world_com(s);
+    if (s->use_cpic) {  /* pipeline.rs:393-405 rigid update */
+        if (s->rp_dirty) build_rigid_particles(s);
+        transform_rigid_particles(s);
+    }
     orc_sort(s);
-    if (s->use_cpic) {
+    if (s->use_cpic) {  /* pipeline.rs:433-460 */
         orc_grid_update_cdf(s);
+        orc_p2g_cdf(s);
         orc_g2p_cdf(s);
     }
     orc_p2g(s);

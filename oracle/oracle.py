@@ -63,7 +63,9 @@ def lib(precision: str = "f32"):
     for name in ("orc_p2g", "orc_grid_update", "orc_g2p", "orc_particle_update", "orc_grid_update_cdf",
                  "orc_g2p_cdf"):
         getattr(L, name).argtypes = [C.c_void_p]
-    for name in ("orc_num_blocks", "orc_status", "orc_capacity", "orc_sorted_len", "orc_timestep_bound_bits"):
+    L.orc_get_rigid.argtypes = [C.c_void_p, _f]
+    for name in ("orc_num_blocks", "orc_status", "orc_capacity", "orc_sorted_len", "orc_timestep_bound_bits",
+                 "orc_num_rigid"):
         getattr(L, name).argtypes = [C.c_void_p]
         getattr(L, name).restype = C.c_uint32
     L.orc_get_headers.argtypes = [C.c_void_p, _i]
@@ -128,6 +130,23 @@ class OracleScene:
 
     def grid_update_cdf(self):
         self.L.orc_grid_update_cdf(self.h)
+
+    def collider_pose(self, index: int) -> np.ndarray:
+        """Quaternion x, y, z, w then translation of collider `index`."""
+        out = np.zeros(7, np.float32)
+        self.L.orc_get_collider_pose(self.h, index, _ptr(out, _f))
+        return out
+
+    def rigid_particles(self) -> dict:
+        """CPIC rigid particles (trimesh surface samples, sampling step = cell
+        width): local position, collider index, triangle index inside the
+        collider's triangle range."""
+        n = self.L.orc_num_rigid(self.h)
+        out = np.zeros((n, 5), np.float32)
+        if n:
+            self.L.orc_get_rigid(self.h, _ptr(out, _f))
+        return dict(local=out[:, :3], collider=out[:, 3].copy().view(np.uint32),
+                    triangle=out[:, 4].copy().view(np.uint32))
 
     def g2p_cdf(self):
         self.L.orc_g2p_cdf(self.h)

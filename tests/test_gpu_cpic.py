@@ -39,9 +39,58 @@ def test_cpic_matches_oracle(gpu_lib, oracle_built, deterministic):
         assert (gc["affinity"] == wc["affinity"]).mean() > 0.95
 
 
-def test_cpic_refuses_trimesh(gpu_lib):
-    sc = scenes.trimesh_floor(n_side=4)
+@pytest.mark.parametrize("deterministic", [True, False])
+def test_cpic_trimesh_matches_oracle(gpu_lib, oracle_built, deterministic):
+    """Trimesh colliders under CPIC: the library samples the same rigid
+    particles as the oracle (bit for bit), and stepping the floor mesh plus
+    the moving, spinning box mesh matches the oracle as the analytic case."""
+    from oracle.oracle import OracleScene
+    sc = scenes.cpic_trimesh()
+    pipe = MpmPipeline()
+    st = state_from_scene(sc, deterministic=deterministic, use_cpic=True)
+    o = OracleScene(sc)
+    o.set_use_cpic(True)
+    rg, ro = st.read_rigid_particles(), o.rigid_particles()
+    assert len(ro["local"]) > 10000
+    assert np.array_equal(rg["local"].view(np.uint32), ro["local"].view(np.uint32))
+    assert np.array_equal(rg["collider"], ro["collider"]) and np.array_equal(rg["triangle"], ro["triangle"])
+    for _ in range(sc.steps):
+        pipe.step(st)
+    st.synchronize()
+    o.step(sc.steps)
+    g, want = st.read_particles(), o.particles()
+    gc, wc = st.read_cdf(), o.cdf()
+    err = rel_l2(g["pos"], want["pos"])
+    agree = (gc["affinity"] == wc["affinity"]).mean()
+    print(f"cpic trimesh, deterministic={deterministic}: rel L2 {err:.3e}, affinity agreement {agree:.4f}")
+    assert np.array_equal(g["enabled"], want["enabled"])
+    for bit in (5, 6):  # the floor mesh and the box mesh
+        assert ((wc["affinity"] >> bit) & 1).sum() > 100
+    if deterministic:
+        assert err < 1e-5 and agree > 0.99
+    else:
+        assert err < 1e-3 and agree > 0.95
+    np.testing.assert_allclose(st.collider_pose(6), o.collider_pose(6), rtol=0, atol=1e-5)
+
+
+def test_cpic_trimesh_resamples_with_the_cell_width(gpu_lib):
+    """Rigid particles exist only with CPIC on, and follow the cell width."""
+    sc = scenes.cpic_trimesh()
     st = state_from_scene(sc)
+    assert st.num_rigid_particles() == 0
+    st.set_use_cpic(True)
+    n = st.num_rigid_particles()
+    assert n > 10000
+    st.set_cell_width(sc.dx * 2.0, sc.grid_capacity)
+    assert 0 < st.num_rigid_particles() < n / 2
+    st.set_use_cpic(False)
+    assert st.num_rigid_particles() == 0
+
+
+def test_cpic_trimesh_refused_in_batched_scenes(gpu_lib):
+    """Trimesh CPIC samples the rigid particles of a single scene only."""
+    from nexus_b200.mpm import batched_state_from_scenes
+    st, _ = batched_state_from_scenes([scenes.trimesh_floor(n_side=4)])
     with pytest.raises(NexusError) as e:
         st.set_use_cpic(True)
     assert e.value.code == NXM_E_UNSUPPORTED

@@ -327,3 +327,75 @@ def test_cpic_keeps_particles_at_the_colliders(oracle_built):
     assert (c["affinity"] != 0).sum() > 100
     assert p["pos"][:, 2].min() < 0.5 * 1.5 * sc.dx < runs[False][0]["pos"][:, 2].min()
     assert np.linalg.norm(p["pos"] - ball, axis=1).min() > 2.0 - 0.5 * sc.dx
+
+
+def _mesh_scene(tri, meshes, dx, particle_pos=None):
+    """A scene whose colliders are the trimeshes `meshes` ((first, count) each)
+    over the triangles `tri` (k, 3, 3), with a few particles."""
+    from nexus_b200.scenes import Scene, lattice_block
+    pos = particle_pos if particle_pos is not None else lattice_block((50.0, 50.0, 50.0), (2, 2, 2), dx, 1)
+    b = ParticleBatch.from_positions(pos, np.float32(dx) / np.float32(4.0), 1000.0,
+                                     ParticleModel.elastic_neo_hookean(1.0e5, 0.3))
+    cols = collider_array([Collider.trimesh(f, c, (0.0, 0.0, 0.0), BoundaryCondition.slip()) for f, c in meshes])
+    return Scene("mesh", dx, 1.0e-3, (0.0, 0.0, 0.0), b, cols, 1, 1024,
+                 tri_vertices=np.asarray(tri, np.float32).reshape(-1, 3))
+
+
+def _rigid(sc):
+    from oracle.oracle import OracleScene
+    o = OracleScene(sc)
+    o.set_use_cpic(True)
+    return o.rigid_particles()
+
+
+def test_trimesh_sampling_covers_the_triangle(oracle_built):
+    """sample_trimesh.rs: every sample lies on the triangle (here in the plane
+    z = 0.25) and every cell of the x-y grid of the sampling step that lies
+    inside the triangle holds at least one sample."""
+    step = 0.1
+    tri = [[[0.0, 0.0, 0.25], [2.0, 0.0, 0.25], [0.0, 1.5, 0.25]]]
+    r = _rigid(_mesh_scene(tri, [(0, 1)], step))
+    p = r["local"]
+    assert len(p) > 200 and (r["collider"] == 0).all() and (r["triangle"] == 0).all()
+    assert (p[:, 2] == np.float32(0.25)).all()
+    assert (p[:, 0] >= -1e-6).all() and (p[:, 1] >= -1e-6).all()
+    assert (p[:, 0] / 2.0 + p[:, 1] / 1.5 <= 1.0 + 1e-5).all()
+    cells = {(int(math.floor(x / step)), int(math.floor(y / step))) for x, y in p[:, :2]}
+    for i in range(20):
+        for j in range(15):
+            if (i + 1) * step / 2.0 + (j + 1) * step / 1.5 <= 1.0 - 1e-6:  # cell fully inside
+                assert (i, j) in cells, (i, j)
+
+
+def test_trimesh_sampling_samples_a_shared_edge_once(oracle_built):
+    """sample_trimesh.rs:73-81: an edge shared by two triangles of one mesh is
+    sampled once; as two separate meshes it is sampled twice."""
+    tri = [[[0.0, 0.0, 0.0], [1.0, 0.0, 0.0], [1.0, 1.0, 0.0]],
+           [[0.0, 0.0, 0.0], [1.0, 1.0, 0.0], [0.0, 1.0, 0.0]]]
+    one = _rigid(_mesh_scene(tri, [(0, 2)], 0.1))["local"]
+    two = _rigid(_mesh_scene(tri, [(0, 1), (1, 1)], 0.1))["local"]
+    on_diag = lambda p: int((np.abs(p[:, 0] - p[:, 1]) < 1e-6).sum())
+    assert on_diag(two) > 0 and on_diag(two) == 2 * on_diag(one)
+    assert len(two) - len(one) == on_diag(one)
+
+
+def test_cpic_trimesh_plane_distance_field(oracle_built):
+    """p2g_cdf + g2p_cdf on a flat two-triangle floor z = 1: the particle
+    distance field of the particles within reach is the plane's signed
+    distance z - 1 with normal +z (exact in the FP64 oracle: the MLS fit
+    reproduces a linear field), and the FP32 oracle agrees to 1e-4."""
+    from oracle.oracle import OracleScene
+    from nexus_b200.scenes import lattice_block
+    L, dx = 32.0, 0.5
+    tri = [[[0, 0, 1], [L, 0, 1], [L, L, 1]], [[0, 0, 1], [L, L, 1], [0, L, 1]]]
+    pos = lattice_block((10.0, 10.0, 1.3), (8, 8, 6), dx, 5)
+    sc = _mesh_scene(tri, [(0, 2)], dx, pos)
+    for prec, tol in (("f64", 1e-12), ("f32", 1e-4)):
+        o = OracleScene(sc, precision=prec)
+        o.set_use_cpic(True)
+        o.step(1)
+        c = o.cdf()
+        m = c["affinity"] != 0
+        assert m.sum() > 50 and (c["affinity"][m] == 1).all()
+        assert np.abs(c["signed_distance"][m] - (pos[m, 2] - 1.0)).max() <= tol
+        assert np.abs(c["normal"][m] - np.array([0.0, 0.0, 1.0])).max() <= tol
