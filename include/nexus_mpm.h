@@ -94,9 +94,10 @@ typedef struct nxm_particle {
  * as nxm_particle; any pointer except position and model may be NULL to
  * take the Particle::new default: zero velocity/affine/force/vel_grad_det,
  * identity F, damping 0, phase 1, boundary_friction 1, group 0, enabled 1,
- * fixed 0; init_volume/mass are then required).  init_radius, phase,
- * boundary_friction and group_id are part of the layout; the step does not
- * read them and the library does not keep them. */
+ * fixed 0; init_volume/mass are then required; a missing init_radius is
+ * taken from init_volume = (2 r)^3).  boundary_friction scales the colliders'
+ * friction under CPIC; init_radius, phase and group_id only feed the render
+ * data (nxm_prep_readback). */
 typedef struct nxm_particles_soa {
     const float* position;        /* n*3 */
     const float* velocity;        /* n*3 */
@@ -229,6 +230,51 @@ NXM_API int nxm_state_num_rigid_particles(const nxm_state* state, uint32_t* coun
  * bits), 5 floats each (the reference's sample_points + sample_ids,
  * sampling/sample_trimesh.rs:33-56). */
 NXM_API int nxm_read_rigid_particles(nxm_state* state, float* out);
+
+/* Render data, headless (src_mpm/solver/prep_readback.rs, shader
+ * src_mpm_shaders/solver/prep_readback.rs).  RenderConfig modes: */
+#define NXM_RENDER_DEFAULT 0u       /* the group color */
+#define NXM_RENDER_VOLUME 1u        /* (1 - singular values of F) / 0.005 + 0.2 */
+#define NXM_RENDER_VELOCITY 2u      /* |v| dt 100 + 0.2 */
+#define NXM_RENDER_PHASE 3u         /* (0, 0.4 phase, 0.4 (1 - phase)) */
+#define NXM_RENDER_CDF_NORMALS 4u   /* (CPIC normal + 1) / 2 */
+#define NXM_RENDER_CDF_DISTANCES 5u /* CPIC signed distance / 1.5 dx: green outside, red inside */
+#define NXM_RENDER_CDF_SIGNS 6u     /* black: no affinity, green: no sign bit, red: a sign bit */
+
+/* ReadbackData (prep_readback.rs:81-93, 3D): color rgba (alpha of the group
+ * color; disabled particles (1, 0, 0, 1)), deformation diag(2 init_radius) *
+ * clamp(F, -4, 4) as a column-major 4x4 (Mat4::from_mat3), position. */
+typedef struct nxm_readback_data {
+    float color[4];
+    float deformation[16];
+    float position[3];
+    float pad;
+} nxm_readback_data;
+
+/* WgPrepReadback::launch (prep_readback.rs:152-200) for the particles: one
+ * record per particle, in particle-id order, read back into `out`
+ * (n records); synchronizes.  `palette` holds `num_groups` rgba colors
+ * indexed by group_id modulo num_groups (NULL or 0: the reference's default
+ * six-color palette). */
+NXM_API int nxm_prep_readback(nxm_state* state, uint32_t mode, const float* palette, uint32_t num_groups,
+                              nxm_readback_data* out);
+
+/* WgPrepReadback::launch_render (gpu_mpm_prep_render): the same data written
+ * straight into caller-owned DEVICE buffers, per particle in id order:
+ * positions (3 floats), deformations (9, the column-major 3x3), colors (4,
+ * 16-byte aligned); asynchronous on the state's stream (headless: plain CUDA
+ * buffers where the reference writes a renderer's instance buffers). */
+NXM_API int nxm_prep_render(nxm_state* state, uint32_t mode, const float* palette, uint32_t num_groups,
+                            float* positions, float* deformations, float* colors);
+
+/* gpu_prep_readback_rigid (prep_readback.rs:420-469): one record per CPIC
+ * rigid particle (sampling order): base color (`colors`, 4 floats per rigid
+ * particle, or NULL for the palette cycled over the particles as
+ * GpuReadbackData::new does), deformation diag(0.4 cell width), world
+ * position as of the start of the last step (the local sample before any
+ * step); synchronizes. */
+NXM_API int nxm_prep_readback_rigid(nxm_state* state, const float* colors, const float* palette,
+                                    uint32_t num_groups, nxm_readback_data* out);
 /* Particle Cdf (solver/particle.rs:35-50) of every particle: normal xyz,
  * signed distance, rigid velocity xyz, affinity bits (u32 bits), 8 floats
  * each; synchronizes. */

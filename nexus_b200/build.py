@@ -26,6 +26,7 @@ UNITS = {
     "nxm_transfer_fast.cu": [],
     "nxm_transfer_det.cu": ["--fmad=false"],
     "nxm_noalloc.cu": [],
+    "nxm_readback.cu": ["--fmad=false"],
 }
 
 HEADERS = ["nxm_device.cuh", "nxm_layout.h", "nxm_kernels.h", "nxm_transfer.inc.cuh"]

@@ -46,10 +46,11 @@ struct DevPtrs {
     // [x, x + y) in `colliders`
     const uint32_t* pscene;
     const uint2* scene_cols;
-    // CPIC (analytic colliders): node distance field (distance bits, affinity
-    // + sign bits, closest collider, unused), the nodes' incompatible
-    // momentum / velocity + mass, and per particle id 3 float4: normal +
-    // signed distance, rigid velocity + affinity bits, boundary friction.
+    // CPIC: node distance field (distance bits, affinity + sign bits, closest
+    // collider, unused), the nodes' incompatible momentum / velocity + mass,
+    // and per particle id 3 float4: normal + signed distance, rigid velocity
+    // + affinity bits, and the properties the step does not move (boundary
+    // friction, then the render-only init radius, phase, group id bits).
     uint4* ncdf;
     float4* nodes_inc;
     float4* pcdf;
@@ -114,6 +115,34 @@ void launch_p2g_cdf(const DevPtrs& P, const LaunchCfg& c, cudaStream_t s);
 void launch_grid_update(const DevPtrs& P, const LaunchCfg& c, cudaStream_t s);
 void launch_g2p_update(const DevPtrs& P, const LaunchCfg& c, cudaStream_t s);
 }  // namespace exact
+
+// Render data (prep_readback.rs): the particle records, the slot -> id map of
+// block-ordered storage (null: slot = id), the render mode and palette.
+enum : uint32_t {
+    RENDER_DEFAULT = 0,
+    RENDER_VOLUME = 1,
+    RENDER_VELOCITY = 2,
+    RENDER_PHASE = 3,
+    RENDER_CDF_NORMALS = 4,
+    RENDER_CDF_DISTANCES = 5,
+    RENDER_CDF_SIGNS = 6,
+};
+struct RenderSrc {
+    const PKin* kin;
+    const PDef* def;
+    const float4* pcdf;  // per id: normal + signed distance, rigid velocity + affinity, render properties
+    const uint32_t* pid;
+    uint32_t n;
+    uint32_t mode;
+    const float4* palette;
+    uint32_t num_groups;
+    float dx, dt;
+    int sm_count;
+};
+void launch_prep_readback(const RenderSrc& in, float4* out, cudaStream_t s);
+void launch_prep_render(const RenderSrc& in, float* positions, float* deformations, float* colors, cudaStream_t s);
+void launch_prep_readback_rigid(const RenderSrc& in, const float4* world, uint32_t nrp, const float4* colors,
+                                float4* out, cudaStream_t s);
 
 // Primary-only block sort of plain float4 positions (x, y, z, unused): no
 // per-particle scratch; P.sorted receives the ids, P.nodes may be null.

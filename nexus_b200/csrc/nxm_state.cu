@@ -260,12 +260,13 @@ __global__ void k_set_velocities(DevCollider* __restrict__ cols, const float* __
     }
 }
 
-// Fresh CPIC records: empty distance field, the particle's boundary friction (1 if none given).
-__global__ void k_init_pcdf(float4* __restrict__ pcdf, const float* __restrict__ bfric, uint32_t count) {
+// Fresh CPIC records: empty distance field, then the uploaded properties
+// (boundary friction, init radius, phase, group id).
+__global__ void k_init_pcdf(float4* __restrict__ pcdf, const float4* __restrict__ props, uint32_t count) {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
         pcdf[3 * (size_t)i] = make_float4(0.f, 0.f, 0.f, 0.f);
         pcdf[3 * (size_t)i + 1] = make_float4(0.f, 0.f, 0.f, 0.f);
-        pcdf[3 * (size_t)i + 2] = make_float4(bfric ? bfric[i] : 1.0f, 0.f, 0.f, 0.f);
+        pcdf[3 * (size_t)i + 2] = props[i];
     }
 }
 
@@ -409,6 +410,12 @@ struct nxm_state {
     bool graph_valid[2] = {false, false};
     int graph_kernels = 0;
     uint64_t launches = 0;
+
+    // render data (prep_readback): record scratch and palette
+    float4* d_render = nullptr;
+    size_t render_cap = 0;  // float4s
+    float4* d_palette = nullptr;
+    uint32_t palette_cap = 0;
 
     // scratch for readback packing
     uint32_t* d_pack = nullptr;
@@ -921,7 +928,7 @@ int upload_particles(nxm_state* s, const nxm_particles_soa* p, uint32_t count) {
     if (rc) return rc;
     std::vector<PKin> hk(count);
     std::vector<PDef> hd(count);
-    std::vector<float4> hs(count);
+    std::vector<float4> hs(count), hr(count);
     static const float I9[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
     uint32_t last_mid = 0;
     for (uint32_t i = 0; i < count; ++i) {
@@ -957,6 +964,11 @@ int upload_particles(nxm_state* s, const nxm_particles_soa* p, uint32_t count) {
         float st[4] = {0, 0, 0, 0};
         for (int w = 0; w < ns; ++w) st[w] = bits_f(m.data[w]);
         hs[i] = make_float4(st[0], st[1], st[2], st[3]);
+        // defaults of ParticleDynamics::new (solver/particle.rs:100-122); the
+        // radius, when not given, from init_volume = (2 r)^3
+        hr[i] = make_float4(p->boundary_friction ? p->boundary_friction[i] : 1.0f,
+                            p->init_radius ? p->init_radius[i] : 0.5f * std::cbrt(p->init_volume[i]),
+                            p->phase ? p->phase[i] : 1.0f, bits_f(p->group_id ? p->group_id[i] : 0u));
     }
     if (s->chunks_used) s->slot2chunk.insert(s->slot2chunk.end(), count, NONE);
     rc = sync_materials(s);
@@ -964,20 +976,16 @@ int upload_particles(nxm_state* s, const nxm_particles_soa* p, uint32_t count) {
     NXM_TRY(cudaMemcpyAsync(s->kin + s->n, hk.data(), sizeof(PKin) * count, cudaMemcpyHostToDevice, s->stream));
     NXM_TRY(cudaMemcpyAsync(s->def + s->n, hd.data(), sizeof(PDef) * count, cudaMemcpyHostToDevice, s->stream));
     NXM_TRY(cudaMemcpyAsync(s->pstate + s->n, hs.data(), sizeof(float4) * count, cudaMemcpyHostToDevice, s->stream));
-    {  // CPIC fields start empty; boundary friction (default 1) scales the colliders' friction there
-        const float* bf = nullptr;
-        if (p->boundary_friction) {
-            if (count > s->pack_cap) {
-                NXM_TRY(cudaStreamSynchronize(s->stream));
-                dfree(s->d_pack);
-                NXM_TRY(dalloc(&s->d_pack, count));
-                s->pack_cap = count;
-            }
-            NXM_TRY(cudaMemcpyAsync(s->d_pack, p->boundary_friction, 4 * (size_t)count, cudaMemcpyHostToDevice,
-                                    s->stream));
-            bf = reinterpret_cast<const float*>(s->d_pack);
+    {  // CPIC fields start empty; the properties record follows them
+        if (4 * (size_t)count > s->pack_cap) {
+            NXM_TRY(cudaStreamSynchronize(s->stream));
+            dfree(s->d_pack);
+            NXM_TRY(dalloc(&s->d_pack, 4 * (size_t)count));
+            s->pack_cap = 4 * (size_t)count;
         }
-        k_init_pcdf<<<grid_for_n(s, count), 256, 0, s->stream>>>(s->d_pcdf + 3 * (size_t)s->n, bf, count);
+        NXM_TRY(cudaMemcpyAsync(s->d_pack, hr.data(), sizeof(float4) * count, cudaMemcpyHostToDevice, s->stream));
+        k_init_pcdf<<<grid_for_n(s, count), 256, 0, s->stream>>>(s->d_pcdf + 3 * (size_t)s->n,
+                                                                  reinterpret_cast<const float4*>(s->d_pack), count);
         s->launches += 1;
         NXM_TRY(cudaGetLastError());
     }
@@ -1332,6 +1340,9 @@ int rebuild_rigid_particles(nxm_state* s) {
         NXM_TRY(dalloc(&s->d_rp_sorted, 8 * (size_t)s->nrp));
         NXM_TRY(cudaMemcpyAsync(s->d_rp_local, s->rp_host.data(), sizeof(float4) * s->nrp, cudaMemcpyHostToDevice,
                                 s->stream));
+        // world = local until the first step (solver/particle.rs:272-276)
+        NXM_TRY(cudaMemcpyAsync(s->d_rp_world, s->d_rp_local, sizeof(float4) * s->nrp, cudaMemcpyDeviceToDevice,
+                                s->stream));
         NXM_TRY(cudaStreamSynchronize(s->stream));
     }
     if (had || s->nrp) invalidate_graph(s);
@@ -1430,6 +1441,7 @@ void nxm_state_destroy(nxm_state* s) {
     dfree(s->d_materials); dfree(s->d_colliders); dfree(s->d_tris); dfree(s->d_bvh); dfree(s->d_scene_cols); dfree(s->d_vel6); dfree(s->d_params); dfree(s->d_counters);
     dfree(s->d_pack); dfree(s->d_offsets);
     dfree(s->d_rp_local); dfree(s->d_rp_world); dfree(s->d_rp_need); dfree(s->d_rp_sorted);
+    dfree(s->d_render); dfree(s->d_palette);
     if (s->h_counters) cudaFreeHost(s->h_counters);
     if (s->stream) cudaStreamDestroy(s->stream);
     delete s;
@@ -1530,6 +1542,110 @@ int nxm_state_set_use_cpic(nxm_state* s, int enabled) {
     s->use_cpic = enabled != 0;
     s->params_dirty = true;
     return rebuild_rigid_particles(s);
+}
+
+// ---- render data (headless prep_readback) -----------------------------------
+
+static_assert(sizeof(nxm_readback_data) == 96, "ReadbackData layout");
+static_assert(NXM_RENDER_DEFAULT == RENDER_DEFAULT && NXM_RENDER_VOLUME == RENDER_VOLUME &&
+                  NXM_RENDER_VELOCITY == RENDER_VELOCITY && NXM_RENDER_PHASE == RENDER_PHASE &&
+                  NXM_RENDER_CDF_NORMALS == RENDER_CDF_NORMALS && NXM_RENDER_CDF_DISTANCES == RENDER_CDF_DISTANCES &&
+                  NXM_RENDER_CDF_SIGNS == RENDER_CDF_SIGNS,
+              "render modes");
+
+// GpuReadbackData::DEFAULT_GROUP_COLORS (src_mpm/solver/prep_readback.rs).
+static const float kDefaultPalette[6][4] = {
+    {124.0f / 255.0f, 144.0f / 255.0f, 1.0f, 1.0f},          {8.0f / 255.0f, 144.0f / 255.0f, 1.0f, 1.0f},
+    {124.0f / 255.0f, 7.0f / 255.0f, 1.0f, 1.0f},            {124.0f / 255.0f, 144.0f / 255.0f, 7.0f / 255.0f, 1.0f},
+    {200.0f / 255.0f, 37.0f / 255.0f, 1.0f, 1.0f},           {124.0f / 255.0f, 230.0f / 255.0f, 25.0f / 255.0f, 1.0f}};
+
+// Uploads the palette (null or empty: the default one) and fills `in`.
+static int render_source(nxm_state* s, uint32_t mode, const float* palette, uint32_t num_groups, RenderSrc& in) {
+    if (!palette || num_groups == 0) {
+        palette = &kDefaultPalette[0][0];
+        num_groups = 6;
+    }
+    if (num_groups > s->palette_cap) {
+        NXM_TRY(cudaStreamSynchronize(s->stream));
+        dfree(s->d_palette);
+        NXM_TRY(dalloc(&s->d_palette, num_groups));
+        s->palette_cap = num_groups;
+    }
+    NXM_TRY(cudaMemcpyAsync(s->d_palette, palette, sizeof(float4) * num_groups, cudaMemcpyHostToDevice, s->stream));
+    in.kin = s->kin;
+    in.def = s->def;
+    in.pcdf = s->d_pcdf;
+    in.pid = s->permuted ? s->pid : nullptr;
+    in.n = s->n;
+    in.mode = mode;
+    in.palette = s->d_palette;
+    in.num_groups = num_groups;
+    in.dx = s->dx;
+    in.dt = s->dt;
+    in.sm_count = s->sm_count;
+    return NXM_OK;
+}
+
+static int render_scratch(nxm_state* s, size_t records) {
+    if (6 * records <= s->render_cap) return NXM_OK;
+    NXM_TRY(cudaStreamSynchronize(s->stream));
+    dfree(s->d_render);
+    NXM_TRY(dalloc(&s->d_render, 6 * records));
+    s->render_cap = 6 * records;
+    return NXM_OK;
+}
+
+int nxm_prep_readback(nxm_state* s, uint32_t mode, const float* palette, uint32_t num_groups, nxm_readback_data* out) {
+    if (!s || (s->n && !out)) return NXM_E_INVALID;
+    if (s->n == 0) return NXM_OK;
+    RenderSrc in{};
+    int rc = render_source(s, mode, palette, num_groups, in);
+    if (rc) return rc;
+    rc = render_scratch(s, s->n);
+    if (rc) return rc;
+    launch_prep_readback(in, s->d_render, s->stream);
+    s->launches += 1;
+    NXM_TRY(cudaGetLastError());
+    NXM_TRY(cudaMemcpyAsync(out, s->d_render, sizeof(nxm_readback_data) * s->n, cudaMemcpyDeviceToHost, s->stream));
+    NXM_TRY(cudaStreamSynchronize(s->stream));
+    return NXM_OK;
+}
+
+int nxm_prep_render(nxm_state* s, uint32_t mode, const float* palette, uint32_t num_groups, float* positions,
+                    float* deformations, float* colors) {
+    if (!s || (s->n && (!positions || !deformations || !colors))) return NXM_E_INVALID;
+    if (reinterpret_cast<uintptr_t>(colors) % 16 != 0) return NXM_E_INVALID;
+    if (s->n == 0) return NXM_OK;
+    RenderSrc in{};
+    int rc = render_source(s, mode, palette, num_groups, in);
+    if (rc) return rc;
+    launch_prep_render(in, positions, deformations, colors, s->stream);
+    s->launches += 1;
+    NXM_TRY(cudaGetLastError());
+    return NXM_OK;
+}
+
+int nxm_prep_readback_rigid(nxm_state* s, const float* colors, const float* palette, uint32_t num_groups,
+                            nxm_readback_data* out) {
+    if (!s || (s->nrp && !out)) return NXM_E_INVALID;
+    if (s->nrp == 0) return NXM_OK;
+    RenderSrc in{};
+    int rc = render_source(s, RENDER_DEFAULT, palette, num_groups, in);
+    if (rc) return rc;
+    rc = render_scratch(s, (size_t)s->nrp * (colors ? 2 : 1));
+    if (rc) return rc;
+    const float4* d_colors = nullptr;
+    if (colors) {  // per rigid particle base colors, staged after the records
+        NXM_TRY(cudaMemcpyAsync(s->d_render + 6 * (size_t)s->nrp, colors, sizeof(float4) * s->nrp,
+                                cudaMemcpyHostToDevice, s->stream));
+        d_colors = s->d_render + 6 * (size_t)s->nrp;
+    }
+    launch_prep_readback_rigid(in, s->d_rp_world, s->nrp, d_colors, s->d_render, s->stream);
+    s->launches += 1;
+    NXM_TRY(cudaGetLastError());
+    NXM_TRY(cudaMemcpyAsync(out, s->d_render, sizeof(nxm_readback_data) * s->nrp, cudaMemcpyDeviceToHost, s->stream));
+    NXM_TRY(cudaStreamSynchronize(s->stream));
+    return NXM_OK;
 }
 
 int nxm_state_num_rigid_particles(const nxm_state* s, uint32_t* count) {

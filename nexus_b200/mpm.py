@@ -28,6 +28,10 @@ NXM_E_NO_DEVICE = -5
 NXM_E_UNSUPPORTED = -6
 NXM_E_OOM = -7
 
+# RenderConfig modes of the render data (solver/prep_readback.rs:16-21)
+RENDER_DEFAULT, RENDER_VOLUME, RENDER_VELOCITY, RENDER_PHASE = 0, 1, 2, 3
+RENDER_CDF_NORMALS, RENDER_CDF_DISTANCES, RENDER_CDF_SIGNS = 4, 5, 6
+
 HEADER_FIELDS = 23
 
 # Every function the header declares, with its ctypes signature.
@@ -94,6 +98,9 @@ SIGNATURES = {
     "nxm_read_cdf": (C.c_int, [_vp, _f]),
     "nxm_state_num_rigid_particles": (C.c_int, [_vp, _u]),
     "nxm_read_rigid_particles": (C.c_int, [_vp, _f]),
+    "nxm_prep_readback": (C.c_int, [_vp, C.c_uint32, _f, C.c_uint32, _f]),
+    "nxm_prep_render": (C.c_int, [_vp, C.c_uint32, _f, C.c_uint32, _vp, _vp, _vp]),
+    "nxm_prep_readback_rigid": (C.c_int, [_vp, _f, _f, C.c_uint32, _f]),
     "nxm_state_set_collider_velocities": (C.c_int, [_vp, C.c_uint32, C.c_uint32, _f]),
     "nxm_state_enable_scenes": (C.c_int, [_vp, C.c_uint32]),
     "nxm_scene_capacity": (C.c_uint32, [_vp]),
@@ -404,6 +411,48 @@ class MpmState:
         out = out[:n]
         return dict(local=out[:, :3], collider=out[:, 3].copy().view(np.uint32),
                     triangle=out[:, 4].copy().view(np.uint32))
+
+    @staticmethod
+    def _render_records(out: np.ndarray) -> dict:
+        return dict(color=out[:, 0:4], deformation=out[:, 4:20].reshape(-1, 4, 4), position=out[:, 20:23])
+
+    @staticmethod
+    def _palette(palette):
+        if palette is None:
+            return None, 0
+        pal = np.ascontiguousarray(palette, np.float32).reshape(-1, 4)
+        return pal, len(pal)
+
+    def prep_readback(self, mode: int = 0, palette=None) -> dict:
+        """``WgPrepReadback::launch`` (headless): per particle in id order its
+        render color for `mode` (RENDER_*), deformation (n, 4, 4) as columns
+        of Mat4::from_mat3(diag(2 r) clamp(F, -4, 4)) and position."""
+        pal, ng = self._palette(palette)
+        out = np.zeros((max(len(self), 1), 24), np.float32)
+        _check(self.lib.nxm_prep_readback(self.h, mode, None if pal is None else _p(pal, _f), ng, _p(out, _f)),
+               "prep_readback")
+        return self._render_records(out[:len(self)])
+
+    def prep_render(self, mode: int, positions: int, deformations: int, colors: int, palette=None):
+        """``WgPrepReadback::launch_render``: the render data written into
+        caller-owned device buffers (device pointers as ints: n x 3, n x 9,
+        n x 4 floats), asynchronously on the state's stream."""
+        pal, ng = self._palette(palette)
+        _check(self.lib.nxm_prep_render(self.h, mode, None if pal is None else _p(pal, _f), ng,
+                                        C.c_void_p(positions), C.c_void_p(deformations), C.c_void_p(colors)),
+               "prep_render")
+
+    def prep_readback_rigid(self, colors=None, palette=None) -> dict:
+        """``gpu_prep_readback_rigid``: per CPIC rigid particle its base color,
+        deformation diag(0.4 dx) and world position."""
+        n = self.num_rigid_particles()
+        pal, ng = self._palette(palette)
+        cols = None if colors is None else np.ascontiguousarray(colors, np.float32).reshape(-1, 4)
+        out = np.zeros((max(n, 1), 24), np.float32)
+        _check(self.lib.nxm_prep_readback_rigid(self.h, None if cols is None else _p(cols, _f),
+                                                None if pal is None else _p(pal, _f), ng, _p(out, _f)),
+               "prep_readback_rigid")
+        return self._render_records(out[:n])
 
     def estimate_timestep_bound(self) -> tuple[float, int]:
         """``WgTimestepBounds::compute_bounds``: (max dt in seconds, fixed-point bits)."""

@@ -633,6 +633,8 @@ typedef struct {
     uint32_t *enabled, *fixed, *tag;
     REAL *words; /* n * 24 */
     REAL *bfric; /* boundary_friction */
+    float *init_radius, *phase; /* render-only properties (ParticleProperties) */
+    uint32_t *group_id;
     /* particle Cdf (solver/particle.rs:35-50): normal, signed distance, rigid velocity, affinity bits */
     v3 *cdf_normal, *cdf_rigid_vel;
     REAL *cdf_sd;
@@ -690,6 +692,9 @@ scene_t *orc_create(uint32_t n, double dx, uint32_t grid_capacity) {
     s->damping = xcalloc(n, sizeof(REAL));
     s->enabled = xcalloc(n, sizeof(uint32_t));
     s->bfric = xcalloc(n, sizeof(REAL));
+    s->init_radius = xcalloc(n, sizeof(float));
+    s->phase = xcalloc(n, sizeof(float));
+    s->group_id = xcalloc(n, sizeof(uint32_t));
     for (uint32_t i = 0; i < n; ++i) s->bfric[i] = (REAL)1.0;
     s->cdf_normal = xcalloc(n, sizeof(v3));
     s->cdf_rigid_vel = xcalloc(n, sizeof(v3));
@@ -714,7 +719,7 @@ void orc_destroy(scene_t *s) {
     if (!s) return;
     free(s->pos); free(s->vel); free(s->aff); free(s->F); free(s->vgd); free(s->mass);
     free(s->init_volume); free(s->damping); free(s->enabled); free(s->fixed); free(s->tag);
-    free(s->bfric); free(s->cdf_normal); free(s->cdf_rigid_vel); free(s->cdf_sd); free(s->cdf_aff);
+    free(s->bfric); free(s->init_radius); free(s->phase); free(s->group_id); free(s->cdf_normal); free(s->cdf_rigid_vel); free(s->cdf_sd); free(s->cdf_aff);
     free(s->words); free(s->hstate); free(s->hvalue); free(s->howner); free(s->hdr);
     free(s->nodes); free(s->sorted); free(s->scan); free(s->col); free(s->tri);
     free(s->rp_local); free(s->rp_world); free(s->rp_col); free(s->rp_tri); free(s->rp_need); free(s->rp_sorted);
@@ -753,6 +758,14 @@ void orc_set_particles(scene_t *s, const float *pos, const float *vel, const flo
 
 void orc_set_boundary_friction(scene_t *s, const float *bf) {
     for (uint32_t i = 0; i < s->n; ++i) s->bfric[i] = bf[i];
+}
+
+void orc_set_render_props(scene_t *s, const float *init_radius, const float *phase, const uint32_t *group_id) {
+    for (uint32_t i = 0; i < s->n; ++i) {
+        s->init_radius[i] = init_radius[i];
+        s->phase[i] = phase[i];
+        s->group_id[i] = group_id[i];
+    }
 }
 
 static float f2bitsf(uint32_t u) { float f; memcpy(&f, &u, 4); return f; }
@@ -1017,6 +1030,7 @@ static void build_rigid_particles(scene_t *s) {
     s->rp_sorted = xcalloc((size_t)s->nrp * 8, sizeof(uint32_t));
     for (uint32_t i = 0; i < s->nrp; ++i) {
         s->rp_local[i] = V(all.pt[i].x, all.pt[i].y, all.pt[i].z);
+        s->rp_world[i] = s->rp_local[i];  /* solver/particle.rs:272-276: world = local until the first step */
         s->rp_col[i] = cols[i];
         s->rp_tri[i] = all.tri[i];
     }
@@ -2126,4 +2140,87 @@ static proj_t trimesh_project(const scene_t *s, const collider_t *c, v3 pt, REAL
     out.point = bp.point;
     out.inside = vdot(pn, vsub(pt, bp.point)) <= 0;
     return out;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Render data: src_mpm_shaders/solver/prep_readback.rs (3D)                 */
+/* ------------------------------------------------------------------------ */
+
+/* GpuReadbackData::DEFAULT_GROUP_COLORS (src_mpm/solver/prep_readback.rs). */
+static const float DEFAULT_PALETTE[6][4] = {
+    {124.0f / 255.0f, 144.0f / 255.0f, 1.0f, 1.0f},           {8.0f / 255.0f, 144.0f / 255.0f, 1.0f, 1.0f},
+    {124.0f / 255.0f, 7.0f / 255.0f, 1.0f, 1.0f},             {124.0f / 255.0f, 144.0f / 255.0f, 7.0f / 255.0f, 1.0f},
+    {200.0f / 255.0f, 37.0f / 255.0f, 1.0f, 1.0f},            {124.0f / 255.0f, 230.0f / 255.0f, 25.0f / 255.0f, 1.0f}};
+
+static inline void put4(float *o, float a, float b, float c, float d) { o[0] = a; o[1] = b; o[2] = c; o[3] = d; }
+
+/* One ReadbackData record, 24 floats: color, deformation as a column-major
+ * 4x4 (Mat4::from_mat3), position, padding. */
+static void readback_record(float *o, const float color[4], m3 def, v3 pos) {
+    put4(o, color[0], color[1], color[2], color[3]);
+    put4(o + 4, (float)def.c0.x, (float)def.c0.y, (float)def.c0.z, 0.0f);
+    put4(o + 8, (float)def.c1.x, (float)def.c1.y, (float)def.c1.z, 0.0f);
+    put4(o + 12, (float)def.c2.x, (float)def.c2.y, (float)def.c2.z, 0.0f);
+    put4(o + 16, 0.0f, 0.0f, 0.0f, 1.0f);
+    put4(o + 20, (float)pos.x, (float)pos.y, (float)pos.z, 0.0f);
+}
+
+/* prep_readback.rs:241-295 gpu_prep_readback: per particle (id order) its
+ * color for the render mode (compute_color, :176-237), its deformation
+ * diag(2 r) * clamp(F, -4, 4) (compute_deformation, :111-123) and position.
+ * `palette` holds `num_groups` rgba colors (NULL: the default palette). */
+void orc_prep_readback(const scene_t *s, uint32_t mode, const float *palette, uint32_t num_groups, float *out24) {
+    if (!palette || num_groups == 0) { palette = &DEFAULT_PALETTE[0][0]; num_groups = 6; }
+    for (uint32_t i = 0; i < s->n; ++i) {
+        const float *bc = palette + 4 * (size_t)(s->group_id[i] % num_groups);
+        float col[4] = {bc[0], bc[1], bc[2], bc[3]};  /* every mode keeps the base alpha */
+        if (mode == 2) { /* velocity */
+            v3 c = vadd(vmul(vmul(vabs(s->vel[i]), s->dt), (REAL)100.0), vsplat((REAL)0.2));
+            col[0] = (float)c.x; col[1] = (float)c.y; col[2] = (float)c.z;
+        } else if (mode == 1) { /* volume */
+            svd3 d = svd(s->F[i]);
+            v3 c = vadd(vdiv(vsub(vsplat((REAL)1.0), d.s), (REAL)0.005), vsplat((REAL)0.2));
+            col[0] = (float)c.x; col[1] = (float)c.y; col[2] = (float)c.z;
+        } else if (mode == 3) { /* phase */
+            const REAL ph = s->phase[i];
+            col[0] = 0.0f; col[1] = (float)((REAL)0.4 * ph); col[2] = (float)((REAL)0.4 * ((REAL)1.0 - ph));
+        } else if (mode == 4) { /* cdf normals */
+            v3 nrm = s->cdf_normal[i];
+            if (nrm.x == 0 && nrm.y == 0 && nrm.z == 0) { col[0] = col[1] = col[2] = 0.0f; }
+            else {
+                v3 c = vmul(vadd(nrm, vsplat((REAL)1.0)), (REAL)0.5);
+                col[0] = (float)c.x; col[1] = (float)c.y; col[2] = (float)c.z;
+            }
+        } else if (mode == 5) { /* cdf distances */
+            REAL d = s->cdf_sd[i] / (s->dx * (REAL)1.5);
+            if (d > 0) { col[0] = 0.0f; col[1] = (float)fabs(d); col[2] = 0.0f; }
+            else { col[0] = (float)fabs(d); col[1] = 0.0f; col[2] = 0.0f; }
+        } else if (mode == 6) { /* cdf signs */
+            uint32_t a = s->cdf_aff[i];
+            uint32_t both = (a >> 16) & (a & 0x0000FFFFu);
+            col[0] = (a != 0 && both != 0) ? 1.0f : 0.0f;
+            col[1] = (a != 0 && both == 0) ? 1.0f : 0.0f;
+            col[2] = 0.0f;
+        }
+        if (!s->enabled[i]) put4(col, 1.0f, 0.0f, 0.0f, 1.0f);
+        const REAL r2 = (REAL)s->init_radius[i] * (REAL)2.0;
+        m3 cl = M(vclamp(s->F[i].c0, -4, 4), vclamp(s->F[i].c1, -4, 4), vclamp(s->F[i].c2, -4, 4));
+        m3 def = mm(mdiag(vsplat(r2)), cl);
+        readback_record(out24 + 24 * (size_t)i, col, def, s->pos[i]);
+    }
+}
+
+/* prep_readback.rs:420-469 gpu_prep_readback_rigid: per rigid particle its
+ * base color (`colors`, 4 per particle; NULL: the palette cycled over the
+ * particles, GpuReadbackData::new), the deformation diag(0.4 dx) and its
+ * world position. */
+void orc_prep_readback_rigid(scene_t *s, const float *colors, const float *palette, uint32_t num_groups,
+                             float *out24) {
+    if (s->rp_dirty) build_rigid_particles(s);
+    if (!palette || num_groups == 0) { palette = &DEFAULT_PALETTE[0][0]; num_groups = 6; }
+    const REAL scale = s->dx * (REAL)0.4;
+    for (uint32_t i = 0; i < s->nrp; ++i) {
+        const float *c = colors ? colors + 4 * (size_t)i : palette + 4 * (size_t)(i % num_groups);
+        readback_record(out24 + 24 * (size_t)i, c, mdiag(vsplat(scale)), s->rp_world[i]);
+    }
 }

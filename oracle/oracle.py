@@ -64,6 +64,9 @@ def lib(precision: str = "f32"):
                  "orc_g2p_cdf"):
         getattr(L, name).argtypes = [C.c_void_p]
     L.orc_get_rigid.argtypes = [C.c_void_p, _f]
+    L.orc_set_render_props.argtypes = [C.c_void_p, _f, _f, _u]
+    L.orc_prep_readback.argtypes = [C.c_void_p, C.c_uint32, _f, C.c_uint32, _f]
+    L.orc_prep_readback_rigid.argtypes = [C.c_void_p, _f, _f, C.c_uint32, _f]
     for name in ("orc_num_blocks", "orc_status", "orc_capacity", "orc_sorted_len", "orc_timestep_bound_bits",
                  "orc_num_rigid"):
         getattr(L, name).argtypes = [C.c_void_p]
@@ -120,6 +123,33 @@ class OracleScene:
         self.L.orc_set_particles(self.h, *[_ptr(a, _f) for a in arrs], *[_ptr(a, _u) for a in ints])
         bf = np.ascontiguousarray(p.boundary_friction, dtype=np.float32)
         self.L.orc_set_boundary_friction(self.h, _ptr(bf, _f))
+        r, ph = (np.ascontiguousarray(a, dtype=np.float32) for a in (p.init_radius, p.phase))
+        g = np.ascontiguousarray(p.group_id, dtype=np.uint32)
+        self.L.orc_set_render_props(self.h, _ptr(r, _f), _ptr(ph, _f), _ptr(g, _u))
+
+    @staticmethod
+    def _records(out: np.ndarray) -> dict:
+        return dict(color=out[:, 0:4], deformation=out[:, 4:20].reshape(-1, 4, 4), position=out[:, 20:23])
+
+    def prep_readback(self, mode: int, palette=None) -> dict:
+        """ReadbackData of every particle (prep_readback.rs): color (n, 4),
+        deformation (n, 4, 4) as columns, position (n, 3)."""
+        pal = None if palette is None else np.ascontiguousarray(palette, np.float32).reshape(-1, 4)
+        out = np.zeros((self.n, 24), np.float32)
+        self.L.orc_prep_readback(self.h, mode, None if pal is None else _ptr(pal, _f),
+                                 0 if pal is None else len(pal), _ptr(out, _f))
+        return self._records(out)
+
+    def prep_readback_rigid(self, colors=None, palette=None) -> dict:
+        """ReadbackData of every rigid particle (prep_readback.rs:420-469)."""
+        n = self.L.orc_num_rigid(self.h)
+        cols = None if colors is None else np.ascontiguousarray(colors, np.float32).reshape(-1, 4)
+        pal = None if palette is None else np.ascontiguousarray(palette, np.float32).reshape(-1, 4)
+        out = np.zeros((max(n, 1), 24), np.float32)
+        self.L.orc_prep_readback_rigid(self.h, None if cols is None else _ptr(cols, _f),
+                                       None if pal is None else _ptr(pal, _f), 0 if pal is None else len(pal),
+                                       _ptr(out, _f))
+        return self._records(out[:n])
 
     def cdf(self) -> dict:
         """Particle Cdf (CPIC): normal, signed distance, rigid velocity, affinity bits."""

@@ -399,3 +399,43 @@ def test_cpic_trimesh_plane_distance_field(oracle_built):
         assert m.sum() > 50 and (c["affinity"][m] == 1).all()
         assert np.abs(c["signed_distance"][m] - (pos[m, 2] - 1.0)).max() <= tol
         assert np.abs(c["normal"][m] - np.array([0.0, 0.0, 1.0])).max() <= tol
+
+
+def test_readback_record_closed_form(oracle_built):
+    """prep_readback.rs compute_deformation / compute_color on hand-set
+    particles: deformation diag(2 r) clamp(F, -4, 4) as Mat4::from_mat3,
+    the velocity, phase and default colors, group ids wrapping the palette,
+    and a disabled particle drawn red."""
+    from oracle.oracle import OracleScene
+    from nexus_b200.scenes import Scene
+    rng = np.random.default_rng(5)
+    n = 8
+    b = ParticleBatch.from_positions(rng.uniform(0.3, 0.7, (n, 3)), np.float32(0.01), 1000.0,
+                                     ParticleModel.elastic_neo_hookean(1.0e5, 0.3))
+    b.def_grad = rng.uniform(-6.0, 6.0, (n, 9)).astype(np.float32)
+    b.vel = rng.uniform(-3.0, 3.0, (n, 3)).astype(np.float32)
+    b.init_radius = rng.uniform(0.005, 0.02, n).astype(np.float32)
+    b.phase = rng.uniform(0.0, 1.0, n).astype(np.float32)
+    b.group_id = np.arange(n, dtype=np.uint32) * 3
+    b.enabled[5] = 0
+    sc = Scene("readback", 0.02, 1.0e-4, (0.0, 0.0, 0.0), b, collider_array([]), 1, 64)
+    o = OracleScene(sc)
+    pal = rng.uniform(0.0, 1.0, (5, 4)).astype(np.float32)
+    F = b.def_grad.reshape(n, 3, 3)  # [particle, column, row]
+    for mode in (0, 2, 3):
+        r = o.prep_readback(mode, pal)
+        base = pal[b.group_id % 5]
+        want = {0: base,
+                2: np.concatenate([np.abs(b.vel) * np.float32(1e-4) * np.float32(100.0) + np.float32(0.2),
+                                   base[:, 3:]], 1),
+                3: np.stack([np.zeros(n, np.float32), np.float32(0.4) * b.phase,
+                             np.float32(0.4) * (np.float32(1.0) - b.phase), base[:, 3]], 1)}[mode].copy()
+        want[5] = (1.0, 0.0, 0.0, 1.0)
+        np.testing.assert_allclose(r["color"], want, rtol=1e-6, atol=1e-7)
+        d = r["deformation"]  # [particle, column, row]
+        np.testing.assert_allclose(d[:, :3, :3], 2.0 * b.init_radius[:, None, None] * np.clip(F, -4.0, 4.0),
+                                   rtol=1e-6)
+        assert (d[:, :3, 3] == 0).all() and (d[:, 3] == np.array([0, 0, 0, 1], np.float32)).all()
+        np.testing.assert_array_equal(r["position"], b.pos)
+    default = o.prep_readback(0)["color"]
+    np.testing.assert_allclose(default[0], [124 / 255, 144 / 255, 1.0, 1.0], rtol=1e-6)
