@@ -196,7 +196,9 @@ NXM_API int nxm_state_set_colliders(nxm_state* state, const nxm_collider* collid
                             const float* tri_vertices, uint32_t num_triangles);
 
 /* Overwrites the velocity of collider i (kinematic driving, e.g. velocity =
- * d(pose)/dt each step; the step integrates the pose from it). */
+ * d(pose)/dt each step; the step integrates the pose from it).  Ordered on
+ * the state's stream before the next step, without a host synchronisation
+ * (the values travel as kernel arguments). */
 NXM_API int nxm_state_set_collider_velocity(nxm_state* state, uint32_t index, const float linvel[3], const float angvel[3]);
 
 /* Kinematic driving of colliders [first, first + count) at once: 6 floats
@@ -439,6 +441,11 @@ NXM_API int nxm_state_estimate_timestep_bound(nxm_state* state, float* max_dt, u
 NXM_API int nxm_synchronize(nxm_state* state);
 /* Device status bits (NXM_STATUS_*); synchronizes.  `clear` resets them. */
 NXM_API int nxm_state_status(nxm_state* state, uint32_t* bits, int clear);
+/* Pipelined status read for a step loop: enqueues a copy of the status word
+ * after the work issued so far and returns in `*bits` the word the previous
+ * call enqueued (waiting only for that copy, so the stream never drains;
+ * 0 on the first call).  Each step's status reaches the host one call late. */
+NXM_API int nxm_state_status_pipelined(nxm_state* state, uint32_t* bits);
 NXM_API const char* nxm_error_string(int code);
 
 /* The CUDA stream (cudaStream_t) every call on this state is ordered on,

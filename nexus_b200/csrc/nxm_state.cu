@@ -17,6 +17,7 @@
 #include <map>
 #include <new>
 #include <set>
+#include <thread>
 #include <vector>
 
 #include "../../include/nexus_mpm.h"
@@ -260,13 +261,15 @@ __global__ void k_set_velocities(DevCollider* __restrict__ cols, const float* __
     }
 }
 
-// Fresh CPIC records: empty distance field, then the uploaded properties
-// (boundary friction, init radius, phase, group id).
-__global__ void k_init_pcdf(float4* __restrict__ pcdf, const float4* __restrict__ props, uint32_t count) {
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
-        pcdf[3 * (size_t)i] = make_float4(0.f, 0.f, 0.f, 0.f);
-        pcdf[3 * (size_t)i + 1] = make_float4(0.f, 0.f, 0.f, 0.f);
-        pcdf[3 * (size_t)i + 2] = props[i];
+// One collider's velocity, passed by value (no host staging, no stream sync).
+struct Vel6 {
+    float v[6];
+};
+__global__ void k_set_velocity(DevCollider* __restrict__ cols, uint32_t index, Vel6 vel) {
+    if (threadIdx.x == 0) {
+        DevCollider& c = cols[index];
+        c.linvel[0] = vel.v[0]; c.linvel[1] = vel.v[1]; c.linvel[2] = vel.v[2];
+        c.angvel[0] = vel.v[3]; c.angvel[1] = vel.v[4]; c.angvel[2] = vel.v[5];
     }
 }
 
@@ -357,8 +360,18 @@ struct nxm_state {
     std::vector<DevCollider> colliders;
     DevCollider* d_colliders = nullptr;
     uint32_t col_cap = 0;
-    float* d_vel6 = nullptr;  // staging of bulk collider velocities
-    size_t vel_cap = 0;
+    // bulk collider velocities: pinned host slots (a ring, each reused only
+    // after the copy issued from it has run) and their device copies
+    static constexpr int kVelSlots = 4;
+    float* d_vel6 = nullptr;
+    float* h_vel6 = nullptr;
+    cudaEvent_t vel_done[kVelSlots] = {};
+    size_t vel_cap = 0;  // floats per slot
+    int vel_slot = 0;
+    // pipelined status reads: pinned words and their copy events
+    uint32_t* h_status = nullptr;
+    cudaEvent_t status_done[2] = {};
+    uint64_t status_calls = 0;
 
     // batched scenes (scene_blocks != 0): scene slots on the block-key grid
     // (see Params), each a contiguous range of particle ids with its own colliders
@@ -918,6 +931,98 @@ int remove_id_ranges(nxm_state* s, std::vector<uint2> ranges) {
     return invalidate_codes(s);
 }
 
+// Material runs of an upload: consecutive particles with byte-identical models
+// share one material and one initial model state (a new run starts wherever
+// the model differs from the previous particle's).  The comparison runs in
+// parallel over slices of the particles; the lookups, one per run, serially.
+struct MaterialRuns {
+    std::vector<uint32_t> start, mid;
+    std::vector<float4> state;
+};
+
+static int material_runs(nxm_state* s, const nxm_particle_model* models, uint32_t count, MaterialRuns& r) {
+    const unsigned hw = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    const uint32_t nt = count < (1u << 16) ? 1u : hw;
+    std::vector<std::vector<uint32_t>> starts(nt);
+    auto scan = [&](uint32_t t) {
+        const uint32_t lo = (uint32_t)((uint64_t)count * t / nt), hi = (uint32_t)((uint64_t)count * (t + 1) / nt);
+        for (uint32_t i = lo; i < hi; ++i)
+            if (i == 0 || std::memcmp(&models[i], &models[i - 1], sizeof(nxm_particle_model)) != 0)
+                starts[t].push_back(i);
+    };
+    if (nt == 1) {
+        scan(0);
+    } else {
+        std::vector<std::thread> th;
+        for (uint32_t t = 0; t < nt; ++t) th.emplace_back(scan, t);
+        for (auto& x : th) x.join();
+    }
+    for (const auto& v : starts) r.start.insert(r.start.end(), v.begin(), v.end());
+    r.mid.resize(r.start.size());
+    r.state.resize(r.start.size());
+    for (size_t k = 0; k < r.start.size(); ++k) {
+        const nxm_particle_model& m = models[r.start[k]];
+        r.mid[k] = material_of(s, m);
+        float st[4] = {0, 0, 0, 0};
+        for (int w = 0; w < model_state_words(m.tag); ++w) st[w] = bits_f(m.data[w]);
+        r.state[k] = make_float4(st[0], st[1], st[2], st[3]);
+    }
+    return NXM_OK;
+}
+
+// Device-side record packing of an upload: the SoA fields (null = the
+// ParticleDynamics::new default) of particles [base, base + count) of the
+// upload, written as PKin / PDef / model state / CPIC + properties records.
+struct UploadSrc {
+    const float *pos, *vel, *F, *A, *vgd, *v0, *rad, *mass, *damp, *phase, *bf;
+    const uint32_t *gid, *en, *fx;
+    const uint32_t* run_start;
+    const uint32_t* run_mid;
+    const float4* run_state;
+    uint32_t nruns;
+};
+
+__global__ void k_pack_particles(UploadSrc u, uint32_t base, uint32_t count, PKin* __restrict__ kin,
+                                 PDef* __restrict__ def, float4* __restrict__ pstate, float4* __restrict__ pcdf) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+        // the material run holding particle base + i
+        uint32_t lo = 0, hi = u.nruns;
+        while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (u.run_start[mid] <= base + i) lo = mid; else hi = mid;
+        }
+        const float* x = u.pos + 3 * (size_t)i;
+        const float* v = u.vel ? u.vel + 3 * (size_t)i : nullptr;
+        const float* a = u.A ? u.A + 9 * (size_t)i : nullptr;
+        const float* F = u.F ? u.F + 9 * (size_t)i : nullptr;
+        uint32_t flags = 0;
+        if (!u.en || u.en[i]) flags |= PFLAG_ENABLED;
+        if (u.fx && u.fx[i]) flags |= PFLAG_FIXED;
+        float4* k = reinterpret_cast<float4*>(&kin[i]);
+        k[0] = make_float4(x[0], x[1], x[2], u.mass[i]);
+        k[1] = make_float4(v ? v[0] : 0.f, v ? v[1] : 0.f, v ? v[2] : 0.f, __uint_as_float(flags));
+        k[2] = make_float4(a ? a[0] : 0.f, a ? a[1] : 0.f, a ? a[2] : 0.f, u.vgd ? u.vgd[i] : 0.f);
+        k[3] = make_float4(a ? a[3] : 0.f, a ? a[4] : 0.f, a ? a[5] : 0.f, 0.f);
+        k[4] = make_float4(a ? a[6] : 0.f, a ? a[7] : 0.f, a ? a[8] : 0.f, 0.f);
+        float4* d = reinterpret_cast<float4*>(&def[i]);
+        d[0] = make_float4(F ? F[0] : 1.f, F ? F[1] : 0.f, F ? F[2] : 0.f, u.v0[i]);
+        d[1] = make_float4(F ? F[3] : 0.f, F ? F[4] : 1.f, F ? F[5] : 0.f, u.damp ? u.damp[i] : 0.f);
+        d[2] = make_float4(F ? F[6] : 0.f, F ? F[7] : 0.f, F ? F[8] : 1.f, __uint_as_float(u.run_mid[lo]));
+        pstate[i] = u.run_state[lo];
+        // CPIC fields start empty; then the properties: defaults of
+        // ParticleDynamics::new (solver/particle.rs:100-122), the radius, when
+        // not given, from init_volume = (2 r)^3
+        pcdf[3 * (size_t)i] = make_float4(0.f, 0.f, 0.f, 0.f);
+        pcdf[3 * (size_t)i + 1] = make_float4(0.f, 0.f, 0.f, 0.f);
+        pcdf[3 * (size_t)i + 2] = make_float4(u.bf ? u.bf[i] : 1.0f, u.rad ? u.rad[i] : 0.5f * cbrtf(u.v0[i]),
+                                              u.phase ? u.phase[i] : 1.0f, __uint_as_float(u.gid ? u.gid[i] : 0u));
+    }
+}
+
+// Appends `count` particles: the caller's SoA arrays are copied as they are
+// (fast from pinned memory) into a stream-ordered scratch, chunk by chunk, and
+// packed into the particle records on the device; only the material runs are
+// resolved on the host.
 int upload_particles(nxm_state* s, const nxm_particles_soa* p, uint32_t count) {
     if (count == 0) return NXM_OK;
     if (!p || !p->position || !p->model) return NXM_E_INVALID;
@@ -926,69 +1031,84 @@ int upload_particles(nxm_state* s, const nxm_particles_soa* p, uint32_t count) {
     if (need > 0x7FFFFFFFull / 8) return NXM_E_INVALID;
     int rc = reserve_particles(s, (uint32_t)need);
     if (rc) return rc;
-    std::vector<PKin> hk(count);
-    std::vector<PDef> hd(count);
-    std::vector<float4> hs(count), hr(count);
-    static const float I9[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
-    uint32_t last_mid = 0;
-    for (uint32_t i = 0; i < count; ++i) {
-        const float* x = p->position + 3 * (size_t)i;
-        const float* v = p->velocity ? p->velocity + 3 * (size_t)i : nullptr;
-        const float* a = p->affine ? p->affine + 9 * (size_t)i : nullptr;
-        const float* F = p->def_grad ? p->def_grad + 9 * (size_t)i : I9;
-        uint32_t flags = 0;
-        if (!p->enabled || p->enabled[i]) flags |= PFLAG_ENABLED;
-        if (p->fixed && p->fixed[i]) flags |= PFLAG_FIXED;
-        PKin& k = hk[i];
-        k.x = x[0]; k.y = x[1]; k.z = x[2];
-        k.mass = p->mass[i];
-        k.vx = v ? v[0] : 0.f; k.vy = v ? v[1] : 0.f; k.vz = v ? v[2] : 0.f;
-        k.flags = bits_f(flags);
-        k.c00 = a ? a[0] : 0.f; k.c10 = a ? a[1] : 0.f; k.c20 = a ? a[2] : 0.f;
-        k.c01 = a ? a[3] : 0.f; k.c11 = a ? a[4] : 0.f; k.c21 = a ? a[5] : 0.f;
-        k.c02 = a ? a[6] : 0.f; k.c12 = a ? a[7] : 0.f; k.c22 = a ? a[8] : 0.f;
-        k.vgd = p->vel_grad_det ? p->vel_grad_det[i] : 0.f;
-        k.pad1 = 0.f; k.pad2 = 0.f;
-        const nxm_particle_model& m = p->model[i];
-        // consecutive particles mostly share a model: look up only on a change
-        if (i == 0 || std::memcmp(&m, &p->model[i - 1], sizeof(m)) != 0) last_mid = material_of(s, m);
-        const uint32_t mid = last_mid;
-        PDef& d = hd[i];
-        d.f00 = F[0]; d.f10 = F[1]; d.f20 = F[2];
-        d.f01 = F[3]; d.f11 = F[4]; d.f21 = F[5];
-        d.f02 = F[6]; d.f12 = F[7]; d.f22 = F[8];
-        d.init_volume = p->init_volume[i];
-        d.damping = p->damping ? p->damping[i] : 0.f;
-        d.material = bits_f(mid);
-        const int ns = model_state_words(m.tag);
-        float st[4] = {0, 0, 0, 0};
-        for (int w = 0; w < ns; ++w) st[w] = bits_f(m.data[w]);
-        hs[i] = make_float4(st[0], st[1], st[2], st[3]);
-        // defaults of ParticleDynamics::new (solver/particle.rs:100-122); the
-        // radius, when not given, from init_volume = (2 r)^3
-        hr[i] = make_float4(p->boundary_friction ? p->boundary_friction[i] : 1.0f,
-                            p->init_radius ? p->init_radius[i] : 0.5f * std::cbrt(p->init_volume[i]),
-                            p->phase ? p->phase[i] : 1.0f, bits_f(p->group_id ? p->group_id[i] : 0u));
-    }
-    if (s->chunks_used) s->slot2chunk.insert(s->slot2chunk.end(), count, NONE);
+    MaterialRuns runs;
+    rc = material_runs(s, p->model, count, runs);
+    if (rc) return rc;
     rc = sync_materials(s);
     if (rc) return rc;
-    NXM_TRY(cudaMemcpyAsync(s->kin + s->n, hk.data(), sizeof(PKin) * count, cudaMemcpyHostToDevice, s->stream));
-    NXM_TRY(cudaMemcpyAsync(s->def + s->n, hd.data(), sizeof(PDef) * count, cudaMemcpyHostToDevice, s->stream));
-    NXM_TRY(cudaMemcpyAsync(s->pstate + s->n, hs.data(), sizeof(float4) * count, cudaMemcpyHostToDevice, s->stream));
-    {  // CPIC fields start empty; the properties record follows them
-        if (4 * (size_t)count > s->pack_cap) {
-            NXM_TRY(cudaStreamSynchronize(s->stream));
-            dfree(s->d_pack);
-            NXM_TRY(dalloc(&s->d_pack, 4 * (size_t)count));
-            s->pack_cap = 4 * (size_t)count;
+    if (s->chunks_used) s->slot2chunk.insert(s->slot2chunk.end(), count, NONE);
+
+    // scratch: the run table, then per chunk the fields that are given
+    const uint32_t nruns = (uint32_t)runs.start.size();
+    const uint32_t chunk = std::min<uint32_t>(count, 1u << 20);
+    struct Field {
+        const void* src;
+        size_t elem;  // bytes per particle
+    };
+    const Field fields[14] = {{p->position, 12}, {p->velocity, 12}, {p->def_grad, 36},   {p->affine, 36},
+                              {p->vel_grad_det, 4}, {p->init_volume, 4}, {p->init_radius, 4}, {p->mass, 4},
+                              {p->damping, 4},  {p->phase, 4},     {p->boundary_friction, 4}, {p->group_id, 4},
+                              {p->enabled, 4},  {p->fixed, 4}};
+    size_t per_particle = 0;
+    for (const Field& f : fields)
+        if (f.src) per_particle += f.elem;
+    const size_t run_bytes = ((size_t)nruns * 8 + 15) / 16 * 16 + (size_t)nruns * 16;
+    char* scratch = nullptr;
+    NXM_TRY(cudaMallocAsync(reinterpret_cast<void**>(&scratch), run_bytes + per_particle * chunk, s->stream));
+    UploadSrc u{};
+    u.nruns = nruns;
+    {
+        uint32_t* rs = reinterpret_cast<uint32_t*>(scratch);
+        uint32_t* rm = rs + nruns;
+        float4* rst = reinterpret_cast<float4*>(scratch + ((size_t)nruns * 8 + 15) / 16 * 16);
+        cudaError_t e = cudaMemcpyAsync(rs, runs.start.data(), 4 * (size_t)nruns, cudaMemcpyHostToDevice, s->stream);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(rm, runs.mid.data(), 4 * (size_t)nruns, cudaMemcpyHostToDevice, s->stream);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(rst, runs.state.data(), 16 * (size_t)nruns, cudaMemcpyHostToDevice, s->stream);
+        if (e != cudaSuccess) {
+            cudaFreeAsync(scratch, s->stream);
+            return NXM_E_CUDA;
         }
-        NXM_TRY(cudaMemcpyAsync(s->d_pack, hr.data(), sizeof(float4) * count, cudaMemcpyHostToDevice, s->stream));
-        k_init_pcdf<<<grid_for_n(s, count), 256, 0, s->stream>>>(s->d_pcdf + 3 * (size_t)s->n,
-                                                                  reinterpret_cast<const float4*>(s->d_pack), count);
-        s->launches += 1;
-        NXM_TRY(cudaGetLastError());
+        u.run_start = rs;
+        u.run_mid = rm;
+        u.run_state = rst;
     }
+    cudaError_t err = cudaSuccess;
+    for (uint32_t c0 = 0; c0 < count && err == cudaSuccess; c0 += chunk) {
+        const uint32_t cn = std::min(chunk, count - c0);
+        const void* dst[14] = {};
+        char* at = scratch + run_bytes;
+        for (int f = 0; f < 14 && err == cudaSuccess; ++f) {
+            if (!fields[f].src) continue;
+            dst[f] = at;
+            err = cudaMemcpyAsync(at, static_cast<const char*>(fields[f].src) + fields[f].elem * c0, fields[f].elem * cn,
+                                  cudaMemcpyHostToDevice, s->stream);
+            at += fields[f].elem * chunk;
+        }
+        if (err != cudaSuccess) break;
+        u.pos = static_cast<const float*>(dst[0]);
+        u.vel = static_cast<const float*>(dst[1]);
+        u.F = static_cast<const float*>(dst[2]);
+        u.A = static_cast<const float*>(dst[3]);
+        u.vgd = static_cast<const float*>(dst[4]);
+        u.v0 = static_cast<const float*>(dst[5]);
+        u.rad = static_cast<const float*>(dst[6]);
+        u.mass = static_cast<const float*>(dst[7]);
+        u.damp = static_cast<const float*>(dst[8]);
+        u.phase = static_cast<const float*>(dst[9]);
+        u.bf = static_cast<const float*>(dst[10]);
+        u.gid = static_cast<const uint32_t*>(dst[11]);
+        u.en = static_cast<const uint32_t*>(dst[12]);
+        u.fx = static_cast<const uint32_t*>(dst[13]);
+        const size_t at0 = (size_t)s->n + c0;
+        k_pack_particles<<<grid_for_n(s, cn), 256, 0, s->stream>>>(u, c0, cn, s->kin + at0, s->def + at0,
+                                                                   s->pstate + at0, s->d_pcdf + 3 * at0);
+        s->launches += 1;
+        err = cudaGetLastError();
+    }
+    cudaFreeAsync(scratch, s->stream);
+    if (err != cudaSuccess) return NXM_E_CUDA;
     if (s->permuted) {  // appended particles sit at slots == their ids
         k_iota<<<grid_for_n(s, count), 256, 0, s->stream>>>(s->pid + s->n, s->n, count);
         s->launches += 1;
@@ -1442,6 +1562,12 @@ void nxm_state_destroy(nxm_state* s) {
     dfree(s->d_pack); dfree(s->d_offsets);
     dfree(s->d_rp_local); dfree(s->d_rp_world); dfree(s->d_rp_need); dfree(s->d_rp_sorted);
     dfree(s->d_render); dfree(s->d_palette);
+    if (s->h_vel6) cudaFreeHost(s->h_vel6);
+    if (s->h_status) cudaFreeHost(s->h_status);
+    for (cudaEvent_t e : s->vel_done)
+        if (e) cudaEventDestroy(e);
+    for (cudaEvent_t e : s->status_done)
+        if (e) cudaEventDestroy(e);
     if (s->h_counters) cudaFreeHost(s->h_counters);
     if (s->stream) cudaStreamDestroy(s->stream);
     delete s;
@@ -1491,10 +1617,11 @@ int nxm_state_set_colliders(nxm_state* s, const nxm_collider* cols, uint32_t nco
 
 int nxm_state_set_collider_velocity(nxm_state* s, uint32_t index, const float linvel[3], const float angvel[3]) {
     if (!s || !linvel || !angvel || index >= s->colliders.size()) return NXM_E_INVALID;
-    float buf[8] = {linvel[0], linvel[1], linvel[2], 0.f, angvel[0], angvel[1], angvel[2], 0.f};
-    char* base = reinterpret_cast<char*>(s->d_colliders + index);
-    NXM_TRY(cudaMemcpyAsync(base + offsetof(DevCollider, linvel), buf, 32, cudaMemcpyHostToDevice, s->stream));
-    NXM_TRY(cudaStreamSynchronize(s->stream));
+    // the values travel as a kernel argument: ordered on the stream, no host wait
+    const Vel6 v{{linvel[0], linvel[1], linvel[2], angvel[0], angvel[1], angvel[2]}};
+    k_set_velocity<<<1, 32, 0, s->stream>>>(s->d_colliders, index, v);
+    s->launches += 1;
+    NXM_TRY(cudaGetLastError());
     return NXM_OK;
 }
 
@@ -1504,14 +1631,28 @@ int nxm_state_set_collider_velocities(nxm_state* s, uint32_t first, uint32_t cou
     if (count == 0) return NXM_OK;
     const size_t need = 6 * (size_t)count;
     if (need > s->vel_cap) {
-        NXM_TRY(cudaStreamSynchronize(s->stream));  // the old staging buffer may still be read
+        NXM_TRY(cudaStreamSynchronize(s->stream));  // the old slots may still be read
         dfree(s->d_vel6);
-        NXM_TRY(dalloc(&s->d_vel6, need));
+        if (s->h_vel6) cudaFreeHost(s->h_vel6);
+        s->h_vel6 = nullptr;
+        s->vel_cap = 0;
+        NXM_TRY(dalloc(&s->d_vel6, need * nxm_state::kVelSlots));
+        NXM_TRY(cudaMallocHost(reinterpret_cast<void**>(&s->h_vel6), 4 * need * nxm_state::kVelSlots));
+        for (cudaEvent_t& e : s->vel_done)
+            if (!e) NXM_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
         s->vel_cap = need;
     }
-    // pageable source: the copy has taken the data when the call returns
-    NXM_TRY(cudaMemcpyAsync(s->d_vel6, vel6, 4 * need, cudaMemcpyHostToDevice, s->stream));
-    k_set_velocities<<<(count + 127) / 128, 128, 0, s->stream>>>(s->d_colliders, s->d_vel6, first, count);
+    // copy into a pinned slot (its previous copy, kVelSlots calls ago, has run),
+    // then a truly asynchronous transfer: the caller's array is free on return
+    const int slot = s->vel_slot;
+    s->vel_slot = (slot + 1) % nxm_state::kVelSlots;
+    NXM_TRY(cudaEventSynchronize(s->vel_done[slot]));
+    float* h = s->h_vel6 + s->vel_cap * slot;
+    float* d = s->d_vel6 + s->vel_cap * slot;
+    std::memcpy(h, vel6, 4 * need);
+    NXM_TRY(cudaMemcpyAsync(d, h, 4 * need, cudaMemcpyHostToDevice, s->stream));
+    NXM_TRY(cudaEventRecord(s->vel_done[slot], s->stream));
+    k_set_velocities<<<(count + 127) / 128, 128, 0, s->stream>>>(s->d_colliders, d, first, count);
     s->launches += 1;
     NXM_TRY(cudaGetLastError());
     return NXM_OK;
@@ -2095,6 +2236,26 @@ int nxm_synchronize(nxm_state* s) {
     if (rc) return rc;
     if (bits & NXM_STATUS_HASH_FULL) return NXM_E_HASH_FULL;
     if (bits & (NXM_STATUS_BLOCK_CAPACITY | NXM_STATUS_MISSING_BLOCK | NXM_STATUS_SORT_CAPACITY)) return NXM_E_CAPACITY;
+    return NXM_OK;
+}
+
+int nxm_state_status_pipelined(nxm_state* s, uint32_t* bits) {
+    if (!s || !bits) return NXM_E_INVALID;
+    if (!s->h_status) {
+        NXM_TRY(cudaMallocHost(reinterpret_cast<void**>(&s->h_status), 2 * sizeof(uint32_t)));
+        s->h_status[0] = s->h_status[1] = 0;
+        for (cudaEvent_t& e : s->status_done) NXM_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    }
+    const int cur = (int)(s->status_calls & 1u), prev = cur ^ 1;
+    NXM_TRY(cudaMemcpyAsync(&s->h_status[cur], reinterpret_cast<const char*>(s->d_counters) + offsetof(Counters, status),
+                            sizeof(uint32_t), cudaMemcpyDeviceToHost, s->stream));
+    NXM_TRY(cudaEventRecord(s->status_done[cur], s->stream));
+    *bits = 0;
+    if (s->status_calls > 0) {
+        NXM_TRY(cudaEventSynchronize(s->status_done[prev]));
+        *bits = s->h_status[prev];
+    }
+    ++s->status_calls;
     return NXM_OK;
 }
 

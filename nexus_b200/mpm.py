@@ -96,6 +96,7 @@ SIGNATURES = {
     "nxm_debug_sort": (C.c_int, [_vp, _vp, C.c_int]),
     "nxm_state_estimate_timestep_bound": (C.c_int, [_vp, _f, _u]),
     "nxm_read_cdf": (C.c_int, [_vp, _f]),
+    "nxm_state_status_pipelined": (C.c_int, [_vp, _u]),
     "nxm_state_num_rigid_particles": (C.c_int, [_vp, _u]),
     "nxm_read_rigid_particles": (C.c_int, [_vp, _f]),
     "nxm_prep_readback": (C.c_int, [_vp, C.c_uint32, _f, C.c_uint32, _f]),
@@ -498,6 +499,13 @@ class MpmState:
     def status(self, clear: bool = False) -> int:
         v = C.c_uint32()
         _check(self.lib.nxm_state_status(self.h, C.byref(v), int(clear)), "state_status")
+        return v.value
+
+    def status_pipelined(self) -> int:
+        """Status word of the previous call's point in the stream, without
+        draining the stream (the read for this point is enqueued)."""
+        v = C.c_uint32()
+        _check(self.lib.nxm_state_status_pipelined(self.h, C.byref(v)), "state_status_pipelined")
         return v.value
 
     def kernel_launches(self) -> int:
