@@ -480,15 +480,19 @@ def measure_e2e(scene, args, torch):
     st.set_cell_width(scene.dx, scene.grid_capacity)
     st.set_simulation_params(scene.gravity, scene.dt)
     st.set_colliders(scene.colliders)
+    t1 = time.perf_counter()
     st.append(batch)
+    t2 = time.perf_counter()
     for _ in range(steps):
         st.set_collider_velocity(0, zeros, zeros)
         pipe.step(st)
         st.status_pipelined()  # the previous step's status word; this step's is in flight
     st.status_pipelined()  # the last step's
+    t3 = time.perf_counter()
     st.read_positions_into(out)
     st.synchronize()
-    dt = time.perf_counter() - t0
+    t4 = time.perf_counter()
+    dt = t4 - t0
     # the SoA arrays copied to the device (the per-particle models stay on the
     # host: only their material runs travel)
     upload = sum(a.nbytes for k, a in batch.__dict__.items() if k != "model")
@@ -497,7 +501,9 @@ def measure_e2e(scene, args, torch):
             "h2d_bytes_per_step": int(upload / steps + 24), "d2h_bytes_per_step": int(p.n * 12 / steps + 4),
             "how": "host wall clock: state create + SoA upload from pinned memory (packed into records on the "
                    "device) + per step (collider velocity write, step, pipelined status D2H read one step late) + "
-                   "final positions D2H"}
+                   "final positions D2H",
+            "phases_ms": {"create": (t1 - t0) * 1e3, "upload": (t2 - t1) * 1e3, "steps": (t3 - t2) * 1e3,
+                          "readback": (t4 - t3) * 1e3}}
 
 
 def main():
