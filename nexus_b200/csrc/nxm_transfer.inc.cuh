@@ -184,6 +184,9 @@ __device__ __forceinline__ void g2p_particle(const DevPtrs& P, const Params& prm
     uint32_t flags = __float_as_uint(vf.w);
     const v3 pt = mk(xm.x, xm.y, xm.z);
     float mass = xm.w;
+    // the deformation record, loaded ahead of the gather
+    const float4* dr = reinterpret_cast<const float4*>(&P.def[src]);
+    const float4 d0 = dr[0], d1 = dr[1], d2 = dr[2];
 
 #if NXM_CPIC
     // particle Cdf (normal, signed distance, affinity) from this step's g2p_cdf pass
@@ -302,8 +305,6 @@ __device__ __forceinline__ void g2p_particle(const DevPtrs& P, const Params& prm
 #endif
 
     // ---- particle update (particle_update.rs:60-201, non-CPIC: Cdf = 0)
-    const float4* dr = reinterpret_cast<const float4*>(&P.def[src]);
-    const float4 d0 = dr[0], d1 = dr[1], d2 = dr[2];
     m3 F = mkm(mk(d0.x, d0.y, d0.z), mk(d1.x, d1.y, d1.z), mk(d2.x, d2.y, d2.z));
     const float init_volume = d0.w, damping = d1.w;
     const uint32_t mid = __float_as_uint(d2.w);
