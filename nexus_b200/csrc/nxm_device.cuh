@@ -267,6 +267,85 @@ __device__ __forceinline__ Svd svd3(const m3& f) {
     return out;
 }
 
+// Fast-build SVD: the same Jacobi sweeps with the orthogonality test on
+// squares (no square roots), the rotation's division by an approximate
+// reciprocal (__fdividef), and the singular values and U columns from one
+// reciprocal square root per column.  Agrees with svd3 to a few ulp.
+__device__ __forceinline__ bool jacobi_pair_fast(float (&a)[3][3], float (&v)[3][3], int p, int q) {
+    const float alpha = a[0][p] * a[0][p] + a[1][p] * a[1][p] + a[2][p] * a[2][p];
+    const float beta = a[0][q] * a[0][q] + a[1][q] * a[1][q] + a[2][q] * a[2][q];
+    const float gamma = a[0][p] * a[0][q] + a[1][p] * a[1][q] + a[2][p] * a[2][q];
+    if (gamma * gamma <= 1.0e-12f * alpha * beta || fabsf(gamma) <= 1.0e-30f) return false;
+    const float zeta = __fdividef(beta - alpha, 2.0f * gamma);
+    const float t = __fdividef(copysignf(1.0f, zeta), fabsf(zeta) + sqrtf(1.0f + zeta * zeta));
+    const float c = rsqrtf(1.0f + t * t);
+    const float s = c * t;
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+        const float ap = a[r][p], aq = a[r][q];
+        a[r][p] = c * ap - s * aq;
+        a[r][q] = s * ap + c * aq;
+        const float vp = v[r][p], vq = v[r][q];
+        v[r][p] = c * vp - s * vq;
+        v[r][q] = s * vp + c * vq;
+    }
+    return true;
+}
+
+__device__ __forceinline__ Svd svd3_fast(const m3& f) {
+    float a[3][3] = {{f.c0.x, f.c1.x, f.c2.x}, {f.c0.y, f.c1.y, f.c2.y}, {f.c0.z, f.c1.z, f.c2.z}};
+    float v[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
+#pragma unroll 1
+    for (int sweep = 0; sweep < 10; ++sweep) {
+        bool rot = jacobi_pair_fast(a, v, 0, 1);
+        rot |= jacobi_pair_fast(a, v, 0, 2);
+        rot |= jacobi_pair_fast(a, v, 1, 2);
+        if (!rot) break;
+    }
+    float sig[3], inv[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        const float n2 = a[0][c] * a[0][c] + a[1][c] * a[1][c] + a[2][c] * a[2][c];
+        inv[c] = n2 > 1.0e-36f ? rsqrtf(n2) : 0.0f;
+        sig[c] = n2 * inv[c];
+    }
+    auto swapc = [&](int i, int j) {
+        float t = sig[i]; sig[i] = sig[j]; sig[j] = t;
+        t = inv[i]; inv[i] = inv[j]; inv[j] = t;
+#pragma unroll
+        for (int r = 0; r < 3; ++r) {
+            float ta = a[r][i]; a[r][i] = a[r][j]; a[r][j] = ta;
+            float tv = v[r][i]; v[r][i] = v[r][j]; v[r][j] = tv;
+        }
+    };
+    if (sig[1] > sig[0]) swapc(0, 1);
+    if (sig[2] > sig[0]) swapc(0, 2);
+    if (sig[2] > sig[1]) swapc(1, 2);
+    float u[3][3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+        for (int r = 0; r < 3; ++r) u[r][c] = a[r][c] * inv[c];
+    if (!(sig[1] > 1.0e-18f)) {
+        float ux = u[0][0], uy = u[1][0], uz = u[2][0];
+        float ox, oy, oz;
+        if (fabsf(ux) < 0.9f) { ox = 0; oy = -uz; oz = uy; } else { ox = uz; oy = 0; oz = -ux; }
+        float on = sqrtf(ox * ox + oy * oy + oz * oz);
+        if (on == 0.0f) { ox = 1; oy = 0; oz = 0; on = 1; }
+        u[0][1] = ox / on; u[1][1] = oy / on; u[2][1] = oz / on;
+    }
+    if (!(sig[2] > 1.0e-18f)) {
+        u[0][2] = u[1][0] * u[2][1] - u[2][0] * u[1][1];
+        u[1][2] = u[2][0] * u[0][1] - u[0][0] * u[2][1];
+        u[2][2] = u[0][0] * u[1][1] - u[1][0] * u[0][1];
+    }
+    Svd out;
+    out.u = mkm(mk(u[0][0], u[1][0], u[2][0]), mk(u[0][1], u[1][1], u[2][1]), mk(u[0][2], u[1][2], u[2][2]));
+    out.s = mk(sig[0], sig[1], sig[2]);
+    out.vt = mkm(mk(v[0][0], v[0][1], v[0][2]), mk(v[1][0], v[1][1], v[1][2]), mk(v[2][0], v[2][1], v[2][2]));
+    return out;
+}
+
 // ---------------------------------------------------------------------------
 // Constitutive models (src_mpm_shaders/models/*.rs).
 // ---------------------------------------------------------------------------
@@ -365,6 +444,63 @@ __device__ __forceinline__ m3 dp_project_svd(const float* pl, float* state, cons
     d.s = sv;
     return (d.u * diag(sv)) * d.vt;
 }
+// Fast-build Drucker-Prager projection: dp_project_svd's return map with the
+// hardware approximations of log, exp and sin (__logf, __expf, __sinf), and
+// the determinants' logarithms taken from the strains (log det = sum of the
+// log singular values), so no further logarithm is needed.
+__device__ __forceinline__ m3 dp_project_fast(const float* pl, float* state, const m3& F, Svd& d) {
+    d = svd3_fast(F);
+    if (pl[4] == 0.0f) return F;
+    const float q = state[1];
+    const float angle = pl[0] + (pl[1] * q - pl[3]) * __expf(-pl[2] * q);
+    const float s_angle = __sinf(angle);
+    const float alpha = sqrtf(2.0f / 3.0f) * __fdividef(2.0f * s_angle, 3.0f - s_angle);
+    const float dd = 3.0f;
+    const v3 ls = mk(__logf(d.s.x), __logf(d.s.y), __logf(d.s.z));
+    const v3 strain = ls + splat(state[2] / dd);
+    const float tr = strain.x + strain.y + strain.z;
+    const v3 dev = strain - splat(tr / dd);
+    const float shifted = tr - pl[6];
+    v3 sv;
+    float hard, log_new;
+    if (shifted > 0.0f || (dev.x == 0.0f && dev.y == 0.0f && dev.z == 0.0f)) {
+        sv = splat(__expf(pl[6] / dd));
+        hard = length(strain);
+        log_new = pl[6];
+    } else {
+        const float dnorm = length(dev);
+        const float gamma = dnorm + (dd * pl[4] + 2.0f * pl[5]) / (2.0f * pl[5]) * shifted * alpha;
+        if (gamma <= 0.0f) return F;  // invalid projection: state and F unchanged
+        const v3 h = strain - dev * __fdividef(gamma, dnorm);
+        sv = mk(__expf(h.x), __expf(h.y), __expf(h.z));
+        hard = gamma;
+        log_new = h.x + h.y + h.z;
+    }
+    const float log_prev = ls.x + ls.y + ls.z;
+    state[0] = state[0] * __expf(log_prev - log_new);
+    state[1] = state[1] + hard;
+    state[2] = state[2] + log_prev - log_new;
+    d.s = sv;
+    return (d.u * diag(sv)) * d.vt;
+}
+
+// Fast-build corotated linear stress from the SVD of F: with F = U S V^T,
+// U (S - I) V^T F^T = U diag((s - 1) s) U^T, a symmetric product.
+__device__ __forceinline__ m3 linear_stress_fast(float lambda, float mu, const Svd& d) {
+    const float j = d.s.x * d.s.y * d.s.z;
+    const v3 e = mk((d.s.x - 1.0f) * d.s.x, (d.s.y - 1.0f) * d.s.y, (d.s.z - 1.0f) * d.s.z) * (2.0f * mu);
+    const m3& U = d.u;
+    const v3 u0e = U.c0 * e.x, u1e = U.c1 * e.y, u2e = U.c2 * e.z;
+    const float xx = u0e.x * U.c0.x + u1e.x * U.c1.x + u2e.x * U.c2.x;
+    const float yy = u0e.y * U.c0.y + u1e.y * U.c1.y + u2e.y * U.c2.y;
+    const float zz = u0e.z * U.c0.z + u1e.z * U.c1.z + u2e.z * U.c2.z;
+    const float xy = u0e.x * U.c0.y + u1e.x * U.c1.y + u2e.x * U.c2.y;
+    const float xz = u0e.x * U.c0.z + u1e.x * U.c1.z + u2e.x * U.c2.z;
+    const float yz = u0e.y * U.c0.z + u1e.y * U.c1.z + u2e.y * U.c2.z;
+    const float diag_val = lambda * (j - 1.0f) * j;
+    return mkm(mk(xx + diag_val, xy, xz), mk(xy, yy + diag_val, yz), mk(xz, yz, zz + diag_val));
+}
+
 __device__ __forceinline__ m3 dp_project(const float* pl, float* state, const m3& F) {
     Svd d;
     return dp_project_svd(pl, state, F, d);
@@ -390,28 +526,35 @@ __device__ __forceinline__ m3 snow_project(const float* pl, float* state, const 
 
 // models/default.rs:208-264.  `w` holds the material's 24 model words; the
 // per-particle state words (Drucker-Prager words 0..2, snow word 0) are in `st`
-// and updated in place.  With kReuseSvd, Drucker-Prager sand on a linear
-// backbone computes the stress from the projection's SVD instead of taking
-// the SVD of the projected F a second time (the reference recomputes it; the
-// two agree to rounding).
+// and updated in place.  kReuseSvd selects the fast build's forms, which
+// agree with the reference's to rounding: Drucker-Prager sand on a linear
+// backbone takes its stress from the projection's SVD instead of a second SVD
+// of the projected F, with the fast SVD, projection and stress above; the
+// deterministic build keeps the reference's operation order.
 template <bool kReuseSvd>
 __device__ __forceinline__ m3 model_update(uint32_t tag, const float* w, float* st, m3& F, const m3& vel_grad) {
     switch (tag) {
     case MODEL_ELASTIC_LINEAR:
+        if (kReuseSvd) return linear_stress_fast(w[0], w[1], svd3_fast(F));
         return linear_stress(w[0], w[1], F);
     case MODEL_ELASTIC_NEO_HOOKEAN:
         return neo_hookean_stress(w[0], w[1], F);
     case MODEL_SAND_LINEAR:
         if (kReuseSvd) {
             Svd d;
-            F = dp_project_svd(&w[3], st, F, d);
-            return linear_stress_svd(w[10], w[11], F, d);
+            F = dp_project_fast(&w[3], st, F, d);
+            return linear_stress_fast(w[10], w[11], d);
         } else {
             F = dp_project(&w[3], st, F);
             return linear_stress(w[10], w[11], F);
         }
     case MODEL_SAND_NEO_HOOKEAN:
-        F = dp_project(&w[3], st, F);
+        if (kReuseSvd) {
+            Svd d;
+            F = dp_project_fast(&w[3], st, F, d);
+        } else {
+            F = dp_project(&w[3], st, F);
+        }
         return neo_hookean_stress(w[10], w[11], F);
     case MODEL_FLUID: {
         m3 sr = (vel_grad + transpose(vel_grad)) * 0.5f;
