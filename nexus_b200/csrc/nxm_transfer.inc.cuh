@@ -50,8 +50,19 @@ __device__ __forceinline__ Collision collide(const DevPtrs& P, const DevCollider
         const DevCollider& c = cols[i];
         quat q = quat{c.rot[0], c.rot[1], c.rot[2], c.rot[3]};
         v3 tra = mk(c.tra[0], c.tra[1], c.tra[2]);
+        // fast build: an unrotated collider (the usual box walls) skips the
+        // two rotations (the deterministic build keeps them: they turn -0 into +0)
+        const bool ident = NXM_FAST && q.x == 0.f && q.y == 0.f && q.z == 0.f && q.w == 1.f;
         Proj pr;
-        if (c.type == SHAPE_TRIMESH) {
+        if (ident && c.type != SHAPE_TRIMESH) {
+            const v3 local = point - tra;
+            if (c.type == SHAPE_BALL) pr = ball_project_local(c.a[0], local);
+            else if (c.type == SHAPE_CUBOID) pr = cuboid_project_local(mk(c.a[0], c.a[1], c.a[2]), local);
+            else if (c.type == SHAPE_CAPSULE)
+                pr = capsule_project_local(mk(c.a[0], c.a[1], c.a[2]), mk(c.b[0], c.b[1], c.b[2]), c.b[3], local);
+            else { pr.point = local; pr.inside = false; }
+            pr.point = pr.point + tra;
+        } else if (c.type == SHAPE_TRIMESH) {
             // pose.inverse() * point, as the inverse isometry applies it
             const quat ci = qconj(q);
             const v3 local = qrot(ci, point) + (-qrot(ci, tra));
@@ -64,7 +75,7 @@ __device__ __forceinline__ Collision collide(const DevPtrs& P, const DevCollider
                 pr = capsule_project_local(mk(c.a[0], c.a[1], c.a[2]), mk(c.b[0], c.b[1], c.b[2]), c.b[3], local);
             else { pr.point = local; pr.inside = false; }
         }
-        pr.point = qrot(q, pr.point) + tra;
+        if (!(ident && c.type != SHAPE_TRIMESH)) pr.point = qrot(q, pr.point) + tra;
         v3 dpt = pr.point - point;
         v3 ad = vabs(dpt);
         bool within = ad.x <= cap && ad.y <= cap && ad.z <= cap;
@@ -318,7 +329,8 @@ __device__ __forceinline__ void g2p_particle(const DevPtrs& P, const Params& prm
 #endif
     const float vl = length(v);
     if (vl > dx / dt) v = ((v / vl) * dx) / dt;
-    v = v / (1.0f + damping * dt);
+    if (NXM_FAST) v = v * (1.0f / (1.0f + damping * dt));  // one division instead of three
+    else v = v / (1.0f + damping * dt);
     if (flags & PFLAG_FIXED) v = splat(0.f);
     const v3 np_ = pt + v * dt;
 #if NXM_CPIC
