@@ -448,9 +448,11 @@ __device__ __forceinline__ m3 dp_project_svd(const float* pl, float* state, cons
 // hardware approximations of log, exp and sin (__logf, __expf, __sinf), and
 // the determinants' logarithms taken from the strains (log det = sum of the
 // log singular values), so no further logarithm is needed.
+// The paths that leave F unchanged return it as U S V^T (equal to rounding),
+// so F itself need not stay live across the SVD.
 __device__ __forceinline__ m3 dp_project_fast(const float* pl, float* state, const m3& F, Svd& d) {
     d = svd3_fast(F);
-    if (pl[4] == 0.0f) return F;
+    if (pl[4] == 0.0f) return (d.u * diag(d.s)) * d.vt;
     const float q = state[1];
     const float angle = pl[0] + (pl[1] * q - pl[3]) * __expf(-pl[2] * q);
     const float s_angle = __sinf(angle);
@@ -470,7 +472,7 @@ __device__ __forceinline__ m3 dp_project_fast(const float* pl, float* state, con
     } else {
         const float dnorm = length(dev);
         const float gamma = dnorm + (dd * pl[4] + 2.0f * pl[5]) / (2.0f * pl[5]) * shifted * alpha;
-        if (gamma <= 0.0f) return F;  // invalid projection: state and F unchanged
+        if (gamma <= 0.0f) return (d.u * diag(d.s)) * d.vt;  // invalid projection: state and F unchanged
         const v3 h = strain - dev * __fdividef(gamma, dnorm);
         sv = mk(__expf(h.x), __expf(h.y), __expf(h.z));
         hard = gamma;
