@@ -188,7 +188,7 @@ __device__ __forceinline__ float4 halo_node(const DevPtrs& P, uint32_t b, uint32
 // `dst` of the output records, together with the block key of its new position.
 __device__ __forceinline__ void g2p_particle(const DevPtrs& P, const Params& prm, const float4* __restrict__ halo,
                                              uint32_t src, uint32_t dst, float4 xm, float4 vf, int3 key_off,
-                                             const CpicCtx& cx) {
+                                             const CpicCtx& cx, volatile float* stash) {
     const float dx = prm.dx, dt = prm.dt;
     const float inv_d = 4.0f / (dx * dx);
     float4* kr = reinterpret_cast<float4*>(&P.kin_out[dst]);
@@ -365,15 +365,34 @@ __device__ __forceinline__ void g2p_particle(const DevPtrs& P, const Params& prm
         float4 s4 = P.pstate[src];
         st[0] = s4.x; st[1] = s4.y; st[2] = s4.z; st[3] = s4.w;
     }
-    const m3 tau = model_update<NXM_FAST>(tag, mat.w, st, F, A);
-    m3 aff = A * mass - tau * (init_volume * inv_d * dt);
+    m3 aff;
+    if (stash && tag != MODEL_FLUID) {
+        // m A waits in this thread's shared-memory slots (stride 256) across
+        // the model update instead of in registers
+        const m3 am = A * mass;
+        const float* e = &am.c0.x;
+#pragma unroll
+        for (int i = 0; i < 9; ++i) stash[256 * i] = e[i];
+        const m3 tau = model_update<NXM_FAST>(tag, mat.w, st, F, mzero());
+        float r[9];
+#pragma unroll
+        for (int i = 0; i < 9; ++i) r[i] = stash[256 * i];
+        aff = mkm(mk(r[0], r[1], r[2]), mk(r[3], r[4], r[5]), mk(r[6], r[7], r[8])) -
+              tau * (init_volume * inv_d * dt);
+    } else {
+        const m3 tau = model_update<NXM_FAST>(tag, mat.w, st, F, A);
+        aff = A * mass - tau * (init_volume * inv_d * dt);
+    }
     if (nan || !(det(F) > 0.0f)) {  // disabled: rewrite what was written ahead
         flags &= ~PFLAG_ENABLED;
         F = mident();
         aff = mzero();
-        kr[0] = make_float4(pt.x, pt.y, pt.z, 0.f);
+        // the fast build always writes to the other buffer: the old position
+        // is re-read there instead of staying live across the model update
+        const v3 op = NXM_FAST ? mk(P.kin[src].x, P.kin[src].y, P.kin[src].z) : pt;
+        kr[0] = make_float4(op.x, op.y, op.z, 0.f);
         kr[1] = make_float4(0.f, 0.f, 0.f, __uint_as_float(flags));
-        const CellInfo oc = cell_info(dx, pt);
+        const CellInfo oc = cell_info(dx, op);
         P.pcode[dst] = make_uint2(pack_key(oc.bx + key_off.x, oc.by + key_off.y, oc.bz + key_off.z),
                                   oc.ax | (oc.ay << 2) | (oc.az << 4));
     }
@@ -401,8 +420,17 @@ __device__ __forceinline__ void g2p_particle(const DevPtrs& P, const Params& prm
 // j = first + k goes to output slot j; particles the sort could not place
 // (their block was not created: capacity or hash overflow, reported in the
 // status word) are copied unchanged to the slots after the sorted ones.
+#ifndef NXM_G2P_STASH
+#define NXM_G2P_STASH 1  // m A waits in shared memory across the model update (fast build)
+#endif
 __global__ void __launch_bounds__(256, NXM_G2P_MIN_CTAS) k_g2p_update(DevPtrs P) {
     __shared__ float4 halo[216];
+#if NXM_G2P_STASH
+    __shared__ float stash_mem[9 * 256];
+    volatile float* stash = NXM_FAST ? stash_mem + threadIdx.x : nullptr;
+#else
+    volatile float* stash = nullptr;
+#endif
 #if NXM_CPIC
     __shared__ float4 halo_inc[216];
     __shared__ uint2 halo_cdf[216];
@@ -477,7 +505,7 @@ __global__ void __launch_bounds__(256, NXM_G2P_MIN_CTAS) k_g2p_update(DevPtrs P)
                 xm = kr[0];
                 vf = kr[1];
             }
-            g2p_particle(P, prm, halo, pid, reorder ? first + k : pid, xm, vf, key_off, cx);
+            g2p_particle(P, prm, halo, pid, reorder ? first + k : pid, xm, vf, key_off, cx, stash);
         }
         __syncthreads();
         b = bn;
