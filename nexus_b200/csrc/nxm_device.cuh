@@ -140,6 +140,20 @@ struct CellInfo {
     uint32_t ax, ay, az;  // associated cell inside the block, in [0, 3]
 };
 
+// Block and associated cell from the quotient q = pt / dx, already formed.
+__device__ __forceinline__ CellInfo cell_info_scaled(v3 q) {
+    const v3 a = mk(roundf(q.x) - 1.0f, roundf(q.y) - 1.0f, roundf(q.z) - 1.0f);
+    float fx = floorf(a.x / 4.0f), fy = floorf(a.y / 4.0f), fz = floorf(a.z / 4.0f);
+    CellInfo c;
+    c.bx = f2i_sat(fx);
+    c.by = f2i_sat(fy);
+    c.bz = f2i_sat(fz);
+    c.ax = (uint32_t)__float2uint_rz(a.x - fx * 4.0f);
+    c.ay = (uint32_t)__float2uint_rz(a.y - fy * 4.0f);
+    c.az = (uint32_t)__float2uint_rz(a.z - fz * 4.0f);
+    return c;
+}
+
 __device__ __forceinline__ CellInfo cell_info(float dx, v3 pt) {
     v3 a = assoc_cell_of(dx, pt);
     float fx = floorf(a.x / 4.0f), fy = floorf(a.y / 4.0f), fz = floorf(a.z / 4.0f);

@@ -103,6 +103,14 @@ __global__ void __launch_bounds__(kP2gThreads, NXM_P2G_MIN_CTAS) k_p2g(DevPtrs P
 
     const float dx = P.params->dx;
     const float inv_dx = P.params->inv_dx;
+#ifndef NXM_P2G_POW2
+#define NXM_P2G_POW2 1
+#endif
+    // a power-of-two cell width divides exactly by multiplying with its
+    // reciprocal (the association must round as the reference's division)
+    const uint32_t dxb = __float_as_uint(dx);
+    const bool pow2 = NXM_P2G_POW2 && (dxb & 0x807FFFFFu) == 0u && (dxb >> 23) - 1u < 253u;
+    const float rdx = __uint_as_float((254u << 23) - dxb);
     const uint32_t nbp = min(__ldcg(&P.counters->num_primary), __ldcg(&P.counters->num_blocks));
     const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
     // cell-phase roles; lanes 27..31 idle (zero weight, never write)
@@ -146,7 +154,7 @@ __global__ void __launch_bounds__(kP2gThreads, NXM_P2G_MIN_CTAS) k_p2g(DevPtrs P
                 } else {
                     const v3 pt = mk(raw.xm.x, raw.xm.y, raw.xm.z);
                     const float m = raw.xm.w;
-                    const CellInfo ci = cell_info(dx, pt);
+                    const CellInfo ci = pow2 ? cell_info_scaled(pt * rdx) : cell_info(dx, pt);
                     const v3 r = mk((float)(vid.x * 4 + (int)ci.ax), (float)(vid.y * 4 + (int)ci.ay),
                                     (float)(vid.z * 4 + (int)ci.az)) * dx - pt;
                     const v3 wx = kernel_eval_all(-r.x * inv_dx);
