@@ -97,7 +97,6 @@ constexpr int kRigidSortLaunches = 5;
 void launch_p2g(const DevPtrs& P, const LaunchCfg& c, cudaStream_t s);
 void launch_grid_update(const DevPtrs& P, const LaunchCfg& c, cudaStream_t s);
 void launch_g2p_update(const DevPtrs& P, const LaunchCfg& c, cudaStream_t s);
-void launch_colliders_begin(const DevPtrs& P, cudaStream_t s);
 void launch_colliders_end(const DevPtrs& P, cudaStream_t s);
 }  // namespace fast
 
@@ -154,6 +153,6 @@ int sort_launches(bool canonical);
 constexpr int kP2gLaunches = 1;
 constexpr int kGridLaunches = 1;
 constexpr int kG2pLaunches = 1;
-constexpr int kColliderLaunches = 2;
+constexpr int kColliderLaunches = 1;
 
 }  // namespace nxm

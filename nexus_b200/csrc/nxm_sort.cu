@@ -122,9 +122,22 @@ __device__ __forceinline__ uint32_t extra_bucket(uint32_t az, int sz) {
 
 // ---------------------------------------------------------------------------
 
+// Clears the hash and the step counters; the last CTA also refreshes the
+// colliders' world centres of mass from their poses (rigid_impulses.rs:167-185),
+// which the grid update reads.
 __global__ void k_sort_reset(DevPtrs P, uint32_t hash_cap) {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < hash_cap; i += gridDim.x * blockDim.x)
         P.hkey[i] = NONE;
+    if (P.colliders && blockIdx.x == gridDim.x - 1) {
+        const Params& prm = *P.params;
+        const uint32_t ncol = prm.scene_blocks ? prm.ncol : min(prm.ncol, (uint32_t)MAX_COLLIDERS);
+        for (uint32_t i = threadIdx.x; i < ncol; i += blockDim.x) {
+            DevCollider& c = P.colliders[i];
+            const quat q = quat{c.rot[0], c.rot[1], c.rot[2], c.rot[3]};
+            const v3 com = qrot(q, mk(c.local_com[0], c.local_com[1], c.local_com[2])) + mk(c.tra[0], c.tra[1], c.tra[2]);
+            c.com[0] = com.x; c.com[1] = com.y; c.com[2] = com.z;
+        }
+    }
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         P.counters->num_primary = 0;
         P.counters->num_extra = 0;

@@ -745,7 +745,7 @@ int enqueue_step(nxm_state* s, cudaStream_t st, cudaEvent_t* ev /* 5 events or n
     int k = 0;
     const bool has_col = !s->colliders.empty();
     if (ev) cudaEventRecord(ev[0], st);
-    if (has_col) { fast::launch_colliders_begin(P, st); ++k; }
+    // the colliders' centres of mass are refreshed by the sort's first kernel
     // CPIC runs the reference's gather-form transfers, so it needs the sort's extras
     const bool exact_path = s->deterministic || s->use_cpic;
     const bool rigid = P.nrp > 0;  // CPIC with trimesh colliders

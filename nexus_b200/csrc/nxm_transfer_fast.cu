@@ -274,19 +274,9 @@ __global__ void __launch_bounds__(kP2gThreads, NXM_P2G_MIN_CTAS) k_p2g(DevPtrs P
     }
 }
 
-// rigid_impulses.rs:167-185: world centre of mass from the current pose.
+// Colliders a step moves: all (at most 16), or every scene's in batched mode.
 __device__ __forceinline__ uint32_t collider_count(const Params& p) {
     return p.scene_blocks ? p.ncol : min(p.ncol, (uint32_t)MAX_COLLIDERS);
-}
-
-__global__ void k_colliders_begin(DevPtrs P) {
-    const uint32_t ncol = collider_count(*P.params);
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < ncol; i += gridDim.x * blockDim.x) {
-    DevCollider& c = P.colliders[i];
-    quat q = quat{c.rot[0], c.rot[1], c.rot[2], c.rot[3]};
-    v3 com = qrot(q, mk(c.local_com[0], c.local_com[1], c.local_com[2])) + mk(c.tra[0], c.tra[1], c.tra[2]);
-    c.com[0] = com.x; c.com[1] = com.y; c.com[2] = com.z;
-    }
 }
 
 // dynamics/body.rs Velocity::integrate for one-way coupled bodies
@@ -329,7 +319,6 @@ void launch_p2g(const DevPtrs& P, const LaunchCfg& c, cudaStream_t s) {
     k_p2g<<<c.sm_count * NXM_P2G_MIN_CTAS, kP2gThreads, kP2gSmem, s>>>(P);
 }
 
-void launch_colliders_begin(const DevPtrs& P, cudaStream_t s) { k_colliders_begin<<<8, 128, 0, s>>>(P); }
 void launch_colliders_end(const DevPtrs& P, cudaStream_t s) { k_colliders_end<<<8, 128, 0, s>>>(P); }
 
 }  // namespace fast
