@@ -46,10 +46,10 @@ UNIT = "particle-steps/s"
 # read; Drucker-Prager state, 3 floats, read and written for sand).
 B_ALG_ELASTIC = 204
 B_ALG_SAND = 228
-# DRAM bytes read + written per step by the two transfer kernels (77 % of the
-# step) on the sand_water scene, from one ncu capture of the full scene
-# (k_p2g 182 MB + k_g2p_update 614 MB; the sort and grid kernels are not included).
-TRAFFIC_PER_STEP = 174.2e6 + 8.0e6 + 317.5e6 + 296.5e6
+# DRAM bytes read + written per step by the two transfer kernels (79 % of the
+# step's kernel time) on the sand_water scene, from one ncu capture of the full
+# scene (k_p2g 180 MB + k_g2p_update 601 MB; the sort and grid kernels are not included).
+TRAFFIC_PER_STEP = 174.2e6 + 6.1e6 + 322.1e6 + 279.0e6
 
 
 def b_alg_per_particle(model_tags: np.ndarray) -> float:
