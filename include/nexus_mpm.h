@@ -436,6 +436,16 @@ NXM_API int nxm_chunk_of_particles(const nxm_state* state, uint32_t* out);
  * 0xFFFFFFFF when no particle is enabled. */
 NXM_API int nxm_state_estimate_timestep_bound(nxm_state* state, float* max_dt, uint32_t* bits);
 
+/* NexusPipeline::simulate's MPM part (src/pipeline.rs:75-87) with adaptive
+ * substeps: the frame's dt (the simulation params' dt) is split into n
+ * substeps, n = clamp(ceil(dt / CFL bound), min_substeps, max_substeps), the
+ * bound taken as nxm_state_estimate_timestep_bound gives it at the start of
+ * the frame (the reference runs a fixed count, state.rs:136-137, which
+ * min_substeps = max_substeps reproduces); then write_substep_params(n) and n
+ * steps.  Synchronizes once (the bound); `substeps` (nullable) receives n. */
+NXM_API int nxm_simulate_frame(nxm_pipeline* pipeline, nxm_state* state, uint32_t min_substeps,
+                               uint32_t max_substeps, uint32_t* substeps);
+
 /* ---- synchronisation and status ------------------------------------------ */
 
 NXM_API int nxm_synchronize(nxm_state* state);

@@ -2228,6 +2228,31 @@ int nxm_state_estimate_timestep_bound(nxm_state* s, float* max_dt, uint32_t* bit
     return NXM_OK;
 }
 
+int nxm_simulate_frame(nxm_pipeline* pipeline, nxm_state* s, uint32_t min_substeps, uint32_t max_substeps,
+                       uint32_t* substeps) {
+    if (!pipeline || !s || max_substeps == 0 || min_substeps > max_substeps) return NXM_E_INVALID;
+    float bound = 0.f;
+    uint32_t bits = 0;
+    int rc = nxm_state_estimate_timestep_bound(s, &bound, &bits);
+    if (rc) return rc;
+    uint32_t n = std::max<uint32_t>(min_substeps, 1u);
+    if (bits == 0u) {
+        n = max_substeps;  // a zero bound (a degenerate particle): as many substeps as allowed
+    } else if (bits != 0xFFFFFFFFu) {  // 0xFFFFFFFF: no enabled particle, no constraint
+        const double need = std::ceil((double)s->base_dt / ((double)bits / 1.0e12));
+        if (need > (double)n) n = need >= (double)max_substeps ? max_substeps : (uint32_t)need;
+    }
+    n = std::min(n, max_substeps);
+    rc = nxm_state_write_substep_params(s, n);
+    if (rc) return rc;
+    for (uint32_t i = 0; i < n; ++i) {
+        rc = nxm_step(pipeline, s, nullptr);
+        if (rc) return rc;
+    }
+    if (substeps) *substeps = n;
+    return NXM_OK;
+}
+
 int nxm_synchronize(nxm_state* s) {
     if (!s) return NXM_E_INVALID;
     NXM_TRY(cudaStreamSynchronize(s->stream));

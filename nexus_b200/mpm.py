@@ -96,6 +96,7 @@ SIGNATURES = {
     "nxm_debug_sort": (C.c_int, [_vp, _vp, C.c_int]),
     "nxm_state_estimate_timestep_bound": (C.c_int, [_vp, _f, _u]),
     "nxm_read_cdf": (C.c_int, [_vp, _f]),
+    "nxm_simulate_frame": (C.c_int, [_vp, _vp, C.c_uint32, C.c_uint32, _u]),
     "nxm_state_status_pipelined": (C.c_int, [_vp, _u]),
     "nxm_state_num_rigid_particles": (C.c_int, [_vp, _u]),
     "nxm_read_rigid_particles": (C.c_int, [_vp, _f]),
@@ -169,6 +170,13 @@ class MpmPipeline:
         h = C.c_void_p()
         _check(self.lib.nxm_pipeline_create(C.byref(h)), "nxm_pipeline_create")
         self.h = h
+
+    def simulate_frame(self, state: "MpmState", min_substeps: int = 1, max_substeps: int = 1000) -> int:
+        """``NexusPipeline::simulate`` (MPM part) with the substep count from the
+        CFL bound: returns the number of substeps run."""
+        n = np.zeros(1, np.uint32)
+        _check(self.lib.nxm_simulate_frame(self.h, state.h, min_substeps, max_substeps, _p(n, _u)), "simulate_frame")
+        return int(n[0])
 
     def step(self, state: "MpmState", timestamps: bool = False):
         """``MpmPipeline::step`` (src_mpm/pipeline.rs:385-526).  Enqueued; with
