@@ -181,6 +181,11 @@ __device__ __forceinline__ float4 halo_node(const DevPtrs& P, uint32_t b, uint32
     return make_float4(nd.x, nd.y, nd.z, 0.f);
 }
 
+#ifndef NXM_G2P_THREADS
+#define NXM_G2P_THREADS 256
+#endif
+constexpr uint32_t kG2pThreads = NXM_G2P_THREADS;  // threads per G2P CTA
+
 // g2p.rs:150-270 (non-CPIC) fused with particle_update.rs:60-201 for one
 // particle: gathers velocity and velocity gradient from the 6x6x6 halo of its
 // block (shared memory), then advects, updates F and the model, and writes the
@@ -367,16 +372,16 @@ __device__ __forceinline__ void g2p_particle(const DevPtrs& P, const Params& prm
     }
     m3 aff;
     if (stash && tag != MODEL_FLUID) {
-        // m A waits in this thread's shared-memory slots (stride 256) across
+        // m A waits in this thread's shared-memory slots (stride kG2pThreads) across
         // the model update instead of in registers
         const m3 am = A * mass;
         const float* e = &am.c0.x;
 #pragma unroll
-        for (int i = 0; i < 9; ++i) stash[256 * i] = e[i];
+        for (int i = 0; i < 9; ++i) stash[kG2pThreads * i] = e[i];
         const m3 tau = model_update<NXM_FAST>(tag, mat.w, st, F, mzero());
         float r[9];
 #pragma unroll
-        for (int i = 0; i < 9; ++i) r[i] = stash[256 * i];
+        for (int i = 0; i < 9; ++i) r[i] = stash[kG2pThreads * i];
         aff = mkm(mk(r[0], r[1], r[2]), mk(r[3], r[4], r[5]), mk(r[6], r[7], r[8])) -
               tau * (init_volume * inv_d * dt);
     } else {
@@ -408,7 +413,7 @@ __device__ __forceinline__ void g2p_particle(const DevPtrs& P, const Params& prm
 }
 
 #ifndef NXM_G2P_MIN_CTAS
-#define NXM_G2P_MIN_CTAS 4  // CTAs of 256 threads per SM the register budget is sized for
+#define NXM_G2P_MIN_CTAS 4  // CTAs per SM the register budget is sized for
 #endif
 
 // One CTA per primary block (ids [0, num_primary); the other blocks hold no
@@ -423,10 +428,10 @@ __device__ __forceinline__ void g2p_particle(const DevPtrs& P, const Params& prm
 #ifndef NXM_G2P_STASH
 #define NXM_G2P_STASH 1  // m A waits in shared memory across the model update (fast build)
 #endif
-__global__ void __launch_bounds__(256, NXM_G2P_MIN_CTAS) k_g2p_update(DevPtrs P) {
+__global__ void __launch_bounds__(kG2pThreads, NXM_G2P_MIN_CTAS) k_g2p_update(DevPtrs P) {
     __shared__ float4 halo[216];
 #if NXM_G2P_STASH
-    __shared__ float stash_mem[9 * 256];
+    __shared__ float stash_mem[9 * kG2pThreads];
     volatile float* stash = NXM_FAST ? stash_mem + threadIdx.x : nullptr;
 #else
     volatile float* stash = nullptr;
@@ -544,7 +549,7 @@ void launch_grid_update(const DevPtrs& P, const LaunchCfg& c, cudaStream_t s) {
 }
 
 void launch_g2p_update(const DevPtrs& P, const LaunchCfg& c, cudaStream_t s) {
-    k_g2p_update<<<c.sm_count * NXM_G2P_MIN_CTAS, 256, 0, s>>>(P);
+    k_g2p_update<<<c.sm_count * NXM_G2P_MIN_CTAS, kG2pThreads, 0, s>>>(P);
 }
 
 }  // namespace NXM_NS
