@@ -153,6 +153,5 @@ int sort_launches(bool canonical);
 constexpr int kP2gLaunches = 1;
 constexpr int kGridLaunches = 1;
 constexpr int kG2pLaunches = 1;
-constexpr int kColliderLaunches = 1;
 
 }  // namespace nxm
