@@ -18,6 +18,7 @@
 #include <new>
 #include <set>
 #include <thread>
+#include <deque>
 #include <vector>
 
 #include "../../include/nexus_mpm.h"
@@ -430,6 +431,16 @@ struct nxm_state {
     float4* d_palette = nullptr;
     uint32_t palette_cap = 0;
 
+    // pinned staging ring for host -> device copies (see upload_async)
+    struct StagingSpan {
+        size_t begin, end;
+        cudaEvent_t done;
+    };
+    char* stg = nullptr;
+    size_t stg_cap = 0, stg_head = 0;
+    std::deque<StagingSpan> stg_live;
+    std::vector<cudaEvent_t> event_pool;
+
     // scratch for readback packing
     uint32_t* d_pack = nullptr;
     size_t pack_cap = 0;
@@ -504,6 +515,84 @@ LaunchCfg launch_cfg(nxm_state* s) {
     c.block_capacity = s->block_cap;
     c.particle_capacity = s->pcap;
     return c;
+}
+
+// ---- pinned staging -------------------------------------------------------------
+//
+// Host data bound for the device is copied into a ring of pinned memory and
+// sent from there with cudaMemcpyAsync, so the copy is ordered on the stream
+// behind the queued work without the host waiting for it (a copy from
+// pageable memory would first drain the stream).  An event recorded after
+// each copy marks when its ring region may be written again.
+
+cudaError_t take_event(nxm_state* s, cudaEvent_t* e) {
+    if (!s->event_pool.empty()) {
+        *e = s->event_pool.back();
+        s->event_pool.pop_back();
+        return cudaSuccess;
+    }
+    return cudaEventCreateWithFlags(e, cudaEventDisableTiming);
+}
+
+// A ring region of `bytes` (256-aligned) whose earlier copies have run.
+cudaError_t staging_reserve(nxm_state* s, size_t bytes, char** out) {
+    bytes = (bytes + 255) & ~size_t(255);
+    if (bytes * 2 > s->stg_cap) {  // grow: every copy from the old ring has to be done
+        cudaError_t e = cudaStreamSynchronize(s->stream);
+        if (e != cudaSuccess) return e;
+        for (const auto& sp : s->stg_live) s->event_pool.push_back(sp.done);
+        s->stg_live.clear();
+        if (s->stg) cudaFreeHost(s->stg);
+        s->stg = nullptr;
+        s->stg_cap = 0;
+        const size_t cap = std::max<size_t>(bytes * 4, size_t(64) << 20);
+        e = cudaMallocHost(reinterpret_cast<void**>(&s->stg), cap);
+        if (e != cudaSuccess) return e;
+        s->stg_cap = cap;
+        s->stg_head = 0;
+    }
+    if (s->stg_head + bytes > s->stg_cap) s->stg_head = 0;
+    const size_t lo = s->stg_head, hi = lo + bytes;
+    int newest = -1;  // copies complete in stream order: waiting for the newest overlap covers the older
+    for (size_t i = 0; i < s->stg_live.size(); ++i)
+        if (s->stg_live[i].begin < hi && lo < s->stg_live[i].end) newest = (int)i;
+    if (newest >= 0) {
+        cudaError_t e = cudaEventSynchronize(s->stg_live[newest].done);
+        if (e != cudaSuccess) return e;
+        for (int i = 0; i <= newest; ++i) s->event_pool.push_back(s->stg_live[i].done);
+        s->stg_live.erase(s->stg_live.begin(), s->stg_live.begin() + newest + 1);
+    }
+    *out = s->stg + lo;
+    s->stg_head = hi;
+    return cudaSuccess;
+}
+
+bool host_pinned(const void* p) {
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeHost;
+}
+
+// Copies `bytes` of host data to `dst` in stream order; the caller's buffer
+// is free when the call returns and the host never waits for queued work.
+cudaError_t upload_async(nxm_state* s, void* dst, const void* src, size_t bytes) {
+    if (bytes == 0) return cudaSuccess;
+    char* h = nullptr;
+    cudaError_t e = staging_reserve(s, bytes, &h);
+    if (e != cudaSuccess) return e;
+    std::memcpy(h, src, bytes);
+    e = cudaMemcpyAsync(dst, h, bytes, cudaMemcpyHostToDevice, s->stream);
+    if (e != cudaSuccess) return e;
+    cudaEvent_t done;
+    e = take_event(s, &done);
+    if (e != cudaSuccess) return e;
+    e = cudaEventRecord(done, s->stream);
+    if (e != cudaSuccess) return e;
+    s->stg_live.push_back(nxm_state::StagingSpan{(size_t)(h - s->stg), (size_t)(h - s->stg) + bytes, done});
+    return cudaSuccess;
 }
 
 void invalidate_graph(nxm_state* s) {
@@ -696,9 +785,7 @@ int sync_materials(nxm_state* s) {
         s->mat_cap = cap;
         invalidate_graph(s);
     }
-    NXM_TRY(cudaMemcpyAsync(s->d_materials, s->materials.data(), sizeof(Material) * need, cudaMemcpyHostToDevice,
-                            s->stream));
-    NXM_TRY(cudaStreamSynchronize(s->stream));
+    NXM_TRY(upload_async(s, s->d_materials, s->materials.data(), sizeof(Material) * need));
     s->materials_dirty = false;
     return NXM_OK;
 }
@@ -732,8 +819,7 @@ int sync_params(nxm_state* s) {
         p.scene_cmin[k] = s->scene_cmin[k];
         p.scene_cells[k] = s->scene_cells[k];
     }
-    NXM_TRY(cudaMemcpyAsync(s->d_params, &p, sizeof(Params), cudaMemcpyHostToDevice, s->stream));
-    NXM_TRY(cudaStreamSynchronize(s->stream));
+    NXM_TRY(upload_async(s, s->d_params, &p, sizeof(Params)));
     s->params_dirty = false;
     return NXM_OK;
 }
@@ -1020,9 +1106,12 @@ __global__ void k_pack_particles(UploadSrc u, uint32_t base, uint32_t count, PKi
 }
 
 // Appends `count` particles: the caller's SoA arrays are copied as they are
-// (fast from pinned memory) into a stream-ordered scratch, chunk by chunk, and
-// packed into the particle records on the device; only the material runs are
-// resolved on the host.
+// into a stream-ordered scratch, chunk by chunk, and packed into the particle
+// records on the device; only the material runs are resolved on the host.
+// Arrays in pinned memory are copied directly (the call then waits for the
+// copies before returning, as the caller owns them); pageable ones go through
+// the staging ring, so the upload is queued behind the running steps without
+// the host waiting for them.
 int upload_particles(nxm_state* s, const nxm_particles_soa* p, uint32_t count) {
     if (count == 0) return NXM_OK;
     if (!p || !p->position || !p->model) return NXM_E_INVALID;
@@ -1053,6 +1142,10 @@ int upload_particles(nxm_state* s, const nxm_particles_soa* p, uint32_t count) {
     for (const Field& f : fields)
         if (f.src) per_particle += f.elem;
     const size_t run_bytes = ((size_t)nruns * 8 + 15) / 16 * 16 + (size_t)nruns * 16;
+    bool pinned[14] = {};
+    bool direct = false;  // some copy reads the caller's pinned memory
+    for (int f = 0; f < 14; ++f)
+        if (fields[f].src) direct |= (pinned[f] = host_pinned(fields[f].src));
     char* scratch = nullptr;
     NXM_TRY(cudaMallocAsync(reinterpret_cast<void**>(&scratch), run_bytes + per_particle * chunk, s->stream));
     UploadSrc u{};
@@ -1061,11 +1154,9 @@ int upload_particles(nxm_state* s, const nxm_particles_soa* p, uint32_t count) {
         uint32_t* rs = reinterpret_cast<uint32_t*>(scratch);
         uint32_t* rm = rs + nruns;
         float4* rst = reinterpret_cast<float4*>(scratch + ((size_t)nruns * 8 + 15) / 16 * 16);
-        cudaError_t e = cudaMemcpyAsync(rs, runs.start.data(), 4 * (size_t)nruns, cudaMemcpyHostToDevice, s->stream);
-        if (e == cudaSuccess)
-            e = cudaMemcpyAsync(rm, runs.mid.data(), 4 * (size_t)nruns, cudaMemcpyHostToDevice, s->stream);
-        if (e == cudaSuccess)
-            e = cudaMemcpyAsync(rst, runs.state.data(), 16 * (size_t)nruns, cudaMemcpyHostToDevice, s->stream);
+        cudaError_t e = upload_async(s, rs, runs.start.data(), 4 * (size_t)nruns);
+        if (e == cudaSuccess) e = upload_async(s, rm, runs.mid.data(), 4 * (size_t)nruns);
+        if (e == cudaSuccess) e = upload_async(s, rst, runs.state.data(), 16 * (size_t)nruns);
         if (e != cudaSuccess) {
             cudaFreeAsync(scratch, s->stream);
             return NXM_E_CUDA;
@@ -1082,8 +1173,9 @@ int upload_particles(nxm_state* s, const nxm_particles_soa* p, uint32_t count) {
         for (int f = 0; f < 14 && err == cudaSuccess; ++f) {
             if (!fields[f].src) continue;
             dst[f] = at;
-            err = cudaMemcpyAsync(at, static_cast<const char*>(fields[f].src) + fields[f].elem * c0, fields[f].elem * cn,
-                                  cudaMemcpyHostToDevice, s->stream);
+            const char* from = static_cast<const char*>(fields[f].src) + fields[f].elem * c0;
+            err = pinned[f] ? cudaMemcpyAsync(at, from, fields[f].elem * cn, cudaMemcpyHostToDevice, s->stream)
+                            : upload_async(s, at, from, fields[f].elem * cn);
             at += fields[f].elem * chunk;
         }
         if (err != cudaSuccess) break;
@@ -1114,7 +1206,7 @@ int upload_particles(nxm_state* s, const nxm_particles_soa* p, uint32_t count) {
         s->launches += 1;
         NXM_TRY(cudaGetLastError());
     }
-    NXM_TRY(cudaStreamSynchronize(s->stream));
+    if (direct) NXM_TRY(cudaStreamSynchronize(s->stream));
     s->n += count;
     s->params_dirty = true;
     return invalidate_codes(s);
@@ -1393,7 +1485,11 @@ int install_colliders(nxm_state* s, std::vector<DevCollider> dc, const float* tr
         trimesh_bvh(tris, base, d.tri_count, d.bvh_first, bvh);
         d.bvh_count = (uint32_t)bvh.size() - d.bvh_first;
     }
-    NXM_TRY(cudaStreamSynchronize(s->stream));
+    // buffers the queued steps read are replaced only after they ran; a table
+    // that fits is rewritten in stream order, without waiting
+    const bool had_mesh = s->d_tris != nullptr;
+    const bool replace = dc.size() > s->col_cap || had_mesh || !tris.empty();
+    if (replace) NXM_TRY(cudaStreamSynchronize(s->stream));
     bool realloc_graph = false;
     if (dc.size() > s->col_cap) {
         const uint32_t cap = std::max<uint32_t>((uint32_t)dc.size(), 2 * s->col_cap);
@@ -1404,21 +1500,17 @@ int install_colliders(nxm_state* s, std::vector<DevCollider> dc, const float* tr
         s->col_cap = cap;
         realloc_graph = true;
     }
-    if (!dc.empty())
-        NXM_TRY(cudaMemcpyAsync(s->d_colliders, dc.data(), sizeof(DevCollider) * dc.size(), cudaMemcpyHostToDevice,
-                                s->stream));
-    const bool had_mesh = s->d_tris != nullptr;
-    dfree(s->d_tris);
-    dfree(s->d_bvh);
-    if (!tris.empty()) {
-        NXM_TRY(dalloc(&s->d_tris, tris.size()));
-        NXM_TRY(dalloc(&s->d_bvh, bvh.size()));
-        NXM_TRY(cudaMemcpyAsync(s->d_tris, tris.data(), sizeof(DevTri) * tris.size(), cudaMemcpyHostToDevice,
-                                s->stream));
-        NXM_TRY(cudaMemcpyAsync(s->d_bvh, bvh.data(), sizeof(DevBvhNode) * bvh.size(), cudaMemcpyHostToDevice,
-                                s->stream));
+    if (!dc.empty()) NXM_TRY(upload_async(s, s->d_colliders, dc.data(), sizeof(DevCollider) * dc.size()));
+    if (replace) {
+        dfree(s->d_tris);
+        dfree(s->d_bvh);
+        if (!tris.empty()) {
+            NXM_TRY(dalloc(&s->d_tris, tris.size()));
+            NXM_TRY(dalloc(&s->d_bvh, bvh.size()));
+            NXM_TRY(upload_async(s, s->d_tris, tris.data(), sizeof(DevTri) * tris.size()));
+            NXM_TRY(upload_async(s, s->d_bvh, bvh.data(), sizeof(DevBvhNode) * bvh.size()));
+        }
     }
-    NXM_TRY(cudaStreamSynchronize(s->stream));
     const bool had = !s->colliders.empty();
     s->colliders = dc;
     s->tris_host = std::move(tris);
@@ -1432,6 +1524,7 @@ int install_colliders(nxm_state* s, std::vector<DevCollider> dc, const float* tr
 // without CPIC), as the reference does when the coupling is set
 // (src_mpm/pipeline.rs:211-245).
 int rebuild_rigid_particles(nxm_state* s) {
+    if (!s->use_cpic && s->nrp == 0) return NXM_OK;  // nothing sampled, nothing to free
     NXM_TRY(cudaStreamSynchronize(s->stream));
     dfree(s->d_rp_local); dfree(s->d_rp_world); dfree(s->d_rp_need); dfree(s->d_rp_sorted);
     const bool had = s->nrp != 0;
@@ -1564,6 +1657,9 @@ void nxm_state_destroy(nxm_state* s) {
     dfree(s->d_render); dfree(s->d_palette);
     if (s->h_vel6) cudaFreeHost(s->h_vel6);
     if (s->h_status) cudaFreeHost(s->h_status);
+    if (s->stg) cudaFreeHost(s->stg);
+    for (const auto& sp : s->stg_live) cudaEventDestroy(sp.done);
+    for (cudaEvent_t e : s->event_pool) cudaEventDestroy(e);
     for (cudaEvent_t e : s->vel_done)
         if (e) cudaEventDestroy(e);
     for (cudaEvent_t e : s->status_done)
@@ -1910,8 +2006,7 @@ static int rebuild_scene_colliders(nxm_state* s) {
         }
         tri.insert(tri.end(), sc.tri.begin(), sc.tri.end());
     }
-    NXM_TRY(cudaMemcpyAsync(s->d_scene_cols, ranges.data(), sizeof(uint2) * ranges.size(), cudaMemcpyHostToDevice,
-                            s->stream));
+    NXM_TRY(upload_async(s, s->d_scene_cols, ranges.data(), sizeof(uint2) * ranges.size()));
     return install_colliders(s, dc, tri.data());
 }
 
