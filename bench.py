@@ -247,8 +247,14 @@ def run_ours(args, world, rank, local):
     peak, peak_kind = load_peaks()
     achieved = bytes_per_step / step_s / 1e9
 
-    # end to end through the C ABI from pinned host buffers
+    # end to end through the C ABI from pinned host buffers (every rank its own
+    # replica; the whole job's rate over the slowest rank's wall time)
     e2e = measure_e2e(scene, args, torch) if args.e2e else None
+    if e2e is not None and world > 1:
+        wall = all_max(n * e2e["steps"] / e2e["value"], world)
+        e2e["value"] = n * world * e2e["steps"] / wall
+        e2e["h2d_bytes_per_step"] *= world
+        e2e["d2h_bytes_per_step"] *= world
     del st
     batched = measure_batched(args, world, rank, torch) if args.batched_steps > 0 else None
     serving = measure_serving(args, torch) if (args.serving_requests > 0 and world == 1) else None
