@@ -545,7 +545,7 @@ cudaError_t staging_reserve(nxm_state* s, size_t bytes, char** out) {
         if (s->stg) cudaFreeHost(s->stg);
         s->stg = nullptr;
         s->stg_cap = 0;
-        const size_t cap = std::max<size_t>(bytes * 4, size_t(64) << 20);
+        const size_t cap = std::max<size_t>(bytes * 4, size_t(1) << 20);
         e = cudaMallocHost(reinterpret_cast<void**>(&s->stg), cap);
         if (e != cudaSuccess) return e;
         s->stg_cap = cap;
