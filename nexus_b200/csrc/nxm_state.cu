@@ -319,6 +319,7 @@ struct nxm_state {
     // become current (`parity` counts the swaps mod 2); pid[slot] is the
     // particle id of a slot while `permuted`, otherwise slot == id.
     uint32_t n = 0, pcap = 0;
+    char* pslab = nullptr;  // the one allocation the per-particle arrays below are carved from
     PKin* kin = nullptr;
     PDef* def = nullptr;
     float4* pstate = nullptr;
@@ -349,6 +350,7 @@ struct nxm_state {
 
     // grid
     uint32_t block_cap = 0, hash_cap = 0;
+    char* gslab = nullptr;  // the one allocation the grid arrays below are carved from
     uint32_t* hkey = nullptr;
     uint32_t* hval = nullptr;
     int4* bvid = nullptr;
@@ -638,10 +640,53 @@ int canonicalize(nxm_state* s) {
     return NXM_OK;
 }
 
+// Arrays carved from one device allocation (each piece 256-byte aligned):
+// one cudaMalloc instead of one per array, which is most of the cost of
+// creating a state.
+struct Slab {
+    std::vector<std::pair<void**, size_t>> parts;
+    size_t bytes = 0;
+    template <class T>
+    void add(T** p, size_t count) {
+        parts.emplace_back(reinterpret_cast<void**>(p), bytes);
+        bytes += (std::max<size_t>(count, 1) * sizeof(T) + 255) & ~size_t(255);
+    }
+    // Allocates and points every added array into the allocation (or leaves them null).
+    cudaError_t alloc(char** base) {
+        *base = nullptr;
+        const cudaError_t e = cudaMalloc(reinterpret_cast<void**>(base), bytes);
+        if (e != cudaSuccess) {
+            *base = nullptr;
+            return e;
+        }
+        for (auto& [ptr, off] : parts) *ptr = *base + off;
+        return cudaSuccess;
+    }
+    void clear() {
+        for (auto& [ptr, off] : parts) *ptr = nullptr;
+    }
+};
+
+void grid_arrays(nxm_state* s, Slab& g) {
+    g.add(&s->hkey, s->hash_cap);
+    g.add(&s->hval, s->hash_cap);
+    g.add(&s->bvid, s->block_cap);
+    g.add(&s->first, s->block_cap);
+    g.add(&s->nprim, s->block_cap);
+    g.add(&s->nwx, s->block_cap);
+    g.add(&s->cursors, (size_t)s->block_cap * NUM_BUCKETS);
+    g.add(&s->nbh, (size_t)s->block_cap * NUM_NBH);
+    g.add(&s->nodes, (size_t)s->block_cap * 64);
+    g.add(&s->scan_tmp, s->block_cap);
+    g.add(&s->tile_sums, s->block_cap / kScanTile + 2);
+}
+
 int free_grid(nxm_state* s) {
     dfree(s->d_ncdf); dfree(s->d_nodes_inc); dfree(s->d_rp_count); dfree(s->d_rp_first);
-    dfree(s->hkey); dfree(s->hval); dfree(s->bvid); dfree(s->first); dfree(s->nprim); dfree(s->nwx);
-    dfree(s->cursors); dfree(s->nbh); dfree(s->nodes); dfree(s->scan_tmp); dfree(s->tile_sums);
+    Slab g;
+    grid_arrays(s, g);
+    g.clear();
+    dfree(s->gslab);
     return NXM_OK;
 }
 
@@ -660,20 +705,23 @@ int alloc_cpic_grid(nxm_state* s) {
 }
 
 int alloc_grid(nxm_state* s, uint32_t grid_capacity) {
+    const uint32_t block_cap = next_pow2(std::max<uint32_t>(grid_capacity, 1));
+    if (s->hkey && block_cap == s->block_cap) {  // same capacity: keep the buffers, clear the hash
+        NXM_TRY(cudaMemsetAsync(s->hkey, 0xFF, sizeof(uint32_t) * s->hash_cap, s->stream));
+        if (s->use_cpic && !s->d_ncdf) {
+            int rc = alloc_cpic_grid(s);
+            if (rc) return rc;
+        }
+        invalidate_graph(s);
+        s->params_dirty = true;
+        return NXM_OK;
+    }
     free_grid(s);
-    s->block_cap = next_pow2(std::max<uint32_t>(grid_capacity, 1));
+    s->block_cap = block_cap;
     s->hash_cap = next_pow2(std::max<uint32_t>(2u * s->block_cap, 1024u));
-    NXM_TRY(dalloc(&s->hkey, s->hash_cap));
-    NXM_TRY(dalloc(&s->hval, s->hash_cap));
-    NXM_TRY(dalloc(&s->bvid, s->block_cap));
-    NXM_TRY(dalloc(&s->first, s->block_cap));
-    NXM_TRY(dalloc(&s->nprim, s->block_cap));
-    NXM_TRY(dalloc(&s->nwx, s->block_cap));
-    NXM_TRY(dalloc(&s->cursors, (size_t)s->block_cap * NUM_BUCKETS));
-    NXM_TRY(dalloc(&s->nbh, (size_t)s->block_cap * NUM_NBH));
-    NXM_TRY(dalloc(&s->nodes, (size_t)s->block_cap * 64));
-    NXM_TRY(dalloc(&s->scan_tmp, s->block_cap));
-    NXM_TRY(dalloc(&s->tile_sums, s->block_cap / kScanTile + 2));
+    Slab g;
+    grid_arrays(s, g);
+    NXM_TRY(g.alloc(&s->gslab));
     NXM_TRY(cudaMemsetAsync(s->hkey, 0xFF, sizeof(uint32_t) * s->hash_cap, s->stream));
     if (s->use_cpic) {
         int rc = alloc_cpic_grid(s);
@@ -686,6 +734,7 @@ int alloc_grid(nxm_state* s, uint32_t grid_capacity) {
 
 // The particle arrays of a state (owned; freed on destruction unless released).
 struct ParticleBuffers {
+    char* slab = nullptr;
     PKin *kin = nullptr, *kin_alt = nullptr;
     PDef *def = nullptr, *def_alt = nullptr;
     float4 *pstate = nullptr, *pstate_alt = nullptr;
@@ -694,33 +743,30 @@ struct ParticleBuffers {
     uint2* pcode = nullptr;
     float4 *pcdf = nullptr, *pcdf_alt = nullptr;
     cudaError_t alloc(uint32_t cap) {
-        cudaError_t e = cudaSuccess;
-        auto a = [&](auto** p, size_t count) {
-            if (e == cudaSuccess) e = dalloc(p, count);
-        };
-        a(&kin, cap); a(&def, cap); a(&pstate, cap);
-        a(&kin_alt, cap); a(&def_alt, cap); a(&pstate_alt, cap);
-        a(&pid, cap); a(&pid_alt, cap); a(&pcode, cap); a(&phdr, cap);
-        a(&sorted, (size_t)cap * 8);
-        a(&pscene, cap);
-        a(&pscene_alt, cap);
-        a(&pcdf, 3 * (size_t)cap);
-        a(&pcdf_alt, 3 * (size_t)cap);
-        a(&tiles, cap / 1024 + 2);
-        return e;
+        Slab a;
+        a.add(&kin, cap); a.add(&def, cap); a.add(&pstate, cap);
+        a.add(&kin_alt, cap); a.add(&def_alt, cap); a.add(&pstate_alt, cap);
+        a.add(&pid, cap); a.add(&pid_alt, cap); a.add(&pcode, cap); a.add(&phdr, cap);
+        a.add(&sorted, (size_t)cap * 8);
+        a.add(&pscene, cap);
+        a.add(&pscene_alt, cap);
+        a.add(&pcdf, 3 * (size_t)cap);
+        a.add(&pcdf_alt, 3 * (size_t)cap);
+        a.add(&tiles, cap / 1024 + 2);
+        return a.alloc(&slab);
     }
     void release() { *this = ParticleBuffers{}; }
-    ~ParticleBuffers() {
-        dfree(kin); dfree(def); dfree(pstate); dfree(kin_alt); dfree(def_alt); dfree(pstate_alt);
-        dfree(pid); dfree(pid_alt); dfree(pcode); dfree(phdr); dfree(sorted); dfree(pscene); dfree(pscene_alt); dfree(tiles);
-        dfree(pcdf); dfree(pcdf_alt);
-    }
+    ~ParticleBuffers() { dfree(slab); }
 };
 
 void free_particles(nxm_state* s) {
-    dfree(s->kin); dfree(s->def); dfree(s->pstate); dfree(s->kin_alt); dfree(s->def_alt); dfree(s->pstate_alt);
-    dfree(s->pid); dfree(s->pid_alt); dfree(s->pcode); dfree(s->phdr); dfree(s->sorted);
-    dfree(s->d_pscene); dfree(s->d_pscene_alt); dfree(s->d_tiles); dfree(s->d_pcdf); dfree(s->d_pcdf_alt);
+    dfree(s->pslab);
+    s->kin = s->kin_alt = nullptr;
+    s->def = s->def_alt = nullptr;
+    s->pstate = s->pstate_alt = nullptr;
+    s->pid = s->pid_alt = s->phdr = s->sorted = s->d_pscene = s->d_pscene_alt = s->d_tiles = nullptr;
+    s->pcode = nullptr;
+    s->d_pcdf = s->d_pcdf_alt = nullptr;
 }
 
 int reserve_particles(nxm_state* s, uint32_t need) {
@@ -739,6 +785,7 @@ int reserve_particles(nxm_state* s, uint32_t need) {
     }
     NXM_TRY(cudaStreamSynchronize(s->stream));
     free_particles(s);
+    s->pslab = t.slab;
     s->kin = t.kin; s->def = t.def; s->pstate = t.pstate;
     s->kin_alt = t.kin_alt; s->def_alt = t.def_alt; s->pstate_alt = t.pstate_alt;
     s->pid = t.pid; s->pid_alt = t.pid_alt;
@@ -1568,13 +1615,14 @@ bool device_ok(int* dev, int* sms) {
         (void)cudaGetLastError();
         return false;
     }
-    int d = 0;
+    int d = 0, major = 0, count_sm = 0;
     if (cudaGetDevice(&d) != cudaSuccess) return false;
-    cudaDeviceProp prop;
-    if (cudaGetDeviceProperties(&prop, d) != cudaSuccess) return false;
-    if (prop.major != 10) return false;  // kernels are built for sm_100a only
+    // two attribute queries (a full property query costs milliseconds)
+    if (cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, d) != cudaSuccess) return false;
+    if (cudaDeviceGetAttribute(&count_sm, cudaDevAttrMultiProcessorCount, d) != cudaSuccess) return false;
+    if (major != 10) return false;  // kernels are built for sm_100a only
     *dev = d;
-    *sms = prop.multiProcessorCount;
+    *sms = count_sm;
     return true;
 }
 
