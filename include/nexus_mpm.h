@@ -451,10 +451,12 @@ NXM_API int nxm_simulate_frame(nxm_pipeline* pipeline, nxm_state* state, uint32_
 NXM_API int nxm_synchronize(nxm_state* state);
 /* Device status bits (NXM_STATUS_*); synchronizes.  `clear` resets them. */
 NXM_API int nxm_state_status(nxm_state* state, uint32_t* bits, int clear);
-/* Pipelined status read for a step loop: enqueues a copy of the status word
- * after the work issued so far and returns in `*bits` the word the previous
- * call enqueued (waiting only for that copy, so the stream never drains;
- * 0 on the first call).  Each step's status reaches the host one call late. */
+/* Pipelined status read for a step loop: enqueues, after the work issued so
+ * far, a one-thread kernel that stores the status word into mapped pinned
+ * host memory (no copy engine between steps), and returns in `*bits` the
+ * word the previous call enqueued (waiting only for that store, so the stream
+ * never drains; 0 on the first call).  Each step's status reaches the host
+ * one call late. */
 NXM_API int nxm_state_status_pipelined(nxm_state* state, uint32_t* bits);
 NXM_API const char* nxm_error_string(int code);
 

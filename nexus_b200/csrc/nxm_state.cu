@@ -278,6 +278,16 @@ __global__ void k_fill(uint32_t* __restrict__ out, uint32_t value, uint32_t coun
     for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < count; t += gridDim.x * blockDim.x) out[t] = value;
 }
 
+// The status word stored straight into mapped pinned host memory: no copy
+// engine between two steps (a 4-byte device-to-host copy costs tens of
+// microseconds of stream time there).
+__global__ void k_post_status(const Counters* __restrict__ c, volatile uint32_t* out) {
+    if (threadIdx.x == 0) {
+        *out = c->status;
+        __threadfence_system();
+    }
+}
+
 __global__ void k_iota(uint32_t* __restrict__ out, uint32_t first, uint32_t count) {
     for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < count; t += gridDim.x * blockDim.x) out[t] = first + t;
 }
@@ -372,7 +382,8 @@ struct nxm_state {
     size_t vel_cap = 0;  // floats per slot
     int vel_slot = 0;
     // pipelined status reads: pinned words and their copy events
-    uint32_t* h_status = nullptr;
+    uint32_t* h_status = nullptr;    // two mapped pinned words (host view)
+    uint32_t* h_status_dev = nullptr;  // the same words, device view
     cudaEvent_t status_done[2] = {};
     uint64_t status_calls = 0;
 
@@ -826,7 +837,7 @@ int sync_materials(nxm_state* s) {
         uint32_t cap = std::max<uint32_t>(need, s->mat_cap ? s->mat_cap * 2 : 16);
         Material* m;
         NXM_TRY(dalloc(&m, cap));
-        NXM_TRY(cudaStreamSynchronize(s->stream));
+        if (s->d_materials) NXM_TRY(cudaStreamSynchronize(s->stream));  // queued steps may still read it
         dfree(s->d_materials);
         s->d_materials = m;
         s->mat_cap = cap;
@@ -1167,15 +1178,8 @@ int upload_particles(nxm_state* s, const nxm_particles_soa* p, uint32_t count) {
     if (need > 0x7FFFFFFFull / 8) return NXM_E_INVALID;
     int rc = reserve_particles(s, (uint32_t)need);
     if (rc) return rc;
-    MaterialRuns runs;
-    rc = material_runs(s, p->model, count, runs);
-    if (rc) return rc;
-    rc = sync_materials(s);
-    if (rc) return rc;
-    if (s->chunks_used) s->slot2chunk.insert(s->slot2chunk.end(), count, NONE);
 
-    // scratch: the run table, then per chunk the fields that are given
-    const uint32_t nruns = (uint32_t)runs.start.size();
+    // scratch for one chunk of the fields that are given
     const uint32_t chunk = std::min<uint32_t>(count, 1u << 20);
     struct Field {
         const void* src;
@@ -1188,43 +1192,60 @@ int upload_particles(nxm_state* s, const nxm_particles_soa* p, uint32_t count) {
     size_t per_particle = 0;
     for (const Field& f : fields)
         if (f.src) per_particle += f.elem;
-    const size_t run_bytes = ((size_t)nruns * 8 + 15) / 16 * 16 + (size_t)nruns * 16;
     bool pinned[14] = {};
     bool direct = false;  // some copy reads the caller's pinned memory
     for (int f = 0; f < 14; ++f)
         if (fields[f].src) direct |= (pinned[f] = host_pinned(fields[f].src));
     char* scratch = nullptr;
-    NXM_TRY(cudaMallocAsync(reinterpret_cast<void**>(&scratch), run_bytes + per_particle * chunk, s->stream));
-    UploadSrc u{};
-    u.nruns = nruns;
-    {
-        uint32_t* rs = reinterpret_cast<uint32_t*>(scratch);
-        uint32_t* rm = rs + nruns;
-        float4* rst = reinterpret_cast<float4*>(scratch + ((size_t)nruns * 8 + 15) / 16 * 16);
-        cudaError_t e = upload_async(s, rs, runs.start.data(), 4 * (size_t)nruns);
-        if (e == cudaSuccess) e = upload_async(s, rm, runs.mid.data(), 4 * (size_t)nruns);
-        if (e == cudaSuccess) e = upload_async(s, rst, runs.state.data(), 16 * (size_t)nruns);
-        if (e != cudaSuccess) {
-            cudaFreeAsync(scratch, s->stream);
-            return NXM_E_CUDA;
-        }
-        u.run_start = rs;
-        u.run_mid = rm;
-        u.run_state = rst;
-    }
-    cudaError_t err = cudaSuccess;
-    for (uint32_t c0 = 0; c0 < count && err == cudaSuccess; c0 += chunk) {
-        const uint32_t cn = std::min(chunk, count - c0);
-        const void* dst[14] = {};
-        char* at = scratch + run_bytes;
-        for (int f = 0; f < 14 && err == cudaSuccess; ++f) {
+    NXM_TRY(cudaMallocAsync(reinterpret_cast<void**>(&scratch), std::max<size_t>(per_particle, 4) * chunk, s->stream));
+    const void* dst[14] = {};
+    auto copy_chunk = [&](uint32_t c0, uint32_t cn) {
+        char* at = scratch;
+        cudaError_t e = cudaSuccess;
+        for (int f = 0; f < 14 && e == cudaSuccess; ++f) {
+            dst[f] = nullptr;
             if (!fields[f].src) continue;
             dst[f] = at;
             const char* from = static_cast<const char*>(fields[f].src) + fields[f].elem * c0;
-            err = pinned[f] ? cudaMemcpyAsync(at, from, fields[f].elem * cn, cudaMemcpyHostToDevice, s->stream)
-                            : upload_async(s, at, from, fields[f].elem * cn);
+            e = pinned[f] ? cudaMemcpyAsync(at, from, fields[f].elem * cn, cudaMemcpyHostToDevice, s->stream)
+                          : upload_async(s, at, from, fields[f].elem * cn);
             at += fields[f].elem * chunk;
         }
+        return e;
+    };
+    // The first chunk's copies are queued before the host looks for the
+    // material runs, so the scan over the model words overlaps the transfer.
+    cudaError_t err = copy_chunk(0, std::min(chunk, count));
+    MaterialRuns runs;
+    if (err == cudaSuccess) rc = material_runs(s, p->model, count, runs);
+    else rc = NXM_E_CUDA;
+    if (!rc) rc = sync_materials(s);
+    char* run_scratch = nullptr;
+    UploadSrc u{};
+    if (!rc) {
+        const uint32_t nruns = (uint32_t)runs.start.size();
+        const size_t mid_at = (size_t)nruns * 4, state_at = ((size_t)nruns * 8 + 15) / 16 * 16;
+        cudaError_t e = cudaMallocAsync(reinterpret_cast<void**>(&run_scratch), state_at + (size_t)nruns * 16, s->stream);
+        if (e == cudaSuccess) e = upload_async(s, run_scratch, runs.start.data(), 4 * (size_t)nruns);
+        if (e == cudaSuccess) e = upload_async(s, run_scratch + mid_at, runs.mid.data(), 4 * (size_t)nruns);
+        if (e == cudaSuccess) e = upload_async(s, run_scratch + state_at, runs.state.data(), 16 * (size_t)nruns);
+        if (e != cudaSuccess) rc = NXM_E_CUDA;
+        u.nruns = nruns;
+        u.run_start = reinterpret_cast<const uint32_t*>(run_scratch);
+        u.run_mid = reinterpret_cast<const uint32_t*>(run_scratch + mid_at);
+        u.run_state = reinterpret_cast<const float4*>(run_scratch + state_at);
+    }
+    if (rc) {
+        cudaFreeAsync(scratch, s->stream);
+        if (run_scratch) cudaFreeAsync(run_scratch, s->stream);
+        if (direct) (void)cudaStreamSynchronize(s->stream);  // no copy reads the caller's memory after return
+        (void)cudaGetLastError();
+        return rc;
+    }
+    if (s->chunks_used) s->slot2chunk.insert(s->slot2chunk.end(), count, NONE);
+    for (uint32_t c0 = 0; c0 < count && err == cudaSuccess; c0 += chunk) {
+        const uint32_t cn = std::min(chunk, count - c0);
+        if (c0 > 0) err = copy_chunk(c0, cn);  // queued after the previous chunk's packing
         if (err != cudaSuccess) break;
         u.pos = static_cast<const float*>(dst[0]);
         u.vel = static_cast<const float*>(dst[1]);
@@ -1247,7 +1268,11 @@ int upload_particles(nxm_state* s, const nxm_particles_soa* p, uint32_t count) {
         err = cudaGetLastError();
     }
     cudaFreeAsync(scratch, s->stream);
-    if (err != cudaSuccess) return NXM_E_CUDA;
+    cudaFreeAsync(run_scratch, s->stream);
+    if (err != cudaSuccess) {
+        if (direct) (void)cudaStreamSynchronize(s->stream);
+        return NXM_E_CUDA;
+    }
     if (s->permuted) {  // appended particles sit at slots == their ids
         k_iota<<<grid_for_n(s, count), 256, 0, s->stream>>>(s->pid + s->n, s->n, count);
         s->launches += 1;
@@ -2410,13 +2435,16 @@ int nxm_synchronize(nxm_state* s) {
 int nxm_state_status_pipelined(nxm_state* s, uint32_t* bits) {
     if (!s || !bits) return NXM_E_INVALID;
     if (!s->h_status) {
-        NXM_TRY(cudaMallocHost(reinterpret_cast<void**>(&s->h_status), 2 * sizeof(uint32_t)));
+        NXM_TRY(cudaHostAlloc(reinterpret_cast<void**>(&s->h_status), 2 * sizeof(uint32_t), cudaHostAllocMapped));
         s->h_status[0] = s->h_status[1] = 0;
+        NXM_TRY(cudaHostGetDevicePointer(reinterpret_cast<void**>(&s->h_status_dev), s->h_status, 0));
         for (cudaEvent_t& e : s->status_done) NXM_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     }
     const int cur = (int)(s->status_calls & 1u), prev = cur ^ 1;
-    NXM_TRY(cudaMemcpyAsync(&s->h_status[cur], reinterpret_cast<const char*>(s->d_counters) + offsetof(Counters, status),
-                            sizeof(uint32_t), cudaMemcpyDeviceToHost, s->stream));
+    // slot `cur` was read by the previous call (after its write completed): free to be written again
+    k_post_status<<<1, 32, 0, s->stream>>>(s->d_counters, s->h_status_dev + cur);
+    s->launches += 1;
+    NXM_TRY(cudaGetLastError());
     NXM_TRY(cudaEventRecord(s->status_done[cur], s->stream));
     *bits = 0;
     if (s->status_calls > 0) {

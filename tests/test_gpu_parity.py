@@ -225,6 +225,25 @@ def test_grid_capacity_overflow_is_reported(pipe):
     assert np.abs(got - sc.particles.pos).max() <= sc.dx
 
 
+def test_pipelined_status_arrives_one_call_late(pipe):
+    """The status word a pipelined read enqueues (stored into mapped host
+    memory by a kernel) is returned by the next call, in stream order."""
+    sc = scenes.elastic_cube(n_side=16)
+    ok = state_from_scene(sc)
+    for _ in range(5):
+        pipe.step(ok)
+        assert ok.status_pipelined() == 0
+    assert ok.status_pipelined() == 0
+    bad = state_from_scene(sc, grid_capacity=8)
+    assert bad.status_pipelined() == 0  # first call: nothing enqueued before it
+    pipe.step(bad)
+    assert bad.status_pipelined() == 0  # the word enqueued before the step
+    assert bad.status_pipelined() & 2  # the step's overflow
+    assert bad.status(clear=True) & 2
+    assert bad.status_pipelined() & 2  # enqueued before the clear
+    assert bad.status_pipelined() == 0  # enqueued after it
+
+
 def test_sort_on_reordered_storage_matches_oracle(pipe):
     """After fast steps the records sit in block order; the sort of that storage
     reports particle ids and matches the oracle's sort of the same positions."""
