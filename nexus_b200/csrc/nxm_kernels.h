@@ -34,6 +34,11 @@ struct DevPtrs {
     uint32_t* phdr;          // per particle: primary header id
     uint32_t* scan_tmp;      // per block: offset inside its scan tile
     uint32_t* tile_sums;     // per scan tile of kScanTile blocks: its total
+    // per run of kRangeChunk sorted positions: the block holding its first
+    // position (written by the scan; the fast G2P walks the sorted list in
+    // these runs)
+    uint32_t* chunk_blk;
+    uint32_t chunk_cap;
     // G2P output.  In place: the *_out pointers equal the inputs and pid_in is
     // null.  Reordering: sorted entry j is written to slot j of the *_out
     // records, pid_out[j] = pid_in[its source slot] (pid = particle id).
@@ -68,6 +73,7 @@ struct DevPtrs {
 };
 
 constexpr uint32_t kScanTile = 256;  // blocks per scan tile (one per thread of a scan CTA)
+constexpr uint32_t kRangeChunk = 256;  // sorted positions per fast-G2P run (one per thread of its CTA)
 
 struct LaunchCfg {
     int sm_count;

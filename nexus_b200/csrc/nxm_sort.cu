@@ -405,6 +405,10 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_apply(DevPtrs P) {
                 running += cnt[j][k];
             }
             P.nwx[b] = running - first;
+            // the runs of kRangeChunk sorted positions that start inside this block
+            if (P.chunk_blk)
+                for (uint32_t c = (first + kRangeChunk - 1u) / kRangeChunk; c * kRangeChunk < running && c < P.chunk_cap; ++c)
+                    P.chunk_blk[c] = b;
             if (b == total - 1) {
                 P.counters->sorted_len = running;
                 if (running > P.params->sorted_capacity) set_status(P.counters, STATUS_SORT_CAPACITY);

@@ -56,6 +56,10 @@ void dfree(T*& p) {
     p = nullptr;
 }
 
+// Runs of kRangeChunk sorted positions a state of `cap` particles needs
+// (the fast path lists each particle once).
+uint32_t chunk_cap_for(uint32_t cap) { return cap / kRangeChunk + 2; }
+
 float bits_f(uint32_t u) {
     float f;
     std::memcpy(&f, &u, 4);
@@ -408,6 +412,7 @@ struct nxm_state {
     uint32_t* d_pscene_alt = nullptr;
     uint2* d_scene_cols = nullptr;      // per scene slot: its colliders in the table
     uint32_t* d_tiles = nullptr;        // compaction scratch, one word per 1024 particles
+    uint32_t* d_chunk_blk = nullptr;    // block of each run of kRangeChunk sorted positions
     DevTri* d_tris = nullptr;       // triangles of every trimesh collider (one copy per collider)
     DevBvhNode* d_bvh = nullptr;    // their BVHs
     std::vector<DevTri> tris_host;  // host copy of d_tris
@@ -518,6 +523,8 @@ DevPtrs dev_ptrs(nxm_state* s) {
     P.phdr = s->phdr;
     P.scan_tmp = s->scan_tmp;
     P.tile_sums = s->tile_sums;
+    P.chunk_blk = s->d_chunk_blk;
+    P.chunk_cap = chunk_cap_for(s->pcap);
     return P;
 }
 
@@ -750,7 +757,7 @@ struct ParticleBuffers {
     PDef *def = nullptr, *def_alt = nullptr;
     float4 *pstate = nullptr, *pstate_alt = nullptr;
     uint32_t *pid = nullptr, *pid_alt = nullptr, *phdr = nullptr, *sorted = nullptr, *pscene = nullptr,
-             *pscene_alt = nullptr, *tiles = nullptr;
+             *pscene_alt = nullptr, *tiles = nullptr, *chunk_blk = nullptr;
     uint2* pcode = nullptr;
     float4 *pcdf = nullptr, *pcdf_alt = nullptr;
     cudaError_t alloc(uint32_t cap) {
@@ -764,6 +771,7 @@ struct ParticleBuffers {
         a.add(&pcdf, 3 * (size_t)cap);
         a.add(&pcdf_alt, 3 * (size_t)cap);
         a.add(&tiles, cap / 1024 + 2);
+        a.add(&chunk_blk, chunk_cap_for(cap));
         return a.alloc(&slab);
     }
     void release() { *this = ParticleBuffers{}; }
@@ -776,6 +784,7 @@ void free_particles(nxm_state* s) {
     s->def = s->def_alt = nullptr;
     s->pstate = s->pstate_alt = nullptr;
     s->pid = s->pid_alt = s->phdr = s->sorted = s->d_pscene = s->d_pscene_alt = s->d_tiles = nullptr;
+    s->d_chunk_blk = nullptr;
     s->pcode = nullptr;
     s->d_pcdf = s->d_pcdf_alt = nullptr;
 }
@@ -803,6 +812,7 @@ int reserve_particles(nxm_state* s, uint32_t need) {
     s->pcode = t.pcode; s->phdr = t.phdr; s->sorted = t.sorted;
     s->d_pscene = t.pscene; s->d_pscene_alt = t.pscene_alt; s->d_tiles = t.tiles;
     s->d_pcdf = t.pcdf; s->d_pcdf_alt = t.pcdf_alt;
+    s->d_chunk_blk = t.chunk_blk;
     t.release();
     s->sort_pid = nullptr;
     s->pcap = cap;

@@ -412,6 +412,36 @@ __device__ __forceinline__ void g2p_particle(const DevPtrs& P, const Params& prm
     if (P.pid_in) P.pid_out[dst] = P.pid_in[src];
 }
 
+// End of a G2P launch: when reordering, the particles the sort could not
+// place (their block was not created: capacity or hash overflow, reported in
+// the status word) are copied unchanged to the slots after the sorted ones;
+// then the cached block keys are marked valid.
+__device__ __forceinline__ void g2p_finish(const DevPtrs& P, const Params& prm) {
+    if (P.pid_in) {
+        const uint32_t n = prm.n, sl = __ldcg(&P.counters->sorted_len);
+        for (uint32_t p = sl < n ? blockIdx.x * blockDim.x + threadIdx.x : n; p < n; p += gridDim.x * blockDim.x) {
+            if (__ldcg(&P.phdr[p]) != NONE) continue;
+            const uint32_t dst = sl + atomicAdd(&P.counters->unsorted, 1u);
+            if (dst >= n) continue;  // not reached: exactly n - sl particles have no header
+            const float4* ks = reinterpret_cast<const float4*>(&P.kin[p]);
+            float4* kd = reinterpret_cast<float4*>(&P.kin_out[dst]);
+#pragma unroll
+            for (int w = 0; w < 5; ++w) kd[w] = ks[w];
+            const float4* ds = reinterpret_cast<const float4*>(&P.def[p]);
+            float4* dd = reinterpret_cast<float4*>(&P.def_out[dst]);
+#pragma unroll
+            for (int w = 0; w < 3; ++w) dd[w] = ds[w];
+            P.pstate_out[dst] = P.pstate[p];
+            P.pid_out[dst] = P.pid_in[p];
+            const CellInfo nc = cell_info(prm.dx, mk(ks[0].x, ks[0].y, ks[0].z));
+            const int3 o = prm.scene_blocks ? scene_base_of(prm, P.pscene[P.pid_in[p]]) : make_int3(0, 0, 0);
+            P.pcode[dst] = make_uint2(pack_key(nc.bx + o.x, nc.by + o.y, nc.bz + o.z),
+                                      nc.ax | (nc.ay << 2) | (nc.az << 4));
+        }
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) P.counters->codes_valid = 1u;
+}
+
 #ifndef NXM_G2P_MIN_CTAS
 #define NXM_G2P_MIN_CTAS 4  // CTAs per SM the register budget is sized for
 #endif
@@ -517,30 +547,89 @@ __global__ void __launch_bounds__(kG2pThreads, NXM_G2P_MIN_CTAS) k_g2p_update(De
         first = nfirst;
         np = nnp;
     }
-    if (P.pid_in) {
-        const uint32_t n = prm.n, sl = __ldcg(&P.counters->sorted_len);
-        for (uint32_t p = sl < n ? blockIdx.x * blockDim.x + tid : n; p < n; p += gridDim.x * blockDim.x) {
-            if (__ldcg(&P.phdr[p]) != NONE) continue;
-            const uint32_t dst = sl + atomicAdd(&P.counters->unsorted, 1u);
-            if (dst >= n) continue;  // not reached: exactly n - sl particles have no header
-            const float4* ks = reinterpret_cast<const float4*>(&P.kin[p]);
-            float4* kd = reinterpret_cast<float4*>(&P.kin_out[dst]);
-#pragma unroll
-            for (int w = 0; w < 5; ++w) kd[w] = ks[w];
-            const float4* ds = reinterpret_cast<const float4*>(&P.def[p]);
-            float4* dd = reinterpret_cast<float4*>(&P.def_out[dst]);
-#pragma unroll
-            for (int w = 0; w < 3; ++w) dd[w] = ds[w];
-            P.pstate_out[dst] = P.pstate[p];
-            P.pid_out[dst] = P.pid_in[p];
-            const CellInfo nc = cell_info(prm.dx, mk(ks[0].x, ks[0].y, ks[0].z));
-            const int3 o = prm.scene_blocks ? scene_base_of(prm, P.pscene[P.pid_in[p]]) : make_int3(0, 0, 0);
-            P.pcode[dst] = make_uint2(pack_key(nc.bx + o.x, nc.by + o.y, nc.bz + o.z),
-                                      nc.ax | (nc.ay << 2) | (nc.az << 4));
+    g2p_finish(P, prm);
+}
+
+#if NXM_FAST && !NXM_CPIC
+// The fast build's G2P walks the sorted list in runs of kRangeChunk
+// positions, one particle per thread, instead of one CTA per block: a block
+// holds some 1-600 particles, so per-block rounds of 256 threads run part
+// empty (three quarters full on a settled scene); a run fills every thread
+// but one run's worth at the end.  A run spans the tail of one block and the
+// head of the next (a few more where blocks are small): the halos of up to
+// kRangeHalos of its blocks are staged at a time, in passes if it spans more.
+// The run's first block comes from the scan (chunk_blk); the blocks after it
+// are found from the nondecreasing `first` (primary particles of block b sit
+// at sorted positions [first[b], first[b] + nprim[b]); the fast path lists no
+// extras, so the positions [0, sorted_len) are exactly the primary particles).
+constexpr uint32_t kRangeHalos = 4;
+static_assert(kG2pThreads == kRangeChunk, "one sorted position per thread");
+static_assert(kRangeHalos < 32u, "one lane per staged block, plus one");
+__global__ void __launch_bounds__(kG2pThreads, NXM_G2P_MIN_CTAS) k_g2p_range(DevPtrs P) {
+    __shared__ float4 halo[kRangeHalos * 216];
+#if NXM_G2P_STASH
+    __shared__ float stash_mem[9 * kG2pThreads];
+    volatile float* stash = stash_mem + threadIdx.x;
+#else
+    volatile float* stash = nullptr;
+#endif
+    const Params prm = *P.params;
+    const uint32_t nbp = min(__ldcg(&P.counters->num_primary), __ldcg(&P.counters->num_blocks));
+    const uint32_t len = min(__ldcg(&P.counters->sorted_len), prm.n);
+    const uint32_t nchunks = min((len + kRangeChunk - 1u) / kRangeChunk, P.chunk_cap);
+    const uint32_t tid = threadIdx.x, lane = tid & 31u;
+    const bool reorder = P.pid_in != nullptr;
+    const CpicCtx cx{nullptr, nullptr, P.colliders, 0u};
+    for (uint32_t c = blockIdx.x; c < nchunks; c += gridDim.x) {
+        const uint32_t j0 = c * kRangeChunk, j1 = min(j0 + kRangeChunk, len);
+        const uint32_t j = j0 + tid;
+        // this thread's particle, fetched while the halos load
+        const uint32_t pid = j < j1 ? __ldg(&P.sorted[j]) : NONE;
+        float4 xm = make_float4(0.f, 0.f, 0.f, 0.f), vf = xm;
+        if (pid != NONE) {
+            const float4* kr = reinterpret_cast<const float4*>(&P.kin[pid]);
+            xm = kr[0];
+            vf = kr[1];
+        }
+        const uint32_t b0 = __ldg(&P.chunk_blk[c]);
+        for (uint32_t done = 0;;) {
+            // every warp finds the same blocks: lane i < kRangeHalos looks at
+            // block b0 + done + i, lane kRangeHalos at the one after them
+            const uint32_t bq = b0 + done + min(lane, kRangeHalos);
+            uint32_t f = NONE, e = 0u;
+            if (bq < nbp) {
+                f = __ldcg(&P.first[bq]);
+                e = f + __ldcg(&P.nprim[bq]);
+            }
+            const uint32_t m = __ballot_sync(0xFFFFFFFFu, lane <= kRangeHalos && bq < nbp && f < j1);
+            const uint32_t cnt = min((uint32_t)__popc(m & ((1u << kRangeHalos) - 1u)), kRangeHalos);
+            const bool more = (m >> kRangeHalos) & 1u;
+            if (cnt == 0u && done == 0u && tid == 0u) set_status(P.counters, STATUS_MISSING_BLOCK);  // not reached
+            // this thread's block among them (none: its block is in another pass)
+            int slot = -1;
+            for (uint32_t i = 0; i < cnt; ++i) {
+                const uint32_t fi = __shfl_sync(0xFFFFFFFFu, f, i), ei = __shfl_sync(0xFFFFFFFFu, e, i);
+                if (j >= fi && j < ei && j < j1) slot = (int)i;
+            }
+            for (uint32_t t = tid; t < cnt * 216u; t += kG2pThreads) {
+                const uint32_t i = t / 216u;
+                halo[t] = halo_node(P, b0 + done + i, t - 216u * i);
+            }
+            __syncthreads();
+            if (slot >= 0 && pid != NONE) {
+                const uint32_t b = b0 + done + (uint32_t)slot;
+                const int3 key_off = prm.scene_blocks ? scene_base_of_block(prm, P.bvid[b]) : make_int3(0, 0, 0);
+                g2p_particle(P, prm, halo + 216u * (uint32_t)slot, pid, reorder ? j : pid, xm, vf, key_off, cx,
+                             stash);
+            }
+            __syncthreads();
+            done += cnt;
+            if (!more || cnt == 0u) break;
         }
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0) P.counters->codes_valid = 1u;
+    g2p_finish(P, prm);
 }
+#endif
 
 }  // namespace
 
@@ -549,6 +638,12 @@ void launch_grid_update(const DevPtrs& P, const LaunchCfg& c, cudaStream_t s) {
 }
 
 void launch_g2p_update(const DevPtrs& P, const LaunchCfg& c, cudaStream_t s) {
+#if NXM_FAST && !NXM_CPIC && !defined(NXM_G2P_PER_BLOCK)
+    if (P.chunk_blk) {
+        k_g2p_range<<<c.sm_count * NXM_G2P_MIN_CTAS, kG2pThreads, 0, s>>>(P);
+        return;
+    }
+#endif
     k_g2p_update<<<c.sm_count * NXM_G2P_MIN_CTAS, kG2pThreads, 0, s>>>(P);
 }
 

@@ -110,6 +110,30 @@ def test_elastic_cube_100_steps(pipe, deterministic):
     assert rel_l2(g["def_grad"], o["def_grad"]) < (1e-6 if deterministic else 1e-4)
 
 
+def test_sparse_blocks_fast_matches_oracle(pipe):
+    """Particles scattered about two per block: each 256-position run of the
+    fast G2P spans far more blocks than the four it stages at once, so it
+    takes many passes; mixed with a dense cube (runs of one or two blocks)."""
+    from nexus_b200.models import BoundaryCondition, ParticleModel
+    from nexus_b200.particles import ParticleBatch, box_walls, collider_array
+    rng = np.random.default_rng(12)
+    dx = 1.0 / 64.0
+    model = ParticleModel.elastic_neo_hookean(1.0e5, 0.3)
+    sparse = ParticleBatch.from_positions(rng.uniform(0.15, 0.85, (3000, 3)), np.float32(dx / 4), 1000.0, model)
+    sparse.vel = rng.normal(0.0, 0.5, (3000, 3)).astype(np.float32)
+    dense = scenes.elastic_cube(n_side=16).particles
+    batch = ParticleBatch.concat([sparse, dense])
+    cols = collider_array(box_walls(0.0, 1.0, BoundaryCondition.slip(), BoundaryCondition.slip()))
+    sc = scenes.Scene("sparse_blocks", dx, 1.0e-4, (0.0, 0.0, -9.81), batch, cols, 30, 16384)
+    g, o, o64 = _run_both(sc, False, 30)
+    err32 = rel_l2(g["pos"], o["pos"])
+    print(f"sparse blocks, fast: rel L2 vs f32 {err32:.3e}, vs f64 {rel_l2(g['pos'], o64):.3e}")
+    assert np.array_equal(g["enabled"], o["enabled"])
+    assert err32 < FAST_TOL
+    assert rel_l2(g["vel"], o["vel"]) < 1e-2
+    assert rel_l2(g["def_grad"], o["def_grad"]) < 1e-4
+
+
 @pytest.mark.parametrize("deterministic", [False, True])
 def test_every_material_50_steps(pipe, deterministic):
     sc = scenes.mixed_materials(n_side=10)
