@@ -102,7 +102,7 @@ void launch_sort(const DevPtrs& P, const LaunchCfg& c, bool with_extras, bool ca
 constexpr int kRigidSortLaunches = 5;
 void launch_p2g(const DevPtrs& P, const LaunchCfg& c, cudaStream_t s);
 void launch_grid_update(const DevPtrs& P, const LaunchCfg& c, cudaStream_t s);
-void launch_g2p_update(const DevPtrs& P, const LaunchCfg& c, cudaStream_t s);
+int launch_g2p_update(const DevPtrs& P, const LaunchCfg& c, cudaStream_t s);  // returns the kernels issued
 void launch_colliders_end(const DevPtrs& P, cudaStream_t s);
 }  // namespace fast
 
@@ -118,7 +118,7 @@ void launch_g2p_cdf(const DevPtrs& P, const LaunchCfg& c, cudaStream_t s);
 void launch_rigid_transform(const DevPtrs& P, const LaunchCfg& c, cudaStream_t s);
 void launch_p2g_cdf(const DevPtrs& P, const LaunchCfg& c, cudaStream_t s);
 void launch_grid_update(const DevPtrs& P, const LaunchCfg& c, cudaStream_t s);
-void launch_g2p_update(const DevPtrs& P, const LaunchCfg& c, cudaStream_t s);
+int launch_g2p_update(const DevPtrs& P, const LaunchCfg& c, cudaStream_t s);  // returns the kernels issued
 }  // namespace exact
 
 // Render data (prep_readback.rs): the particle records, the slot -> id map of
@@ -158,6 +158,5 @@ constexpr int kSortPositionsLaunches = 8;
 int sort_launches(bool canonical);
 constexpr int kP2gLaunches = 1;
 constexpr int kGridLaunches = 1;
-constexpr int kG2pLaunches = 1;
 
 }  // namespace nxm

@@ -921,9 +921,7 @@ int enqueue_step(nxm_state* s, cudaStream_t st, cudaEvent_t* ev /* 5 events or n
     else fast::launch_grid_update(P, c, st);
     k += kGridLaunches;
     if (ev) cudaEventRecord(ev[3], st);
-    if (exact_path) exact::launch_g2p_update(P, c, st);
-    else fast::launch_g2p_update(P, c, st);
-    k += kG2pLaunches;
+    k += exact_path ? exact::launch_g2p_update(P, c, st) : fast::launch_g2p_update(P, c, st);
     if (has_col) { fast::launch_colliders_end(P, st); ++k; }
     if (ev) cudaEventRecord(ev[4], st);
     return k;

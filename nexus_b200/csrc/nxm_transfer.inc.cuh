@@ -458,19 +458,28 @@ __device__ __forceinline__ void g2p_finish(const DevPtrs& P, const Params& prm) 
 #ifndef NXM_G2P_STASH
 #define NXM_G2P_STASH 1  // m A waits in shared memory across the model update (fast build)
 #endif
-__global__ void __launch_bounds__(kG2pThreads, NXM_G2P_MIN_CTAS) k_g2p_update(DevPtrs P) {
-    __shared__ float4 halo[216];
-#if NXM_G2P_STASH
-    __shared__ float stash_mem[9 * kG2pThreads];
-    volatile float* stash = NXM_FAST ? stash_mem + threadIdx.x : nullptr;
-#else
-    volatile float* stash = nullptr;
+// Below kRangeMinFill particles a block on average, a run of the fast G2P
+// (k_g2p_range) would span more blocks than one pass stages: such a launch
+// (decided on the device from this step's counts, the same in every CTA)
+// runs the per-block loop, where the blocks of a small sparse scene are
+// side by side on many CTAs instead of passes in a row on a few.
+#ifndef NXM_RANGE_MIN_FILL
+#define NXM_RANGE_MIN_FILL 64
 #endif
-#if NXM_CPIC
-    __shared__ float4 halo_inc[216];
-    __shared__ uint2 halo_cdf[216];
-#endif
-    const Params prm = *P.params;
+constexpr uint32_t kRangeMinFill = NXM_RANGE_MIN_FILL;
+__device__ __forceinline__ bool g2p_sparse(const DevPtrs& P, const Params& prm) {
+    const uint32_t nbp = min(__ldcg(&P.counters->num_primary), __ldcg(&P.counters->num_blocks));
+    const uint32_t len = min(__ldcg(&P.counters->sorted_len), prm.n);
+    return (uint64_t)len < (uint64_t)kRangeMinFill * nbp;
+}
+
+// The per-block loop: one CTA per primary block (grid-stride), halo of 216
+// nodes in `halo` (CPIC: the incompatible fields and node distance field in
+// halo_inc / halo_cdf).
+__device__ __forceinline__ void g2p_block_loop(const DevPtrs& P, const Params& prm, float4* halo, float4* halo_inc,
+                                               uint2* halo_cdf, volatile float* stash) {
+    (void)halo_inc;
+    (void)halo_cdf;
     const uint32_t nbp = min(__ldcg(&P.counters->num_primary), __ldcg(&P.counters->num_blocks));
     const uint32_t tid = threadIdx.x;
     const uint32_t ht = tid < 216u ? tid : 0u;  // halo node of this thread
@@ -547,6 +556,25 @@ __global__ void __launch_bounds__(kG2pThreads, NXM_G2P_MIN_CTAS) k_g2p_update(De
         first = nfirst;
         np = nnp;
     }
+}
+
+__global__ void __launch_bounds__(kG2pThreads, NXM_G2P_MIN_CTAS) k_g2p_update(DevPtrs P) {
+    __shared__ float4 halo[216];
+#if NXM_G2P_STASH
+    __shared__ float stash_mem[9 * kG2pThreads];
+    volatile float* stash = NXM_FAST ? stash_mem + threadIdx.x : nullptr;
+#else
+    volatile float* stash = nullptr;
+#endif
+#if NXM_CPIC
+    __shared__ float4 halo_inc[216];
+    __shared__ uint2 halo_cdf[216];
+#else
+    float4* halo_inc = nullptr;
+    uint2* halo_cdf = nullptr;
+#endif
+    const Params prm = *P.params;
+    g2p_block_loop(P, prm, halo, halo_inc, halo_cdf, stash);
     g2p_finish(P, prm);
 }
 
@@ -555,16 +583,22 @@ __global__ void __launch_bounds__(kG2pThreads, NXM_G2P_MIN_CTAS) k_g2p_update(De
 // positions, one particle per thread, instead of one CTA per block: a block
 // holds some 1-600 particles, so per-block rounds of 256 threads run part
 // empty (three quarters full on a settled scene); a run fills every thread
-// but one run's worth at the end.  A run spans the tail of one block and the
-// head of the next (a few more where blocks are small): the halos of up to
-// kRangeHalos of its blocks are staged at a time, in passes if it spans more.
-// The run's first block comes from the scan (chunk_blk); the blocks after it
-// are found from the nondecreasing `first` (primary particles of block b sit
-// at sorted positions [first[b], first[b] + nprim[b]); the fast path lists no
-// extras, so the positions [0, sorted_len) are exactly the primary particles).
-constexpr uint32_t kRangeHalos = 4;
+// but one run's worth at the end.  The fast path lists no extras, so the
+// positions [0, sorted_len) are exactly the primary particles, block after
+// block; run c spans the blocks [chunk_blk[c], chunk_blk[c + 1]] (the scan
+// records the block of each run's first position; the last run reaches the
+// last primary block), usually one or two.  Their halos are staged
+// kRangeHalos at a time, and each thread takes its particle's block from the
+// header id the sort's count pass stored for it (phdr).  A run's span is
+// loaded one run ahead, so that a run's own loads (ids, records, halos) are
+// issued together.
+//
+// A launch over sparse blocks (g2p_sparse) takes one block per unit instead
+// (its particles in rounds of 256), through the same loop: a unit is a span
+// of blocks whose halos are staged in passes and a range of sorted positions
+// the threads step through, so the particle update has one call site.
+constexpr uint32_t kRangeHalos = 8;
 static_assert(kG2pThreads == kRangeChunk, "one sorted position per thread");
-static_assert(kRangeHalos < 32u, "one lane per staged block, plus one");
 __global__ void __launch_bounds__(kG2pThreads, NXM_G2P_MIN_CTAS) k_g2p_range(DevPtrs P) {
     __shared__ float4 halo[kRangeHalos * 216];
 #if NXM_G2P_STASH
@@ -576,56 +610,73 @@ __global__ void __launch_bounds__(kG2pThreads, NXM_G2P_MIN_CTAS) k_g2p_range(Dev
     const Params prm = *P.params;
     const uint32_t nbp = min(__ldcg(&P.counters->num_primary), __ldcg(&P.counters->num_blocks));
     const uint32_t len = min(__ldcg(&P.counters->sorted_len), prm.n);
-    const uint32_t nchunks = min((len + kRangeChunk - 1u) / kRangeChunk, P.chunk_cap);
-    const uint32_t tid = threadIdx.x, lane = tid & 31u;
+    const bool sparse = g2p_sparse(P, prm);
+    const uint32_t nunits = !nbp ? 0u : (sparse ? nbp : min((len + kRangeChunk - 1u) / kRangeChunk, P.chunk_cap));
+    const uint32_t tid = threadIdx.x;
     const bool reorder = P.pid_in != nullptr;
     const CpicCtx cx{nullptr, nullptr, P.colliders, 0u};
-    for (uint32_t c = blockIdx.x; c < nchunks; c += gridDim.x) {
-        const uint32_t j0 = c * kRangeChunk, j1 = min(j0 + kRangeChunk, len);
-        const uint32_t j = j0 + tid;
-        // this thread's particle, fetched while the halos load
-        const uint32_t pid = j < j1 ? __ldg(&P.sorted[j]) : NONE;
+    // unit u: blocks [lo, hi], sorted positions [p0, p1)
+    struct Unit {
+        uint32_t lo, hi, p0, p1;
+    };
+    auto unit_of = [&](uint32_t u) {
+        Unit w;
+        if (sparse) {
+            w.lo = w.hi = u;
+            w.p0 = __ldcg(&P.first[u]);
+            w.p1 = min(w.p0 + __ldcg(&P.nprim[u]), len);
+        } else {
+            w.lo = __ldcg(&P.chunk_blk[u]);
+            w.hi = min(u + 1u < nunits ? __ldcg(&P.chunk_blk[u + 1u]) : nbp - 1u, nbp - 1u);
+            w.p0 = u * kRangeChunk;
+            w.p1 = min(w.p0 + kRangeChunk, len);
+        }
+        return w;
+    };
+    uint32_t u = blockIdx.x;
+    Unit w{1u, 0u, 0u, 0u};
+    if (u < nunits) w = unit_of(u);
+    for (; u < nunits; u += gridDim.x) {
+        Unit wn{1u, 0u, 0u, 0u};
+        if (u + gridDim.x < nunits) wn = unit_of(u + gridDim.x);
+        // this thread's first particle, fetched while the halos load
+        uint32_t pid = w.p0 + tid < w.p1 ? __ldg(&P.sorted[w.p0 + tid]) : NONE;
         float4 xm = make_float4(0.f, 0.f, 0.f, 0.f), vf = xm;
+        uint32_t blk = w.lo;
         if (pid != NONE) {
             const float4* kr = reinterpret_cast<const float4*>(&P.kin[pid]);
             xm = kr[0];
             vf = kr[1];
+            if (!sparse) blk = __ldcg(&P.phdr[pid]);
         }
-        const uint32_t b0 = __ldg(&P.chunk_blk[c]);
-        for (uint32_t done = 0;;) {
-            // every warp finds the same blocks: lane i < kRangeHalos looks at
-            // block b0 + done + i, lane kRangeHalos at the one after them
-            const uint32_t bq = b0 + done + min(lane, kRangeHalos);
-            uint32_t f = NONE, e = 0u;
-            if (bq < nbp) {
-                f = __ldcg(&P.first[bq]);
-                e = f + __ldcg(&P.nprim[bq]);
-            }
-            const uint32_t m = __ballot_sync(0xFFFFFFFFu, lane <= kRangeHalos && bq < nbp && f < j1);
-            const uint32_t cnt = min((uint32_t)__popc(m & ((1u << kRangeHalos) - 1u)), kRangeHalos);
-            const bool more = (m >> kRangeHalos) & 1u;
-            if (cnt == 0u && done == 0u && tid == 0u) set_status(P.counters, STATUS_MISSING_BLOCK);  // not reached
-            // this thread's block among them (none: its block is in another pass)
-            int slot = -1;
-            for (uint32_t i = 0; i < cnt; ++i) {
-                const uint32_t fi = __shfl_sync(0xFFFFFFFFu, f, i), ei = __shfl_sync(0xFFFFFFFFu, e, i);
-                if (j >= fi && j < ei && j < j1) slot = (int)i;
-            }
+        uint32_t left = 0u;  // particles of this thread not yet updated
+        for (uint32_t p = w.p0 + tid; p < w.p1; p += kG2pThreads) ++left;
+        for (uint32_t b = w.lo; b <= w.hi; b += kRangeHalos) {
+            const uint32_t cnt = min(w.hi - b + 1u, kRangeHalos);
             for (uint32_t t = tid; t < cnt * 216u; t += kG2pThreads) {
                 const uint32_t i = t / 216u;
-                halo[t] = halo_node(P, b0 + done + i, t - 216u * i);
+                halo[t] = halo_node(P, b + i, t - 216u * i);
             }
             __syncthreads();
-            if (slot >= 0 && pid != NONE) {
-                const uint32_t b = b0 + done + (uint32_t)slot;
-                const int3 key_off = prm.scene_blocks ? scene_base_of_block(prm, P.bvid[b]) : make_int3(0, 0, 0);
-                g2p_particle(P, prm, halo + 216u * (uint32_t)slot, pid, reorder ? j : pid, xm, vf, key_off, cx,
-                             stash);
+            for (uint32_t p = w.p0 + tid; p < w.p1; p += kG2pThreads) {
+                if (p != w.p0 + tid) {  // later rounds of a sparse unit
+                    pid = __ldg(&P.sorted[p]);
+                    const float4* kr = reinterpret_cast<const float4*>(&P.kin[pid]);
+                    xm = kr[0];
+                    vf = kr[1];
+                }
+                if (blk >= b && blk - b < cnt) {
+                    const int3 key_off =
+                        prm.scene_blocks ? scene_base_of_block(prm, P.bvid[blk]) : make_int3(0, 0, 0);
+                    g2p_particle(P, prm, halo + 216u * (blk - b), pid, reorder ? p : pid, xm, vf, key_off, cx,
+                                 stash);
+                    --left;
+                }
             }
             __syncthreads();
-            done += cnt;
-            if (!more || cnt == 0u) break;
         }
+        if (left) set_status(P.counters, STATUS_MISSING_BLOCK);  // not reached: a unit holds its particles' blocks
+        w = wn;
     }
     g2p_finish(P, prm);
 }
@@ -637,14 +688,15 @@ void launch_grid_update(const DevPtrs& P, const LaunchCfg& c, cudaStream_t s) {
     k_grid_update<<<c.sm_count * 8, 256, 0, s>>>(P);
 }
 
-void launch_g2p_update(const DevPtrs& P, const LaunchCfg& c, cudaStream_t s) {
+int launch_g2p_update(const DevPtrs& P, const LaunchCfg& c, cudaStream_t s) {
 #if NXM_FAST && !NXM_CPIC && !defined(NXM_G2P_PER_BLOCK)
-    if (P.chunk_blk) {
+    if (P.chunk_blk) {  // runs of the sorted list, or one block per unit over sparse blocks
         k_g2p_range<<<c.sm_count * NXM_G2P_MIN_CTAS, kG2pThreads, 0, s>>>(P);
-        return;
+        return 1;
     }
 #endif
     k_g2p_update<<<c.sm_count * NXM_G2P_MIN_CTAS, kG2pThreads, 0, s>>>(P);
+    return 1;
 }
 
 }  // namespace NXM_NS
