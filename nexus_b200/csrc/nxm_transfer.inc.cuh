@@ -615,51 +615,54 @@ __global__ void __launch_bounds__(kG2pThreads, NXM_G2P_MIN_CTAS) k_g2p_range(Dev
     const uint32_t tid = threadIdx.x;
     const bool reorder = P.pid_in != nullptr;
     const CpicCtx cx{nullptr, nullptr, P.colliders, 0u};
-    // unit u: blocks [lo, hi], sorted positions [p0, p1)
-    struct Unit {
-        uint32_t lo, hi, p0, p1;
-    };
-    auto unit_of = [&](uint32_t u) {
-        Unit w;
+    // unit u: blocks [lo, hi], sorted positions [p0, p1), from two loaded
+    // words (dense: the run's first and last block; sparse: first, nprim of
+    // the block), loaded one unit ahead
+    auto words_of = [&](uint32_t u, uint32_t& a, uint32_t& b) {
         if (sparse) {
-            w.lo = w.hi = u;
-            w.p0 = __ldcg(&P.first[u]);
-            w.p1 = min(w.p0 + __ldcg(&P.nprim[u]), len);
+            a = __ldcg(&P.first[u]);
+            b = __ldcg(&P.nprim[u]);
         } else {
-            w.lo = __ldcg(&P.chunk_blk[u]);
-            w.hi = min(u + 1u < nunits ? __ldcg(&P.chunk_blk[u + 1u]) : nbp - 1u, nbp - 1u);
-            w.p0 = u * kRangeChunk;
-            w.p1 = min(w.p0 + kRangeChunk, len);
+            a = __ldcg(&P.chunk_blk[u]);
+            b = u + 1u < nunits ? __ldcg(&P.chunk_blk[u + 1u]) : nbp - 1u;
         }
-        return w;
     };
-    uint32_t u = blockIdx.x;
-    Unit w{1u, 0u, 0u, 0u};
-    if (u < nunits) w = unit_of(u);
+    uint32_t u = blockIdx.x, wa = 0u, wb = 0u;
+    if (u < nunits) words_of(u, wa, wb);
     for (; u < nunits; u += gridDim.x) {
-        Unit wn{1u, 0u, 0u, 0u};
-        if (u + gridDim.x < nunits) wn = unit_of(u + gridDim.x);
+        uint32_t lo, hi, p0, p1;
+        if (sparse) {
+            lo = hi = u;
+            p0 = wa;
+            p1 = min(wa + wb, len);
+        } else {
+            lo = wa;
+            hi = min(wb, nbp - 1u);
+            p0 = u * kRangeChunk;
+            p1 = min(p0 + kRangeChunk, len);
+        }
+        if (u + gridDim.x < nunits) words_of(u + gridDim.x, wa, wb);
         // this thread's first particle, fetched while the halos load
-        uint32_t pid = w.p0 + tid < w.p1 ? __ldg(&P.sorted[w.p0 + tid]) : NONE;
+        uint32_t pid = p0 + tid < p1 ? __ldg(&P.sorted[p0 + tid]) : NONE;
         float4 xm = make_float4(0.f, 0.f, 0.f, 0.f), vf = xm;
-        uint32_t blk = w.lo;
+        uint32_t blk = lo;
         if (pid != NONE) {
             const float4* kr = reinterpret_cast<const float4*>(&P.kin[pid]);
             xm = kr[0];
             vf = kr[1];
             if (!sparse) blk = __ldcg(&P.phdr[pid]);
         }
-        uint32_t left = 0u;  // particles of this thread not yet updated
-        for (uint32_t p = w.p0 + tid; p < w.p1; p += kG2pThreads) ++left;
-        for (uint32_t b = w.lo; b <= w.hi; b += kRangeHalos) {
-            const uint32_t cnt = min(w.hi - b + 1u, kRangeHalos);
+        bool pending = pid != NONE;  // dense: this thread's one particle not yet updated
+        for (uint32_t b = lo; b <= hi; b += kRangeHalos) {
+            const uint32_t cnt = min(hi - b + 1u, kRangeHalos);
             for (uint32_t t = tid; t < cnt * 216u; t += kG2pThreads) {
                 const uint32_t i = t / 216u;
                 halo[t] = halo_node(P, b + i, t - 216u * i);
             }
             __syncthreads();
-            for (uint32_t p = w.p0 + tid; p < w.p1; p += kG2pThreads) {
-                if (p != w.p0 + tid) {  // later rounds of a sparse unit
+            // dense: one position per thread; sparse: the block's positions in rounds
+            for (uint32_t p = p0 + tid; p < p1; p += kG2pThreads) {
+                if (p != p0 + tid) {
                     pid = __ldg(&P.sorted[p]);
                     const float4* kr = reinterpret_cast<const float4*>(&P.kin[pid]);
                     xm = kr[0];
@@ -670,13 +673,12 @@ __global__ void __launch_bounds__(kG2pThreads, NXM_G2P_MIN_CTAS) k_g2p_range(Dev
                         prm.scene_blocks ? scene_base_of_block(prm, P.bvid[blk]) : make_int3(0, 0, 0);
                     g2p_particle(P, prm, halo + 216u * (blk - b), pid, reorder ? p : pid, xm, vf, key_off, cx,
                                  stash);
-                    --left;
+                    pending = false;
                 }
             }
             __syncthreads();
         }
-        if (left) set_status(P.counters, STATUS_MISSING_BLOCK);  // not reached: a unit holds its particles' blocks
-        w = wn;
+        if (!sparse && pending) set_status(P.counters, STATUS_MISSING_BLOCK);  // not reached: a run holds its blocks
     }
     g2p_finish(P, prm);
 }
