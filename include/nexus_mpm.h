@@ -19,6 +19,7 @@
 #ifndef NEXUS_MPM_H
 #define NEXUS_MPM_H
 
+#include <stddef.h>
 #include <stdint.h>
 
 #if defined(__GNUC__)
@@ -458,6 +459,25 @@ NXM_API int nxm_state_status(nxm_state* state, uint32_t* bits, int clear);
  * never drains; 0 on the first call).  Each step's status reaches the host
  * one call late. */
 NXM_API int nxm_state_status_pipelined(nxm_state* state, uint32_t* bits);
+/* Tickets: nxm_state_fence marks the work queued on the state's stream so
+ * far; nxm_state_ticket_done tells (without waiting) whether that work has
+ * run, nxm_state_ticket_wait waits for it.  Tickets complete in the order
+ * they were taken.  They stand for the futures of the reference's async
+ * reads (below): done = the future is ready, wait = .await. */
+NXM_API int nxm_state_fence(nxm_state* state, uint64_t* ticket);
+NXM_API int nxm_state_ticket_done(nxm_state* state, uint64_t ticket, int* done);
+NXM_API int nxm_state_ticket_wait(nxm_state* state, uint64_t ticket);
+/* GpuParticles::read_positions (src_mpm/solver/particle.rs:634-648, an async
+ * read) for the ids [first, first + count): positions into `out` (count x 3
+ * floats) without waiting; `*ticket` completes when `out` holds them.  `out`
+ * must stay valid until then; with pinned memory (nxm_host_alloc) the copy
+ * queues behind the steps in flight, with pageable memory the call waits for
+ * them. */
+NXM_API int nxm_read_positions_range_async(nxm_state* state, uint32_t first, uint32_t count, float* out,
+                                           uint64_t* ticket);
+/* Pinned (page-locked) host memory for asynchronous reads and uploads. */
+NXM_API int nxm_host_alloc(size_t bytes, void** out);
+NXM_API void nxm_host_free(void* ptr);
 NXM_API const char* nxm_error_string(int code);
 
 /* The CUDA stream (cudaStream_t) every call on this state is ordered on,

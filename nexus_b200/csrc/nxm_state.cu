@@ -457,7 +457,13 @@ struct nxm_state {
     char* stg = nullptr;
     size_t stg_cap = 0, stg_head = 0;
     std::deque<StagingSpan> stg_live;
+    std::vector<char*> stg_retired;  // outgrown rings, freed once the stream has drained
     std::vector<cudaEvent_t> event_pool;
+
+    // stream-ordered tickets (nxm_state_fence): the events of tickets not yet
+    // known complete, oldest first; tickets up to done_ticket are complete
+    std::deque<std::pair<uint64_t, cudaEvent_t>> fences;
+    uint64_t next_ticket = 1, done_ticket = 0;
 
     // scratch for readback packing
     uint32_t* d_pack = nullptr;
@@ -554,28 +560,55 @@ cudaError_t take_event(nxm_state* s, cudaEvent_t* e) {
     return cudaEventCreateWithFlags(e, cudaEventDisableTiming);
 }
 
+// Frees the outgrown staging rings (their copies have all run: call only
+// with the stream drained).
+void free_retired_rings(nxm_state* s) {
+    for (char* r : s->stg_retired) cudaFreeHost(r);
+    s->stg_retired.clear();
+}
+
+// A new ring of at least `bytes` * 4 (twice the old one, 1 MB at least, up
+// to kRingMax).  The old ring is kept, not freed, until the stream drains:
+// its copies may still be queued behind other work, and the host does not
+// wait for them here.
+constexpr size_t kRingMax = size_t(1) << 30;
+cudaError_t staging_grow(nxm_state* s, size_t bytes) {
+    for (const auto& sp : s->stg_live) s->event_pool.push_back(sp.done);  // an event may be recorded again
+    s->stg_live.clear();
+    if (s->stg) s->stg_retired.push_back(s->stg);
+    s->stg = nullptr;
+    const size_t cap = std::max({bytes * 4, std::min(s->stg_cap * 2, kRingMax), size_t(1) << 20});
+    s->stg_cap = 0;
+    s->stg_head = 0;
+    const cudaError_t e = cudaMallocHost(reinterpret_cast<void**>(&s->stg), cap);
+    if (e != cudaSuccess) {
+        s->stg = nullptr;
+        return e;
+    }
+    s->stg_cap = cap;
+    return cudaSuccess;
+}
+
 // A ring region of `bytes` (256-aligned) whose earlier copies have run.
 cudaError_t staging_reserve(nxm_state* s, size_t bytes, char** out) {
     bytes = (bytes + 255) & ~size_t(255);
-    if (bytes * 2 > s->stg_cap) {  // grow: every copy from the old ring has to be done
-        cudaError_t e = cudaStreamSynchronize(s->stream);
+    if (bytes * 2 > s->stg_cap) {
+        const cudaError_t e = staging_grow(s, bytes);
         if (e != cudaSuccess) return e;
-        for (const auto& sp : s->stg_live) s->event_pool.push_back(sp.done);
-        s->stg_live.clear();
-        if (s->stg) cudaFreeHost(s->stg);
-        s->stg = nullptr;
-        s->stg_cap = 0;
-        const size_t cap = std::max<size_t>(bytes * 4, size_t(1) << 20);
-        e = cudaMallocHost(reinterpret_cast<void**>(&s->stg), cap);
-        if (e != cudaSuccess) return e;
-        s->stg_cap = cap;
-        s->stg_head = 0;
     }
     if (s->stg_head + bytes > s->stg_cap) s->stg_head = 0;
-    const size_t lo = s->stg_head, hi = lo + bytes;
+    size_t lo = s->stg_head, hi = lo + bytes;
     int newest = -1;  // copies complete in stream order: waiting for the newest overlap covers the older
     for (size_t i = 0; i < s->stg_live.size(); ++i)
         if (s->stg_live[i].begin < hi && lo < s->stg_live[i].end) newest = (int)i;
+    if (newest >= 0 && s->stg_cap < kRingMax && cudaEventQuery(s->stg_live[newest].done) == cudaErrorNotReady) {
+        // that region is still queued behind other work: a larger ring instead of a wait
+        const cudaError_t e = staging_grow(s, bytes);
+        if (e != cudaSuccess) return e;
+        lo = 0;
+        hi = bytes;
+        newest = -1;
+    }
     if (newest >= 0) {
         cudaError_t e = cudaEventSynchronize(s->stg_live[newest].done);
         if (e != cudaSuccess) return e;
@@ -596,6 +629,26 @@ bool host_pinned(const void* p) {
     return a.type == cudaMemoryTypeHost;
 }
 
+// memcpy, split over host threads when large (one thread copies a few GB/s;
+// a big upload would otherwise keep the host from queueing work).
+void host_copy(void* dst, const void* src, size_t bytes) {
+    constexpr size_t kPerThread = size_t(4) << 20;
+    const unsigned hw = std::max(1u, std::min(8u, std::thread::hardware_concurrency()));
+    const unsigned nt = (unsigned)std::min<size_t>(hw, bytes / kPerThread);
+    if (nt <= 1) {
+        std::memcpy(dst, src, bytes);
+        return;
+    }
+    std::vector<std::thread> th;
+    const size_t per = (bytes / nt + 63) & ~size_t(63);
+    for (unsigned t = 0; t < nt; ++t) {
+        const size_t lo = std::min(bytes, per * t), hi = std::min(bytes, per * (t + 1));
+        if (lo < hi)
+            th.emplace_back([=] { std::memcpy(static_cast<char*>(dst) + lo, static_cast<const char*>(src) + lo, hi - lo); });
+    }
+    for (auto& x : th) x.join();
+}
+
 // Copies `bytes` of host data to `dst` in stream order; the caller's buffer
 // is free when the call returns and the host never waits for queued work.
 cudaError_t upload_async(nxm_state* s, void* dst, const void* src, size_t bytes) {
@@ -603,7 +656,7 @@ cudaError_t upload_async(nxm_state* s, void* dst, const void* src, size_t bytes)
     char* h = nullptr;
     cudaError_t e = staging_reserve(s, bytes, &h);
     if (e != cudaSuccess) return e;
-    std::memcpy(h, src, bytes);
+    host_copy(h, src, bytes);
     e = cudaMemcpyAsync(dst, h, bytes, cudaMemcpyHostToDevice, s->stream);
     if (e != cudaSuccess) return e;
     cudaEvent_t done;
@@ -982,18 +1035,21 @@ void finish_step(nxm_state* s) {
 
 // Fields of particles [first, first + count) (ids), in id order, into `out`.
 int pack_read_range(nxm_state* s, const void* records, uint32_t stride_bytes, const int* offsets, int nfields,
-                    uint32_t first, uint32_t count, void* out) {
+                    uint32_t first, uint32_t count, void* out, bool wait = true) {
     if (!out) return NXM_E_INVALID;
     if (first > s->n || count > s->n - first) return NXM_E_INVALID;
     if (count == 0) return NXM_OK;
     const size_t words = (size_t)count * nfields;
-    if (words > s->pack_cap) {
-        dfree(s->d_pack);
-        NXM_TRY(dalloc(&s->d_pack, words));
-        s->pack_cap = words;
+    if (words > s->pack_cap) {  // stream-ordered: queued reads of the old scratch finish first
+        const size_t cap = std::max(words, s->pack_cap * 2);
+        if (s->d_pack) NXM_TRY(cudaFreeAsync(s->d_pack, s->stream));
+        s->d_pack = nullptr;
+        s->pack_cap = 0;
+        NXM_TRY(cudaMallocAsync(reinterpret_cast<void**>(&s->d_pack), cap * 4, s->stream));
+        s->pack_cap = cap;
     }
     if (!s->d_offsets) NXM_TRY(dalloc(&s->d_offsets, 32));
-    NXM_TRY(cudaMemcpyAsync(s->d_offsets, offsets, sizeof(int) * nfields, cudaMemcpyHostToDevice, s->stream));
+    NXM_TRY(upload_async(s, s->d_offsets, offsets, sizeof(int) * nfields));
     const size_t threads = (s->permuted ? (size_t)s->n : (size_t)count) * nfields;
     int grid = (int)std::min<size_t>((threads + 255) / 256, (size_t)s->sm_count * 8);
     if (grid < 1) grid = 1;
@@ -1007,7 +1063,7 @@ int pack_read_range(nxm_state* s, const void* records, uint32_t stride_bytes, co
     s->launches += 1;
     NXM_TRY(cudaGetLastError());
     NXM_TRY(cudaMemcpyAsync(out, s->d_pack, words * 4, cudaMemcpyDeviceToHost, s->stream));
-    NXM_TRY(cudaStreamSynchronize(s->stream));
+    if (wait) NXM_TRY(cudaStreamSynchronize(s->stream));
     return NXM_OK;
 }
 
@@ -1037,12 +1093,14 @@ int remove_id_ranges(nxm_state* s, std::vector<uint2> ranges) {
         removed += rr[i].y - rr[i].x;
     }
     const uint32_t n0 = s->n, ntiles = (n0 + 1023u) / 1024u;
-    uint2* d_r = nullptr;
-    uint32_t* d_cum = nullptr;
-    cudaError_t e = dalloc(&d_r, rr.size());
-    if (e == cudaSuccess) e = dalloc(&d_cum, cum.size());
-    if (e == cudaSuccess) e = cudaMemcpyAsync(d_r, rr.data(), sizeof(uint2) * rr.size(), cudaMemcpyHostToDevice, s->stream);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(d_cum, cum.data(), 4 * cum.size(), cudaMemcpyHostToDevice, s->stream);
+    // stream-ordered scratch and staged uploads: the removal queues behind the
+    // steps in flight without waiting for them
+    char* scratch = nullptr;
+    cudaError_t e = cudaMallocAsync(reinterpret_cast<void**>(&scratch), 16 * rr.size() + 16, s->stream);
+    uint2* d_r = reinterpret_cast<uint2*>(scratch);
+    uint32_t* d_cum = reinterpret_cast<uint32_t*>(scratch + 8 * rr.size());
+    if (e == cudaSuccess) e = upload_async(s, d_r, rr.data(), sizeof(uint2) * rr.size());
+    if (e == cudaSuccess) e = upload_async(s, d_cum, cum.data(), 4 * cum.size());
     const uint32_t* pid = s->permuted ? s->pid : nullptr;
     const uint32_t nr = (uint32_t)rr.size();
     if (e == cudaSuccess) {
@@ -1060,9 +1118,7 @@ int remove_id_ranges(nxm_state* s, std::vector<uint2> ranges) {
         s->launches += 1;
         e = cudaGetLastError();
     }
-    if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
-    if (d_r) cudaFree(d_r);
-    if (d_cum) cudaFree(d_cum);
+    if (scratch) cudaFreeAsync(scratch, s->stream);
     NXM_TRY(e);
     swap_buffers(s);  // the compacted records (and, when permuted, their ids) are current
     if (s->scene_blocks) std::swap(s->d_pscene, s->d_pscene_alt);
@@ -1739,7 +1795,9 @@ void nxm_state_destroy(nxm_state* s) {
     if (s->h_vel6) cudaFreeHost(s->h_vel6);
     if (s->h_status) cudaFreeHost(s->h_status);
     if (s->stg) cudaFreeHost(s->stg);
+    free_retired_rings(s);
     for (const auto& sp : s->stg_live) cudaEventDestroy(sp.done);
+    for (const auto& f : s->fences) cudaEventDestroy(f.second);
     for (cudaEvent_t e : s->event_pool) cudaEventDestroy(e);
     for (cudaEvent_t e : s->vel_done)
         if (e) cudaEventDestroy(e);
@@ -2100,12 +2158,44 @@ int nxm_scene_add(nxm_state* s, const nxm_particles_soa* particles, uint32_t cou
         int rc = collider_from_abi(colliders[i], tri_vertices, num_triangles, 0, d);
         if (rc) return rc;
     }
-    // every particle's block (and its +1 neighbours) must stay inside the scene's key region
+    // every particle's block (and its +1 neighbours) must stay inside the scene's
+    // key region: the floor of a coordinate / block width grows with the
+    // coordinate, so the extremes (and no NaN) decide it; found on host threads
     const float bw = 4.0f * s->dx;
     const int M = s->scene_margin, S = (int)s->scene_blocks;
-    for (size_t i = 0; i < 3 * (size_t)count; ++i) {
-        const float b = std::floor(particles->position[i] / bw);
-        if (!(b >= (float)(1 - M) && b <= (float)(S - M - 3))) return NXM_E_INVALID;
+    if (count) {
+        const float* x = particles->position;
+        const size_t total = 3 * (size_t)count;
+        const unsigned hw = std::max(1u, std::min(8u, std::thread::hardware_concurrency()));
+        const unsigned nt = total < (size_t(1) << 18) ? 1u : hw;
+        std::vector<std::array<float, 7>> ext(nt);  // per thread: min xyz, max xyz, NaN seen
+        auto scan = [&](unsigned t) {
+            std::array<float, 7> e{INFINITY, INFINITY, INFINITY, -INFINITY, -INFINITY, -INFINITY, 0.f};
+            const size_t lo = count * (size_t)t / nt, hi = count * (size_t)(t + 1) / nt;
+            for (size_t i = lo; i < hi; ++i)
+                for (int a = 0; a < 3; ++a) {
+                    const float v = x[3 * i + a];
+                    if (v != v) e[6] = 1.f;
+                    e[a] = std::min(e[a], v);
+                    e[3 + a] = std::max(e[3 + a], v);
+                }
+            ext[t] = e;
+        };
+        if (nt == 1) {
+            scan(0);
+        } else {
+            std::vector<std::thread> th;
+            for (unsigned t = 0; t < nt; ++t) th.emplace_back(scan, t);
+            for (auto& t : th) t.join();
+        }
+        for (const auto& e : ext) {
+            if (e[6] != 0.f) return NXM_E_INVALID;
+            for (int a = 0; a < 3; ++a) {
+                if (e[a] > e[3 + a]) continue;  // this thread saw no particle
+                const float blo = std::floor(e[a] / bw), bhi = std::floor(e[3 + a] / bw);
+                if (!(blo >= (float)(1 - M) && bhi <= (float)(S - M - 3))) return NXM_E_INVALID;
+            }
+        }
     }
     uint32_t slot = 0;
     while (slot < s->scenes.size() && s->scenes[slot].live) ++slot;
@@ -2432,6 +2522,7 @@ int nxm_simulate_frame(nxm_pipeline* pipeline, nxm_state* s, uint32_t min_subste
 int nxm_synchronize(nxm_state* s) {
     if (!s) return NXM_E_INVALID;
     NXM_TRY(cudaStreamSynchronize(s->stream));
+    free_retired_rings(s);
     uint32_t bits = 0;
     int rc = nxm_state_status(s, &bits, 0);
     if (rc) return rc;
@@ -2461,6 +2552,83 @@ int nxm_state_status_pipelined(nxm_state* s, uint32_t* bits) {
     }
     ++s->status_calls;
     return NXM_OK;
+}
+
+// ---- tickets ----------------------------------------------------------------
+//
+// A ticket marks the work queued on the state's stream so far; tickets
+// complete in the order they were taken (one stream).
+
+namespace {
+
+// Retires the oldest fences: those already complete, and (wait) every one up
+// to `upto`, waiting for it.
+int retire_fences(nxm_state* s, uint64_t upto, bool wait) {
+    while (!s->fences.empty()) {
+        auto [t, e] = s->fences.front();
+        if (wait && t <= upto) {
+            NXM_TRY(cudaEventSynchronize(e));
+        } else {
+            const cudaError_t q = cudaEventQuery(e);
+            if (q == cudaErrorNotReady) break;
+            NXM_TRY(q);
+        }
+        s->done_ticket = t;
+        s->event_pool.push_back(e);
+        s->fences.pop_front();
+    }
+    return NXM_OK;
+}
+
+}  // namespace
+
+int nxm_state_fence(nxm_state* s, uint64_t* ticket) {
+    if (!s || !ticket) return NXM_E_INVALID;
+    cudaEvent_t e;
+    NXM_TRY(take_event(s, &e));
+    NXM_TRY(cudaEventRecord(e, s->stream));
+    s->fences.emplace_back(s->next_ticket, e);
+    *ticket = s->next_ticket++;
+    int rc = retire_fences(s, 0, false);
+    // a caller that never asks keeps at most 1024 events: wait for the oldest
+    while (!rc && s->fences.size() > 1024u) rc = retire_fences(s, s->fences.front().first, true);
+    return rc;
+}
+
+int nxm_state_ticket_done(nxm_state* s, uint64_t ticket, int* done) {
+    if (!s || !done || ticket == 0 || ticket >= s->next_ticket) return NXM_E_INVALID;
+    const int rc = retire_fences(s, 0, false);
+    *done = ticket <= s->done_ticket;
+    return rc;
+}
+
+int nxm_state_ticket_wait(nxm_state* s, uint64_t ticket) {
+    if (!s || ticket == 0 || ticket >= s->next_ticket) return NXM_E_INVALID;
+    return retire_fences(s, ticket, true);
+}
+
+int nxm_read_positions_range_async(nxm_state* s, uint32_t first, uint32_t count, float* out, uint64_t* ticket) {
+    if (!s || !ticket) return NXM_E_INVALID;
+    static const int off[3] = {0, 1, 2};
+    const int rc = pack_read_range(s, s->kin, sizeof(PKin), off, 3, first, count, out, /*wait=*/false);
+    if (rc) return rc;
+    return nxm_state_fence(s, ticket);
+}
+
+int nxm_host_alloc(size_t bytes, void** out) {
+    if (!out) return NXM_E_INVALID;
+    *out = nullptr;
+    const cudaError_t e = cudaMallocHost(out, std::max<size_t>(bytes, 1));
+    if (e != cudaSuccess) {
+        (void)cudaGetLastError();
+        *out = nullptr;
+        return e == cudaErrorMemoryAllocation ? NXM_E_OOM : NXM_E_CUDA;
+    }
+    return NXM_OK;
+}
+
+void nxm_host_free(void* p) {
+    if (p) cudaFreeHost(p);
 }
 
 int nxm_state_status(nxm_state* s, uint32_t* bits, int clear) {

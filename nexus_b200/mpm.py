@@ -98,6 +98,12 @@ SIGNATURES = {
     "nxm_read_cdf": (C.c_int, [_vp, _f]),
     "nxm_simulate_frame": (C.c_int, [_vp, _vp, C.c_uint32, C.c_uint32, _u]),
     "nxm_state_status_pipelined": (C.c_int, [_vp, _u]),
+    "nxm_state_fence": (C.c_int, [_vp, C.POINTER(C.c_uint64)]),
+    "nxm_state_ticket_done": (C.c_int, [_vp, C.c_uint64, C.POINTER(C.c_int)]),
+    "nxm_state_ticket_wait": (C.c_int, [_vp, C.c_uint64]),
+    "nxm_read_positions_range_async": (C.c_int, [_vp, C.c_uint32, C.c_uint32, _f, C.POINTER(C.c_uint64)]),
+    "nxm_host_alloc": (C.c_int, [C.c_size_t, _pp]),
+    "nxm_host_free": (None, [_vp]),
     "nxm_state_num_rigid_particles": (C.c_int, [_vp, _u]),
     "nxm_read_rigid_particles": (C.c_int, [_vp, _f]),
     "nxm_prep_readback": (C.c_int, [_vp, C.c_uint32, _f, C.c_uint32, _f]),
@@ -160,6 +166,31 @@ def _check(rc: int, what: str):
 
 def _p(a, t=_f):
     return a.ctypes.data_as(t)
+
+
+class PinnedArray:
+    """Page-locked host memory (nxm_host_alloc) seen as a numpy array
+    (``.array``); freed with the object, so keep it while a copy may still
+    write into it."""
+
+    def __init__(self, shape, dtype=np.float32):
+        self.lib = load()
+        count = int(np.prod(shape))
+        nbytes = max(count * np.dtype(dtype).itemsize, 1)
+        ptr = C.c_void_p()
+        _check(self.lib.nxm_host_alloc(nbytes, C.byref(ptr)), "host_alloc")
+        self.ptr = ptr
+        buf = (C.c_char * nbytes).from_address(ptr.value)
+        self.array = np.frombuffer(buf, dtype=dtype, count=count).reshape(shape)
+
+    def close(self):
+        if getattr(self, "ptr", None) is not None and self.ptr.value:
+            self.array = None
+            self.lib.nxm_host_free(self.ptr)
+            self.ptr = None
+
+    def __del__(self):
+        self.close()
 
 
 class MpmPipeline:
@@ -318,6 +349,34 @@ class MpmState:
 
     def read_scene_positions(self, scene: int) -> np.ndarray:
         return self.read_positions_range(*self.scene_range(scene))
+
+    # -- asynchronous reads and tickets --------------------------------------------
+    def fence(self) -> int:
+        """A ticket for the work queued on the state's stream so far."""
+        t = C.c_uint64()
+        _check(self.lib.nxm_state_fence(self.h, C.byref(t)), "state_fence")
+        return t.value
+
+    def ticket_done(self, ticket: int) -> bool:
+        d = C.c_int()
+        _check(self.lib.nxm_state_ticket_done(self.h, ticket, C.byref(d)), "state_ticket_done")
+        return bool(d.value)
+
+    def ticket_wait(self, ticket: int):
+        _check(self.lib.nxm_state_ticket_wait(self.h, ticket), "state_ticket_wait")
+
+    def read_positions_range_async(self, first: int, count: int, out: np.ndarray) -> int:
+        """``GpuParticles::read_positions`` as an async read: positions of ids
+        [first, first + count) into ``out`` ((count, 3) float32, best pinned:
+        ``PinnedArray``); returns the ticket after which ``out`` holds them."""
+        assert out.dtype == np.float32 and out.shape == (count, 3) and out.flags.c_contiguous
+        t = C.c_uint64()
+        _check(self.lib.nxm_read_positions_range_async(self.h, first, count, _p(out, _f), C.byref(t)),
+               "read_positions_range_async")
+        return t.value
+
+    def read_scene_positions_async(self, scene: int, out: np.ndarray) -> int:
+        return self.read_positions_range_async(*self.scene_range(scene), out)
 
     # -- particle chunks (NexusState, src/state.rs:665-774) ------------------------
     def add_chunk(self, batch: ParticleBatch) -> int:

@@ -9,6 +9,11 @@ state with batched scenes).  When a scene has taken its step budget, its
 particles are read back and the scene is removed, freeing memory for the next
 arrivals.  Scenes that arrive while others run start on the next step.
 
+The host never drains the GPU: a finished scene's positions are read
+asynchronously into pinned memory and its slot is freed at once (both queue
+behind the steps in flight), and its result is collected when the read's
+ticket completes; each batched state keeps at most a few steps queued ahead.
+
 Each scene steps exactly as it would alone (scene-local coordinates, its own
 block-key region and colliders), so a result does not depend on what else was
 in the mix or on when it was admitted.
@@ -16,11 +21,12 @@ in the mix or on when it was admitted.
 from __future__ import annotations
 
 import time
+from collections import deque
 from dataclasses import dataclass, field
 
 import numpy as np
 
-from .mpm import MpmPipeline, MpmState
+from .mpm import MpmPipeline, MpmState, PinnedArray
 from .scenes import Scene
 
 # Estimated device bytes per particle of a batched state: two copies of the
@@ -72,6 +78,7 @@ class _Group:
         self.active = {}  # slot -> [request, remaining steps, admitted time]
         self.particles = 0
         self.grid = 0
+        self.steps = deque()  # tickets of the steps queued on this state
 
 
 class MpmServer:
@@ -89,6 +96,15 @@ class MpmServer:
         self.in_use = 0
         self.steps_taken = 0
         self.particle_steps = 0
+        self._pinned = {}  # capacity (particles) -> free pinned result buffers
+
+    def _buffer(self, n: int) -> PinnedArray:
+        cap = 1 << max(int(n) - 1, 0).bit_length()
+        free = self._pinned.get(cap)
+        return free.pop() if free else PinnedArray((cap, 3))
+
+    def _release(self, buf: PinnedArray):
+        self._pinned.setdefault(buf.array.shape[0], []).append(buf)
 
     def _group(self, sc: Scene) -> _Group:
         key = (float(sc.dx), float(sc.dt), tuple(float(g) for g in sc.gravity))
@@ -108,13 +124,15 @@ class MpmServer:
         return (self.in_use + footprint(sc) <= self.budget and g.particles + sc.n <= self.particles_capacity
                 and g.grid + sc.grid_capacity <= self.grid_capacity)
 
-    def run(self, requests, clock=time.perf_counter, idle_sleep: float = 1e-4):
+    def run(self, requests, clock=time.perf_counter, idle_sleep: float = 1e-4, depth: int = 32):
         """Serves ``requests`` (any order; by arrival) and returns the results by
-        request id, plus requests that can never fit (rejected)."""
+        request id, plus requests that can never fit (rejected).  ``depth``:
+        steps each batched state may have queued ahead of the GPU."""
         pending = sorted(requests, key=lambda r: (r.arrival, r.rid))
         results, rejected = {}, []
+        reads = deque()  # (group, ticket, request, admitted time, pinned buffer), in issue order per state
         t0 = clock()
-        while pending or any(g.active for g in self.groups.values()):
+        while pending or reads or any(g.active for g in self.groups.values()):
             now = clock() - t0
             # admission, first come first served
             while pending and pending[0].arrival <= now:
@@ -132,13 +150,26 @@ class MpmServer:
                 g.particles += r.scene.n
                 g.grid += r.scene.grid_capacity
                 self.in_use += footprint(r.scene)
+            # results whose reads have landed
+            for _ in range(len(reads)):
+                g, ticket, r, admitted, buf = reads[0]
+                reads.rotate(-1)
+                if g.state.ticket_done(ticket):
+                    reads.pop()
+                    results[r.rid] = Result(r.rid, r.scene.n, r.steps, r.arrival, admitted, clock() - t0,
+                                            buf.array[:r.scene.n].copy())
+                    self._release(buf)
             busy = [g for g in self.groups.values() if g.active]
             if not busy:
-                if pending:
-                    time.sleep(min(idle_sleep, max(0.0, pending[0].arrival - (clock() - t0))))
+                if reads or pending:
+                    wait = idle_sleep if reads else max(0.0, pending[0].arrival - (clock() - t0))
+                    time.sleep(min(idle_sleep, wait))
                 continue
             for g in busy:
+                if len(g.steps) >= depth:  # keep at most `depth` steps queued on this state
+                    g.state.ticket_wait(g.steps.popleft())
                 self.pipe.step(g.state)
+                g.steps.append(g.state.fence())
                 self.steps_taken += 1
                 self.particle_steps += g.particles
             for g in busy:
@@ -149,9 +180,10 @@ class MpmServer:
                         done.append(slot)
                 for slot in done:
                     r, _, admitted = g.active.pop(slot)
-                    pos = g.state.read_scene_positions(slot)  # waits for the scene's last step
-                    results[r.rid] = Result(r.rid, r.scene.n, r.steps, r.arrival, admitted, clock() - t0, pos)
-                if done:
+                    buf = self._buffer(r.scene.n)
+                    ticket = g.state.read_scene_positions_async(slot, buf.array[:r.scene.n])
+                    reads.append((g, ticket, r, admitted, buf))
+                if done:  # queued behind the reads above
                     g.state.remove_scenes(done)
                     g.particles = sum(rec[0].scene.n for rec in g.active.values())
                     g.grid = sum(rec[0].scene.grid_capacity for rec in g.active.values())
