@@ -46,10 +46,10 @@ UNIT = "particle-steps/s"
 # read; Drucker-Prager state, 3 floats, read and written for sand).
 B_ALG_ELASTIC = 204
 B_ALG_SAND = 228
-# DRAM bytes read + written per step by the two transfer kernels (79 % of the
+# DRAM bytes read + written per step by the two transfer kernels (75 % of the
 # step's kernel time) on the sand_water scene, from one ncu capture of the full
-# scene (k_p2g 180 MB + k_g2p_update 601 MB; the sort and grid kernels are not included).
-TRAFFIC_PER_STEP = 174.2e6 + 6.1e6 + 322.1e6 + 279.0e6
+# scene (k_p2g 180 MB + k_g2p_range 590 MB; the sort and grid kernels are not included).
+TRAFFIC_PER_STEP = 174.2e6 + 5.6e6 + 322.0e6 + 267.5e6
 
 
 def b_alg_per_particle(model_tags: np.ndarray) -> float:
@@ -532,7 +532,7 @@ def main():
     ap.add_argument("--coupled-steps", type=int, default=50, help="timed steps of the coupled mix (0: skip it)")
     ap.add_argument("--coupled-scenes", type=int, default=64)
     ap.add_argument("--traffic", type=float, default=TRAFFIC_PER_STEP,
-                    help="DRAM bytes per step from an ncu capture (profiles/k_p2g_k_g2p_update_sand_water_2M.md)")
+                    help="DRAM bytes per step from an ncu capture (profiles/k_p2g_k_g2p_range_sand_water_2M.md)")
     args = ap.parse_args()
     if args.impl == "reference":
         # CPU baseline arm: rank 0 alone runs it; other ranks exit without work.
