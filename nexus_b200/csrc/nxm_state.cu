@@ -460,6 +460,11 @@ struct nxm_state {
     std::vector<char*> stg_retired;  // outgrown rings, freed once the stream has drained
     std::vector<cudaEvent_t> event_pool;
 
+    // scratch of uploads, removals and reads: a memory pool of this state that
+    // keeps what it has grown to (the device's default pool hands memory back
+    // at every synchronisation, so each upload would map its scratch anew)
+    cudaMemPool_t pool = nullptr;
+
     // stream-ordered tickets (nxm_state_fence): the events of tickets not yet
     // known complete, oldest first; tickets up to done_ticket are complete
     std::deque<std::pair<uint64_t, cudaEvent_t>> fences;
@@ -550,6 +555,12 @@ LaunchCfg launch_cfg(nxm_state* s) {
 // behind the queued work without the host waiting for it (a copy from
 // pageable memory would first drain the stream).  An event recorded after
 // each copy marks when its ring region may be written again.
+
+// Stream-ordered scratch from the state's pool (freed with cudaFreeAsync).
+template <class T>
+cudaError_t scratch_alloc(nxm_state* s, T** p, size_t bytes) {
+    return cudaMallocFromPoolAsync(reinterpret_cast<void**>(p), bytes, s->pool, s->stream);
+}
 
 cudaError_t take_event(nxm_state* s, cudaEvent_t* e) {
     if (!s->event_pool.empty()) {
@@ -1045,7 +1056,7 @@ int pack_read_range(nxm_state* s, const void* records, uint32_t stride_bytes, co
         if (s->d_pack) NXM_TRY(cudaFreeAsync(s->d_pack, s->stream));
         s->d_pack = nullptr;
         s->pack_cap = 0;
-        NXM_TRY(cudaMallocAsync(reinterpret_cast<void**>(&s->d_pack), cap * 4, s->stream));
+        NXM_TRY(scratch_alloc(s, &s->d_pack, cap * 4));
         s->pack_cap = cap;
     }
     if (!s->d_offsets) NXM_TRY(dalloc(&s->d_offsets, 32));
@@ -1096,7 +1107,7 @@ int remove_id_ranges(nxm_state* s, std::vector<uint2> ranges) {
     // stream-ordered scratch and staged uploads: the removal queues behind the
     // steps in flight without waiting for them
     char* scratch = nullptr;
-    cudaError_t e = cudaMallocAsync(reinterpret_cast<void**>(&scratch), 16 * rr.size() + 16, s->stream);
+    cudaError_t e = scratch_alloc(s, &scratch, 16 * rr.size() + 16);
     uint2* d_r = reinterpret_cast<uint2*>(scratch);
     uint32_t* d_cum = reinterpret_cast<uint32_t*>(scratch + 8 * rr.size());
     if (e == cudaSuccess) e = upload_async(s, d_r, rr.data(), sizeof(uint2) * rr.size());
@@ -1261,7 +1272,7 @@ int upload_particles(nxm_state* s, const nxm_particles_soa* p, uint32_t count) {
     for (int f = 0; f < 14; ++f)
         if (fields[f].src) direct |= (pinned[f] = host_pinned(fields[f].src));
     char* scratch = nullptr;
-    NXM_TRY(cudaMallocAsync(reinterpret_cast<void**>(&scratch), std::max<size_t>(per_particle, 4) * chunk, s->stream));
+    NXM_TRY(scratch_alloc(s, &scratch, std::max<size_t>(per_particle, 4) * chunk));
     const void* dst[14] = {};
     auto copy_chunk = [&](uint32_t c0, uint32_t cn) {
         char* at = scratch;
@@ -1289,7 +1300,7 @@ int upload_particles(nxm_state* s, const nxm_particles_soa* p, uint32_t count) {
     if (!rc) {
         const uint32_t nruns = (uint32_t)runs.start.size();
         const size_t mid_at = (size_t)nruns * 4, state_at = ((size_t)nruns * 8 + 15) / 16 * 16;
-        cudaError_t e = cudaMallocAsync(reinterpret_cast<void**>(&run_scratch), state_at + (size_t)nruns * 16, s->stream);
+        cudaError_t e = scratch_alloc(s, &run_scratch, state_at + (size_t)nruns * 16);
         if (e == cudaSuccess) e = upload_async(s, run_scratch, runs.start.data(), 4 * (size_t)nruns);
         if (e == cudaSuccess) e = upload_async(s, run_scratch + mid_at, runs.mid.data(), 4 * (size_t)nruns);
         if (e == cudaSuccess) e = upload_async(s, run_scratch + state_at, runs.state.data(), 16 * (size_t)nruns);
@@ -1764,6 +1775,17 @@ int nxm_state_create(const nxm_capacities* caps, nxm_state** out) {
     s->sm_count = sms;
     int rc = NXM_OK;
     if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess) rc = NXM_E_CUDA;
+    if (!rc) {
+        cudaMemPoolProps pp{};
+        pp.allocType = cudaMemAllocationTypePinned;
+        pp.handleTypes = cudaMemHandleTypeNone;
+        pp.location.type = cudaMemLocationTypeDevice;
+        pp.location.id = dev;
+        uint64_t keep = UINT64_MAX;
+        if (cudaMemPoolCreate(&s->pool, &pp) != cudaSuccess ||
+            cudaMemPoolSetAttribute(s->pool, cudaMemPoolAttrReleaseThreshold, &keep) != cudaSuccess)
+            rc = NXM_E_CUDA;
+    }
     if (!rc && dalloc(&s->d_params, 1) != cudaSuccess) rc = NXM_E_OOM;
     if (!rc && dalloc(&s->d_counters, 1) != cudaSuccess) rc = NXM_E_OOM;
     if (!rc && cudaMallocHost(reinterpret_cast<void**>(&s->h_counters), sizeof(Counters)) != cudaSuccess) rc = NXM_E_OOM;
@@ -1804,6 +1826,7 @@ void nxm_state_destroy(nxm_state* s) {
     for (cudaEvent_t e : s->status_done)
         if (e) cudaEventDestroy(e);
     if (s->h_counters) cudaFreeHost(s->h_counters);
+    if (s->pool) cudaMemPoolDestroy(s->pool);  // after d_pack, its last allocation, was freed above
     if (s->stream) cudaStreamDestroy(s->stream);
     delete s;
 }
