@@ -107,7 +107,10 @@ __device__ __forceinline__ void warp_range(uint32_t n, uint32_t& lo, uint32_t& h
     hi = min(lo + per_warp, n);
 }
 
-constexpr int kSortBatch = 4;  // passes of 32 particles whose loads are issued together
+#ifndef NXM_SORT_BATCH
+#define NXM_SORT_BATCH 4
+#endif
+constexpr int kSortBatch = NXM_SORT_BATCH;  // passes of 32 particles whose loads are issued together
 
 __device__ __forceinline__ bool spills(uint32_t ax, uint32_t ay, uint32_t az, int sx, int sy, int sz) {
     // sort.rs:320-329, EXTRA_PARTICLE_MIN_SHIFT = 2
