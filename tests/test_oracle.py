@@ -144,6 +144,34 @@ def test_drucker_prager_tensile_and_inside_cone(oracle_built):
     assert np.allclose(_from_cm(F), np.eye(3) * math.exp(0.001), atol=1e-6)
 
 
+def test_snow_band_clamp_and_hardening(oracle_built):
+    """snow.rs:452-488 in closed form: singular values inside [1 - theta_c,
+    1 + theta_s] leave F and the plastic determinant alone (stress = the
+    corotated stress of the same Lame parameters); outside, F is clamped,
+    the plastic determinant takes the ratio (clamped to [0.1, 4]) and the
+    Lame parameters scale by exp(h (1 - J_p))."""
+    o = oracle_built
+    E, nu = 1.4e5, 0.2
+    m = ParticleModel.snow(E, nu).gpu_words()
+    lin = ParticleModel.elastic(E, nu).gpu_words()
+    tc, ts, h = float(np.float32(2.5e-2)), float(np.float32(7.5e-3)), 10.0
+    Fin = _rot([1, 2, 0.5], 0.3) @ np.diag([1.004, 0.99, 0.98])
+    tau, F, w = o.model_update(m, _cm(Fin), np.zeros(9), "f64")
+    tl, _, _ = o.model_update(lin, _cm(Fin), np.zeros(9), "f64")
+    assert np.allclose(_from_cm(F), Fin, atol=1e-6)
+    assert abs(float(w.view(np.float32)[1]) - 1.0) < 1e-6
+    assert np.allclose(tau, tl, rtol=1e-5, atol=1e-3)
+    for s_, c in ((1.02, 1.0 + ts), (0.96, 1.0 - tc)):
+        tau, F, w = o.model_update(m, _cm(np.eye(3) * s_), np.zeros(9), "f64")
+        assert np.allclose(_from_cm(F), np.eye(3) * c, atol=1e-6)
+        pdet = (float(np.float32(s_)) / c) ** 3
+        assert abs(float(w.view(np.float32)[1]) - pdet) < 1e-5
+        tl, _, _ = o.model_update(lin, _cm(np.eye(3) * c), np.zeros(9), "f64")
+        assert np.allclose(tau, tl * math.exp(h * (1.0 - pdet)), rtol=1e-4, atol=1e-2)
+    _, _, w = o.model_update(m, _cm(np.eye(3) * 2.0), np.zeros(9), "f64")
+    assert w.view(np.float32)[1] == np.float32(4.0)
+
+
 def test_fluid_pressure_and_volume_only(oracle_built):
     o = oracle_built
     m = ParticleModel.water(1e5).gpu_words()
