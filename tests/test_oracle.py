@@ -105,6 +105,30 @@ def test_linear_corotated_rest_and_rotation(oracle_built):
         assert np.abs(tau).max() < 2e-6 * 2e4
 
 
+def test_elastic_stresses_closed_form(oracle_built):
+    """Corotated (linear.rs): tau = 2 mu (F - R) F^T + lambda (J - 1) J I,
+    for F = Q diag(s): 2 mu Q diag((s - 1) s) Q^T + lambda (J - 1) J I.
+    Neo-Hookean (neo_hookean_elasticity.rs): tau = mu (F F^T - I) + lambda ln(J) I."""
+    o = oracle_built
+    lam, mu = (float(v) for v in lame_lambda_mu(3e4, 0.3))
+    lin = ParticleModel.elastic(3e4, 0.3).gpu_words()
+    nh = ParticleModel.elastic_neo_hookean(3e4, 0.3).gpu_words()
+    rng = np.random.default_rng(8)
+    for _ in range(5):
+        Q = _rot(rng.standard_normal(3), rng.uniform(-1.0, 1.0))
+        sv = rng.uniform(0.9, 1.1, 3)
+        F = (Q @ np.diag(sv)).astype(np.float32).astype(np.float64)
+        j = float(np.linalg.det(F))
+        tau, _, _ = o.model_update(lin, _cm(F), np.zeros(9), "f64")
+        want = 2 * mu * Q @ np.diag((sv - 1) * sv) @ Q.T + lam * (j - 1) * j * np.eye(3)
+        assert np.allclose(_from_cm(tau), want, rtol=1e-4, atol=2e-2)
+        G = F + 0.05 * rng.standard_normal((3, 3))  # a general F (shear too)
+        G = G.astype(np.float32).astype(np.float64)
+        tau, _, _ = o.model_update(nh, _cm(G), np.zeros(9), "f64")
+        want = mu * (G @ G.T - np.eye(3)) + lam * math.log(np.linalg.det(G)) * np.eye(3)
+        assert np.allclose(_from_cm(tau), want, rtol=1e-5, atol=1e-3)
+
+
 def test_svd_reconstructs(oracle_built):
     o = oracle_built
     rng = np.random.default_rng(3)
@@ -181,6 +205,21 @@ def test_fluid_pressure_and_volume_only(oracle_built):
     tau, _, _ = o.model_update(m, _cm(np.eye(3) * 0.97), np.zeros(9), "f64")
     p = 1e5 * (j ** -7 - 1)
     assert np.allclose(_from_cm(tau), -p * j * np.eye(3), rtol=1e-5)
+
+
+def test_fluid_viscous_stress(oracle_built):
+    """fluid.rs: tau = 2 eta J dev(S) - p(J) J I with S = (L + L^T) / 2."""
+    o = oracle_built
+    eta, k, gamma = 0.5, 1e5, 7.0
+    m = ParticleModel.fluid(k, gamma, eta).gpu_words()
+    L = np.random.default_rng(4).standard_normal((3, 3))
+    S = 0.5 * (L + L.T)
+    dev = S - np.trace(S) / 3.0 * np.eye(3)
+    for c in (1.0, 0.98):
+        tau, _, _ = o.model_update(m, _cm(np.eye(3) * c), _cm(L), "f64")
+        j = float(np.float32(c)) ** 3
+        p = k * (j ** -gamma - 1.0)
+        assert np.allclose(_from_cm(tau), 2 * eta * j * dev - p * j * np.eye(3), rtol=1e-5, atol=1e-4)
 
 
 def test_boundary_condition_projection(oracle_built):
