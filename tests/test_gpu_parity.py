@@ -110,6 +110,31 @@ def test_elastic_cube_100_steps(pipe, deterministic):
     assert rel_l2(g["def_grad"], o["def_grad"]) < (1e-6 if deterministic else 1e-4)
 
 
+@pytest.mark.parametrize("deterministic", [False, True])
+def test_affine_velocity_field_is_transferred_exactly(pipe, deterministic):
+    """APIC property on the CUDA path: an affine velocity field carried by
+    the particles (C = A) comes back from P2G + G2P, v_p = A x_p + c, C = A."""
+    from nexus_b200.models import ParticleModel
+    from nexus_b200.particles import ParticleBatch, collider_array
+    rng = np.random.default_rng(9)
+    dx = 1.0 / 64.0
+    pos = scenes.lattice_block((0.4, 0.4, 0.4), (12, 12, 12), dx, 5)
+    b = ParticleBatch.from_positions(pos, np.float32(dx / 4), 1000.0, ParticleModel.elastic_neo_hookean(1e-3, 0.3))
+    A = 0.5 * rng.standard_normal((3, 3))
+    c = 0.3 * rng.standard_normal(3)
+    x = pos.astype(np.float64)
+    b.vel = (x @ A.T + c).astype(np.float32)
+    b.aff = (b.mass.astype(np.float64)[:, None] * A.T.reshape(1, 9)).astype(np.float32)
+    sc = scenes.Scene("affine", dx, 1.0e-4, (0.0, 0.0, 0.0), b, collider_array([]), 1, 4096)
+    st = state_from_scene(sc, deterministic=deterministic)
+    pipe.step(st)
+    st.synchronize()
+    g = st.read_particles()
+    np.testing.assert_allclose(g["vel"], x @ A.T + c, rtol=0, atol=1e-5)
+    aff = g["aff"].astype(np.float64).reshape(-1, 3, 3).transpose(0, 2, 1) / g["mass"][:, None, None]
+    np.testing.assert_allclose(aff, np.broadcast_to(A, aff.shape), rtol=0, atol=1e-4)
+
+
 def test_sparse_blocks_fast_matches_oracle(pipe):
     """Particles scattered about two per block: each 256-position run of the
     fast G2P spans far more blocks than the four it stages at once, so it

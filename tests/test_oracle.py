@@ -331,6 +331,34 @@ def test_free_fall_and_uniform_translation(oracle_built):
     assert np.abs(disp - disp.mean(0)).max() < 1e-6
 
 
+def test_affine_velocity_field_is_transferred_exactly(oracle_built):
+    """APIC (p2g.rs / g2p.rs): particles carrying an affine velocity field
+    v(x) = A x + c with C = A give it back after P2G + G2P, v_p = A x_p + c and
+    C = A, since quadratic B-splines reproduce linear functions.  No gravity,
+    no colliders, a vanishing stiffness (the stored affine is m A minus the
+    stress term)."""
+    from oracle.oracle import OracleScene
+    from nexus_b200.particles import ParticleBatch, collider_array
+    from nexus_b200.scenes import Scene, lattice_block
+    rng = np.random.default_rng(9)
+    dx = 1.0 / 64.0
+    pos = lattice_block((0.4, 0.4, 0.4), (12, 12, 12), dx, 5)
+    b = ParticleBatch.from_positions(pos, np.float32(dx / 4), 1000.0, ParticleModel.elastic_neo_hookean(1e-3, 0.3))
+    A = 0.5 * rng.standard_normal((3, 3))
+    c = 0.3 * rng.standard_normal(3)
+    x = pos.astype(np.float64)
+    b.vel = (x @ A.T + c).astype(np.float32)
+    b.aff = (b.mass.astype(np.float64)[:, None] * A.T.reshape(1, 9)).astype(np.float32)  # column-major m A
+    sc = Scene("affine", dx, 1.0e-4, (0.0, 0.0, 0.0), b, collider_array([]), 1, 4096)
+    o = OracleScene(sc, "f64")
+    o.step(1)
+    got = o.particles()
+    np.testing.assert_allclose(got["vel"], x @ A.T + c, rtol=0, atol=2e-6)
+    aff = got["aff"].astype(np.float64).reshape(-1, 3, 3).transpose(0, 2, 1) / got["mass"][:, None, None]
+    np.testing.assert_allclose(aff, np.broadcast_to(A, aff.shape), rtol=0, atol=1e-5)
+    np.testing.assert_allclose(got["pos"], x + got["vel"].astype(np.float64) * 1.0e-4, rtol=0, atol=1e-7)
+
+
 def test_fp32_and_fp64_oracles_agree_on_elastic_cube(oracle_built):
     from oracle.oracle import OracleScene
     sc = scenes.elastic_cube(n_side=12, steps=20)
