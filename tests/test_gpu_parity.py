@@ -135,6 +135,23 @@ def test_affine_velocity_field_is_transferred_exactly(pipe, deterministic):
     np.testing.assert_allclose(aff, np.broadcast_to(A, aff.shape), rtol=0, atol=1e-4)
 
 
+@pytest.mark.parametrize("deterministic", [False, True])
+def test_linear_momentum_is_conserved(pipe, deterministic):
+    """No gravity, no colliders: the total momentum survives 20 steps of a
+    stiff body with random velocities on the CUDA path."""
+    from tests.test_oracle import _momentum_scene
+    sc = _momentum_scene()
+    p0 = (sc.particles.mass[:, None].astype(np.float64) * sc.particles.vel).sum(0)
+    st = state_from_scene(sc, deterministic=deterministic)
+    for _ in range(20):
+        pipe.step(st)
+    st.synchronize()
+    g = st.read_particles()
+    p1 = (g["mass"][:, None].astype(np.float64) * g["vel"]).sum(0)
+    scale = (sc.particles.mass[:, None] * np.abs(sc.particles.vel)).sum()
+    assert np.abs(p1 - p0).max() < 1e-5 * scale
+
+
 def test_sparse_blocks_fast_matches_oracle(pipe):
     """Particles scattered about two per block: each 256-position run of the
     fast G2P spans far more blocks than the four it stages at once, so it

@@ -359,6 +359,32 @@ def test_affine_velocity_field_is_transferred_exactly(oracle_built):
     np.testing.assert_allclose(got["pos"], x + got["vel"].astype(np.float64) * 1.0e-4, rtol=0, atol=1e-7)
 
 
+def _momentum_scene():
+    from nexus_b200.particles import ParticleBatch, collider_array
+    from nexus_b200.scenes import Scene, lattice_block
+    dx = 1.0 / 64.0
+    pos = lattice_block((0.4, 0.4, 0.4), (12, 12, 12), dx, 6)
+    b = ParticleBatch.from_positions(pos, np.float32(dx / 4), 1000.0, ParticleModel.elastic_neo_hookean(1e5, 0.3))
+    b.vel = (0.5 * np.random.default_rng(10).standard_normal(pos.shape)).astype(np.float32)
+    return Scene("momentum", dx, 1.0e-4, (0.0, 0.0, 0.0), b, collider_array([]), 20, 4096)
+
+
+def test_linear_momentum_is_conserved(oracle_built):
+    """No gravity, no colliders: P2G, the grid update and G2P keep the total
+    momentum (the APIC term sums to zero over a stencil, internal forces
+    cancel), while the random velocities deform the body."""
+    from oracle.oracle import OracleScene
+    sc = _momentum_scene()
+    p0 = (sc.particles.mass[:, None].astype(np.float64) * sc.particles.vel).sum(0)
+    o = OracleScene(sc, "f64")
+    o.step(20)
+    got = o.particles()
+    p1 = (got["mass"][:, None].astype(np.float64) * got["vel"]).sum(0)
+    scale = (sc.particles.mass[:, None] * np.abs(sc.particles.vel)).sum()
+    assert np.abs(p1 - p0).max() < 1e-6 * scale
+    assert np.abs(got["vel"] - sc.particles.vel).max() > 1e-3  # the velocities did change
+
+
 def test_fp32_and_fp64_oracles_agree_on_elastic_cube(oracle_built):
     from oracle.oracle import OracleScene
     sc = scenes.elastic_cube(n_side=12, steps=20)
