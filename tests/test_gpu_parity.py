@@ -152,6 +152,23 @@ def test_linear_momentum_is_conserved(pipe, deterministic):
     assert np.abs(p1 - p0).max() < 1e-5 * scale
 
 
+@pytest.mark.parametrize("deterministic", [False, True])
+def test_angular_momentum_is_conserved(pipe, deterministic):
+    """APIC angular momentum (the affine part included) over 20 steps of a
+    stiff body with random velocities on the CUDA path."""
+    from tests.test_oracle import _momentum_scene, apic_angular_momentum
+    sc = _momentum_scene()
+    p = sc.particles
+    l0, scale = apic_angular_momentum(p.pos, p.vel, p.aff, p.mass, sc.dx)
+    st = state_from_scene(sc, deterministic=deterministic)
+    for _ in range(20):
+        pipe.step(st)
+    st.synchronize()
+    g = st.read_particles()
+    l1, _ = apic_angular_momentum(g["pos"], g["vel"], g["aff"], g["mass"], sc.dx)
+    assert np.abs(l1 - l0).max() < 1e-5 * scale
+
+
 def test_sparse_blocks_fast_matches_oracle(pipe):
     """Particles scattered about two per block: each 256-position run of the
     fast G2P spans far more blocks than the four it stages at once, so it

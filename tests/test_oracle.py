@@ -385,6 +385,35 @@ def test_linear_momentum_is_conserved(oracle_built):
     assert np.abs(got["vel"] - sc.particles.vel).max() > 1e-3  # the velocities did change
 
 
+def apic_angular_momentum(pos, vel, aff, mass, dx):
+    """Total angular momentum of APIC particles: sum of m x x v plus the
+    affine part D eps : M with D = dx^2 / 4 (quadratic B-splines) and M the
+    stored affine matrix (m C minus a symmetric stress term, which the
+    contraction with eps drops).  Returns it and the scale sum m |x| |v|."""
+    x, v, m = pos.astype(np.float64), vel.astype(np.float64), mass.astype(np.float64)
+    M = aff.astype(np.float64).reshape(-1, 3, 3).transpose(0, 2, 1)
+    spin = np.stack([M[:, 2, 1] - M[:, 1, 2], M[:, 0, 2] - M[:, 2, 0], M[:, 1, 0] - M[:, 0, 1]], 1)
+    total = (m[:, None] * np.cross(x, v)).sum(0) + dx * dx / 4.0 * spin.sum(0)
+    scale = (m * np.linalg.norm(x, axis=1) * np.linalg.norm(v, axis=1)).sum()
+    return total, scale
+
+
+def test_angular_momentum_is_conserved(oracle_built):
+    """APIC conserves angular momentum (its affine part included) through
+    the transfers, the symmetric stress and the advection."""
+    from oracle.oracle import OracleScene
+    sc = _momentum_scene()
+    p = sc.particles
+    l0, scale = apic_angular_momentum(p.pos, p.vel, p.aff, p.mass, sc.dx)
+    o = OracleScene(sc, "f64")
+    o.step(20)
+    g = o.particles()
+    l1, _ = apic_angular_momentum(g["pos"], g["vel"], g["aff"], g["mass"], sc.dx)
+    assert np.abs(l1 - l0).max() < 1e-7 * scale
+    spin1 = apic_angular_momentum(g["pos"], g["vel"], np.zeros_like(g["aff"]), g["mass"], sc.dx)[0]
+    assert np.abs(spin1 - l0).max() > 1e-5 * scale  # without the affine part it would not hold
+
+
 def test_fp32_and_fp64_oracles_agree_on_elastic_cube(oracle_built):
     from oracle.oracle import OracleScene
     sc = scenes.elastic_cube(n_side=12, steps=20)
