@@ -25,8 +25,10 @@ the scenes are sharded over the ranks (no collective on the data path).
 from __future__ import annotations
 
 import argparse
+import hashlib
 import json
 import os
+import re
 import statistics
 import subprocess
 import sys
@@ -46,15 +48,63 @@ UNIT = "particle-steps/s"
 # read; Drucker-Prager state, 3 floats, read and written for sand).
 B_ALG_ELASTIC = 204
 B_ALG_SAND = 228
-# DRAM bytes read + written per step by the two transfer kernels (75 % of the
-# step's kernel time) on the sand_water scene, from one ncu capture of the full
-# scene (k_p2g 180 MB + k_g2p_range 590 MB; the sort and grid kernels are not included).
-TRAFFIC_PER_STEP = 174.2e6 + 5.6e6 + 322.0e6 + 267.5e6
+# Per phase (the roofline of each kernel group of one step), bytes per particle:
+#   sort: the 4-byte block key read and the 4-byte sorted index written;
+#   p2g:  x, mass, v, C read (12 + 4 + 12 + 36);
+#   grid: node momentum + mass read and velocity + mass written, 32 bytes a
+#         node, at the scene's nodes per particle (counted from the grid);
+#   g2p:  x, v, F, V0, material read, x, v, C, F written (+ 24 for the
+#         Drucker-Prager state words of sand).
+PHASE_BYTES = {"sort": 8.0, "p2g": 64.0}
+G2P_BYTES_ELASTIC = 24 + 36 + 8 + 96
+G2P_BYTES_SAND = G2P_BYTES_ELASTIC + 24
+
+# The DRAM traffic of one step (dram__bytes_read.sum + dram__bytes_write.sum
+# over every kernel of the step) comes from an ncu capture summarised in a
+# profiles/ file, which records the hash of the kernel sources it was taken
+# on; the bench reports it only while the sources are unchanged.
+TRAFFIC_PROFILE = os.path.join(ROOT, "profiles", "step_traffic_sand_water_2M.md")
+KERNEL_SOURCES = os.path.join(ROOT, "nexus_b200", "csrc")
 
 
 def b_alg_per_particle(model_tags: np.ndarray) -> float:
     sand = np.isin(model_tags, (2, 3))
     return float(np.where(sand, B_ALG_SAND, B_ALG_ELASTIC).mean())
+
+
+def kernel_sources_hash() -> str:
+    """sha256 (first 16 hex digits) of the CUDA library's sources."""
+    h = hashlib.sha256()
+    for name in sorted(os.listdir(KERNEL_SOURCES)):
+        path = os.path.join(KERNEL_SOURCES, name)
+        if os.path.isfile(path) and name.endswith((".cu", ".cuh", ".h")):
+            h.update(name.encode())
+            with open(path, "rb") as f:
+                h.update(f.read())
+    return h.hexdigest()[:16]
+
+
+def load_traffic(workload: str):
+    """(bytes per step or None, details): the captured traffic of this build's
+    step, None when the capture predates the current kernel sources."""
+    current = kernel_sources_hash()
+    info = {"sources": current, "profile": os.path.basename(TRAFFIC_PROFILE)}
+    if workload != "sand_water" or not os.path.exists(TRAFFIC_PROFILE):
+        info["note"] = "no capture for this workload"
+        return None, info
+    text = open(TRAFFIC_PROFILE).read()
+    m = re.search(r"traffic_bytes_per_step:\s*([0-9.eE+]+)\s+sources:\s*([0-9a-f]{16})", text)
+    if not m:
+        info["note"] = "no traffic line in the profile"
+        return None, info
+    captured, src = float(m.group(1)), m.group(2)
+    info["captured_sources"] = src
+    if src != current:
+        info["stale"] = True
+        info["last_capture_bytes"] = captured
+        return None, info
+    info["stale"] = False
+    return captured, info
 
 
 def load_peaks():
@@ -172,27 +222,96 @@ def cpu_oracle_rate(scene, steps: int, warmup: int):
     return scene.n * steps / dt, dt
 
 
+def workload_config(scene, world: int) -> dict:
+    """The `config` of both arms' lines (the same dict, so that they compare)."""
+    return {"workload": scene.name, "particles_per_gpu": scene.n, "dx": scene.dx, "dt": scene.dt,
+            "parallelism": f"replicas{world}" if world > 1 else "single",
+            "l2": "inputs larger than L2 (particle state %.0f MB per GPU)" % (scene.n * 144 / 1e6)}
+
+
+# The reference arm times whole oracle steps of the full scene; it runs at
+# most this many seconds of steps (about half a second each on 16 cores for
+# the 2 M-particle scene), fewer than K when K would take longer.
+REFERENCE_BUDGET_S = 150.0
+
+
 def run_reference(args, world, rank):
     if rank != 0:
         return
     os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count()))
+    from oracle.oracle import OracleScene
     scene = make_scene(args.workload)
     cores = int(os.environ["OMP_NUM_THREADS"])
-    rate, secs = cpu_oracle_rate(scene, args.ref_steps, args.ref_warmup)
+    o = OracleScene(scene, "f32")
+    warm = min(args.warmup, 2)
+    t0 = time.perf_counter()
+    if warm:
+        o.step(warm)
+    per_step = (time.perf_counter() - t0) / warm if warm else None
+    steps = args.steps
+    if per_step:
+        steps = max(1, min(steps, int(REFERENCE_BUDGET_S / per_step)))
+    t0 = time.perf_counter()
+    o.step(steps)
+    secs = time.perf_counter() - t0
+    rate = scene.n * steps / secs
     line = {
         "impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus,
-        "steps": args.ref_steps, "warmup": args.ref_warmup, "ms_per_step": secs / args.ref_steps * 1e3,
+        "steps": steps, "warmup": warm, "ms_per_step": secs / steps * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": args.workload, "particles": scene.n, "dx": scene.dx, "dt": scene.dt},
+        "config": workload_config(scene, args.gpus),
         "cpu_baseline": {"value": rate, "unit": UNIT, "cores": cores, "kind": "port",
-                         "sample": f"{args.ref_steps} full steps of the {scene.n}-particle scene after "
-                                   f"{args.ref_warmup} warm-up steps (C restatement of the reference step, "
+                         "sample": f"{steps} full steps of the {scene.n}-particle scene after {warm} warm-up "
+                                   f"steps (of --steps {args.steps} / --warmup {args.warmup}: at most "
+                                   f"{REFERENCE_BUDGET_S:.0f} s of steps; C restatement of the reference step, "
                                    f"FP32, OpenMP)"},
         "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "note": "the reference's own GPU (wgpu) and CPU (Rust) paths cannot run on this box: no Rust toolchain, "
                 "no graphics stack",
     }
     print(json.dumps(line), flush=True)
+
+
+def phase_rooflines(phases: dict, scene, st, peak: float) -> dict:
+    """Achieved GB/s and fraction of the measured peak of each phase of one
+    timestamped step, from the algorithmic bytes of that phase."""
+    n = scene.n
+    tags = scene.particles.model[:, 0]
+    sand = np.isin(tags, (2, 3))
+    nodes = st.num_blocks() * 64
+    bytes_ = {"sort": PHASE_BYTES["sort"] * n, "p2g": PHASE_BYTES["p2g"] * n, "grid_update": 32.0 * nodes,
+              "g2p": float(np.where(sand, G2P_BYTES_SAND, G2P_BYTES_ELASTIC).sum())}
+    out = {}
+    for k, b in bytes_.items():
+        ms = phases.get(f"{k}_ms")
+        if not ms:
+            continue
+        gbs = b / (ms / 1e3) / 1e9
+        out[k] = {"ms": ms, "algorithmic_bytes": b, "achieved_gbs": gbs, "frac": gbs / peak}
+    return out
+
+
+def measure_cube(torch, steps: int = 100):
+    """the 32,768-particle elastic cube, 100 steps, one graph per step."""
+    from nexus_b200 import scenes
+    from nexus_b200.mpm import MpmPipeline, state_from_scene
+    sc = scenes.elastic_cube()
+    st = state_from_scene(sc)
+    pipe = MpmPipeline()
+    stream = torch.cuda.ExternalStream(st.cuda_stream())
+    for _ in range(5):
+        pipe.step(st)
+    st.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    for _ in range(steps):
+        pipe.step(st)
+    b.record(stream)
+    b.synchronize()
+    ms = a.elapsed_time(b)
+    st.synchronize()
+    return {"workload": "elastic_cube", "particles": sc.n, "steps": steps, "value": sc.n * steps / (ms / 1e3),
+            "unit": UNIT, "ms_per_step": ms / steps, "dx": sc.dx, "dt": sc.dt}
 
 
 def run_ours(args, world, rank, local):
@@ -246,10 +365,13 @@ def run_ours(args, world, rank, local):
     step_s = ms / args.steps / 1e3
     peak, peak_kind = load_peaks()
     achieved = bytes_per_step / step_s / 1e9
+    traffic, traffic_info = load_traffic(args.workload)
+    phase_roof = phase_rooflines(phases, scene, st, peak)
 
     # end to end through the C ABI from pinned host buffers (every rank its own
     # replica; the whole job's rate over the slowest rank's wall time)
     e2e = measure_e2e(scene, args, torch) if args.e2e else None
+    e2e_pageable = measure_e2e(scene, args, torch, pinned=False) if (args.e2e and world == 1) else None
     if e2e is not None and world > 1:
         wall = all_max(n * e2e["steps"] / e2e["value"], world)
         e2e["value"] = n * world * e2e["steps"] / wall
@@ -259,6 +381,7 @@ def run_ours(args, world, rank, local):
     batched = measure_batched(args, world, rank, torch) if args.batched_steps > 0 else None
     serving = measure_serving(args, torch) if (args.serving_requests > 0 and world == 1) else None
     coupled = measure_coupled(args, torch) if (args.coupled_steps > 0 and world == 1) else None
+    cube = measure_cube(torch) if (args.cube and world == 1) else None
 
     if rank != 0:
         return
@@ -273,18 +396,19 @@ def run_ours(args, world, rank, local):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": args.workload, "particles_per_gpu": n, "dx": scene.dx, "dt": scene.dt,
-                   "parallelism": f"replicas{world}" if world > 1 else "single",
-                   "l2": "inputs larger than L2 (particle state %.0f MB per GPU)" % (n * 144 / 1e6)},
+        "config": workload_config(scene, world),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": args.traffic, "peak_kind": peak_kind,
+                     "traffic": traffic, "traffic_source": traffic_info, "peak_kind": peak_kind,
                      "launch": "one step = one CUDA-graph launch of all step kernels",
                      "algorithmic_bytes_per_launch": bytes_per_step},
         "phases_ms": phases,
+        "phase_roofline": phase_roof,
         "clocks": clk,
         "e2e": e2e,
+        "e2e_pageable": e2e_pageable,
         "gpu_launches": launches,
         "cpu_baseline": cpu,
+        "elastic_cube": cube,
         "batched": batched,
         "serving": serving,
         "coupled": coupled,
@@ -457,9 +581,10 @@ def measure_serving(args, torch):
             "note": f"{len(reqs)} requests of the 4000-request stream (same arrival rate and distributions)"}
 
 
-def measure_e2e(scene, args, torch):
+def measure_e2e(scene, args, torch, pinned: bool = True):
     """Same metric through the C ABI with host buffers: upload the scene from
-    pinned host memory, then per step write the (kinematic) collider
+    host memory (pinned buffers; or, `pinned` False, the plain numpy arrays an
+    ordinary caller holds), then per step write the (kinematic) collider
     velocity, step, and read back the device status word; finally read the
     positions back.  Host wall clock around everything."""
     from nexus_b200.mpm import MpmPipeline, MpmState
@@ -467,6 +592,8 @@ def measure_e2e(scene, args, torch):
     from nexus_b200.particles import ParticleBatch
 
     def pinned_like(a):
+        if not pinned:
+            return np.array(a, copy=True)
         t = torch.empty(a.nbytes, dtype=torch.uint8, pin_memory=True)
         v = t.numpy().view(a.dtype).reshape(a.shape)
         v[...] = a
@@ -505,9 +632,9 @@ def measure_e2e(scene, args, torch):
     return {"value": p.n * steps / dt, "unit": UNIT, "steps": steps,
             # per step: a 24-byte collider velocity write (kernel arguments), a 4-byte status word read
             "h2d_bytes_per_step": int(upload / steps + 24), "d2h_bytes_per_step": int(p.n * 12 / steps + 4),
-            "how": "host wall clock: state create + SoA upload from pinned memory (packed into records on the "
+            "how": "host wall clock: state create + SoA upload from %s (packed into records on the "
                    "device) + per step (collider velocity write, step, pipelined status D2H read one step late) + "
-                   "final positions D2H",
+                   "final positions D2H" % ("pinned memory" if pinned else "pageable numpy arrays"),
             "phases_ms": {"create": (t1 - t0) * 1e3, "upload": (t2 - t1) * 1e3, "steps": (t3 - t2) * 1e3,
                           "readback": (t4 - t3) * 1e3}}
 
@@ -519,20 +646,18 @@ def main():
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="sand_water", choices=["sand_water", "elastic_cube"])
-    ap.add_argument("--ref-steps", type=int, default=10)
-    ap.add_argument("--ref-warmup", type=int, default=1)
+    ap.add_argument("--ref-steps", type=int, default=10, help="oracle steps of the cpu_baseline leg")
     ap.add_argument("--e2e-steps", type=int, default=500)
     ap.add_argument("--no-e2e", dest="e2e", action="store_false")
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
-    ap.add_argument("--batched-steps", type=int, default=50,
+    ap.add_argument("--batched-steps", type=int, default=200,
                     help="timed steps of the batched mix (0: skip it)")
     ap.add_argument("--batched-scenes", type=int, default=256)
     ap.add_argument("--plain-steps", type=int, default=10)
     ap.add_argument("--serving-requests", type=int, default=200, help="0: skip the serving measurement")
-    ap.add_argument("--coupled-steps", type=int, default=50, help="timed steps of the coupled mix (0: skip it)")
+    ap.add_argument("--coupled-steps", type=int, default=300, help="timed steps of the coupled mix (0: skip it)")
     ap.add_argument("--coupled-scenes", type=int, default=64)
-    ap.add_argument("--traffic", type=float, default=TRAFFIC_PER_STEP,
-                    help="DRAM bytes per step from an ncu capture (profiles/k_p2g_k_g2p_range_sand_water_2M.md)")
+    ap.add_argument("--no-cube", dest="cube", action="store_false", help="skip the 32k elastic cube leg")
     args = ap.parse_args()
     if args.impl == "reference":
         # CPU baseline arm: rank 0 alone runs it; other ranks exit without work.

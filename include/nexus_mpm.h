@@ -345,17 +345,21 @@ NXM_API int nxm_debug_sort(nxm_pipeline* pipeline, nxm_state* state, int with_p2
 #define NXM_NOALLOC_MAX_BLOCKS 16384u
 #define NXM_NOALLOC_MAX_PARTICLES (1u << 26)
 
-/* Block activation and particle sort for callers that cannot allocate device
- * memory: code recorded into a CUDA graph (where cudaMalloc is not allowed),
- * allocator-less embedded runtimes, or services that size their memory pools
- * once at start-up.  No counterpart in the reference: nexus_mpm always sorts
- * inside MpmPipeline::step on state-owned buffers.
+/* Block activation and particle sort for callers that may not allocate GPU
+ * memory: a host program (a game engine, a simulation service) that reserves
+ * all of its device memory once at start-up and forbids allocations inside
+ * its frame loop, so that a frame can neither fail for lack of memory nor
+ * stall while the allocator synchronizes the device, or a plugin running in
+ * such a program that is handed device buffers but no allocator.  No
+ * counterpart in the reference: nexus_mpm always sorts inside
+ * MpmPipeline::step on state-owned buffers.
  *
  * Computes the same activation and primary ordering as the sort of nxm_step
  * (every particle's 2x2x2 block neighbourhood is active; each block's primary
- * particles are grouped by z-slab) without allocating anything: the grid
- * tables live in one fixed device array of the library (about 1.9 MB per GPU,
- * held until the process exits).  The caller passes device buffers:
+ * particles are grouped by z-slab) without allocating anything (no cudaMalloc,
+ * cudaFree or allocating library call): the grid tables live in one fixed
+ * device array of the library (about 1.9 MB per GPU, held until the process
+ * exits).  The caller passes device buffers:
  *   positions     n x 4 floats (x, y, z, unused), 16-byte aligned;
  *   sorted_ids    n uint32: particle ids grouped by primary block;
  *   block_vids    max_blocks x 4 int32 (16-byte aligned): block x, y, z and
@@ -364,16 +368,18 @@ NXM_API int nxm_debug_sort(nxm_pipeline* pipeline, nxm_state* state, int with_p2
  *                 sorted_ids and number of primary particles of each block
  *                 (0 for blocks that are only +1 neighbours).
  * `num_blocks` (host) receives the number of active blocks.  `stream` is a
- * cudaStream_t (NULL = legacy default stream); the call waits for it before
- * returning.
+ * cudaStream_t (NULL = legacy default stream); the call reads the result
+ * back and waits for the stream before returning, so it blocks the host.
  *
- * Limits: more than min(max_blocks, NXM_NOALLOC_MAX_BLOCKS) active blocks or
- * more than NXM_NOALLOC_MAX_PARTICLES particles return NXM_E_CAPACITY.
+ * Limits: more than min(max_blocks, NXM_NOALLOC_MAX_BLOCKS) active blocks
+ * (including a scene whose blocks overflow the fixed hash) or more than
+ * NXM_NOALLOC_MAX_PARTICLES particles return NXM_E_CAPACITY.
  * The first call on a device (with that device current) looks up the fixed
- * array's device address; make that first call before any stream capture.
- * Every call reuses the same array and clears what must start at zero, so
- * calls whose GPU work overlaps (other streams or host threads) race and
- * must be serialized by the caller. */
+ * array's device address and keeps it for the life of the process; make that
+ * first call before any stream capture, and do not use this entry point
+ * across a cudaDeviceReset.  Every call reuses the same array and clears what
+ * must start at zero, so calls whose GPU work overlaps (other streams or host
+ * threads) race and must be serialized by the caller. */
 NXM_API int nxm_sort_blocks_noalloc(const float* positions, uint32_t n, float cell_width, uint32_t* sorted_ids,
                                     int32_t* block_vids, uint32_t* block_ranges, uint32_t max_blocks,
                                     uint32_t* num_blocks, void* stream);

@@ -1,21 +1,27 @@
 // nxm_sort_blocks_noalloc: the block activation + particle sort for callers
 // that cannot allocate device memory.
 //
-// Some callers cannot call cudaMalloc: code running inside a CUDA graph
-// capture, allocator-less embedded runtimes, or hosts whose memory pools are
-// sized once at start-up.  This entry point runs the same sort kernels as
-// nxm_step's sort, but keeps all of its grid tables (hash, block headers,
-// bucket cursors, scan tiles, counters) in one file-scope `static __device__`
-// array instead of state-owned allocations; the caller passes the particle
-// positions and the output buffers.  It calls no cudaMalloc, cudaFree or other
-// allocating routine.
+// Some callers of this library may not allocate GPU memory at all: a host
+// program (a game engine, a simulation service) that reserves all of its
+// device memory once at start-up and forbids allocations inside its frame
+// loop, so that a frame can neither fail for lack of memory nor stall while
+// the allocator synchronizes the device; or a plugin that runs inside such a
+// program and is handed device buffers but no allocator.  This entry point
+// runs the same sort kernels as nxm_step's sort, but keeps all of its grid
+// tables (hash, block headers, bucket cursors, scan tiles, counters) in one
+// file-scope `static __device__` array instead of state-owned allocations; the
+// caller passes the particle positions and the output buffers.  It calls no
+// cudaMalloc, cudaFree or other allocating routine.
 //
 // The array holds at most kNoallocMaxBlocks active blocks (about 1.9 MB, kept
-// by every GPU that loads this library until the process exits).  Its device
-// address is looked up once per device (cudaGetSymbolAddress) on the first
-// call made with that device current.  Every call shares the array: calls
-// whose GPU work overlaps (different streams, or concurrent host threads)
-// race on it and must be serialized by the caller.
+// by every GPU that loads this library until the process exits).  In host
+// code the array's name is not a device address: its address is looked up
+// once per device (cudaGetSymbolAddress, return code checked) by the first
+// call made with that device current, and kept for the life of the process,
+// so the library must not be used across a cudaDeviceReset of that device.
+// Every call shares the array: calls whose GPU work overlaps (different
+// streams, or concurrent host threads) race on it and must be serialized by
+// the caller.  A call waits for its stream before returning.
 #include <cuda_runtime.h>
 
 #include <cstring>
@@ -158,8 +164,10 @@ extern "C" int nxm_sort_blocks_noalloc(const float* positions, uint32_t n, float
         (void)cudaGetLastError();
         return NXM_E_CUDA;
     }
-    if (host.status & STATUS_HASH_FULL) return NXM_E_HASH_FULL;
-    if (host.status & (STATUS_BLOCK_CAPACITY | STATUS_MISSING_BLOCK | STATUS_SORT_CAPACITY)) return NXM_E_CAPACITY;
+    // The fixed hash has two slots per block the tables hold, so a full hash
+    // also means more active blocks than the tables hold: one error for both.
+    if (host.status & (STATUS_HASH_FULL | STATUS_BLOCK_CAPACITY | STATUS_MISSING_BLOCK | STATUS_SORT_CAPACITY))
+        return NXM_E_CAPACITY;
     *num_blocks = host.num_blocks;
     return NXM_OK;
 }

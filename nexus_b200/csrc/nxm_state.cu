@@ -457,7 +457,13 @@ struct nxm_state {
     char* stg = nullptr;
     size_t stg_cap = 0, stg_head = 0;
     std::deque<StagingSpan> stg_live;
-    std::vector<char*> stg_retired;  // outgrown rings, freed once the stream has drained
+    // outgrown rings, each with an event recorded after the last copy out of
+    // it; freed once that event has completed (see free_retired_rings)
+    struct RetiredRing {
+        char* ring;
+        cudaEvent_t done;
+    };
+    std::vector<RetiredRing> stg_retired;
     std::vector<cudaEvent_t> event_pool;
 
     // scratch of uploads, removals and reads: a memory pool of this state that
@@ -571,11 +577,27 @@ cudaError_t take_event(nxm_state* s, cudaEvent_t* e) {
     return cudaEventCreateWithFlags(e, cudaEventDisableTiming);
 }
 
-// Frees the outgrown staging rings (their copies have all run: call only
-// with the stream drained).
-void free_retired_rings(nxm_state* s) {
-    for (char* r : s->stg_retired) cudaFreeHost(r);
-    s->stg_retired.clear();
+// Frees the outgrown staging rings whose copies have all run (the event
+// recorded when the ring was retired has completed).  `drained`: the caller
+// has just waited for the stream, so every such event is complete.
+// cudaFreeHost may wait for the device, so calls that must not block (the
+// ring reservation of a queued upload) free only while the stream is idle;
+// ticket waits and nxm_synchronize free as soon as the copies are done.
+// A serving loop that only waits on tickets therefore keeps no outgrown ring
+// past the first ticket wait after its copies ran.
+void free_retired_rings(nxm_state* s, bool drained = true) {
+    size_t kept = 0;
+    for (auto& r : s->stg_retired) {
+        const bool done = drained || cudaEventQuery(r.done) == cudaSuccess;
+        if (done) {
+            cudaFreeHost(r.ring);
+            s->event_pool.push_back(r.done);
+        } else {
+            s->stg_retired[kept++] = r;
+        }
+    }
+    s->stg_retired.resize(kept);
+    (void)cudaGetLastError();  // a not-ready query is not an error
 }
 
 // A new ring of at least `bytes` * 4 (twice the old one, 1 MB at least, up
@@ -586,7 +608,13 @@ constexpr size_t kRingMax = size_t(1) << 30;
 cudaError_t staging_grow(nxm_state* s, size_t bytes) {
     for (const auto& sp : s->stg_live) s->event_pool.push_back(sp.done);  // an event may be recorded again
     s->stg_live.clear();
-    if (s->stg) s->stg_retired.push_back(s->stg);
+    if (s->stg) {
+        cudaEvent_t done;
+        cudaError_t e = take_event(s, &done);
+        if (e == cudaSuccess) e = cudaEventRecord(done, s->stream);  // after the last copy out of the ring
+        if (e != cudaSuccess) return e;
+        s->stg_retired.push_back(nxm_state::RetiredRing{s->stg, done});
+    }
     s->stg = nullptr;
     const size_t cap = std::max({bytes * 4, std::min(s->stg_cap * 2, kRingMax), size_t(1) << 20});
     s->stg_cap = 0;
@@ -603,6 +631,8 @@ cudaError_t staging_grow(nxm_state* s, size_t bytes) {
 // A ring region of `bytes` (256-aligned) whose earlier copies have run.
 cudaError_t staging_reserve(nxm_state* s, size_t bytes, char** out) {
     bytes = (bytes + 255) & ~size_t(255);
+    if (!s->stg_retired.empty() && cudaStreamQuery(s->stream) == cudaSuccess) free_retired_rings(s);
+    (void)cudaGetLastError();
     if (bytes * 2 > s->stg_cap) {
         const cudaError_t e = staging_grow(s, bytes);
         if (e != cudaSuccess) return e;
@@ -2600,6 +2630,7 @@ int retire_fences(nxm_state* s, uint64_t upto, bool wait) {
         s->event_pool.push_back(e);
         s->fences.pop_front();
     }
+    if (wait && !s->stg_retired.empty()) free_retired_rings(s, /*drained=*/false);
     return NXM_OK;
 }
 

@@ -350,6 +350,11 @@ class MpmState:
     def read_scene_positions(self, scene: int) -> np.ndarray:
         return self.read_positions_range(*self.scene_range(scene))
 
+    def read_scene_particles(self, scene: int) -> dict:
+        """Every field of ``read_particles`` for the particles of one scene."""
+        first, count = self.scene_range(scene)
+        return {k: v[first:first + count] for k, v in self.read_particles().items()}
+
     # -- asynchronous reads and tickets --------------------------------------------
     def fence(self) -> int:
         """A ticket for the work queued on the state's stream so far."""

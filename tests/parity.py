@@ -73,3 +73,99 @@ def rel_l2(a, b) -> float:
     b = np.asarray(b, np.float64)
     den = np.linalg.norm(b)
     return float(np.linalg.norm(a - b) / (den if den > 0 else 1.0))
+
+
+# ---------------------------------------------------------------------------
+# Accuracy of a run against the oracle, measured on what the run changed.
+#
+# A relative L2 of positions divides by |x|, which is of order 1 in a unit
+# domain, while 100 steps move the particles by 1e-4 to 1e-3 of that: a step
+# that returned its inputs unchanged would score below a 1e-3 bound.  The
+# errors below divide by the oracle's own change from the starting state
+# instead, so an unmoved result scores exactly 1 in every field that moved.
+# A field that only moves by rounding (F and C of a body in free fall) is
+# measured against a noise floor instead of its change: 100 float32 ulps
+# (1.2e-5) of the field's scale (the largest |x| for positions, the CFL speed
+# dx/dt for v, m/dt for C = m grad v - stress term, 1 for F), so that rounding
+# noise is not scored as error.
+
+STATE_KEYS = ("pos", "vel", "aff", "def_grad")
+
+# Fast mode (atomic scatter P2G, fused multiply-adds, fast model forms) after a
+# full run: bounds on change_rel_l2 per field.  The position bound is the
+# accuracy target of the path (1e-3); v, C and F get looser bounds because
+# Drucker-Prager sand amplifies rounding differences through its return map.
+FAST_BOUNDS = {"pos": 1e-3, "vel": 1e-2, "aff": 5e-2, "def_grad": 1e-2}
+# Deterministic mode (gather P2G in the reference's order, --fmad=false).
+DET_BOUNDS = {"pos": 1e-5, "vel": 1e-4, "aff": 1e-3, "def_grad": 1e-4}
+
+
+def change_rel_l2(got, want, start, floor: float = 0.0) -> float:
+    """||got - want|| / max(||want - start||, floor * sqrt(size)): the error of
+    `got` against the oracle's `want`, relative to how far the oracle moved
+    from `start` (or to the noise floor, per element, when it moved less).
+    Returns 0 when got == want, 1 when got == start (and the change is above
+    the floor), and inf when nothing moved, no floor is given and got differs."""
+    g = np.asarray(got, np.float64)
+    w = np.asarray(want, np.float64)
+    s = np.asarray(start, np.float64)
+    num = float(np.linalg.norm(g - w))
+    den = max(float(np.linalg.norm(w - s)), floor * np.sqrt(w.size))
+    if den == 0.0:
+        return 0.0 if num == 0.0 else float("inf")
+    return num / den
+
+
+def start_state(batch, dx: float | None = None, dt: float | None = None) -> dict:
+    """The fields of a ParticleBatch (or a Scene) that a step changes, as a
+    run's start, with the per-field noise floors of the scene's dx and dt."""
+    if hasattr(batch, "particles"):
+        dx, dt, batch = batch.dx, batch.dt, batch.particles
+    out = {k: np.array(getattr(batch, k), np.float32, copy=True) for k in STATE_KEYS}
+    if dx is not None and dt is not None:
+        m = float(np.mean(batch.mass)) if batch.n else 0.0
+        xmax = float(np.abs(batch.pos).max()) if batch.n else 0.0
+        u = 100.0 * float(np.finfo(np.float32).eps)
+        out["_floor"] = {"pos": u * xmax, "vel": u * dx / dt, "aff": u * m / dt, "def_grad": u}
+    return out
+
+
+def state_errors(got: dict, want: dict, start: dict) -> dict:
+    fl = start.get("_floor", {})
+    return {k: change_rel_l2(got[k], want[k], start[k], fl.get(k, 0.0)) for k in STATE_KEYS}
+
+
+def moved_fields(want: dict, start: dict) -> list:
+    """Fields whose change exceeds its noise floor (an unmoved result must fail these)."""
+    fl = start.get("_floor", {})
+    return [k for k in STATE_KEYS if np.linalg.norm(np.asarray(want[k], np.float64) - start[k]) >
+            fl.get(k, 0.0) * np.sqrt(np.asarray(want[k]).size)]
+
+
+def check_state(got: dict, want: dict, start: dict, bounds: dict):
+    """Errors of `got` against `want` per field (change_rel_l2) and the list of
+    fields over their bound (empty = within tolerance)."""
+    err = state_errors(got, want, start)
+    bad = [f"{k}: {err[k]:.3e} > {bounds[k]:.0e}" for k in STATE_KEYS if not err[k] <= bounds[k]]
+    return err, bad
+
+
+def format_errors(err: dict) -> str:
+    return ", ".join(f"{k} {v:.3e}" for k, v in err.items())
+
+
+def assert_run_matches(label, g, o, o64, start, bounds):
+    """The run's state against the FP32 oracle within `bounds` (change_rel_l2
+    per field), the same particles disabled; FP64-oracle errors printed beside
+    them.  Negative control: the same check on the unmoved input must fail."""
+    err, bad = check_state(g, o, start, bounds)
+    err64 = state_errors(g, o64, start)
+    print(f"{label}: vs f32 [{format_errors(err)}]; vs f64 [{format_errors(err64)}]")
+    assert np.array_equal(g["enabled"], o["enabled"])
+    assert not bad, f"{label}: " + "; ".join(bad)
+    moved = moved_fields(o, start)
+    _, bad0 = check_state({k: start[k] for k in STATE_KEYS}, o, start, bounds)
+    failed = {b.split(":")[0] for b in bad0}
+    assert "pos" in moved and set(moved) <= failed, \
+        f"{label}: the unmoved input passes the check for {sorted(set(moved) - failed)}"
+    return err

@@ -1,11 +1,13 @@
-"""nxm_sort_blocks_noalloc: the block sort for callers that cannot allocate
-device memory (graph-captured code, allocator-less runtimes, fixed memory
-pools).  Its grid tables live in a fixed device array of the library, so this
+"""nxm_sort_blocks_noalloc: the block sort for callers that may not allocate
+GPU memory (a host program that reserves its device memory at start-up and
+forbids allocations in its frame loop; a plugin handed device buffers but no
+allocator).  Its grid tables live in a fixed device array of the library, so this
 checks, through the C ABI, that two calls in a row (on different scenes, so
 that state left in the shared array would show) give the same active blocks
 and the same per-block primary particles, in z-slab order, as the sort of
 the existing entry point (nxm_debug_sort on a state), and that sizes beyond
-the fixed limits are rejected.  Integer results: compared bit for bit.
+the fixed limits are rejected (too many particles, more blocks than
+max_blocks, more distinct blocks than the fixed hash holds).  Integer results: compared bit for bit.
 
 Named to be collected last, so a run that stops at the first failure has
 already run every other test.
@@ -80,5 +82,14 @@ def test_noalloc_sort_rejects_sizes_beyond_its_limits(gpu_lib):
     rc = gpu_lib.nxm_sort_blocks_noalloc(dummy.data_ptr(), (1 << 26) + 1, 0.1, dummy.data_ptr(), dummy.data_ptr(),
                                          dummy.data_ptr(), 1, C.byref(n), None)
     assert rc == NXM_E_CAPACITY
+    # more distinct blocks than the fixed hash has slots (2 x 16384): particles
+    # 8 cells apart, so that each one's 2x2x2 block neighbourhood is its own
+    dx = 1.0 / 64.0
+    k = np.arange(18, dtype=np.float32)
+    grid = np.stack(np.meshgrid(k, k, k, indexing="ij"), -1).reshape(-1, 3)
+    spread = ((grid * 8.0 + 2.5) * np.float32(dx)).astype(np.float32)
+    assert 8 * len(spread) > 2 * 16384
+    rc, nb, *_ = _noalloc_sort(gpu_lib, torch, spread, dx, 16384)
+    assert rc == NXM_E_CAPACITY and nb == 0
     # a valid call right after a rejected one still matches the existing sort
     _check_against_existing_entry_point(gpu_lib, torch, sc)
