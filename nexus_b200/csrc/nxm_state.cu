@@ -692,8 +692,21 @@ void host_copy(void* dst, const void* src, size_t bytes) {
 
 // Copies `bytes` of host data to `dst` in stream order; the caller's buffer
 // is free when the call returns and the host never waits for queued work.
+// Large copies go through the ring in pieces of kUploadPiece: a ring a few
+// pieces long serves a bulk upload of any size (a piece's region is reused
+// once its copy has run, which on an idle stream is by the time the host has
+// filled the next pieces), instead of pinning a ring as large as the upload.
+constexpr size_t kUploadPiece = size_t(16) << 20;
 cudaError_t upload_async(nxm_state* s, void* dst, const void* src, size_t bytes) {
     if (bytes == 0) return cudaSuccess;
+    if (bytes > kUploadPiece) {
+        for (size_t off = 0; off < bytes; off += kUploadPiece) {
+            const cudaError_t e = upload_async(s, static_cast<char*>(dst) + off, static_cast<const char*>(src) + off,
+                                               std::min(kUploadPiece, bytes - off));
+            if (e != cudaSuccess) return e;
+        }
+        return cudaSuccess;
+    }
     char* h = nullptr;
     cudaError_t e = staging_reserve(s, bytes, &h);
     if (e != cudaSuccess) return e;

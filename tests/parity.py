@@ -98,6 +98,13 @@ STATE_KEYS = ("pos", "vel", "aff", "def_grad")
 FAST_BOUNDS = {"pos": 1e-3, "vel": 1e-2, "aff": 5e-2, "def_grad": 1e-2}
 # Deterministic mode (gather P2G in the reference's order, --fmad=false).
 DET_BOUNDS = {"pos": 1e-5, "vel": 1e-4, "aff": 1e-3, "def_grad": 1e-4}
+# Where a run moves the particles by only a few hundred float32 ulps of their
+# positions (the mixed-materials scene moves 2e-4 in 50 steps at |x| ~ 0.5),
+# single precision alone limits these errors: the FP32 oracle itself is
+# 4.6e-4 from the FP64 oracle there.  A field's bound is therefore the larger
+# of its fixed bound and NOISE_FACTOR times the FP32 oracle's own error
+# against the FP64 oracle in that field.
+NOISE_FACTOR = 4.0
 
 
 def change_rel_l2(got, want, start, floor: float = 0.0) -> float:
@@ -154,13 +161,23 @@ def format_errors(err: dict) -> str:
     return ", ".join(f"{k} {v:.3e}" for k, v in err.items())
 
 
+def noise_bounds(bounds: dict, o32: dict, o64: dict, start: dict) -> dict:
+    """Per field: max(bound, NOISE_FACTOR x the FP32 oracle's error against
+    the FP64 oracle), the precision floor of single-precision state."""
+    noise = state_errors(o32, o64, start)
+    return {k: max(bounds[k], NOISE_FACTOR * noise[k]) for k in STATE_KEYS}
+
+
 def assert_run_matches(label, g, o, o64, start, bounds):
-    """The run's state against the FP32 oracle within `bounds` (change_rel_l2
-    per field), the same particles disabled; FP64-oracle errors printed beside
-    them.  Negative control: the same check on the unmoved input must fail."""
+    """The run's state against the FP32 oracle within `bounds` raised to the
+    FP32 precision floor of the scene (noise_bounds; change_rel_l2 per field),
+    the same particles disabled; FP64-oracle errors printed beside them.
+    Negative control: the same check on the unmoved input must fail."""
+    bounds = noise_bounds(bounds, o, o64, start)
     err, bad = check_state(g, o, start, bounds)
     err64 = state_errors(g, o64, start)
-    print(f"{label}: vs f32 [{format_errors(err)}]; vs f64 [{format_errors(err64)}]")
+    print(f"{label}: vs f32 [{format_errors(err)}]; vs f64 [{format_errors(err64)}]; "
+          f"bounds [{format_errors(bounds)}]")
     assert np.array_equal(g["enabled"], o["enabled"])
     assert not bad, f"{label}: " + "; ".join(bad)
     moved = moved_fields(o, start)

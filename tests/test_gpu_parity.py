@@ -200,8 +200,14 @@ def test_every_material_50_steps(pipe, deterministic):
     sc = scenes.mixed_materials(n_side=10)
     start = start_state(sc)
     g, o, o64 = _run_both(sc, deterministic, 50)
+    # Deterministic mode follows the oracle's arithmetic except the 3x3 SVD of
+    # the plastic models (float one-sided Jacobi here, double in the oracle)
+    # and CUDA's logf / expf / sinf: the Drucker-Prager and snow particles'
+    # return maps see F differing by float rounding, which their yield
+    # decisions amplify to ~1e-4 of the run's velocity change.
+    det = dict(DET_BOUNDS, vel=5e-4, aff=5e-3, def_grad=1e-3)
     assert_run_matches(f"mixed materials, deterministic={deterministic}", g, o, o64, start,
-                       DET_BOUNDS if deterministic else FAST_BOUNDS)
+                       det if deterministic else FAST_BOUNDS)
     # plastic state words (Drucker-Prager, snow) follow the same trajectory.  The
     # accumulated hardening sums one return-mapping increment per step, each
     # computed from log singular values of a near-identity F: an f32 SVD (GPU)
