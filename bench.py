@@ -179,10 +179,10 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def make_scene(workload: str, seed_offset: int = 0):
+def make_scene(workload: str, seed_offset: int = 0, scale: float = 1.0):
     from nexus_b200 import scenes
     if workload == "sand_water":
-        return scenes.sand_water(seed=2 + seed_offset)
+        return scenes.sand_water(scale=scale, seed=2 + seed_offset)
     if workload == "elastic_cube":
         return scenes.elastic_cube(seed=1 + seed_offset)
     raise SystemExit(f"unknown workload {workload}")
@@ -240,7 +240,7 @@ def run_reference(args, world, rank):
         return
     os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count()))
     from oracle.oracle import OracleScene
-    scene = make_scene(args.workload)
+    scene = make_scene(args.workload, scale=args.scale)
     cores = int(os.environ["OMP_NUM_THREADS"])
     o = OracleScene(scene, "f32")
     warm = min(args.warmup, 2)
@@ -322,7 +322,7 @@ def run_ours(args, world, rank, local):
     nb.build()
     load()
     torch.cuda.set_device(local)
-    scene = make_scene(args.workload, seed_offset=rank)
+    scene = make_scene(args.workload, seed_offset=rank, scale=args.scale)
     n = scene.n
     pipe = MpmPipeline()
     st = state_from_scene(scene)
@@ -365,7 +365,7 @@ def run_ours(args, world, rank, local):
     step_s = ms / args.steps / 1e3
     peak, peak_kind = load_peaks()
     achieved = bytes_per_step / step_s / 1e9
-    traffic, traffic_info = load_traffic(args.workload)
+    traffic, traffic_info = load_traffic(args.workload if args.scale == 1.0 else "scaled")
     phase_roof = phase_rooflines(phases, scene, st, peak)
 
     # end to end through the C ABI from pinned host buffers (every rank its own
@@ -379,7 +379,7 @@ def run_ours(args, world, rank, local):
         e2e["d2h_bytes_per_step"] *= world
     del st
     batched = measure_batched(args, world, rank, torch) if args.batched_steps > 0 else None
-    serving = measure_serving(args, torch) if (args.serving_requests > 0 and world == 1) else None
+    serving = measure_serving(args, torch, world, rank) if args.serving_requests > 0 else None
     coupled = measure_coupled(args, torch) if (args.coupled_steps > 0 and world == 1) else None
     cube = measure_cube(torch) if (args.cube and world == 1) else None
 
@@ -534,26 +534,31 @@ def measure_coupled(args, torch):
             "how": "timed steps include writing every kinematic body's velocity (one stream-ordered call per step)"}
 
 
-def measure_serving(args, torch):
+def measure_serving(args, torch, world: int = 1, rank: int = 0):
     """Continuous batching of a Poisson request stream (mean 200 scenes/s):
     aggregate particle-steps/s and p50/p99 arrival-to-completion latency,
     beside a FIFO loop that runs each request alone (plain step) in arrival
-    order, whose latencies come from each scene's measured plain step time."""
+    order, whose latencies come from each scene's measured plain step time.
+    With N ranks, each serves its LPT share of the same stream (no exchange on
+    the data path); latencies are gathered and the rate is the whole stream's
+    work over the slowest rank's wall time."""
     from nexus_b200 import scenes as S
     from nexus_b200.mpm import MpmPipeline, state_from_scene
-    from nexus_b200.serving import MpmServer, poisson_requests, latency_summary
+    from nexus_b200.serving import MpmServer, poisson_requests, latency_summary, serve_sharded, shard_requests
     reqs = poisson_requests(args.serving_requests, 200.0, 3000, S.serving_scene, (50, 2000))
+    mine = shard_requests(reqs, world, rank) if world > 1 else reqs
     srv = MpmServer(hbm_budget=150e9, particles_capacity=1 << 26, grid_capacity=1 << 22)
-    srv.prepare([r.scene for r in reqs])  # device states allocated before the first arrival
+    srv.prepare([r.scene for r in mine])  # device states allocated before the first arrival
+    barrier(world)
     t0 = time.perf_counter()
-    results, rejected = srv.run(reqs)
-    wall = time.perf_counter() - t0
+    results, rejected, failed = serve_sharded(srv, reqs, world, rank)
+    wall = all_max(time.perf_counter() - t0, world)
     summ = latency_summary(results)
     del srv
     # FIFO plain loop: per-scene step time measured alone, then a virtual clock
     pipe = MpmPipeline()
     t_done, lat = 0.0, []
-    for r in sorted(reqs, key=lambda q: q.arrival):
+    for r in sorted(mine, key=lambda q: q.arrival):
         one = state_from_scene(r.scene)
         s1 = torch.cuda.ExternalStream(one.cuda_stream())
         for _ in range(3):
@@ -570,10 +575,17 @@ def measure_serving(args, torch):
         del one
         t_done = max(t_done, r.arrival) + run_s
         lat.append(t_done - r.arrival)
+    if world > 1:
+        import torch.distributed as dist
+        parts = [None] * world
+        dist.all_gather_object(parts, lat)
+        lat = [x for p in parts for x in p]
+    t_done = all_max(t_done, world)
     work = sum(r.scene.n * r.steps for r in reqs)
     return {"workload": "serving_poisson_200_per_s", "requests": len(reqs), "rejected": len(rejected),
-            "particles_per_request": "logU(2048, 524288)", "steps_per_request": "U{50..2000}",
+            "failed": len(failed), "particles_per_request": "logU(2048, 524288)", "steps_per_request": "U{50..2000}",
             "value": work / wall, "unit": UNIT, "wall_s": wall, "p50_s": summ["p50_s"], "p99_s": summ["p99_s"],
+            "parallelism": f"request-sharded{world}" if world > 1 else "single",
             "plain_fifo": {"value": work / t_done, "unit": UNIT, "p50_s": float(np.percentile(lat, 50)),
                            "p99_s": float(np.percentile(lat, 99)),
                            "how": "each request alone in its own state, in arrival order; per-scene step time "
@@ -646,6 +658,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="sand_water", choices=["sand_water", "elastic_cube"])
+    ap.add_argument("--scale", type=float, default=1.0,
+                    help="sand_water only: fraction of its particles (smaller cases for profiling)")
     ap.add_argument("--ref-steps", type=int, default=10, help="oracle steps of the cpu_baseline leg")
     ap.add_argument("--e2e-steps", type=int, default=500)
     ap.add_argument("--no-e2e", dest="e2e", action="store_false")
@@ -654,7 +668,7 @@ def main():
                     help="timed steps of the batched mix (0: skip it)")
     ap.add_argument("--batched-scenes", type=int, default=256)
     ap.add_argument("--plain-steps", type=int, default=10)
-    ap.add_argument("--serving-requests", type=int, default=200, help="0: skip the serving measurement")
+    ap.add_argument("--serving-requests", type=int, default=4000, help="0: skip the serving measurement")
     ap.add_argument("--coupled-steps", type=int, default=300, help="timed steps of the coupled mix (0: skip it)")
     ap.add_argument("--coupled-scenes", type=int, default=64)
     ap.add_argument("--no-cube", dest="cube", action="store_false", help="skip the 32k elastic cube leg")

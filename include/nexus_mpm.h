@@ -465,6 +465,12 @@ NXM_API int nxm_state_status(nxm_state* state, uint32_t* bits, int clear);
  * never drains; 0 on the first call).  Each step's status reaches the host
  * one call late. */
 NXM_API int nxm_state_status_pipelined(nxm_state* state, uint32_t* bits);
+/* Non-blocking status poll for loops that keep many steps queued: when the
+ * word posted by an earlier call has been stored (its store ran on the GPU),
+ * returns it with *ready = 1 and posts a new one after the work issued so
+ * far; otherwise returns *ready = 0 at once and posts nothing.  The host
+ * never waits.  No counterpart in the reference (its step has no status). */
+NXM_API int nxm_state_status_poll(nxm_state* state, uint32_t* bits, int* ready);
 /* Tickets: nxm_state_fence marks the work queued on the state's stream so
  * far; nxm_state_ticket_done tells (without waiting) whether that work has
  * run, nxm_state_ticket_wait waits for it.  Tickets complete in the order

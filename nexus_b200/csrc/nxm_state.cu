@@ -390,6 +390,12 @@ struct nxm_state {
     uint32_t* h_status_dev = nullptr;  // the same words, device view
     cudaEvent_t status_done[2] = {};
     uint64_t status_calls = 0;
+    // nxm_state_status_poll: its own posted word (slot 0 of h_poll), the
+    // event after that post, and whether a post is outstanding
+    uint32_t* h_poll = nullptr;
+    uint32_t* h_poll_dev = nullptr;
+    cudaEvent_t poll_done = nullptr;
+    bool poll_outstanding = false;
 
     // batched scenes (scene_blocks != 0): scene slots on the block-key grid
     // (see Params), each a contiguous range of particle ids with its own colliders
@@ -1859,6 +1865,8 @@ void nxm_state_destroy(nxm_state* s) {
     dfree(s->d_render); dfree(s->d_palette);
     if (s->h_vel6) cudaFreeHost(s->h_vel6);
     if (s->h_status) cudaFreeHost(s->h_status);
+    if (s->h_poll) cudaFreeHost(s->h_poll);
+    if (s->poll_done) cudaEventDestroy(s->poll_done);
     if (s->stg) cudaFreeHost(s->stg);
     free_retired_rings(s);
     for (const auto& sp : s->stg_live) cudaEventDestroy(sp.done);
@@ -2594,6 +2602,35 @@ int nxm_synchronize(nxm_state* s) {
     if (rc) return rc;
     if (bits & NXM_STATUS_HASH_FULL) return NXM_E_HASH_FULL;
     if (bits & (NXM_STATUS_BLOCK_CAPACITY | NXM_STATUS_MISSING_BLOCK | NXM_STATUS_SORT_CAPACITY)) return NXM_E_CAPACITY;
+    return NXM_OK;
+}
+
+int nxm_state_status_poll(nxm_state* s, uint32_t* bits, int* ready) {
+    if (!s || !bits || !ready) return NXM_E_INVALID;
+    if (!s->h_poll) {
+        NXM_TRY(cudaHostAlloc(reinterpret_cast<void**>(&s->h_poll), sizeof(uint32_t), cudaHostAllocMapped));
+        s->h_poll[0] = 0;
+        NXM_TRY(cudaHostGetDevicePointer(reinterpret_cast<void**>(&s->h_poll_dev), s->h_poll, 0));
+        NXM_TRY(cudaEventCreateWithFlags(&s->poll_done, cudaEventDisableTiming));
+    }
+    *bits = 0;
+    *ready = 0;
+    if (s->poll_outstanding) {
+        const cudaError_t q = cudaEventQuery(s->poll_done);
+        if (q == cudaErrorNotReady) {
+            (void)cudaGetLastError();
+            return NXM_OK;  // the last post has not run yet: no new one either
+        }
+        NXM_TRY(q);
+        *bits = s->h_poll[0];
+        *ready = 1;
+        s->poll_outstanding = false;
+    }
+    k_post_status<<<1, 32, 0, s->stream>>>(s->d_counters, s->h_poll_dev);
+    s->launches += 1;
+    NXM_TRY(cudaGetLastError());
+    NXM_TRY(cudaEventRecord(s->poll_done, s->stream));
+    s->poll_outstanding = true;
     return NXM_OK;
 }
 

@@ -98,6 +98,7 @@ SIGNATURES = {
     "nxm_read_cdf": (C.c_int, [_vp, _f]),
     "nxm_simulate_frame": (C.c_int, [_vp, _vp, C.c_uint32, C.c_uint32, _u]),
     "nxm_state_status_pipelined": (C.c_int, [_vp, _u]),
+    "nxm_state_status_poll": (C.c_int, [_vp, _u, C.POINTER(C.c_int)]),
     "nxm_state_fence": (C.c_int, [_vp, C.POINTER(C.c_uint64)]),
     "nxm_state_ticket_done": (C.c_int, [_vp, C.c_uint64, C.POINTER(C.c_int)]),
     "nxm_state_ticket_wait": (C.c_int, [_vp, C.c_uint64]),
@@ -579,6 +580,13 @@ class MpmState:
         v = C.c_uint32()
         _check(self.lib.nxm_state_status_pipelined(self.h, C.byref(v)), "state_status_pipelined")
         return v.value
+
+    def status_poll(self):
+        """Non-blocking: the status word posted by an earlier call once its
+        store has run on the GPU, else None (nothing waits)."""
+        v, ready = C.c_uint32(), C.c_int()
+        _check(self.lib.nxm_state_status_poll(self.h, C.byref(v), C.byref(ready)), "state_status_poll")
+        return v.value if ready.value else None
 
     def kernel_launches(self) -> int:
         return int(self.lib.nxm_state_kernel_launches(self.h))

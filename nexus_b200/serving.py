@@ -17,6 +17,16 @@ ticket completes; each batched state keeps at most a few steps queued ahead.
 Each scene steps exactly as it would alone (scene-local coordinates, its own
 block-key region and colliders), so a result does not depend on what else was
 in the mix or on when it was admitted.
+
+Failures: the device status word of each batched state (grid blocks or hash
+slots exhausted, a particle without a block) is polled without waiting
+(nxm_state_status_poll: a word posted after some earlier step, once its store
+has run).  When a state reports a status bit, every scene that
+may have taken part in the failing step (those active on the state and those
+whose final read is still in flight) is evicted and reported in
+``MpmServer.failed`` with the status bits; the bits are cleared, the state's
+grid admission estimate is doubled so that the same mix is not admitted
+again, and serving continues with the other requests.
 """
 from __future__ import annotations
 
@@ -43,6 +53,13 @@ class Request:
     scene: Scene
     steps: int
     arrival: float  # seconds after the start of the run
+
+
+@dataclass
+class Failure:
+    rid: int
+    status: int  # NXM_STATUS_* bits the state reported
+    steps_done: int  # steps the scene had taken when it was evicted (its budget if it had finished)
 
 
 @dataclass
@@ -78,6 +95,7 @@ class _Group:
         self.active = {}  # slot -> [request, remaining steps, admitted time]
         self.particles = 0
         self.grid = 0
+        self.grid_factor = 1.0  # admission estimate of a scene's grid blocks, doubled after an overflow
         self.steps = deque()  # tickets of the steps queued on this state
 
 
@@ -93,6 +111,7 @@ class MpmServer:
         self.deterministic = deterministic
         self.scene_blocks = scene_blocks  # None: 64 blocks per scene axis at dx >= 1/128, else 128
         self.groups = {}
+        self.failed = {}  # request id -> Failure
         self.in_use = 0
         self.steps_taken = 0
         self.particle_steps = 0
@@ -122,14 +141,43 @@ class MpmServer:
 
     def _fits(self, sc: Scene, g: _Group) -> bool:
         return (self.in_use + footprint(sc) <= self.budget and g.particles + sc.n <= self.particles_capacity
-                and g.grid + sc.grid_capacity <= self.grid_capacity)
+                and g.grid + sc.grid_capacity * g.grid_factor <= self.grid_capacity)
+
+    def _usage(self, g: _Group):
+        g.particles = sum(rec[0].scene.n for rec in g.active.values())
+        g.grid = sum(rec[0].scene.grid_capacity * g.grid_factor for rec in g.active.values())
+        self.in_use = sum(footprint(rec[0].scene) for gg in self.groups.values() for rec in gg.active.values())
+
+    def _fail(self, g: _Group, bits: int, reads: deque):
+        """Evicts every scene of `g` that may have taken part in the failing
+        step (see the module docstring) and reports it in self.failed."""
+        for slot, (r, left, _) in g.active.items():
+            self.failed[r.rid] = Failure(r.rid, bits, r.steps - left)
+        if g.active:
+            g.state.remove_scenes(list(g.active))
+        g.active.clear()
+        keep = deque()
+        for item in reads:
+            if item[0] is g:
+                self.failed[item[2].rid] = Failure(item[2].rid, bits, item[2].steps)
+                self._release(item[4])
+            else:
+                keep.append(item)
+        reads.clear()
+        reads.extend(keep)
+        g.state.status(clear=True)  # waits for the stream: any earlier post has run
+        g.state.status_poll()  # that post's word predates the clear: dropped
+        g.grid_factor *= 2.0
+        self._usage(g)
 
     def run(self, requests, clock=time.perf_counter, idle_sleep: float = 1e-4, depth: int = 32):
         """Serves ``requests`` (any order; by arrival) and returns the results by
-        request id, plus requests that can never fit (rejected).  ``depth``:
-        steps each batched state may have queued ahead of the GPU."""
+        request id, plus requests that can never fit (rejected); requests
+        evicted after a device status error are in ``self.failed``.
+        ``depth``: steps each batched state may have queued ahead of the GPU."""
         pending = sorted(requests, key=lambda r: (r.arrival, r.rid))
         results, rejected = {}, []
+        self.last_results = results
         reads = deque()  # (group, ticket, request, admitted time, pinned buffer), in issue order per state
         t0 = clock()
         while pending or reads or any(g.active for g in self.groups.values()):
@@ -138,8 +186,9 @@ class MpmServer:
             while pending and pending[0].arrival <= now:
                 r = pending[0]
                 g = self._group(r.scene)
-                if footprint(r.scene) > self.budget or r.scene.n > self.particles_capacity:
-                    rejected.append(pending.pop(0))
+                if (footprint(r.scene) > self.budget or r.scene.n > self.particles_capacity
+                        or r.scene.grid_capacity * g.grid_factor > self.grid_capacity):
+                    rejected.append(pending.pop(0))  # can never fit, even alone
                     continue
                 if not self._fits(r.scene, g):
                     break
@@ -148,7 +197,7 @@ class MpmServer:
                                          r.scene.tri_vertices if r.scene.tri_vertices.size else None)
                 g.active[slot] = [r, r.steps, clock() - t0]
                 g.particles += r.scene.n
-                g.grid += r.scene.grid_capacity
+                g.grid += r.scene.grid_capacity * g.grid_factor
                 self.in_use += footprint(r.scene)
             # results whose reads have landed
             for _ in range(len(reads)):
@@ -172,6 +221,10 @@ class MpmServer:
                 g.steps.append(g.state.fence())
                 self.steps_taken += 1
                 self.particle_steps += g.particles
+                bits = g.state.status_poll()  # an earlier point of this state's stream, or None
+                if bits:
+                    self._fail(g, bits, reads)
+            busy = [g for g in busy if g.active]
             for g in busy:
                 done = []
                 for slot, rec in g.active.items():
@@ -185,10 +238,7 @@ class MpmServer:
                     reads.append((g, ticket, r, admitted, buf))
                 if done:  # queued behind the reads above
                     g.state.remove_scenes(done)
-                    g.particles = sum(rec[0].scene.n for rec in g.active.values())
-                    g.grid = sum(rec[0].scene.grid_capacity for rec in g.active.values())
-                    self.in_use = sum(footprint(rec[0].scene) for gg in self.groups.values()
-                                      for rec in gg.active.values())
+                    self._usage(g)
         return results, rejected
 
 
@@ -210,3 +260,34 @@ def latency_summary(results) -> dict:
     lat = np.array([r.latency for r in results.values()]) if results else np.zeros(0)
     return {"completed": int(lat.size), "p50_s": float(np.percentile(lat, 50)) if lat.size else None,
             "p99_s": float(np.percentile(lat, 99)) if lat.size else None}
+
+
+def shard_requests(requests, world: int, rank: int) -> list:
+    """This rank's share of a request stream for serving on `world` GPUs: the
+    longest-processing-time partition (nexus_b200.sharding) of the requests'
+    particle-steps.  Scenes are independent, so ranks exchange nothing on the
+    data path; every rank computes the same partition from the same stream."""
+    from .sharding import shard_scenes
+    work = [r.scene.n * r.steps for r in requests]
+    return [requests[i] for i in shard_scenes(work, world)[rank]]
+
+
+def serve_sharded(server: "MpmServer", requests, world: int, rank: int, **run_kw):
+    """Runs this rank's shard of `requests` on `server`; returns (results,
+    rejected, failed) of the whole job, gathered on every rank (each result
+    without its positions, which stay on the rank that computed them)."""
+    mine = shard_requests(requests, world, rank) if world > 1 else list(requests)
+    results, rejected = server.run(mine, **run_kw)
+    if world == 1:
+        return results, rejected, dict(server.failed)
+    import torch.distributed as dist
+    light = {rid: Result(r.rid, r.n, r.steps, r.arrival, r.admitted, r.completed, np.zeros((0, 3), np.float32))
+             for rid, r in results.items()}
+    parts = [None] * world
+    dist.all_gather_object(parts, (light, [r.rid for r in rejected], dict(server.failed)))
+    all_results, all_rejected, all_failed = {}, [], {}
+    for res, rej, fail in parts:
+        all_results.update(res)
+        all_rejected.extend(rej)
+        all_failed.update(fail)
+    return all_results, all_rejected, all_failed

@@ -525,3 +525,50 @@ def test_batched_coupled_scenes_step_as_alone(pipe):
     # the bodies moved as driven: pose integrated from the written velocities
     pose = bst.collider_pose(offs[0] + int(mix[0].kinematics[0, 0]))
     assert np.abs(pose[4:] - mix[0].colliders[int(mix[0].kinematics[0, 0])]["translation"]).max() > 0
+
+
+def test_hash_full_is_reported(pipe):
+    """More distinct block keys than the hash has slots (a grid of 8 blocks has
+    a 1024-slot hash; 216 particles 8 cells apart touch 1728 blocks): the step
+    reports STATUS_HASH_FULL, synchronize raises NXM_E_HASH_FULL, and no
+    particle is lost (those without a block are carried over unchanged)."""
+    from nexus_b200.mpm import NXM_E_HASH_FULL
+    from nexus_b200.models import ParticleModel
+    from nexus_b200.particles import ParticleBatch, collider_array
+    dx = 1.0 / 64.0
+    k = np.arange(6, dtype=np.float32)
+    pos = ((np.stack(np.meshgrid(k, k, k, indexing="ij"), -1).reshape(-1, 3) * 8.0 + 6.5) * np.float32(dx))
+    b = ParticleBatch.from_positions(pos.astype(np.float32), np.float32(dx / 4), 1000.0,
+                                     ParticleModel.elastic_neo_hookean(1e5, 0.3))
+    sc = scenes.Scene("spread", dx, 1.0e-4, (0.0, 0.0, -9.81), b, collider_array([]), 1, 8)
+    st = state_from_scene(sc)
+    pipe.step(st)
+    with pytest.raises(NexusError) as e:
+        st.synchronize()
+    assert e.value.code == NXM_E_HASH_FULL
+    bits = st.status(clear=True)
+    assert bits & 1 and bits & 2
+    got = st.read_positions()
+    assert np.isfinite(got).all() and np.abs(got - pos).max() <= dx
+
+
+def test_sort_capacity_is_reported(pipe):
+    """Deterministic mode orders each (block, z-slab) bucket in shared memory,
+    4096 particles at most: a pile of 5000 particles inside one slab reports
+    STATUS_SORT_CAPACITY (synchronize raises NXM_E_CAPACITY) instead of
+    overrunning; the step still completes."""
+    from nexus_b200.models import ParticleModel
+    from nexus_b200.particles import ParticleBatch, collider_array
+    dx = 1.0 / 64.0
+    rng = np.random.default_rng(3)
+    lo = np.float32(32 * dx)
+    pos = (lo + rng.uniform(0.6, 3.4, (5000, 3)).astype(np.float32) * np.float32(dx) * np.array([1, 1, 0.25], np.float32))
+    b = ParticleBatch.from_positions(pos.astype(np.float32), np.float32(dx / 4), 1000.0,
+                                     ParticleModel.elastic_neo_hookean(1e3, 0.3))
+    sc = scenes.Scene("pile", dx, 1.0e-5, (0.0, 0.0, 0.0), b, collider_array([]), 1, 64)
+    st = state_from_scene(sc, deterministic=True)
+    pipe.step(st)
+    with pytest.raises(NexusError) as e:
+        st.synchronize()
+    assert e.value.code == NXM_E_CAPACITY
+    assert st.status(clear=True) & 8

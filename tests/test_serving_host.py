@@ -31,6 +31,9 @@ class FakeState:
         self.ticket = 0
         self.done = 0
         self.max_queued_steps = 0
+        self.bits = 0  # sticky device status word
+        self.posted = 0  # the word a pipelined read returns next (one call late)
+        self.fail_over = None  # particles live at a step above which the step sets bit 2 (grid blocks)
 
     # -- setup calls of _Group
     def set_cell_width(self, dx, cap): pass
@@ -41,6 +44,8 @@ class FakeState:
     def _run_one(self):
         op = self.queue.pop(0)
         if op[0] == "step":
+            if self.fail_over is not None and sum(len(p) for p in self.scenes.values()) > self.fail_over:
+                self.bits |= 2
             for pos in self.scenes.values():
                 pos += 1.0
         elif op[0] == "read":
@@ -84,6 +89,17 @@ class FakeState:
     def ticket_wait(self, t):
         self._drain_to(t)
 
+    def status_poll(self):
+        out, self.posted = self.posted, self.bits
+        return out
+
+    def status(self, clear=False):
+        self._drain_to(self.ticket)
+        out = self.bits
+        if clear:
+            self.bits = 0
+        return out
+
 
 class FakePipeline:
     def step(self, st):
@@ -116,3 +132,89 @@ def test_served_requests_step_their_budget(monkeypatch, depth):
     while g.state.queue:  # the last removals are queued behind the reads
         g.state._run_one()
     assert not g.state.scenes  # every finished scene was removed
+
+
+def test_status_error_evicts_and_reports_the_scenes_of_the_failing_step(monkeypatch):
+    """A state whose step reports a status bit (here: more live particles than
+    its grid holds) has every scene that may have taken part evicted and
+    reported in `failed` with the bits; the bits are cleared, the state's grid
+    estimate doubled, and the other requests are served as usual."""
+    monkeypatch.setattr(serving, "MpmState", FakeState)
+    monkeypatch.setattr(serving, "MpmPipeline", FakePipeline)
+    monkeypatch.setattr(serving, "PinnedArray", FakeArray)
+    reqs = [serving.Request(i, _scene(i, 20), 30, 0.0) for i in range(3)]  # all three at once: 60 particles
+    reqs += [serving.Request(3 + i, _scene(3 + i, 20), 10, 100.0) for i in range(3)]  # later, one at a time fits
+    srv = serving.MpmServer(hbm_budget=1e12, particles_capacity=1 << 20, grid_capacity=192)
+    states = []
+    orig = srv._group
+
+    def group(sc):
+        g = orig(sc)
+        if g.state not in states:
+            g.state.fail_over = 50
+            states.append(g.state)
+        return g
+    srv._group = group
+    results, rejected = srv.run(reqs, clock=iter(np.arange(0.0, 1e6, 1e-2)).__next__, idle_sleep=0.0, depth=4)
+    assert not rejected
+    assert sorted(srv.failed) == [0, 1, 2]
+    assert all(f.status & 2 and 0 < f.steps_done < 30 for f in srv.failed.values())
+    (g,) = srv.groups.values()
+    assert g.grid_factor == 2.0 and g.state.bits == 0
+    # the later requests: the doubled estimate admits at most two at once (2 x 64 x 2 > 192), so they fit
+    assert sorted(results) == [3, 4, 5]
+    for r in reqs[3:]:
+        np.testing.assert_array_equal(results[r.rid].positions, r.scene.particles.pos + np.float32(r.steps))
+
+
+def _serve_rank(rank, world, port, out):
+    import datetime
+    import os
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        serving.MpmState, serving.MpmPipeline, serving.PinnedArray = FakeState, FakePipeline, FakeArray
+        rng = np.random.default_rng(5)
+        reqs = [serving.Request(i, _scene(i, int(rng.integers(1, 40))), int(rng.integers(1, 30)), 0.01 * i)
+                for i in range(20)]
+        mine = serving.shard_requests(reqs, world, rank)
+        srv = serving.MpmServer(hbm_budget=1e12, particles_capacity=1 << 20, grid_capacity=1 << 12)
+        results, rejected, failed = serving.serve_sharded(
+            srv, reqs, world, rank, clock=iter(np.arange(0.0, 1e6, 1e-3)).__next__, idle_sleep=0.0, depth=4)
+        ok = all(np.array_equal(srv_r.positions, reqs[rid].scene.particles.pos + np.float32(reqs[rid].steps))
+                 for rid, srv_r in srv_results(srv, mine, results).items())
+        out.put((rank, [r.rid for r in mine], sorted(results), rejected, sorted(failed), ok,
+                 sum(r.scene.n * r.steps for r in mine)))
+    finally:
+        dist.destroy_process_group()
+
+
+def srv_results(srv, mine, gathered):
+    """This rank's own results (with positions) among the gathered ones."""
+    return {r.rid: srv.last_results[r.rid] for r in mine if r.rid in srv.last_results}
+
+
+def test_two_gloo_ranks_serve_disjoint_shards_of_one_stream():
+    """Serving on two ranks: each serves its LPT share of the same request
+    stream (no exchange on the data path); the gathered results cover every
+    request exactly once, each stepped its budget, and the shares balance."""
+    import socket
+    import torch.multiprocessing as mp
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_serve_rank, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = sorted(q.get(timeout=120) for _ in procs)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    (_, mine0, all0, rej0, f0, ok0, w0), (_, mine1, all1, rej1, f1, ok1, w1) = res
+    assert not set(mine0) & set(mine1) and sorted(mine0 + mine1) == list(range(20))
+    assert all0 == all1 == list(range(20)) and not rej0 and not rej1 and not f0 and not f1
+    assert ok0 and ok1
+    assert abs(w0 - w1) <= max(w0, w1) // 2
