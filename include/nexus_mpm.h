@@ -487,6 +487,12 @@ NXM_API int nxm_state_ticket_wait(nxm_state* state, uint64_t ticket);
  * them. */
 NXM_API int nxm_read_positions_range_async(nxm_state* state, uint32_t first, uint32_t count, float* out,
                                            uint64_t* ticket);
+/* The device status word (NXM_STATUS_*) as of this point of the stream,
+ * copied asynchronously into `out` (pinned host memory, see nxm_host_alloc);
+ * valid once `*ticket` is done.  A serving loop takes one after each result
+ * read, so that a result is only handed out when no step before it reported
+ * a status bit.  No counterpart in the reference (its step has no status). */
+NXM_API int nxm_state_read_status_async(nxm_state* state, uint32_t* out, uint64_t* ticket);
 /* Pinned (page-locked) host memory for asynchronous reads and uploads. */
 NXM_API int nxm_host_alloc(size_t bytes, void** out);
 NXM_API void nxm_host_free(void* ptr);

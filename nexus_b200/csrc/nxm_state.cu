@@ -2719,6 +2719,13 @@ int nxm_read_positions_range_async(nxm_state* s, uint32_t first, uint32_t count,
     return nxm_state_fence(s, ticket);
 }
 
+int nxm_state_read_status_async(nxm_state* s, uint32_t* out, uint64_t* ticket) {
+    if (!s || !out || !ticket) return NXM_E_INVALID;
+    NXM_TRY(cudaMemcpyAsync(out, reinterpret_cast<const char*>(s->d_counters) + offsetof(Counters, status),
+                            sizeof(uint32_t), cudaMemcpyDeviceToHost, s->stream));
+    return nxm_state_fence(s, ticket);
+}
+
 int nxm_host_alloc(size_t bytes, void** out) {
     if (!out) return NXM_E_INVALID;
     *out = nullptr;

@@ -99,6 +99,7 @@ SIGNATURES = {
     "nxm_simulate_frame": (C.c_int, [_vp, _vp, C.c_uint32, C.c_uint32, _u]),
     "nxm_state_status_pipelined": (C.c_int, [_vp, _u]),
     "nxm_state_status_poll": (C.c_int, [_vp, _u, C.POINTER(C.c_int)]),
+    "nxm_state_read_status_async": (C.c_int, [_vp, _u, C.POINTER(C.c_uint64)]),
     "nxm_state_fence": (C.c_int, [_vp, C.POINTER(C.c_uint64)]),
     "nxm_state_ticket_done": (C.c_int, [_vp, C.c_uint64, C.POINTER(C.c_int)]),
     "nxm_state_ticket_wait": (C.c_int, [_vp, C.c_uint64]),
@@ -379,6 +380,14 @@ class MpmState:
         t = C.c_uint64()
         _check(self.lib.nxm_read_positions_range_async(self.h, first, count, _p(out, _f), C.byref(t)),
                "read_positions_range_async")
+        return t.value
+
+    def read_status_async(self, out: np.ndarray) -> int:
+        """The status word at this point of the stream into ``out`` (one uint32,
+        best pinned); returns the ticket after which it holds it."""
+        assert out.dtype == np.uint32 and out.size == 1 and out.flags.c_contiguous
+        t = C.c_uint64()
+        _check(self.lib.nxm_state_read_status_async(self.h, _p(out, _u), C.byref(t)), "read_status_async")
         return t.value
 
     def read_scene_positions_async(self, scene: int, out: np.ndarray) -> int:

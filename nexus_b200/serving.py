@@ -19,11 +19,13 @@ block-key region and colliders), so a result does not depend on what else was
 in the mix or on when it was admitted.
 
 Failures: the device status word of each batched state (grid blocks or hash
-slots exhausted, a particle without a block) is polled without waiting
-(nxm_state_status_poll: a word posted after some earlier step, once its store
-has run).  When a state reports a status bit, every scene that
-may have taken part in the failing step (those active on the state and those
-whose final read is still in flight) is evicted and reported in
+slots exhausted, a particle without a block) is sticky until cleared.  It is
+polled without waiting (nxm_state_status_poll: a word posted after some
+earlier step, once its store has run), and it is also read right after every
+result read (nxm_state_read_status_async), so that a result is only handed
+out when no step before it reported a bit.  When a state reports one, every
+scene that may have taken part in the failing step (those active on the state
+and those whose final read is still in flight) is evicted and reported in
 ``MpmServer.failed`` with the status bits; the bits are cleared, the state's
 grid admission estimate is doubled so that the same mix is not admitted
 again, and serving continues with the other requests.
@@ -116,6 +118,8 @@ class MpmServer:
         self.steps_taken = 0
         self.particle_steps = 0
         self._pinned = {}  # capacity (particles) -> free pinned result buffers
+        self._words = None  # pinned status words, one per result read in flight
+        self._free_words = []
 
     def _buffer(self, n: int) -> PinnedArray:
         cap = 1 << max(int(n) - 1, 0).bit_length()
@@ -125,6 +129,14 @@ class MpmServer:
     def _release(self, buf: PinnedArray):
         self._pinned.setdefault(buf.array.shape[0], []).append(buf)
 
+    def _word(self) -> int:
+        if not self._free_words:
+            old = self._words
+            n = 2 * (len(old.array) if old is not None else 1024)
+            self._words = PinnedArray((n,), np.uint32)
+            self._free_words = list(range(len(old.array) if old is not None else 0, n))
+            self._retired_words = getattr(self, "_retired_words", []) + ([old] if old is not None else [])
+        return self._free_words.pop()
     def _group(self, sc: Scene) -> _Group:
         key = (float(sc.dx), float(sc.dt), tuple(float(g) for g in sc.gravity))
         g = self.groups.get(key)
@@ -161,6 +173,7 @@ class MpmServer:
             if item[0] is g:
                 self.failed[item[2].rid] = Failure(item[2].rid, bits, item[2].steps)
                 self._release(item[4])
+                self._free_words.append(item[5])
             else:
                 keep.append(item)
         reads.clear()
@@ -199,12 +212,21 @@ class MpmServer:
                 g.particles += r.scene.n
                 g.grid += r.scene.grid_capacity * g.grid_factor
                 self.in_use += footprint(r.scene)
-            # results whose reads have landed
+            # results whose reads (and the status word read after them) have landed
             for _ in range(len(reads)):
-                g, ticket, r, admitted, buf = reads[0]
+                if not reads:
+                    break
+                g, ticket, r, admitted, buf, w = reads[0]
                 reads.rotate(-1)
                 if g.state.ticket_done(ticket):
                     reads.pop()
+                    bits = int(self._words.array[w])
+                    self._free_words.append(w)
+                    if bits:  # a step before this read reported a status bit
+                        self.failed[r.rid] = Failure(r.rid, bits, r.steps)
+                        self._release(buf)
+                        self._fail(g, bits, reads)
+                        continue
                     results[r.rid] = Result(r.rid, r.scene.n, r.steps, r.arrival, admitted, clock() - t0,
                                             buf.array[:r.scene.n].copy())
                     self._release(buf)
@@ -234,8 +256,10 @@ class MpmServer:
                 for slot in done:
                     r, _, admitted = g.active.pop(slot)
                     buf = self._buffer(r.scene.n)
-                    ticket = g.state.read_scene_positions_async(slot, buf.array[:r.scene.n])
-                    reads.append((g, ticket, r, admitted, buf))
+                    g.state.read_scene_positions_async(slot, buf.array[:r.scene.n])
+                    w = self._word()
+                    ticket = g.state.read_status_async(self._words.array[w:w + 1])
+                    reads.append((g, ticket, r, admitted, buf, w))
                 if done:  # queued behind the reads above
                     g.state.remove_scenes(done)
                     self._usage(g)

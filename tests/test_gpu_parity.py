@@ -528,16 +528,17 @@ def test_batched_coupled_scenes_step_as_alone(pipe):
 
 
 def test_hash_full_is_reported(pipe):
-    """More distinct block keys than the hash has slots (a grid of 8 blocks has
-    a 1024-slot hash; 216 particles 8 cells apart touch 1728 blocks): the step
-    reports STATUS_HASH_FULL, synchronize raises NXM_E_HASH_FULL, and no
-    particle is lost (those without a block are carried over unchanged)."""
+    """More distinct primary block keys than the hash has slots (a grid of 8
+    blocks has a 1024-slot hash; 1331 particles 4 cells apart each sit in a
+    block of their own): the step reports STATUS_HASH_FULL, synchronize raises
+    NXM_E_HASH_FULL, and no particle is lost (those without a block are
+    carried over unchanged)."""
     from nexus_b200.mpm import NXM_E_HASH_FULL
     from nexus_b200.models import ParticleModel
     from nexus_b200.particles import ParticleBatch, collider_array
     dx = 1.0 / 64.0
-    k = np.arange(6, dtype=np.float32)
-    pos = ((np.stack(np.meshgrid(k, k, k, indexing="ij"), -1).reshape(-1, 3) * 8.0 + 6.5) * np.float32(dx))
+    k = np.arange(11, dtype=np.float32)
+    pos = ((np.stack(np.meshgrid(k, k, k, indexing="ij"), -1).reshape(-1, 3) * 4.0 + 6.5) * np.float32(dx))
     b = ParticleBatch.from_positions(pos.astype(np.float32), np.float32(dx / 4), 1000.0,
                                      ParticleModel.elastic_neo_hookean(1e5, 0.3))
     sc = scenes.Scene("spread", dx, 1.0e-4, (0.0, 0.0, -9.81), b, collider_array([]), 1, 8)
@@ -561,8 +562,11 @@ def test_sort_capacity_is_reported(pipe):
     from nexus_b200.particles import ParticleBatch, collider_array
     dx = 1.0 / 64.0
     rng = np.random.default_rng(3)
-    lo = np.float32(32 * dx)
-    pos = (lo + rng.uniform(0.6, 3.4, (5000, 3)).astype(np.float32) * np.float32(dx) * np.array([1, 1, 0.25], np.float32))
+    # x, y in cells [32.6, 35.4] dx, z in [32.55, 32.95] dx: associated cells
+    # 32..34 in x and y and 32 in z, all in block (8, 8, 8), z-slab 0
+    u = rng.uniform(0.0, 1.0, (5000, 3)).astype(np.float32)
+    pos = (np.float32(32.0) + u * np.array([2.8, 2.8, 0.4], np.float32) +
+           np.array([0.6, 0.6, 0.55], np.float32)) * np.float32(dx)
     b = ParticleBatch.from_positions(pos.astype(np.float32), np.float32(dx / 4), 1000.0,
                                      ParticleModel.elastic_neo_hookean(1e3, 0.3))
     sc = scenes.Scene("pile", dx, 1.0e-5, (0.0, 0.0, 0.0), b, collider_array([]), 1, 64)

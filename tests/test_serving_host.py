@@ -56,6 +56,8 @@ class FakeState:
                 del self.scenes[slot]
         elif op[0] == "fence":
             self.done = op[1]
+        elif op[0] == "status":
+            op[1][0] = self.bits
 
     def _drain_to(self, ticket):
         while self.done < ticket:
@@ -72,6 +74,10 @@ class FakeState:
 
     def read_scene_positions_async(self, slot, out):
         self.queue.append(("read", slot, out))
+        return self.fence()
+
+    def read_status_async(self, out):
+        self.queue.append(("status", out))
         return self.fence()
 
     def fence(self):
@@ -134,7 +140,8 @@ def test_served_requests_step_their_budget(monkeypatch, depth):
     assert not g.state.scenes  # every finished scene was removed
 
 
-def test_status_error_evicts_and_reports_the_scenes_of_the_failing_step(monkeypatch):
+@pytest.mark.parametrize("poll", [True, False])
+def test_status_error_evicts_and_reports_the_scenes_of_the_failing_step(monkeypatch, poll):
     """A state whose step reports a status bit (here: more live particles than
     its grid holds) has every scene that may have taken part evicted and
     reported in `failed` with the bits; the bits are cleared, the state's grid
@@ -142,6 +149,8 @@ def test_status_error_evicts_and_reports_the_scenes_of_the_failing_step(monkeypa
     monkeypatch.setattr(serving, "MpmState", FakeState)
     monkeypatch.setattr(serving, "MpmPipeline", FakePipeline)
     monkeypatch.setattr(serving, "PinnedArray", FakeArray)
+    if not poll:  # the poll never returns in time: the status word read after each result catches it
+        monkeypatch.setattr(FakeState, "status_poll", lambda self: None)
     reqs = [serving.Request(i, _scene(i, 20), 30, 0.0) for i in range(3)]  # all three at once: 60 particles
     reqs += [serving.Request(3 + i, _scene(3 + i, 20), 10, 100.0) for i in range(3)]  # later, one at a time fits
     srv = serving.MpmServer(hbm_budget=1e12, particles_capacity=1 << 20, grid_capacity=192)
@@ -158,7 +167,7 @@ def test_status_error_evicts_and_reports_the_scenes_of_the_failing_step(monkeypa
     results, rejected = srv.run(reqs, clock=iter(np.arange(0.0, 1e6, 1e-2)).__next__, idle_sleep=0.0, depth=4)
     assert not rejected
     assert sorted(srv.failed) == [0, 1, 2]
-    assert all(f.status & 2 and 0 < f.steps_done < 30 for f in srv.failed.values())
+    assert all(f.status & 2 and 0 < f.steps_done <= 30 for f in srv.failed.values())
     (g,) = srv.groups.values()
     assert g.grid_factor == 2.0 and g.state.bits == 0
     # the later requests: the doubled estimate admits at most two at once (2 x 64 x 2 > 192), so they fit
