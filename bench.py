@@ -317,7 +317,7 @@ def measure_cube(torch, steps: int = 100):
 def run_ours(args, world, rank, local):
     import torch
     from nexus_b200 import build as nb
-    from nexus_b200.mpm import MpmPipeline, MpmState, state_from_scene, load
+    from nexus_b200.mpm import MpmPipeline, MpmState, state_from_scene, load, tuning_table
 
     nb.build()
     load()
@@ -328,6 +328,12 @@ def run_ours(args, world, rank, local):
     st = state_from_scene(scene)
     stream = torch.cuda.ExternalStream(st.cuda_stream())
 
+    for _ in range(args.warmup):
+        pipe.step(st)
+    st.synchronize()
+    # launch shapes picked by the autotuner on this state's own steps (the
+    # state advances through the trials), then the timed steps
+    tuning = st.autotune(trial_steps=args.tune_steps) if args.tune_steps > 0 else st.tuning()
     for _ in range(args.warmup):
         pipe.step(st)
     st.synchronize()
@@ -403,6 +409,7 @@ def run_ours(args, world, rank, local):
                      "algorithmic_bytes_per_launch": bytes_per_step},
         "phases_ms": phases,
         "phase_roofline": phase_roof,
+        "tuning": tuning,
         "clocks": clk,
         "e2e": e2e,
         "e2e_pageable": e2e_pageable,
@@ -412,6 +419,7 @@ def run_ours(args, world, rank, local):
         "batched": batched,
         "serving": serving,
         "coupled": coupled,
+        "tuning_table": tuning_table(),
     }
     print(json.dumps(line), flush=True)
 
@@ -429,6 +437,10 @@ def measure_batched(args, world, rank, torch):
     st, _ = batched_state_from_scenes(mine)
     stream = torch.cuda.ExternalStream(st.cuda_stream())
     for _ in range(max(3, args.warmup)):
+        pipe.step(st)
+    st.synchronize()
+    tuning = st.autotune(trial_steps=args.tune_steps) if args.tune_steps > 0 else st.tuning()
+    for _ in range(3):
         pipe.step(st)
     st.synchronize()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -470,7 +482,7 @@ def measure_batched(args, world, rank, torch):
             "plain_scene_by_scene": {"value": plain, "unit": UNIT, "ms_per_step": plain_ms,
                                      "how": f"each scene alone in its own state and graph, {args.plain_steps} "
                                             f"timed steps after 3 warm-up, summed over scenes"},
-            "speedup_vs_plain": value / plain, "dx": mix[0].dx, "dt": mix[0].dt,
+            "speedup_vs_plain": value / plain, "dx": mix[0].dx, "dt": mix[0].dt, "tuning": tuning,
             "parallelism": f"scene-sharded{world}" if world > 1 else "single"}
 
 
@@ -495,6 +507,7 @@ def measure_coupled(args, torch):
         pipe.step(st)
         step += 1
     st.synchronize()
+    tuning = st.autotune(trial_steps=args.tune_steps) if args.tune_steps > 0 else st.tuning()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ev0.record(stream)
     for _ in range(args.coupled_steps):
@@ -530,7 +543,7 @@ def measure_coupled(args, torch):
             "colliders_per_scene": int(len(mix[0].colliders)), "triangles_per_scene": int(len(mix[0].tri_vertices) // 3),
             "value": value, "unit": UNIT, "steps": args.coupled_steps, "ms_per_step": ms / args.coupled_steps,
             "plain_scene_by_scene": {"value": plain, "unit": UNIT, "ms_per_step": plain_ms},
-            "speedup_vs_plain": value / plain, "dx": mix[0].dx, "dt": dt,
+            "speedup_vs_plain": value / plain, "dx": mix[0].dx, "dt": dt, "tuning": tuning,
             "how": "timed steps include writing every kinematic body's velocity (one stream-ordered call per step)"}
 
 
@@ -555,10 +568,21 @@ def measure_serving(args, torch, world: int = 1, rank: int = 0):
     wall = all_max(time.perf_counter() - t0, world)
     summ = latency_summary(results)
     del srv
-    # FIFO plain loop: per-scene step time measured alone, then a virtual clock
+    # FIFO plain loop: each request's plain step time (its scene alone in its
+    # own state), then a virtual clock in arrival order.  The step time is
+    # measured for every `every`-th request and interpolated by particle count
+    # for the others, within their class (cell width, material).
     pipe = MpmPipeline()
-    t_done, lat = 0.0, []
-    for r in sorted(mine, key=lambda q: q.arrival):
+    order = sorted(mine, key=lambda q: q.arrival)
+    every = max(1, len(order) // args.fifo_samples)
+
+    def klass(r):
+        return (r.scene.dx, int(r.scene.particles.model[0, 0]))
+
+    measured = {}
+    for i, r in enumerate(order):
+        if i % every:
+            continue
         one = state_from_scene(r.scene)
         s1 = torch.cuda.ExternalStream(one.cuda_stream())
         for _ in range(3):
@@ -570,10 +594,21 @@ def measure_serving(args, torch, world: int = 1, rank: int = 0):
             pipe.step(one)
         b.record(s1)
         b.synchronize()
-        run_s = a.elapsed_time(b) / args.plain_steps / 1e3 * r.steps
+        measured[r.rid] = a.elapsed_time(b) / args.plain_steps / 1e3
         one.synchronize()
         del one
-        t_done = max(t_done, r.arrival) + run_s
+    samples = {}
+    for r in order:
+        if r.rid in measured:
+            samples.setdefault(klass(r), []).append((r.scene.n, measured[r.rid]))
+    t_done, lat = 0.0, []
+    for r in order:
+        if r.rid in measured:
+            step_s = measured[r.rid]
+        else:
+            pts = sorted(samples.get(klass(r)) or [p for v in samples.values() for p in v])
+            step_s = float(np.interp(r.scene.n, [p[0] for p in pts], [p[1] for p in pts]))
+        t_done = max(t_done, r.arrival) + step_s * r.steps
         lat.append(t_done - r.arrival)
     if world > 1:
         import torch.distributed as dist
@@ -588,8 +623,10 @@ def measure_serving(args, torch, world: int = 1, rank: int = 0):
             "parallelism": f"request-sharded{world}" if world > 1 else "single",
             "plain_fifo": {"value": work / t_done, "unit": UNIT, "p50_s": float(np.percentile(lat, 50)),
                            "p99_s": float(np.percentile(lat, 99)),
-                           "how": "each request alone in its own state, in arrival order; per-scene step time "
-                                  f"measured over {args.plain_steps} steps after 3 warm-up, times its budget"},
+                           "how": "each request alone in its own state, in arrival order, for its step budget; "
+                                  f"the plain step time measured (over {args.plain_steps} steps after 3 warm-up) "
+                                  f"for every {every}-th request ({len(measured)} of {len(order)}), the others "
+                                  "interpolated by particle count within their cell width and material"},
             "note": f"{len(reqs)} requests of the 4000-request stream (same arrival rate and distributions)"}
 
 
@@ -669,9 +706,13 @@ def main():
     ap.add_argument("--batched-scenes", type=int, default=256)
     ap.add_argument("--plain-steps", type=int, default=10)
     ap.add_argument("--serving-requests", type=int, default=4000, help="0: skip the serving measurement")
+    ap.add_argument("--fifo-samples", type=int, default=400,
+                    help="requests whose plain step time the serving leg's FIFO baseline measures")
     ap.add_argument("--coupled-steps", type=int, default=300, help="timed steps of the coupled mix (0: skip it)")
     ap.add_argument("--coupled-scenes", type=int, default=64)
     ap.add_argument("--no-cube", dest="cube", action="store_false", help="skip the 32k elastic cube leg")
+    ap.add_argument("--tune-steps", type=int, default=5,
+                    help="timed steps per candidate of the autotuner before the timed region (0: default shapes)")
     args = ap.parse_args()
     if args.impl == "reference":
         # CPU baseline arm: rank 0 alone runs it; other ranks exit without work.

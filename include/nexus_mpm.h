@@ -338,6 +338,36 @@ NXM_API int nxm_grid_read_nodes(nxm_state* state, float* out, uint32_t max_block
  * particles, leaving the grid readable; particles are not advanced. */
 NXM_API int nxm_debug_sort(nxm_pipeline* pipeline, nxm_state* state, int with_p2g);
 
+/* ---- autotuner --------------------------------------------------------------
+ * Launch shapes of one state's step.  No counterpart in the reference (its
+ * dispatch sizes are fixed per shader). */
+typedef struct nxm_tuning {
+    uint32_t p2g_ctas_per_sm;   /* 1..3 */
+    uint32_t g2p_ctas_per_sm;   /* 1..4 */
+    uint32_t sort_ctas_per_sm;  /* 1, 2, 4, 8 or 16: the sort's particle passes */
+    uint32_t grid_ctas_per_sm;  /* 1, 2, 4, 8 or 16: the grid update */
+    uint32_t sort_batch;        /* 2, 4 or 8 passes of 32 particles a sort warp loads together */
+    uint32_t range_min_fill;    /* below this many particles per block G2P runs one block per unit */
+    uint32_t density;           /* table key: particles per primary block, rounded down to a power of two */
+    uint32_t scenes;            /* table key: live scenes rounded up to a power of two (0: not batched) */
+    float ms_before;            /* ms per step before tuning (0 when no trial ran) */
+    float ms_after;             /* ms per step of the chosen shapes */
+} nxm_tuning;
+
+/* Times the state's own steps under candidate launch shapes (one knob at a
+ * time, the others held; `trial_steps` timed steps per candidate after one
+ * untimed step) and keeps the fastest; the state advances by every step
+ * taken (about 15 x (trial_steps + 1)).  The decision is cached in a
+ * process-wide table keyed by (density, scenes); with trial_steps = 0 the
+ * call only applies the table's entry for this state's key, if there is one.
+ * `out` (may be null) receives the decision and its key. */
+NXM_API int nxm_state_autotune(nxm_state* state, uint32_t trial_steps, nxm_tuning* out);
+NXM_API int nxm_state_get_tuning(const nxm_state* state, nxm_tuning* out);
+/* Sets the launch shapes (values outside the ranges above: NXM_E_INVALID). */
+NXM_API int nxm_state_set_tuning(nxm_state* state, const nxm_tuning* tuning);
+/* The decision table: copies up to `max_entries` entries, returns how many exist. */
+NXM_API uint32_t nxm_tuning_table(nxm_tuning* out, uint32_t max_entries);
+
 /* ---- block sort without device allocation ----------------------------- */
 
 /* Limits of nxm_sort_blocks_noalloc: active blocks its fixed tables hold,

@@ -75,11 +75,22 @@ struct DevPtrs {
 constexpr uint32_t kScanTile = 256;  // blocks per scan tile (one per thread of a scan CTA)
 constexpr uint32_t kRangeChunk = 256;  // sorted positions per fast-G2P run (one per thread of its CTA)
 
+// Launch shapes the autotuner picks per state (nxm_state_autotune); the
+// defaults are the hand-measured best of the 2 M-particle sand + water scene.
+struct Tuning {
+    uint32_t p2g_ctas = 3;    // P2G CTAs per SM (its launch bounds fit 3)
+    uint32_t g2p_ctas = 4;    // G2P CTAs per SM (its launch bounds fit 4)
+    uint32_t sort_ctas = 8;   // CTAs per SM of the sort's particle passes
+    uint32_t grid_ctas = 8;   // grid update CTAs per SM
+    uint32_t sort_batch = 4;  // 2, 4 or 8 passes of 32 particles a sort warp loads together
+};
+
 struct LaunchCfg {
     int sm_count;
     uint32_t hash_capacity;  // host copy, sizes the reset grid
     uint32_t block_capacity;
     uint32_t particle_capacity;
+    Tuning t;
 };
 
 // Number of kernels each launcher issues (for the launch counter).

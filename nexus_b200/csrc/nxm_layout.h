@@ -135,8 +135,12 @@ struct alignas(16) Params {
     int32_t scene_margin;
     int32_t scene_cmin[3];
     uint32_t scene_cells[3];
+    // the fast G2P takes one block per unit (instead of runs of the sorted
+    // list) below this many particles per primary block on average (tuned)
+    uint32_t range_min_fill;
+    uint32_t pad[3];
 };
-static_assert(sizeof(Params) == 80, "Params layout");
+static_assert(sizeof(Params) == 96, "Params layout");
 
 // Device counters (reset each step by the sort).
 struct alignas(16) Counters {

@@ -107,10 +107,8 @@ __device__ __forceinline__ void warp_range(uint32_t n, uint32_t& lo, uint32_t& h
     hi = min(lo + per_warp, n);
 }
 
-#ifndef NXM_SORT_BATCH
-#define NXM_SORT_BATCH 4
-#endif
-constexpr int kSortBatch = NXM_SORT_BATCH;  // passes of 32 particles whose loads are issued together
+// kSortBatch (a template parameter of the particle passes): passes of 32
+// particles whose loads a warp issues together (2, 4 or 8; tuned per state).
 
 __device__ __forceinline__ bool spills(uint32_t ax, uint32_t ay, uint32_t az, int sx, int sy, int sz) {
     // sort.rs:320-329, EXTRA_PARTICLE_MIN_SHIFT = 2
@@ -156,6 +154,7 @@ __global__ void k_sort_reset(DevPtrs P, uint32_t hash_cap) {
 // Each warp walks a contiguous range of particles, so consecutive passes
 // mostly see the block they inserted last: a pass whose lanes all carry the
 // key inserted by the previous pass skips the hash entirely.
+template <int kSortBatch>
 __global__ void __launch_bounds__(256) k_touch_primary(DevPtrs P) {
     const uint32_t n = P.params->n;
     const float dx = P.params->dx;
@@ -246,7 +245,7 @@ __global__ void __launch_bounds__(256) k_block_prep(DevPtrs P) {
 }
 
 // sort.rs:287-349 gpu_update_block_particle_count.
-template <bool kExtras>
+template <bool kExtras, int kSortBatch>
 __global__ void __launch_bounds__(256) k_count(DevPtrs P) {
     const uint32_t n = P.params->n;
     const uint32_t hmask = P.params->hash_capacity - 1;
@@ -421,7 +420,7 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_apply(DevPtrs P) {
 }
 
 // sort.rs:430-491 gpu_finalize_particles_sort.
-template <bool kExtras>
+template <bool kExtras, int kSortBatch>
 __global__ void __launch_bounds__(256) k_finalize(DevPtrs P) {
     const uint32_t n = P.params->n;
     const uint32_t scap = P.params->sorted_capacity;
@@ -701,24 +700,40 @@ namespace fast {
 
 void launch_sort(const DevPtrs& P, const LaunchCfg& c, bool with_extras, bool canonical, cudaStream_t s,
                  bool rigid) {
-    const int g = grid_for(c.sm_count, 8);
+    const int g = grid_for(c.sm_count, (int)c.t.sort_ctas);
     int reset_grid = (int)((c.hash_capacity + 255u) / 256u);
     if (reset_grid > g) reset_grid = g;
     if (reset_grid < 1) reset_grid = 1;
     k_sort_reset<<<reset_grid, 256, 0, s>>>(P, c.hash_capacity);
-    k_touch_primary<<<g, 256, 0, s>>>(P);
+    switch (c.t.sort_batch) {
+    case 2: k_touch_primary<2><<<g, 256, 0, s>>>(P); break;
+    case 8: k_touch_primary<8><<<g, 256, 0, s>>>(P); break;
+    default: k_touch_primary<4><<<g, 256, 0, s>>>(P); break;
+    }
     k_touch_nbh<<<g, 256, 0, s>>>(P);
     if (rigid) {
         k_rigid_mark<<<g, 256, 0, s>>>(P);
         k_rigid_touch<<<g, 256, 0, s>>>(P);
     }
     k_block_prep<<<g, 256, 0, s>>>(P);
-    if (with_extras) k_count<true><<<g, 256, 0, s>>>(P);
-    else k_count<false><<<g, 256, 0, s>>>(P);
+    switch ((with_extras ? 16 : 0) + c.t.sort_batch) {
+    case 2: k_count<false, 2><<<g, 256, 0, s>>>(P); break;
+    case 8: k_count<false, 8><<<g, 256, 0, s>>>(P); break;
+    case 18: k_count<true, 2><<<g, 256, 0, s>>>(P); break;
+    case 20: k_count<true, 4><<<g, 256, 0, s>>>(P); break;
+    case 24: k_count<true, 8><<<g, 256, 0, s>>>(P); break;
+    default: k_count<false, 4><<<g, 256, 0, s>>>(P); break;
+    }
     k_scan_tiles<<<c.sm_count, kScanThreads, 0, s>>>(P);
     k_scan_apply<<<c.sm_count, kScanThreads, 0, s>>>(P);
-    if (with_extras) k_finalize<true><<<g, 256, 0, s>>>(P);
-    else k_finalize<false><<<g, 256, 0, s>>>(P);
+    switch ((with_extras ? 16 : 0) + c.t.sort_batch) {
+    case 2: k_finalize<false, 2><<<g, 256, 0, s>>>(P); break;
+    case 8: k_finalize<false, 8><<<g, 256, 0, s>>>(P); break;
+    case 18: k_finalize<true, 2><<<g, 256, 0, s>>>(P); break;
+    case 20: k_finalize<true, 4><<<g, 256, 0, s>>>(P); break;
+    case 24: k_finalize<true, 8><<<g, 256, 0, s>>>(P); break;
+    default: k_finalize<false, 4><<<g, 256, 0, s>>>(P); break;
+    }
     if (canonical) k_sort_segments<<<grid_for(c.sm_count, 4), 256, 0, s>>>(P);
     if (rigid) {
         k_rigid_count<<<g, 256, 0, s>>>(P);

@@ -14,7 +14,9 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <initializer_list>
 #include <map>
+#include <mutex>
 #include <new>
 #include <set>
 #include <thread>
@@ -42,6 +44,12 @@ uint32_t next_pow2(uint32_t v) {
             (void)cudaGetLastError();                   \
             return e_ == cudaErrorMemoryAllocation ? NXM_E_OOM : NXM_E_CUDA; \
         }                                               \
+    } while (0)
+// Propagates a nonzero NXM_* result.
+#define NXM_TRY_RC(expr)        \
+    do {                        \
+        const int rc_ = (expr); \
+        if (rc_) return rc_;    \
     } while (0)
 
 template <class T>
@@ -397,6 +405,10 @@ struct nxm_state {
     cudaEvent_t poll_done = nullptr;
     bool poll_outstanding = false;
 
+    // launch shapes (nxm_state_autotune); range_min_fill goes to Params
+    Tuning tuning;
+    uint32_t range_min_fill = 64;
+
     // batched scenes (scene_blocks != 0): scene slots on the block-key grid
     // (see Params), each a contiguous range of particle ids with its own colliders
     struct Scene {
@@ -557,6 +569,7 @@ LaunchCfg launch_cfg(nxm_state* s) {
     c.hash_capacity = s->hash_cap;
     c.block_capacity = s->block_cap;
     c.particle_capacity = s->pcap;
+    c.t = s->tuning;
     return c;
 }
 
@@ -1000,6 +1013,7 @@ int sync_params(nxm_state* s) {
         p.scene_cmin[k] = s->scene_cmin[k];
         p.scene_cells[k] = s->scene_cells[k];
     }
+    p.range_min_fill = s->range_min_fill;
     NXM_TRY(upload_async(s, s->d_params, &p, sizeof(Params)));
     s->params_dirty = false;
     return NXM_OK;
@@ -2717,6 +2731,195 @@ int nxm_read_positions_range_async(nxm_state* s, uint32_t first, uint32_t count,
     const int rc = pack_read_range(s, s->kin, sizeof(PKin), off, 3, first, count, out, /*wait=*/false);
     if (rc) return rc;
     return nxm_state_fence(s, ticket);
+}
+
+// ---- autotuner ----------------------------------------------------------------
+//
+// nxm_state_autotune times the state's own steps under candidate launch
+// shapes (coordinate descent over the knobs below, one knob at a time, the
+// others held) and keeps the fastest; the decision is cached in a process-wide
+// table keyed by the scene's density (particles per primary block, rounded
+// down to a power of two) and its active scene count (rounded up to a power
+// of two), which later states of the same kind apply with trial_steps = 0.
+
+namespace {
+
+struct TuneEntry {
+    Tuning t;
+    uint32_t fill;
+    float ms_before, ms_after;
+};
+std::mutex g_tune_mutex;
+std::map<uint64_t, TuneEntry> g_tune_table;
+
+uint32_t floor_pow2(uint32_t v) { return v ? 1u << (31 - __builtin_clz(v)) : 0u; }
+
+// The table key from the counters of the last step (false when no step has
+// set them yet).
+int tune_key(nxm_state* s, uint32_t* density, uint32_t* scenes, bool* known) {
+    NXM_TRY(cudaMemcpyAsync(s->h_counters, s->d_counters, sizeof(Counters), cudaMemcpyDeviceToHost, s->stream));
+    NXM_TRY(cudaStreamSynchronize(s->stream));
+    *known = s->h_counters->num_primary > 0;
+    const uint32_t nbp = std::max<uint32_t>(1u, std::min(s->h_counters->num_primary, s->h_counters->num_blocks));
+    *density = floor_pow2(std::max<uint32_t>(1u, s->n / nbp));
+    uint32_t live = 0;
+    for (const auto& sc : s->scenes) live += sc.live ? 1u : 0u;
+    *scenes = live ? next_pow2(live) : 0u;
+    return NXM_OK;
+}
+
+void apply_tuning(nxm_state* s, const Tuning& t, uint32_t fill) {
+    s->tuning = t;
+    if (s->range_min_fill != fill) {
+        s->range_min_fill = fill;
+        s->params_dirty = true;
+    }
+    invalidate_graph(s);
+}
+
+// ms per step of `steps` graph steps after one untimed step (which captures
+// the graph of the new shapes), CUDA events on the state's stream.
+int time_steps(nxm_pipeline* pipe, nxm_state* s, uint32_t steps, float* ms) {
+    int rc = nxm_step(pipe, s, nullptr);
+    if (rc) return rc;
+    cudaEvent_t a, b;
+    NXM_TRY(cudaEventCreate(&a));
+    NXM_TRY(cudaEventCreate(&b));
+    NXM_TRY(cudaEventRecord(a, s->stream));
+    for (uint32_t i = 0; i < steps && !rc; ++i) rc = nxm_step(pipe, s, nullptr);
+    NXM_TRY(cudaEventRecord(b, s->stream));
+    NXM_TRY(cudaEventSynchronize(b));
+    float t = 0.f;
+    cudaEventElapsedTime(&t, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    *ms = t / (float)std::max<uint32_t>(steps, 1u);
+    return rc;
+}
+
+void to_abi(const Tuning& t, uint32_t fill, uint32_t density, uint32_t scenes, float before, float after,
+            nxm_tuning* out) {
+    out->p2g_ctas_per_sm = t.p2g_ctas;
+    out->g2p_ctas_per_sm = t.g2p_ctas;
+    out->sort_ctas_per_sm = t.sort_ctas;
+    out->grid_ctas_per_sm = t.grid_ctas;
+    out->sort_batch = t.sort_batch;
+    out->range_min_fill = fill;
+    out->density = density;
+    out->scenes = scenes;
+    out->ms_before = before;
+    out->ms_after = after;
+}
+
+}  // namespace
+
+int nxm_state_autotune(nxm_state* s, uint32_t trial_steps, nxm_tuning* out) {
+    if (!s) return NXM_E_INVALID;
+    int rc = ensure_ready(s);
+    if (rc) return rc;
+    if (s->n == 0) return NXM_OK;
+    static nxm_pipeline* pipe = nullptr;  // nxm_step takes a pipeline handle; it holds no state
+    if (!pipe && (rc = nxm_pipeline_create(&pipe))) return rc;
+    uint32_t density = 0, scenes = 0;
+    bool known = false;
+    NXM_TRY_RC(tune_key(s, &density, &scenes, &known));
+    if (!known) {  // the counts come from a step
+        NXM_TRY_RC(nxm_step(pipe, s, nullptr));
+        NXM_TRY_RC(tune_key(s, &density, &scenes, &known));
+    }
+    const uint64_t key = ((uint64_t)density << 32) | scenes;
+    if (trial_steps == 0) {  // apply the table's decision for this kind of state, if any
+        std::lock_guard<std::mutex> lock(g_tune_mutex);
+        auto it = g_tune_table.find(key);
+        if (it != g_tune_table.end()) {
+            apply_tuning(s, it->second.t, it->second.fill);
+            if (out) to_abi(it->second.t, it->second.fill, density, scenes, it->second.ms_before, it->second.ms_after, out);
+        } else if (out) {
+            to_abi(s->tuning, s->range_min_fill, density, scenes, 0.f, 0.f, out);
+        }
+        return NXM_OK;
+    }
+    Tuning best = s->tuning;
+    uint32_t best_fill = s->range_min_fill;
+    float before = 0.f;
+    NXM_TRY_RC(time_steps(pipe, s, trial_steps, &before));
+    float best_ms = before;
+    static const uint32_t kBatch[] = {2, 4, 8}, kSortCtas[] = {4, 8, 16}, kP2g[] = {2, 3}, kG2p[] = {3, 4},
+                          kGrid[] = {4, 8, 16}, kFill[] = {16, 32, 64, 128, 256};
+    struct Knob {
+        uint32_t* field;  // inside `trial`
+        const uint32_t* vals;
+        int nvals;
+    };
+    Tuning trial = best;
+    uint32_t trial_fill = best_fill;
+    const Knob knobs[] = {{&trial.sort_batch, kBatch, 3}, {&trial.sort_ctas, kSortCtas, 3}, {&trial.p2g_ctas, kP2g, 2},
+                          {&trial.g2p_ctas, kG2p, 2},     {&trial.grid_ctas, kGrid, 3},     {&trial_fill, kFill, 5}};
+    for (const Knob& k : knobs) {
+        trial = best;
+        trial_fill = best_fill;
+        const uint32_t keep = *k.field;
+        for (int i = 0; i < k.nvals; ++i) {
+            if (k.vals[i] == keep) continue;
+            trial = best;
+            trial_fill = best_fill;
+            *k.field = k.vals[i];
+            apply_tuning(s, trial, trial_fill);
+            float ms = 0.f;
+            NXM_TRY_RC(time_steps(pipe, s, trial_steps, &ms));
+            if (ms < best_ms * 0.99f) {  // a clear win only
+                best_ms = ms;
+                best = trial;
+                best_fill = trial_fill;
+            }
+        }
+    }
+    apply_tuning(s, best, best_fill);
+    {
+        std::lock_guard<std::mutex> lock(g_tune_mutex);
+        g_tune_table[key] = TuneEntry{best, best_fill, before, best_ms};
+    }
+    if (out) to_abi(best, best_fill, density, scenes, before, best_ms, out);
+    return NXM_OK;
+}
+
+int nxm_state_get_tuning(const nxm_state* s, nxm_tuning* out) {
+    if (!s || !out) return NXM_E_INVALID;
+    to_abi(s->tuning, s->range_min_fill, 0u, 0u, 0.f, 0.f, out);
+    return NXM_OK;
+}
+
+int nxm_state_set_tuning(nxm_state* s, const nxm_tuning* t) {
+    if (!s || !t) return NXM_E_INVALID;
+    auto in = [](uint32_t v, std::initializer_list<uint32_t> ok) {
+        for (uint32_t o : ok)
+            if (v == o) return true;
+        return false;
+    };
+    if (!in(t->p2g_ctas_per_sm, {1, 2, 3}) || !in(t->g2p_ctas_per_sm, {1, 2, 3, 4}) ||
+        !in(t->sort_ctas_per_sm, {1, 2, 4, 8, 16}) || !in(t->grid_ctas_per_sm, {1, 2, 4, 8, 16}) ||
+        !in(t->sort_batch, {2, 4, 8}) || t->range_min_fill == 0)
+        return NXM_E_INVALID;
+    Tuning x;
+    x.p2g_ctas = t->p2g_ctas_per_sm;
+    x.g2p_ctas = t->g2p_ctas_per_sm;
+    x.sort_ctas = t->sort_ctas_per_sm;
+    x.grid_ctas = t->grid_ctas_per_sm;
+    x.sort_batch = t->sort_batch;
+    apply_tuning(s, x, t->range_min_fill);
+    return NXM_OK;
+}
+
+uint32_t nxm_tuning_table(nxm_tuning* out, uint32_t max_entries) {
+    std::lock_guard<std::mutex> lock(g_tune_mutex);
+    uint32_t i = 0;
+    for (const auto& kv : g_tune_table) {
+        if (out && i < max_entries)
+            to_abi(kv.second.t, kv.second.fill, (uint32_t)(kv.first >> 32), (uint32_t)kv.first, kv.second.ms_before,
+                   kv.second.ms_after, &out[i]);
+        ++i;
+    }
+    return i;
 }
 
 int nxm_state_read_status_async(nxm_state* s, uint32_t* out, uint64_t* ticket) {

@@ -458,19 +458,16 @@ __device__ __forceinline__ void g2p_finish(const DevPtrs& P, const Params& prm) 
 #ifndef NXM_G2P_STASH
 #define NXM_G2P_STASH 1  // m A waits in shared memory across the model update (fast build)
 #endif
-// Below kRangeMinFill particles a block on average, a run of the fast G2P
-// (k_g2p_range) would span more blocks than one pass stages: such a launch
-// (decided on the device from this step's counts, the same in every CTA)
-// runs the per-block loop, where the blocks of a small sparse scene are
-// side by side on many CTAs instead of passes in a row on a few.
-#ifndef NXM_RANGE_MIN_FILL
-#define NXM_RANGE_MIN_FILL 64
-#endif
-constexpr uint32_t kRangeMinFill = NXM_RANGE_MIN_FILL;
+// Below prm.range_min_fill particles a block on average (64 unless tuned), a
+// run of the fast G2P (k_g2p_range) would span more blocks than one pass
+// stages: such a launch (decided on the device from this step's counts, the
+// same in every CTA) runs the per-block loop, where the blocks of a small
+// sparse scene are side by side on many CTAs instead of passes in a row on a
+// few.
 __device__ __forceinline__ bool g2p_sparse(const DevPtrs& P, const Params& prm) {
     const uint32_t nbp = min(__ldcg(&P.counters->num_primary), __ldcg(&P.counters->num_blocks));
     const uint32_t len = min(__ldcg(&P.counters->sorted_len), prm.n);
-    return (uint64_t)len < (uint64_t)kRangeMinFill * nbp;
+    return (uint64_t)len < (uint64_t)prm.range_min_fill * nbp;
 }
 
 // The per-block loop: one CTA per primary block (grid-stride), halo of 216
@@ -687,13 +684,13 @@ __global__ void __launch_bounds__(kG2pThreads, NXM_G2P_MIN_CTAS) k_g2p_range(Dev
 }  // namespace
 
 void launch_grid_update(const DevPtrs& P, const LaunchCfg& c, cudaStream_t s) {
-    k_grid_update<<<c.sm_count * 8, 256, 0, s>>>(P);
+    k_grid_update<<<c.sm_count * (int)c.t.grid_ctas, 256, 0, s>>>(P);
 }
 
 int launch_g2p_update(const DevPtrs& P, const LaunchCfg& c, cudaStream_t s) {
 #if NXM_FAST && !NXM_CPIC && !defined(NXM_G2P_PER_BLOCK)
     if (P.chunk_blk) {  // runs of the sorted list, or one block per unit over sparse blocks
-        k_g2p_range<<<c.sm_count * NXM_G2P_MIN_CTAS, kG2pThreads, 0, s>>>(P);
+        k_g2p_range<<<c.sm_count * (int)min(c.t.g2p_ctas, (uint32_t)NXM_G2P_MIN_CTAS), kG2pThreads, 0, s>>>(P);
         return 1;
     }
 #endif

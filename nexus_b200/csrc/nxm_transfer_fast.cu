@@ -316,7 +316,7 @@ __global__ void k_colliders_end(DevPtrs P) {
 
 void launch_p2g(const DevPtrs& P, const LaunchCfg& c, cudaStream_t s) {
     cudaFuncSetAttribute(k_p2g, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kP2gSmem);
-    k_p2g<<<c.sm_count * NXM_P2G_MIN_CTAS, kP2gThreads, kP2gSmem, s>>>(P);
+    k_p2g<<<c.sm_count * (int)min(c.t.p2g_ctas, (uint32_t)NXM_P2G_MIN_CTAS), kP2gThreads, kP2gSmem, s>>>(P);
 }
 
 void launch_colliders_end(const DevPtrs& P, cudaStream_t s) { k_colliders_end<<<8, 128, 0, s>>>(P); }

@@ -56,6 +56,15 @@ class ParticlesSoAC(C.Structure):
         "damping", "phase", "boundary_friction", "group_id", "enabled", "fixed", "model")]
 
 
+class TuningC(C.Structure):
+    _fields_ = [("p2g_ctas_per_sm", C.c_uint32), ("g2p_ctas_per_sm", C.c_uint32), ("sort_ctas_per_sm", C.c_uint32),
+                ("grid_ctas_per_sm", C.c_uint32), ("sort_batch", C.c_uint32), ("range_min_fill", C.c_uint32),
+                ("density", C.c_uint32), ("scenes", C.c_uint32), ("ms_before", C.c_float), ("ms_after", C.c_float)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 class TimestampsC(C.Structure):
     _fields_ = [("sort_ms", C.c_float), ("p2g_ms", C.c_float), ("grid_update_ms", C.c_float),
                 ("g2p_ms", C.c_float), ("total_ms", C.c_float)]
@@ -131,6 +140,10 @@ SIGNATURES = {
     "nxm_state_kernel_launches": (C.c_uint64, [_vp]),
     "nxm_state_cuda_stream": (C.c_void_p, [_vp]),
     "nxm_sort_blocks_noalloc": (C.c_int, [_vp, C.c_uint32, C.c_float, _vp, _vp, _vp, C.c_uint32, _u, _vp]),
+    "nxm_state_autotune": (C.c_int, [_vp, C.c_uint32, C.POINTER(TuningC)]),
+    "nxm_state_get_tuning": (C.c_int, [_vp, C.POINTER(TuningC)]),
+    "nxm_state_set_tuning": (C.c_int, [_vp, C.POINTER(TuningC)]),
+    "nxm_tuning_table": (C.c_uint32, [C.POINTER(TuningC), C.c_uint32]),
 }
 
 _LIB = None
@@ -597,12 +610,41 @@ class MpmState:
         _check(self.lib.nxm_state_status_poll(self.h, C.byref(v), C.byref(ready)), "state_status_poll")
         return v.value if ready.value else None
 
+    def autotune(self, trial_steps: int = 5) -> dict:
+        """Picks the step's launch shapes by timing this state's own steps
+        (the state advances by every step taken); trial_steps = 0 only applies
+        the decision table's entry for this kind of state."""
+        t = TuningC()
+        _check(self.lib.nxm_state_autotune(self.h, trial_steps, C.byref(t)), "state_autotune")
+        return t.as_dict()
+
+    def tuning(self) -> dict:
+        t = TuningC()
+        _check(self.lib.nxm_state_get_tuning(self.h, C.byref(t)), "state_get_tuning")
+        return t.as_dict()
+
+    def set_tuning(self, **kw):
+        t = TuningC()
+        _check(self.lib.nxm_state_get_tuning(self.h, C.byref(t)), "state_get_tuning")
+        for k, v in kw.items():
+            setattr(t, k, v)
+        _check(self.lib.nxm_state_set_tuning(self.h, C.byref(t)), "state_set_tuning")
+
     def kernel_launches(self) -> int:
         return int(self.lib.nxm_state_kernel_launches(self.h))
 
     def cuda_stream(self) -> int:
         """The cudaStream_t (as an integer) all of this state's work runs on."""
         return int(self.lib.nxm_state_cuda_stream(self.h) or 0)
+
+
+def tuning_table() -> list:
+    """The autotuner's decision table of this process (one dict per key)."""
+    lib = load()
+    n = lib.nxm_tuning_table(None, 0)
+    arr = (TuningC * max(n, 1))()
+    lib.nxm_tuning_table(arr, n)
+    return [arr[i].as_dict() for i in range(n)]
 
 
 def state_from_scene(scene, deterministic: bool = False, grid_capacity: int | None = None,
