@@ -387,6 +387,7 @@ def run_ours(args, world, rank, local):
     batched = measure_batched(args, world, rank, torch) if args.batched_steps > 0 else None
     serving = measure_serving(args, torch, world, rank) if args.serving_requests > 0 else None
     coupled = measure_coupled(args, torch) if (args.coupled_steps > 0 and world == 1) else None
+    coupled_cpic = measure_coupled(args, torch, cpic=True) if (args.coupled_steps > 0 and world == 1) else None
     cube = measure_cube(torch) if (args.cube and world == 1) else None
 
     if rank != 0:
@@ -419,6 +420,7 @@ def run_ours(args, world, rank, local):
         "batched": batched,
         "serving": serving,
         "coupled": coupled,
+        "coupled_cpic": coupled_cpic,
         "tuning_table": tuning_table(),
     }
     print(json.dumps(line), flush=True)
@@ -486,11 +488,14 @@ def measure_batched(args, world, rank, torch):
             "parallelism": f"scene-sharded{world}" if world > 1 else "single"}
 
 
-def measure_coupled(args, torch):
+def measure_coupled(args, torch, cpic: bool = False):
     """The coupled batched mix (configs[3]: 64 sand scenes, each with eight
     kinematic bodies on seeded trajectories driven every step and a
     20,000-triangle height-field floor) in one state, against the same scenes
-    stepped one by one with the same driving."""
+    stepped one by one with the same driving.  With `cpic`, every scene runs
+    CPIC coupling (what a NexusState scene with colliders runs): node and
+    particle distance fields, the floor meshes through their rigid particles,
+    the compatible / incompatible P2G and G2P."""
     from nexus_b200 import scenes as S
     from nexus_b200.mpm import (MpmPipeline, batched_state_from_scenes, batched_collider_offsets,
                                 drive_kinematics, state_from_scene)
@@ -498,6 +503,9 @@ def measure_coupled(args, torch):
     n = sum(sc.n for sc in mix)
     pipe = MpmPipeline()
     st, slots = batched_state_from_scenes(mix)
+    if cpic:
+        st.set_use_cpic(True)
+    rigid = st.num_rigid_particles()
     offs = batched_collider_offsets(mix, slots)
     dt = mix[0].dt
     stream = torch.cuda.ExternalStream(st.cuda_stream())
@@ -521,7 +529,7 @@ def measure_coupled(args, torch):
     del st
     plain_ms = 0.0
     for sc in mix:
-        one = state_from_scene(sc)
+        one = state_from_scene(sc, use_cpic=cpic)
         s1 = torch.cuda.ExternalStream(one.cuda_stream())
         for k in range(3):
             drive_kinematics(one, [sc], [0], k * dt)
@@ -539,7 +547,8 @@ def measure_coupled(args, torch):
         del one
     value = n * args.coupled_steps / (ms / 1e3)
     plain = n / (plain_ms / 1e3)
-    return {"workload": f"coupled_mix_{len(mix)}", "scenes": len(mix), "particles": n,
+    return {"workload": f"coupled_mix_{len(mix)}" + ("_cpic" if cpic else ""), "scenes": len(mix), "particles": n,
+            "coupling": "CPIC" if cpic else "one-way collider projection", "rigid_particles": rigid,
             "colliders_per_scene": int(len(mix[0].colliders)), "triangles_per_scene": int(len(mix[0].tri_vertices) // 3),
             "value": value, "unit": UNIT, "steps": args.coupled_steps, "ms_per_step": ms / args.coupled_steps,
             "plain_scene_by_scene": {"value": plain, "unit": UNIT, "ms_per_step": plain_ms},

@@ -47,6 +47,7 @@ extern "C" {
 #define NXM_STATUS_BLOCK_CAPACITY 2u
 #define NXM_STATUS_MISSING_BLOCK 4u
 #define NXM_STATUS_SORT_CAPACITY 8u
+#define NXM_STATUS_COPY_TIMEOUT 16u  /* a kernel's wait for its bulk copies ran out (reported as NXM_E_CUDA) */
 
 /* ---- plain data -------------------------------------------------------- */
 
@@ -221,9 +222,12 @@ NXM_API int nxm_state_read_collider_pose(nxm_state* state, uint32_t index, float
  * (sampling/sample_trimesh.rs, resampled when the colliders or the cell width
  * change), moved with the collider pose each step, sorted into the blocks
  * and projected on the nodes (solver/rigid_particle_update.rs,
- * grid/sort.rs:165-249 and 493-667, solver/p2g_cdf.rs).  Trimesh CPIC is not
- * available in batched-scene mode (NXM_E_UNSUPPORTED).  CPIC steps run the
- * gather-form transfers with particles in id order. */
+ * grid/sort.rs:165-249 and 493-667, solver/p2g_cdf.rs); in batched-scene
+ * mode each scene's samples take its block-key region and its colliders'
+ * scene-local affinity bits (every scene's samples are rebuilt when a scene
+ * is added or removed).  CPIC keeps particles in id order; deterministic
+ * mode runs the gather-form transfers, the fast mode a scatter P2G with the
+ * compatible / incompatible split. */
 NXM_API int nxm_state_set_use_cpic(nxm_state* state, int enabled);
 /* Number of CPIC rigid particles (GpuRigidParticles::len,
  * src_mpm/solver/particle.rs:351-354); 0 without CPIC or trimesh colliders. */
@@ -337,6 +341,11 @@ NXM_API int nxm_grid_read_nodes(nxm_state* state, float* out, uint32_t max_block
 /* Runs only the sort (+ P2G when `with_p2g`) of the next step on the current
  * particles, leaving the grid readable; particles are not advanced. */
 NXM_API int nxm_debug_sort(nxm_pipeline* pipeline, nxm_state* state, int with_p2g);
+/* Test of the bounded waits on bulk copies: enqueues a kernel whose wait on a
+ * copy barrier can never complete (no copy is issued) and runs out after
+ * `limit` rounds, recording NXM_STATUS_COPY_TIMEOUT in the state's status word
+ * (nxm_synchronize then returns NXM_E_CUDA until the status is cleared). */
+NXM_API int nxm_debug_copy_wait_timeout(nxm_state* state, uint32_t limit);
 
 /* ---- autotuner --------------------------------------------------------------
  * Launch shapes of one state's step.  No counterpart in the reference (its

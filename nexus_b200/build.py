@@ -25,6 +25,7 @@ UNITS = {
     "nxm_sort.cu": [],
     "nxm_transfer_fast.cu": [],
     "nxm_transfer_det.cu": ["--fmad=false"],
+    "nxm_transfer_fast_cpic.cu": [],
     "nxm_noalloc.cu": [],
     "nxm_readback.cu": ["--fmad=false"],
 }

@@ -115,7 +115,18 @@ void launch_p2g(const DevPtrs& P, const LaunchCfg& c, cudaStream_t s);
 void launch_grid_update(const DevPtrs& P, const LaunchCfg& c, cudaStream_t s);
 int launch_g2p_update(const DevPtrs& P, const LaunchCfg& c, cudaStream_t s);  // returns the kernels issued
 void launch_colliders_end(const DevPtrs& P, cudaStream_t s);
+// CPIC scatter P2G (compatible and incompatible fields; particles in id order).
+void launch_p2g_cpic(const DevPtrs& P, const LaunchCfg& c, cudaStream_t s);
+// A bulk-copy barrier wait that runs out after `limit` rounds (test of the
+// timeout path: records STATUS_COPY_TIMEOUT).
+void launch_copy_wait_timeout(Counters* counters, uint32_t limit, cudaStream_t s);
 }  // namespace fast
+
+// Fast-arithmetic CPIC grid update and per-block G2P (nxm_transfer_fast_cpic.cu).
+namespace fast_cpic {
+void launch_grid_update(const DevPtrs& P, const LaunchCfg& c, cudaStream_t s);
+int launch_g2p_update(const DevPtrs& P, const LaunchCfg& c, cudaStream_t s);
+}  // namespace fast_cpic
 
 namespace exact {
 void launch_p2g_gather(const DevPtrs& P, const LaunchCfg& c, cudaStream_t s);

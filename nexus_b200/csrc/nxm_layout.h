@@ -46,6 +46,7 @@ enum : uint32_t {
     STATUS_BLOCK_CAPACITY = 2u,   // more active blocks than the grid capacity
     STATUS_MISSING_BLOCK = 4u,    // a particle's block was not found (follows 1 or 2)
     STATUS_SORT_CAPACITY = 8u,    // sorted-id list longer than its buffer
+    STATUS_COPY_TIMEOUT = 16u,    // a bulk copy did not complete within its wait limit
 };
 
 struct alignas(16) PKin {
@@ -86,7 +87,7 @@ struct alignas(16) DevCollider {
     uint32_t type, bc_type, tri_first, tri_count;
     float bc_friction;
     uint32_t bvh_first, bvh_count;  // trimesh: its BVH nodes [bvh_first, bvh_first + bvh_count)
-    uint32_t pad;
+    uint32_t scene;                 // batched scenes: the scene owning it (NONE otherwise)
 };
 static_assert(sizeof(DevCollider) == 176, "DevCollider layout");
 

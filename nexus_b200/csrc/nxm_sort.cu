@@ -231,6 +231,8 @@ __global__ void __launch_bounds__(256) k_block_prep(DevPtrs P) {
     for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < nthreads; t += gridDim.x * blockDim.x) {
         const uint32_t b = t >> 6, k = t & 63u;
         if (P.nodes) P.nodes[t] = make_float4(0.f, 0.f, 0.f, 0.f);
+        // the scatter P2G of CPIC accumulates the incompatible field too
+        if (P.nodes_inc && P.params->use_cpic) P.nodes_inc[t] = make_float4(0.f, 0.f, 0.f, 0.f);
         if (k < NUM_NBH) {
             int4 v = P.bvid[b];
             int sx, sy, sz;
@@ -582,9 +584,20 @@ void launch_sort_positions(const DevPtrs& P, const LaunchCfg& c, const float4* p
 
 namespace {
 
+// Block (global key coordinates: in batched mode offset by the scene of the
+// sample's collider, as the particles' keys are) and associated cell of rigid
+// particle i.
 __device__ __forceinline__ CellInfo rigid_cell(const DevPtrs& P, uint32_t i, float dx) {
     const float4 w = P.rp_world[i];
-    return cell_info(dx, mk(w.x, w.y, w.z));
+    CellInfo ci = cell_info(dx, mk(w.x, w.y, w.z));
+    if (P.params->scene_blocks) {
+        const uint32_t sid = P.colliders[__float_as_uint(w.w) >> kRigidTriBits].scene;
+        const int3 o = scene_base_of(*P.params, sid);
+        ci.bx += o.x;
+        ci.by += o.y;
+        ci.bz += o.z;
+    }
+    return ci;
 }
 
 // sort.rs:200-249 gpu_mark_rigid_particles_needing_block: a rigid particle

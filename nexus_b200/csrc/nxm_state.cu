@@ -820,7 +820,7 @@ void grid_arrays(nxm_state* s, Slab& g) {
     g.add(&s->nwx, s->block_cap);
     g.add(&s->cursors, (size_t)s->block_cap * NUM_BUCKETS);
     g.add(&s->nbh, (size_t)s->block_cap * NUM_NBH);
-    g.add(&s->nodes, (size_t)s->block_cap * 64);
+    g.add(&s->nodes, (size_t)(s->block_cap + 1) * 64);  // + one block of zeros (halos of missing neighbours)
     g.add(&s->scan_tmp, s->block_cap);
     g.add(&s->tile_sums, s->block_cap / kScanTile + 2);
 }
@@ -867,6 +867,7 @@ int alloc_grid(nxm_state* s, uint32_t grid_capacity) {
     grid_arrays(s, g);
     NXM_TRY(g.alloc(&s->gslab));
     NXM_TRY(cudaMemsetAsync(s->hkey, 0xFF, sizeof(uint32_t) * s->hash_cap, s->stream));
+    NXM_TRY(cudaMemsetAsync(s->nodes + (size_t)s->block_cap * 64, 0, 64 * sizeof(float4), s->stream));
     if (s->use_cpic) {
         int rc = alloc_cpic_grid(s);
         if (rc) return rc;
@@ -1027,8 +1028,10 @@ int enqueue_step(nxm_state* s, cudaStream_t st, cudaEvent_t* ev /* 5 events or n
     const bool has_col = !s->colliders.empty();
     if (ev) cudaEventRecord(ev[0], st);
     // the colliders' centres of mass are refreshed by the sort's first kernel
-    // CPIC runs the reference's gather-form transfers, so it needs the sort's extras
-    const bool exact_path = s->deterministic || s->use_cpic;
+    // deterministic mode runs the reference's gather-form transfers (with the
+    // sort's extras); fast CPIC the scatter P2G with the incompatible split
+    const bool exact_path = s->deterministic;
+    const bool fast_cpic = !s->deterministic && s->use_cpic;
     const bool rigid = P.nrp > 0;  // CPIC with trimesh colliders
     if (rigid) { exact::launch_rigid_transform(P, c, st); ++k; }  // pipeline.rs:393-405
     fast::launch_sort(P, c, /*with_extras=*/exact_path, /*canonical=*/s->deterministic, st, rigid);
@@ -1041,14 +1044,18 @@ int enqueue_step(nxm_state* s, cudaStream_t st, cudaEvent_t* ev /* 5 events or n
     }
     if (ev) cudaEventRecord(ev[1], st);
     if (exact_path) exact::launch_p2g_gather(P, c, st);
+    else if (fast_cpic) fast::launch_p2g_cpic(P, c, st);
     else fast::launch_p2g(P, c, st);
     k += kP2gLaunches;
     if (ev) cudaEventRecord(ev[2], st);
     if (exact_path) exact::launch_grid_update(P, c, st);
+    else if (fast_cpic) fast_cpic::launch_grid_update(P, c, st);
     else fast::launch_grid_update(P, c, st);
     k += kGridLaunches;
     if (ev) cudaEventRecord(ev[3], st);
-    k += exact_path ? exact::launch_g2p_update(P, c, st) : fast::launch_g2p_update(P, c, st);
+    k += exact_path   ? exact::launch_g2p_update(P, c, st)
+         : fast_cpic ? fast_cpic::launch_g2p_update(P, c, st)
+                     : fast::launch_g2p_update(P, c, st);
     if (has_col) { fast::launch_colliders_end(P, st); ++k; }
     if (ev) cudaEventRecord(ev[4], st);
     return k;
@@ -1654,6 +1661,7 @@ void sample_mesh(const std::vector<DevTri>& tris, uint32_t base, uint32_t count,
 // Device form of one nxm_collider (triangle indices shifted by `tri_offset`).
 int collider_from_abi(const nxm_collider& c, const float* tri, uint32_t ntri, uint32_t tri_offset, DevCollider& d) {
     std::memset(&d, 0, sizeof(d));
+    d.scene = NONE;
     std::memcpy(d.a, c.shape_a, 16);
     std::memcpy(d.b, c.shape_b, 16);
     std::memcpy(d.c, c.shape_c, 16);
@@ -1682,9 +1690,6 @@ int install_colliders(nxm_state* s, std::vector<DevCollider> dc, const float* tr
     std::vector<DevTri> tris;
     std::vector<DevBvhNode> bvh;
     std::vector<uint32_t> tri_base(dc.size(), 0u);
-    if (s->use_cpic && s->scene_blocks)
-        for (const DevCollider& d : dc)
-            if (d.type == SHAPE_TRIMESH) return NXM_E_UNSUPPORTED;  // rigid particles of one scene only
     for (size_t i = 0; i < dc.size(); ++i) {
         DevCollider& d = dc[i];
         if (d.type != SHAPE_TRIMESH) continue;
@@ -1994,9 +1999,6 @@ int nxm_state_read_collider_pose(nxm_state* s, uint32_t index, float out[7]) {
 int nxm_state_set_use_cpic(nxm_state* s, int enabled) {
     if (!s) return NXM_E_INVALID;
     if (enabled) {
-        if (s->scene_blocks)
-            for (const DevCollider& c : s->colliders)
-                if (c.type == SHAPE_TRIMESH) return NXM_E_UNSUPPORTED;  // rigid particles of one scene only
         int rc = canonicalize(s);  // CPIC steps in place, in id order
         if (rc) return rc;
         rc = alloc_cpic_grid(s);
@@ -2229,6 +2231,7 @@ static int rebuild_scene_colliders(nxm_state* s) {
             DevCollider d;
             int rc = collider_from_abi(c, sc.tri.data(), (uint32_t)(sc.tri.size() / 9), toff, d);
             if (rc) return rc;
+            d.scene = (uint32_t)i;
             dc.push_back(d);
         }
         tri.insert(tri.end(), sc.tri.begin(), sc.tri.end());
@@ -2563,6 +2566,14 @@ int nxm_debug_sort(nxm_pipeline* pipeline, nxm_state* s, int with_p2g) {
     return NXM_OK;
 }
 
+int nxm_debug_copy_wait_timeout(nxm_state* s, uint32_t limit) {
+    if (!s) return NXM_E_INVALID;
+    fast::launch_copy_wait_timeout(s->d_counters, limit, s->stream);
+    s->launches += 1;
+    NXM_TRY(cudaGetLastError());
+    return NXM_OK;
+}
+
 int nxm_state_estimate_timestep_bound(nxm_state* s, float* max_dt, uint32_t* bits) {
     if (!s || !max_dt) return NXM_E_INVALID;
     int rc = ensure_ready(s);
@@ -2614,6 +2625,7 @@ int nxm_synchronize(nxm_state* s) {
     uint32_t bits = 0;
     int rc = nxm_state_status(s, &bits, 0);
     if (rc) return rc;
+    if (bits & NXM_STATUS_COPY_TIMEOUT) return NXM_E_CUDA;
     if (bits & NXM_STATUS_HASH_FULL) return NXM_E_HASH_FULL;
     if (bits & (NXM_STATUS_BLOCK_CAPACITY | NXM_STATUS_MISSING_BLOCK | NXM_STATUS_SORT_CAPACITY)) return NXM_E_CAPACITY;
     return NXM_OK;

@@ -224,7 +224,13 @@ __device__ __forceinline__ void g2p_particle(const DevPtrs& P, const Params& prm
     v3 velocity = splat(0.f);
     m3 grad = mzero();
     float vgd = 0.f;
-    if ((flags & PFLAG_ENABLED) && NXM_FAST) {
+#if NXM_CPIC
+    // a particle with affinity bits may meet incompatible nodes: per-node gather below
+    const bool factored = NXM_FAST && !(cpic && paff != 0u);
+#else
+    const bool factored = NXM_FAST;
+#endif
+    if ((flags & PFLAG_ENABLED) && factored) {
         // Same sums, factored: with dpt_i = ref + s_i dx,
         //   grad = inv_d (v (x) ref + dx [Sx Sy Sz]),  S_a = sum_i w_i v_i s_i,a
         //   vgd  = inv_d (v . ref + dx (Sx.x + Sy.y + Sz.z))
@@ -576,6 +582,101 @@ __global__ void __launch_bounds__(kG2pThreads, NXM_G2P_MIN_CTAS) k_g2p_update(De
 }
 
 #if NXM_FAST && !NXM_CPIC
+// ---- bulk (TMA) copies of node blocks into shared memory -------------------
+// One elected thread issues 1-D cp.async.bulk copies of whole 1 KB node
+// blocks (global memory of this GPU only, no multicast) that complete on an
+// mbarrier in shared memory; every thread then waits on the barrier's phase,
+// with an iteration limit after which the kernel records
+// STATUS_COPY_TIMEOUT instead of waiting on.
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(uint64_t* bar) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+// Waits for the barrier's phase `parity` to complete; false when the limit ran out.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint32_t limit) {
+    for (uint32_t i = 0; i < limit; ++i) {
+        uint32_t done;
+        asm volatile(
+            "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
+            : "=r"(done)
+            : "r"(smem_u32(bar)), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+constexpr uint32_t kCopyWaitLimit = 1u << 20;  // try_wait rounds (each may suspend a few us): over a second
+
+// Stages the 6x6x6 node-velocity halos of blocks [b, b + cnt) into `halo`
+// by bulk copies: per group of kTmaGroup blocks, thread 0 copies the 8 node
+// blocks each halo draws from (the block and its 7 +1 neighbours; a missing
+// one from the zero block after the grid, index block_capacity) into `raw`,
+// 8 KB a block, completing on the CTA's barrier; every thread waits for the
+// phase, then the CTA rearranges them into halo order.  Ends with a CTA
+// barrier.
+constexpr uint32_t kTmaGroup = 2;
+__device__ __forceinline__ void stage_halos_tma(const DevPtrs& P, uint32_t b, uint32_t cnt, float4* halo, float4* raw,
+                                                uint64_t* bar, uint32_t& parity, uint32_t zero_blk) {
+    const uint32_t tid = threadIdx.x;
+    for (uint32_t g0 = 0; g0 < cnt; g0 += kTmaGroup) {
+        const uint32_t gc = min(cnt - g0, kTmaGroup);
+        if (tid == 0) {
+            // the raw area was last read by the generic proxy (the previous group's rearrangement)
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            mbar_expect_tx(bar, gc * 8u * 1024u);
+            for (uint32_t j = 0; j < gc; ++j) {
+                const uint32_t blk = b + g0 + j;
+                uint32_t nb[7];
+#pragma unroll
+                for (uint32_t o = 0; o < 7; ++o) nb[o] = __ldcg(&P.nbh[blk * NUM_NBH + o]);
+                bulk_copy_g2s(raw + (j * 8u) * 64u, P.nodes + (size_t)blk * 64u, 1024u, bar);
+#pragma unroll
+                for (uint32_t o = 1; o < 8; ++o) {
+                    const uint32_t src = nb[o - 1] == NONE ? zero_blk : nb[o - 1];
+                    bulk_copy_g2s(raw + (j * 8u + o) * 64u, P.nodes + (size_t)src * 64u, 1024u, bar);
+                }
+            }
+        }
+        if (!mbar_wait(bar, parity, kCopyWaitLimit)) {
+            if (tid == 0) set_status(P.counters, STATUS_COPY_TIMEOUT);
+            mbar_wait(bar, parity, kCopyWaitLimit);  // the copies may still be in flight: wait once more
+        }
+        parity ^= 1u;
+        for (uint32_t t = tid; t < gc * 216u; t += blockDim.x) {
+            const uint32_t j = t / 216u, node = t - 216u * j;
+            const uint32_t tx = node % 6u, ty = (node / 6u) % 6u, tz = node / 36u;
+            const uint32_t ox = tx >= 4u, oy = ty >= 4u, oz = tz >= 4u;
+            const uint32_t oct = ox * 4u + oy * 2u + oz;
+            const float4 nd = raw[(j * 8u + oct) * 64u + (tx - 4u * ox) + 4u * (ty - 4u * oy) + 16u * (tz - 4u * oz)];
+            halo[(g0 + j) * 216u + node] = make_float4(nd.x, nd.y, nd.z, 0.f);
+        }
+        __syncthreads();  // raw is free again; the halos are complete
+    }
+}
+
+// The wait above, made to run out: a barrier that expects bytes no copy will
+// deliver (nothing is issued), waited on with `limit` rounds; the kernel
+// records STATUS_COPY_TIMEOUT and returns with no copy in flight.
+__global__ void k_copy_wait_timeout(Counters* counters, uint32_t limit) {
+    __shared__ uint64_t bar;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar);
+        mbar_expect_tx(&bar, 16u);
+    }
+    __syncthreads();
+    if (!mbar_wait(&bar, 0u, limit) && threadIdx.x == 0) set_status(counters, STATUS_COPY_TIMEOUT);
+}
+
 // The fast build's G2P walks the sorted list in runs of kRangeChunk
 // positions, one particle per thread, instead of one CTA per block: a block
 // holds some 1-600 particles, so per-block rounds of 256 threads run part
@@ -594,12 +695,37 @@ __global__ void __launch_bounds__(kG2pThreads, NXM_G2P_MIN_CTAS) k_g2p_update(De
 // (its particles in rounds of 256), through the same loop: a unit is a span
 // of blocks whose halos are staged in passes and a range of sorted positions
 // the threads step through, so the particle update has one call site.
+//
+// Halo staging: plain loads by every thread (each node: its block id from the
+// neighbour table, then the node, both L2 hits) by default; with
+// NXM_G2P_TMA_HALO the bulk copies of stage_halos_tma instead (measured
+// slower on the 2 M-particle scene: the rearrangement pass and its barriers
+// cost more than the loads they replace).
+#ifndef NXM_G2P_TMA_HALO
+#define NXM_G2P_TMA_HALO 0
+#endif
 constexpr uint32_t kRangeHalos = 8;
 static_assert(kG2pThreads == kRangeChunk, "one sorted position per thread");
+#if NXM_G2P_TMA_HALO
+constexpr size_t kG2pRangeSmem = (size_t)kRangeHalos * 216 * 16 + (size_t)kTmaGroup * 8 * 64 * 16 +
+                                 (size_t)9 * 4 * kG2pThreads + 16;
+#endif
 __global__ void __launch_bounds__(kG2pThreads, NXM_G2P_MIN_CTAS) k_g2p_range(DevPtrs P) {
+#if NXM_G2P_TMA_HALO
+    extern __shared__ float4 g2p_smem[];
+    float4* halo = g2p_smem;                 // kRangeHalos x 216 nodes
+    float4* raw = halo + kRangeHalos * 216;  // kTmaGroup x 8 node blocks
+    float* stash_mem = reinterpret_cast<float*>(raw + kTmaGroup * 8 * 64);
+    uint64_t* bar = reinterpret_cast<uint64_t*>(stash_mem + 9 * kG2pThreads);
+    if (threadIdx.x == 0) mbar_init(bar);
+    __syncthreads();
+    uint32_t parity = 0;
+    const uint32_t zero_blk = P.params->block_capacity;
+#else
     __shared__ float4 halo[kRangeHalos * 216];
-#if NXM_G2P_STASH
     __shared__ float stash_mem[9 * kG2pThreads];
+#endif
+#if NXM_G2P_STASH
     volatile float* stash = stash_mem + threadIdx.x;
 #else
     volatile float* stash = nullptr;
@@ -652,11 +778,15 @@ __global__ void __launch_bounds__(kG2pThreads, NXM_G2P_MIN_CTAS) k_g2p_range(Dev
         bool pending = pid != NONE;  // dense: this thread's one particle not yet updated
         for (uint32_t b = lo; b <= hi; b += kRangeHalos) {
             const uint32_t cnt = min(hi - b + 1u, kRangeHalos);
+#if NXM_G2P_TMA_HALO
+            stage_halos_tma(P, b, cnt, halo, raw, bar, parity, zero_blk);
+#else
             for (uint32_t t = tid; t < cnt * 216u; t += kG2pThreads) {
                 const uint32_t i = t / 216u;
                 halo[t] = halo_node(P, b + i, t - 216u * i);
             }
             __syncthreads();
+#endif
             // dense: one position per thread; sparse: the block's positions in rounds
             for (uint32_t p = p0 + tid; p < p1; p += kG2pThreads) {
                 if (p != p0 + tid) {
@@ -683,6 +813,12 @@ __global__ void __launch_bounds__(kG2pThreads, NXM_G2P_MIN_CTAS) k_g2p_range(Dev
 
 }  // namespace
 
+#if NXM_FAST && !NXM_CPIC
+void launch_copy_wait_timeout(Counters* counters, uint32_t limit, cudaStream_t s) {
+    k_copy_wait_timeout<<<1, 32, 0, s>>>(counters, limit);
+}
+#endif
+
 void launch_grid_update(const DevPtrs& P, const LaunchCfg& c, cudaStream_t s) {
     k_grid_update<<<c.sm_count * (int)c.t.grid_ctas, 256, 0, s>>>(P);
 }
@@ -690,7 +826,14 @@ void launch_grid_update(const DevPtrs& P, const LaunchCfg& c, cudaStream_t s) {
 int launch_g2p_update(const DevPtrs& P, const LaunchCfg& c, cudaStream_t s) {
 #if NXM_FAST && !NXM_CPIC && !defined(NXM_G2P_PER_BLOCK)
     if (P.chunk_blk) {  // runs of the sorted list, or one block per unit over sparse blocks
+#if NXM_G2P_TMA_HALO
+        cudaFuncSetAttribute(k_g2p_range, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kG2pRangeSmem);
+        cudaFuncSetAttribute(k_g2p_range, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+        k_g2p_range<<<c.sm_count * (int)min(c.t.g2p_ctas, (uint32_t)NXM_G2P_MIN_CTAS), kG2pThreads, kG2pRangeSmem,
+                      s>>>(P);
+#else
         k_g2p_range<<<c.sm_count * (int)min(c.t.g2p_ctas, (uint32_t)NXM_G2P_MIN_CTAS), kG2pThreads, 0, s>>>(P);
+#endif
         return 1;
     }
 #endif

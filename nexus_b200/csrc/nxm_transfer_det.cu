@@ -276,7 +276,17 @@ __global__ void __launch_bounds__(64) k_p2g_cdf(DevPtrs P) {
         const uint32_t num = P.rp_count[b];
         if (num == 0) continue;
         const uint32_t first = P.rp_first[b];
-        const int4 vid = P.bvid[b];
+        int4 vid = P.bvid[b];
+        // batched scenes: scene-local cells, and the scene's colliders numbered
+        // from its first one (the affinity bits and closest-collider index of
+        // the node field are per scene, as for the analytic colliders)
+        uint32_t col0 = 0u;
+        if (P.params->scene_blocks) {
+            const uint32_t sid = scene_of_block(*P.params, vid);
+            col0 = sid != NONE ? P.scene_cols[sid].x : 0u;
+            const int3 o = scene_base_of_block(*P.params, vid);
+            vid.x -= o.x; vid.y -= o.y; vid.z -= o.z;
+        }
         const int cx = vid.x * 4 + (int)(tid & 3u), cy = vid.y * 4 + (int)((tid >> 2) & 3u),
                   cz = vid.z * 4 + (int)(tid >> 4);
         const v3 cell_pos = mk((float)cx, (float)cy, (float)cz) * dx;
@@ -300,7 +310,7 @@ __global__ void __launch_bounds__(64) k_p2g_cdf(DevPtrs P) {
                 sb[tid] = make_float4(bb.x, bb.y, bb.z, 0.f);
                 sc[tid] = make_float4(cc.x, cc.y, cc.z, 0.f);
                 const v3 ac = assoc_cell_of(dx, mk(w.x, w.y, w.z));
-                sassoc[tid] = make_int4(f2i_sat(ac.x), f2i_sat(ac.y), f2i_sat(ac.z), (int)col);
+                sassoc[tid] = make_int4(f2i_sat(ac.x), f2i_sat(ac.y), f2i_sat(ac.z), (int)(col - col0));
             }
             __syncthreads();
             const uint32_t len = min(64u, num - chunk);

@@ -48,20 +48,26 @@ constexpr int kP2gRec = 28;  // floats per staged particle
 //       | [12..15] (C dx).c2, w_z[2] | [16 + i + 3 j] w_x[i] w_y[j] | [25..27] unused
 constexpr size_t kP2gSmem = (size_t)kP2gWarps * 216 * 16 + (size_t)kP2gChunk * kP2gRec * 4 + (64 + 68) * 4 +
                             (size_t)kP2gChunk * (2 + 2 + 1);
+// CPIC adds the warps' incompatible-field tiles and the 216 tile nodes' affinity bits
+constexpr size_t kP2gSmemCpic = kP2gSmem + (size_t)kP2gWarps * 216 * 16 + 216 * 4 + 16;
 static_assert(kP2gChunk <= 65536, "staged particle indices are 16-bit");
 
 __device__ __forceinline__ float4 f4add(float4 a, float4 b) { return make_float4(a.x + b.x, a.y + b.y, a.z + b.z, a.w + b.w); }
 
-// One staged particle's raw record (kin words 0..19) and a block header.
+// One staged particle's raw record (kin words 0..19, CPIC: its affinity
+// bits) and a block header.
 struct P2gRaw {
     float4 xm, vf, c0, c1, c2;
+    float aff;
 };
 struct P2gHdr {
     uint32_t first, np;
 };
 
+template <bool kCpic>
 __device__ __forceinline__ P2gRaw p2g_load_raw(const DevPtrs& P, uint32_t pid) {
     P2gRaw r;
+    r.aff = 0.f;
     if (pid == NONE) {
         r.vf = make_float4(0.f, 0.f, 0.f, 0.f);  // flags 0: not staged
         return r;
@@ -72,6 +78,8 @@ __device__ __forceinline__ P2gRaw p2g_load_raw(const DevPtrs& P, uint32_t pid) {
     r.c0 = __ldg(kr + 2);
     r.c1 = __ldg(kr + 3);
     r.c2 = __ldg(kr + 4);
+    // CPIC keeps particles in id order (slot = id): the affinity of this step's g2p_cdf
+    if (kCpic) r.aff = __ldg(&P.pcdf[3u * pid + 1u].w);
     return r;
 }
 
@@ -89,17 +97,25 @@ __device__ __forceinline__ P2gHdr p2g_load_hdr(const DevPtrs& P, uint32_t b, uin
 // grid strides ahead, the sorted id of the next chunk's particle right after
 // staging, and its 80-byte record at the start of the cell phase, so their
 // latency overlaps the current chunk's shared-memory work.
-__global__ void __launch_bounds__(kP2gThreads, NXM_P2G_MIN_CTAS) k_p2g(DevPtrs P) {
+//
+// CPIC (kCpic; solver/p2g.rs:258-310): a particle whose affinity bits are
+// incompatible with a node's (aff_compatible) feeds that node's second,
+// incompatible field instead: each lane keeps both sums for its three nodes,
+// and the warps keep a second tile flushed into nodes_inc.
+template <bool kCpic>
+__global__ void __launch_bounds__(kP2gThreads, kCpic ? 2 : NXM_P2G_MIN_CTAS) k_p2g(DevPtrs P) {
     static_assert(kP2gChunk == kP2gThreads, "one staged particle per thread");
     static_assert(kP2gThreads >= 216, "one flushed tile node per thread");
     extern __shared__ float4 p2g_smem[];
     float4* tiles = p2g_smem;  // kP2gWarps x 216 nodes of (x, y, z, m)
-    float* rec = reinterpret_cast<float*>(tiles + kP2gWarps * 216);
+    float4* tiles_inc = tiles + kP2gWarps * 216;  // CPIC only
+    float* rec = reinterpret_cast<float*>(tiles + (kCpic ? 2 : 1) * kP2gWarps * 216);
     int* cnt = reinterpret_cast<int*>(rec + kP2gChunk * kP2gRec);
     int* start = cnt + 64;  // 65 used
     uint16_t* perm = reinterpret_cast<uint16_t*>(start + 68);
     uint16_t* prank = perm + kP2gChunk;
     uint8_t* pcell = reinterpret_cast<uint8_t*>(prank + kP2gChunk);
+    uint32_t* node_aff = reinterpret_cast<uint32_t*>(pcell + ((kP2gChunk + 15) & ~15));  // CPIC: 216 tile nodes
 
     const float dx = P.params->dx;
     const float inv_dx = P.params->inv_dx;
@@ -121,6 +137,7 @@ __global__ void __launch_bounds__(kP2gThreads, NXM_P2G_MIN_CTAS) k_p2g(DevPtrs P
     const uint32_t src1 = worker ? sxy + 9u * ((grp + 1u) % 3u) : lane;
     const uint32_t src2 = worker ? sxy + 9u * ((grp + 2u) % 3u) : lane;
     float4* tile = tiles + warp * 216u;
+    float4* tile_inc = tiles_inc + warp * 216u;
     // flush role: tile node `tid` (tid < 216) of octant `foct`
     const uint32_t ftx = tid % 6u, fty = (tid / 6u) % 6u, ftz = tid / 36u;
     const uint32_t fox = ftx >= 4u, foy = fty >= 4u, foz = ftz >= 4u;
@@ -130,12 +147,13 @@ __global__ void __launch_bounds__(kP2gThreads, NXM_P2G_MIN_CTAS) k_p2g(DevPtrs P
     uint32_t b = blockIdx.x;
     if (b >= nbp) return;
     const uint32_t stride = gridDim.x;
-    for (uint32_t t = tid; t < kP2gWarps * 216u; t += kP2gThreads) tiles[t] = make_float4(0.f, 0.f, 0.f, 0.f);
+    for (uint32_t t = tid; t < (kCpic ? 2u : 1u) * kP2gWarps * 216u; t += kP2gThreads)
+        tiles[t] = make_float4(0.f, 0.f, 0.f, 0.f);
     if (tid < 64) cnt[tid] = 0;
     P2gHdr h = p2g_load_hdr(P, b, nbp);
     P2gHdr hn = p2g_load_hdr(P, b + stride, nbp);
     P2gHdr hnn = p2g_load_hdr(P, b + 2u * stride, nbp);
-    P2gRaw raw = p2g_load_raw(P, tid < h.np ? __ldg(&P.sorted[h.first + tid]) : NONE);
+    P2gRaw raw = p2g_load_raw<kCpic>(P, tid < h.np ? __ldg(&P.sorted[h.first + tid]) : NONE);
     __syncthreads();
     for (;;) {
         int4 vid = P.bvid[b];
@@ -144,6 +162,8 @@ __global__ void __launch_bounds__(kP2gThreads, NXM_P2G_MIN_CTAS) k_p2g(DevPtrs P
             vid.x -= o.x; vid.y -= o.y; vid.z -= o.z;
         }
         const uint32_t fblk = (tid < 216u && foct != 0u) ? __ldg(&P.nbh[b * NUM_NBH + foct - 1u]) : b;
+        if (kCpic && tid < 216u)  // read after the staging barrier below
+            node_aff[tid] = fblk == NONE ? 0u : __ldg(&P.ncdf[fblk * 64u + fnode].y);
         for (uint32_t base = 0; base < h.np; base += kP2gChunk) {
             const uint32_t m_chunk = min(h.np - base, (uint32_t)kP2gChunk);
             // 1. stage and bin this thread's particle (base + tid)
@@ -170,7 +190,7 @@ __global__ void __launch_bounds__(kP2gThreads, NXM_P2G_MIN_CTAS) k_p2g(DevPtrs P
                     rr[3] = make_float4(C.c2.x * dx, C.c2.y * dx, C.c2.z * dx, wz.z);
                     rr[4] = make_float4(wx.x * wy.x, wx.y * wy.x, wx.z * wy.x, wx.x * wy.y);
                     rr[5] = make_float4(wx.y * wy.y, wx.z * wy.y, wx.x * wy.z, wx.y * wy.z);
-                    rr[6] = make_float4(wx.z * wy.z, 0.f, 0.f, 0.f);
+                    rr[6] = make_float4(wx.z * wy.z, raw.aff, 0.f, 0.f);
                     const uint32_t c = ci.ax + 4u * ci.ay + 16u * ci.az;
                     pcell[k] = (uint8_t)c;
                     prank[k] = (uint16_t)atomicAdd(&cnt[c], 1);
@@ -205,12 +225,21 @@ __global__ void __launch_bounds__(kP2gThreads, NXM_P2G_MIN_CTAS) k_p2g(DevPtrs P
             }
             __syncthreads();
             if (tid < 64) cnt[tid] = 0;  // counts are consumed; ready for the next chunk
-            raw = p2g_load_raw(P, pid_next);
+            raw = p2g_load_raw<kCpic>(P, pid_next);
             // 3. one warp per cell, three particles per pass
             for (uint32_t c = warp; c < 64u; c += kP2gWarps) {
                 const int s0 = start[c], s1 = start[c + 1];
                 if (s0 == s1) continue;
                 float4 a0 = make_float4(0.f, 0.f, 0.f, 0.f), a1 = a0, a2 = a0;  // s.z = 0, 1, 2
+                float4 i0 = a0, i1 = a0, i2 = a0;  // CPIC: the incompatible sums
+                const uint32_t cx = c & 3u, cy = (c >> 2) & 3u, cz = c >> 4;
+                const uint32_t col = (cx + sxy % 3u) + 6u * (cy + sxy / 3u) + 36u * cz;  // this lane's s.z = 0 node
+                uint32_t na0 = 0u, na1 = 0u, na2 = 0u;
+                if (kCpic && worker) {
+                    na0 = node_aff[col];
+                    na1 = node_aff[col + 36u];
+                    na2 = node_aff[col + 72u];
+                }
                 for (int i = s0; i < s1; i += 3) {
                     const int j = i + (int)grp;
                     const bool valid = worker && j < s1;
@@ -223,46 +252,69 @@ __global__ void __launch_bounds__(kP2gThreads, NXM_P2G_MIN_CTAS) k_p2g(DevPtrs P
                     float bx = qm.x + k0.x * fx + k1.x * fy;
                     float by = qm.y + k0.y * fx + k1.y * fy;
                     float bz = qm.z + k0.z * fx + k1.z * fy;
-                    float w = wxy * k0.w;
-                    a0.x += w * bx; a0.y += w * by; a0.z += w * bz; a0.w += w * qm.w;
-                    bx += k2.x; by += k2.y; bz += k2.z;
-                    w = wxy * k1.w;
-                    a1.x += w * bx; a1.y += w * by; a1.z += w * bz; a1.w += w * qm.w;
-                    bx += k2.x; by += k2.y; bz += k2.z;
-                    w = wxy * k2.w;
-                    a2.x += w * bx; a2.y += w * by; a2.z += w * bz; a2.w += w * qm.w;
+                    if (!kCpic) {
+                        float w = wxy * k0.w;
+                        a0.x += w * bx; a0.y += w * by; a0.z += w * bz; a0.w += w * qm.w;
+                        bx += k2.x; by += k2.y; bz += k2.z;
+                        w = wxy * k1.w;
+                        a1.x += w * bx; a1.y += w * by; a1.z += w * bz; a1.w += w * qm.w;
+                        bx += k2.x; by += k2.y; bz += k2.z;
+                        w = wxy * k2.w;
+                        a2.x += w * bx; a2.y += w * by; a2.z += w * bz; a2.w += w * qm.w;
+                    } else {
+                        const uint32_t paff = __float_as_uint(r[25]);
+                        const auto acc = [&](float4& a, float4& ai, uint32_t na, float w) {
+                            const bool comp = aff_compatible(paff, na);
+                            const float wc = comp ? w : 0.f, wi = comp ? 0.f : w;
+                            a.x += wc * bx; a.y += wc * by; a.z += wc * bz; a.w += wc * qm.w;
+                            ai.x += wi * bx; ai.y += wi * by; ai.z += wi * bz; ai.w += wi * qm.w;
+                        };
+                        acc(a0, i0, na0, wxy * k0.w);
+                        bx += k2.x; by += k2.y; bz += k2.z;
+                        acc(a1, i1, na1, wxy * k1.w);
+                        bx += k2.x; by += k2.y; bz += k2.z;
+                        acc(a2, i2, na2, wxy * k2.w);
+                    }
                 }
                 // lane (sxy, g) collects node (sxy, s.z = g) from the three groups:
                 // from group g+1 its s.z = g sum, which that lane holds as (its g + 2) mod 3,
                 // from group g+2 likewise as (its g + 1) mod 3.
-                const float4 own = grp == 0u ? a0 : (grp == 1u ? a1 : a2);
-                const float4 out1 = grp == 0u ? a2 : (grp == 1u ? a0 : a1);
-                const float4 out2 = grp == 0u ? a1 : (grp == 1u ? a2 : a0);
-                float4 t;
-                t.x = own.x + __shfl_sync(0xFFFFFFFFu, out1.x, src1) + __shfl_sync(0xFFFFFFFFu, out2.x, src2);
-                t.y = own.y + __shfl_sync(0xFFFFFFFFu, out1.y, src1) + __shfl_sync(0xFFFFFFFFu, out2.y, src2);
-                t.z = own.z + __shfl_sync(0xFFFFFFFFu, out1.z, src1) + __shfl_sync(0xFFFFFFFFu, out2.z, src2);
-                t.w = own.w + __shfl_sync(0xFFFFFFFFu, out1.w, src1) + __shfl_sync(0xFFFFFFFFu, out2.w, src2);
-                if (worker) {
-                    const uint32_t cx = c & 3u, cy = (c >> 2) & 3u, cz = c >> 4;
-                    const uint32_t node = (cx + sxy % 3u) + 6u * (cy + sxy / 3u) + 36u * (cz + grp);
-                    tile[node] = f4add(tile[node], t);
+                const auto exchange = [&](float4 x0, float4 x1, float4 x2) {
+                    const float4 own = grp == 0u ? x0 : (grp == 1u ? x1 : x2);
+                    const float4 out1 = grp == 0u ? x2 : (grp == 1u ? x0 : x1);
+                    const float4 out2 = grp == 0u ? x1 : (grp == 1u ? x2 : x0);
+                    float4 t;
+                    t.x = own.x + __shfl_sync(0xFFFFFFFFu, out1.x, src1) + __shfl_sync(0xFFFFFFFFu, out2.x, src2);
+                    t.y = own.y + __shfl_sync(0xFFFFFFFFu, out1.y, src1) + __shfl_sync(0xFFFFFFFFu, out2.y, src2);
+                    t.z = own.z + __shfl_sync(0xFFFFFFFFu, out1.z, src1) + __shfl_sync(0xFFFFFFFFu, out2.z, src2);
+                    t.w = own.w + __shfl_sync(0xFFFFFFFFu, out1.w, src1) + __shfl_sync(0xFFFFFFFFu, out2.w, src2);
+                    return t;
+                };
+                const float4 t = exchange(a0, a1, a2);
+                const uint32_t node = col + 36u * grp;
+                if (worker) tile[node] = f4add(tile[node], t);
+                if (kCpic) {
+                    const float4 ti = exchange(i0, i1, i2);
+                    if (worker) tile_inc[node] = f4add(tile_inc[node], ti);
                 }
             }
             __syncthreads();
         }
         // 4. sum the warp tiles (clearing them) and flush the block's nodes
         if (tid < 216u) {
-            float4 sum = tiles[tid];
-            tiles[tid] = make_float4(0.f, 0.f, 0.f, 0.f);
+            for (int f = 0; f < (kCpic ? 2 : 1); ++f) {
+                float4* tt = f ? tiles_inc : tiles;
+                float4 sum = tt[tid];
+                tt[tid] = make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
-            for (int w = 1; w < kP2gWarps; ++w) {
-                sum = f4add(sum, tiles[w * 216 + tid]);
-                tiles[w * 216 + tid] = make_float4(0.f, 0.f, 0.f, 0.f);
-            }
-            if (sum.x != 0.f || sum.y != 0.f || sum.z != 0.f || sum.w != 0.f) {
-                if (fblk == NONE) set_status_f(P.counters, STATUS_MISSING_BLOCK);
-                else atomicAdd(&P.nodes[fblk * 64u + fnode], sum);
+                for (int w = 1; w < kP2gWarps; ++w) {
+                    sum = f4add(sum, tt[w * 216 + tid]);
+                    tt[w * 216 + tid] = make_float4(0.f, 0.f, 0.f, 0.f);
+                }
+                if (sum.x != 0.f || sum.y != 0.f || sum.z != 0.f || sum.w != 0.f) {
+                    if (fblk == NONE) set_status_f(P.counters, STATUS_MISSING_BLOCK);
+                    else atomicAdd(&(f ? P.nodes_inc : P.nodes)[fblk * 64u + fnode], sum);
+                }
             }
         }
         __syncthreads();
@@ -315,8 +367,13 @@ __global__ void k_colliders_end(DevPtrs P) {
 }  // namespace
 
 void launch_p2g(const DevPtrs& P, const LaunchCfg& c, cudaStream_t s) {
-    cudaFuncSetAttribute(k_p2g, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kP2gSmem);
-    k_p2g<<<c.sm_count * (int)min(c.t.p2g_ctas, (uint32_t)NXM_P2G_MIN_CTAS), kP2gThreads, kP2gSmem, s>>>(P);
+    cudaFuncSetAttribute(k_p2g<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kP2gSmem);
+    k_p2g<false><<<c.sm_count * (int)min(c.t.p2g_ctas, (uint32_t)NXM_P2G_MIN_CTAS), kP2gThreads, kP2gSmem, s>>>(P);
+}
+
+void launch_p2g_cpic(const DevPtrs& P, const LaunchCfg& c, cudaStream_t s) {
+    cudaFuncSetAttribute(k_p2g<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kP2gSmemCpic);
+    k_p2g<true><<<c.sm_count * 2, kP2gThreads, kP2gSmemCpic, s>>>(P);
 }
 
 void launch_colliders_end(const DevPtrs& P, cudaStream_t s) { k_colliders_end<<<8, 128, 0, s>>>(P); }

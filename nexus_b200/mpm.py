@@ -103,6 +103,7 @@ SIGNATURES = {
     "nxm_grid_read_sorted_ids": (C.c_int, [_vp, _u, C.c_uint32]),
     "nxm_grid_read_nodes": (C.c_int, [_vp, _f, C.c_uint32]),
     "nxm_debug_sort": (C.c_int, [_vp, _vp, C.c_int]),
+    "nxm_debug_copy_wait_timeout": (C.c_int, [_vp, C.c_uint32]),
     "nxm_state_estimate_timestep_bound": (C.c_int, [_vp, _f, _u]),
     "nxm_read_cdf": (C.c_int, [_vp, _f]),
     "nxm_simulate_frame": (C.c_int, [_vp, _vp, C.c_uint32, C.c_uint32, _u]),

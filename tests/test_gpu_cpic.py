@@ -1,14 +1,15 @@
 """CPIC coupling on the GPU against the oracle: the deterministic build
 follows the oracle's arithmetic (DET_BOUNDS on what the run changed, the same
-affinity bits); the fast build changes summation order and fuses multiply-adds
-(FAST_BOUNDS).  Errors are change_rel_l2 of positions, v, C and F (the error
+affinity bits); the fast build (scatter P2G with the compatible /
+incompatible split, fast-arithmetic G2P) changes summation order and fuses
+multiply-adds (FAST_BOUNDS).  Errors are change_rel_l2 of positions, v, C and F (the error
 over the oracle's own change from the start), FP64-oracle errors printed
 beside them, and the unmoved input must fail the same check."""
 import numpy as np
 import pytest
 
 from nexus_b200 import scenes
-from nexus_b200.mpm import MpmPipeline, state_from_scene, NexusError, NXM_E_UNSUPPORTED
+from nexus_b200.mpm import MpmPipeline, state_from_scene
 from tests.parity import DET_BOUNDS, FAST_BOUNDS, assert_run_matches, start_state
 
 pytestmark = pytest.mark.gpu
@@ -93,10 +94,40 @@ def test_cpic_trimesh_resamples_with_the_cell_width(gpu_lib):
     assert st.num_rigid_particles() == 0
 
 
-def test_cpic_trimesh_refused_in_batched_scenes(gpu_lib):
-    """Trimesh CPIC samples the rigid particles of a single scene only."""
+def test_cpic_trimesh_in_batched_scenes_matches_alone(gpu_lib, oracle_built):
+    """Trimesh CPIC in batched-scene mode: each scene's rigid samples carry
+    its key offset and its colliders' scene-local affinity bits, so in
+    deterministic mode every scene of the batch steps bit for bit as it does
+    alone, and in the fast mode (scatter P2G with the incompatible split)
+    each stays within the fast bounds of its own oracle run."""
+    from oracle.oracle import OracleScene
     from nexus_b200.mpm import batched_state_from_scenes
-    st, _ = batched_state_from_scenes([scenes.trimesh_floor(n_side=4)])
-    with pytest.raises(NexusError) as e:
-        st.set_use_cpic(True)
-    assert e.value.code == NXM_E_UNSUPPORTED
+    scs = [scenes.cpic_trimesh(), scenes.cpic_drop()]
+    steps = 60
+    pipe = MpmPipeline()
+    alone = []
+    for sc in scs:
+        st = state_from_scene(sc, deterministic=True, use_cpic=True)
+        for _ in range(steps):
+            pipe.step(st)
+        alone.append(st.read_positions())
+    bst, slots = batched_state_from_scenes(scs, deterministic=True)
+    bst.set_use_cpic(True)
+    assert bst.num_rigid_particles() > 10000
+    for _ in range(steps):
+        pipe.step(bst)
+    bst.synchronize()
+    for sc, sl, want in zip(scs, slots, alone):
+        got = bst.read_scene_positions(sl)
+        assert np.array_equal(got, want), (sc.name, np.abs(got - want).max())
+    fst, fslots = batched_state_from_scenes(scs, deterministic=False)
+    fst.set_use_cpic(True)
+    for _ in range(steps):
+        pipe.step(fst)
+    fst.synchronize()
+    for sc, sl in zip(scs, fslots):
+        o = OracleScene(sc)
+        o.set_use_cpic(True)
+        o.step(steps)
+        assert_run_matches(f"batched cpic {sc.name}, fast", fst.read_scene_particles(sl), o.particles(),
+                           _oracle64(sc, steps), start_state(sc), FAST_BOUNDS)

@@ -576,3 +576,22 @@ def test_sort_capacity_is_reported(pipe):
         st.synchronize()
     assert e.value.code == NXM_E_CAPACITY
     assert st.status(clear=True) & 8
+
+
+def test_bulk_copy_wait_runs_out_into_a_status(pipe):
+    """Waits on bulk copies are bounded: a barrier that no copy completes
+    (nothing is issued) runs out of its rounds, the kernel records
+    NXM_STATUS_COPY_TIMEOUT and returns, synchronize reports NXM_E_CUDA, and
+    after the status is cleared the state steps on normally."""
+    from nexus_b200.mpm import NXM_E_CUDA, _check
+    sc = scenes.elastic_cube(n_side=8)
+    st = state_from_scene(sc)
+    _check(st.lib.nxm_debug_copy_wait_timeout(st.h, 1000), "debug_copy_wait_timeout")
+    with pytest.raises(NexusError) as e:
+        st.synchronize()
+    assert e.value.code == NXM_E_CUDA
+    assert st.status(clear=True) & 16
+    for _ in range(3):
+        pipe.step(st)
+    st.synchronize()
+    assert np.isfinite(st.read_positions()).all()
