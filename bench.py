@@ -361,8 +361,9 @@ def run_ours(args, world, rank, local):
     max_ms = all_max(ms, world)
     value = n * world * args.steps / (max_ms / 1e3)
 
-    # per-phase breakdown on one extra (untimed) step
-    phases = pipe.step(st, timestamps=True)
+    # per-phase breakdown: medians over five extra (untimed) timestamped steps
+    ph = [pipe.step(st, timestamps=True) for _ in range(5)]
+    phases = {k: float(np.median([p[k] for p in ph])) for k in ph[0]}
     st.synchronize()
 
     # roofline of one step (the captured graph): algorithmic bytes / step time

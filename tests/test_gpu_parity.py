@@ -138,7 +138,10 @@ def test_affine_velocity_field_is_transferred_exactly(pipe, deterministic):
     g = st.read_particles()
     np.testing.assert_allclose(g["vel"], x @ A.T + c, rtol=0, atol=1e-5)
     aff = g["aff"].astype(np.float64).reshape(-1, 3, 3).transpose(0, 2, 1) / g["mass"][:, None, None]
-    np.testing.assert_allclose(aff, np.broadcast_to(A, aff.shape), rtol=0, atol=1e-4)
+    # C comes from sums of w v (x_i - x_p) scaled by 4 / dx^2: in fast mode the
+    # atomic summation order changes run to run, which moves C by up to ~1e-4
+    # (|A| ~ 0.5); a wrong transfer would be off by O(|A|)
+    np.testing.assert_allclose(aff, np.broadcast_to(A, aff.shape), rtol=0, atol=1e-4 if deterministic else 3e-4)
 
 
 @pytest.mark.parametrize("deterministic", [False, True])
