@@ -35,18 +35,77 @@ struct Collision {
     uint32_t closest;
 };
 
-// grid_update_collide.rs:30-99 collide(): analytic shapes (ball, cuboid,
-// capsule) and triangle meshes (BVH query within 1.5 dx, as the reference's
-// project_local_point with max_dist; a mesh with no triangle that close is
-// skipped).
+// Whether analytic collider c (ball, cuboid, capsule) can touch a node of a
+// block whose 64 nodes lie within rb of `centre` (rb = 1.5 sqrt(3) dx about
+// the block's middle): the exact distance at the centre, then the bound
+// distance(node) >= distance(centre) - rb.  A contributing node is inside the
+// shape or has its projection within cap on every axis (so within sqrt(3)
+// cap): the collider is kept when the centre is inside or the shape lies
+// within rb + sqrt(3) cap of it.  The reach carries a relative and an
+// absolute margin above the rounding of the per-node queries it stands for.
+__device__ __forceinline__ bool analytic_near_block(const DevCollider& c, float cap, float rb, v3 centre) {
+    const quat q = quat{c.rot[0], c.rot[1], c.rot[2], c.rot[3]};
+    const v3 local = qrot(qconj(q), centre - mk(c.tra[0], c.tra[1], c.tra[2]));
+    Proj pr;
+    if (c.type == SHAPE_BALL) pr = ball_project_local(c.a[0], local);
+    else if (c.type == SHAPE_CUBOID) pr = cuboid_project_local(mk(c.a[0], c.a[1], c.a[2]), local);
+    else if (c.type == SHAPE_CAPSULE)
+        pr = capsule_project_local(mk(c.a[0], c.a[1], c.a[2]), mk(c.b[0], c.b[1], c.b[2]), c.b[3], local);
+    else return true;
+    if (pr.inside) return true;
+    const v3 d = pr.point - local;
+    const float reach = (rb + 1.75f * cap) * 1.001f + 1.0e-5f;
+    return !(dot(d, d) > reach * reach);  // a NaN keeps the collider
+}
+
+// Whether trimesh collider c can have a triangle within cap of a node of the
+// block: the box of its BVH root within rb + cap of the centre (a node's
+// query descends only into boxes within cap of the node).  Only the root is
+// tested: one lane's deeper query for the whole block costs the warp about
+// as much as the 32 per-node queries it would save.
+__device__ __forceinline__ bool mesh_near_block(const DevPtrs& P, const DevCollider& c, float cap, float rb,
+                                                v3 centre) {
+    if (c.bvh_count == 0u) return false;
+    const quat ci = qconj(quat{c.rot[0], c.rot[1], c.rot[2], c.rot[3]});
+    const v3 local = qrot(ci, centre) + (-qrot(ci, mk(c.tra[0], c.tra[1], c.tra[2])));
+    return !(aabb_distance(P.bvh[c.bvh_first], local) > (rb + cap) * 1.001f + 1.0e-5f);
+}
+
+// Bit i: collider i (< 32) may touch a node of block `vid` (scene-local
+// block coordinates).  Every lane of the warp calls it for the same block;
+// lane i tests collider i.  Trimeshes are left out when `skip_meshes`.
+__device__ __forceinline__ uint32_t colliders_near_block(const DevPtrs& P, const DevCollider* cols, uint32_t ncol,
+                                                        float dx, int4 vid, bool skip_meshes) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const v3 centre = mk((float)vid.x * 4.0f + 1.5f, (float)vid.y * 4.0f + 1.5f, (float)vid.z * 4.0f + 1.5f) * dx;
+    const float cap = dx * 1.5f, rb = 2.6f * dx;
+    bool near = false;
+    if (lane < ncol) {
+        const DevCollider& c = cols[lane];
+        near = c.type == SHAPE_TRIMESH ? !skip_meshes && mesh_near_block(P, c, cap, rb, centre)
+                                       : analytic_near_block(c, cap, rb, centre);
+    }
+    return __ballot_sync(0xFFFFFFFFu, near);
+}
+
+// `near` (bit i for collider i < 32, from colliders_near_block) leaves out
+// the colliders that cannot reach this node: their projections would find
+// no point within cap and no inside.
 __device__ __forceinline__ Collision collide(const DevPtrs& P, const DevCollider* cols, uint32_t ncol, float dx,
-                                             v3 point) {
+                                             v3 point, uint32_t near) {
     const float cap = dx * 1.5f;
     Collision col;
     col.normal = splat(0.f);
     col.distance = MAX_FLT;
     col.closest = 0;
     for (uint32_t i = 0; i < ncol; ++i) {
+        if (i < 32u && !(near & (1u << i))) {
+            // next candidate: skip the run of unset bits at once
+            const uint32_t rest = near & ~((2u << i) - 1u);
+            if (rest == 0u) i = 31u;
+            else i = (uint32_t)__ffs(rest) - 2u;
+            continue;
+        }
         const DevCollider& c = cols[i];
         quat q = quat{c.rot[0], c.rot[1], c.rot[2], c.rot[3]};
         v3 tra = mk(c.tra[0], c.tra[1], c.tra[2]);
@@ -130,7 +189,9 @@ __global__ void __launch_bounds__(256) k_grid_update(DevPtrs P) {
             }
             v3 cell_pt = mk((float)(vid.x * 4 + (int)(k & 3u)), (float)(vid.y * 4 + (int)((k >> 2) & 3u)),
                             (float)(vid.z * 4 + (int)(k >> 4))) * dx;
-            Collision c = collide(P, cols, nc, dx, cell_pt);
+            // the warp's 32 nodes share one block: its colliders in reach, one lane each
+            const uint32_t near = colliders_near_block(P, cols, nc, dx, vid, false);
+            Collision c = collide(P, cols, nc, dx, cell_pt, near);
             if (c.distance != MAX_FLT) {
                 const DevCollider& cc = cols[c.closest];
                 v3 bv = col_vel_at(cc, cell_pt);
@@ -191,6 +252,9 @@ constexpr uint32_t kG2pThreads = NXM_G2P_THREADS;  // threads per G2P CTA
 // block (shared memory), then advects, updates F and the model, and writes the
 // particle (read from slot `src`, xm / vf = its first two kin words) to slot
 // `dst` of the output records, together with the block key of its new position.
+// kCpicBlock: the CPIC branches (a block whose halo carries affinity bits);
+// the plain instantiation serves every other block without their registers.
+template <bool kCpicBlock>
 __device__ __forceinline__ void g2p_particle(const DevPtrs& P, const Params& prm, const float4* __restrict__ halo,
                                              uint32_t src, uint32_t dst, float4 xm, float4 vf, int3 key_off,
                                              const CpicCtx& cx, volatile float* stash) {
@@ -206,7 +270,7 @@ __device__ __forceinline__ void g2p_particle(const DevPtrs& P, const Params& prm
 
 #if NXM_CPIC
     // particle Cdf (normal, signed distance, affinity) from this step's g2p_cdf pass
-    const bool cpic = prm.use_cpic != 0;
+    const bool cpic = kCpicBlock;
     float4 crec0 = make_float4(0.f, 0.f, 0.f, 0.f), crec1 = crec0;
     float bfric = 1.0f;
     if (cpic) {
@@ -521,7 +585,26 @@ __device__ __forceinline__ void g2p_block_loop(const DevPtrs& P, const Params& p
         for (uint32_t t = tid + blockDim.x; t < 216u; t += blockDim.x) halo[t] = halo_node(P, b, t);
         CpicCtx cx{nullptr, nullptr, P.colliders, 0u};
 #if NXM_CPIC
+        // A halo whose nodes carry no affinity bit gave every particle of the
+        // block an empty affinity and a zero distance record (g2p_cdf): all
+        // nodes are compatible, no body velocity enters and the record stays
+        // zero, so the block runs the plain transfer (halo_cdf left null).
+        bool cpic_block = false;
         if (prm.use_cpic) {
+            uint32_t any = 0u;
+            for (uint32_t t = tid; t < 216u; t += blockDim.x) {
+                const uint32_t tx = t % 6u, ty = (t / 6u) % 6u, tz = t / 36u;
+                const uint32_t ox = tx >= 4u, oy = ty >= 4u, oz = tz >= 4u;
+                const uint32_t oct = ox * 4u + oy * 2u + oz;
+                const uint32_t blk = oct == 0 ? b : P.nbh[b * NUM_NBH + oct - 1u];
+                const uint32_t node = (tx - 4u * ox) + 4u * (ty - 4u * oy) + 16u * (tz - 4u * oz);
+                const uint4 nc = blk == NONE ? make_uint4(0u, 0u, NONE, 0u) : P.ncdf[blk * 64u + node];
+                halo_cdf[t] = make_uint2(nc.y, nc.z);
+                any |= nc.y;
+            }
+            cpic_block = __syncthreads_or((int)(any & 0x0000FFFFu)) != 0;
+        }
+        if (cpic_block) {
             for (uint32_t t = tid; t < 216u; t += blockDim.x) {
                 const uint32_t tx = t % 6u, ty = (t / 6u) % 6u, tz = t / 36u;
                 const uint32_t ox = tx >= 4u, oy = ty >= 4u, oz = tz >= 4u;
@@ -529,8 +612,6 @@ __device__ __forceinline__ void g2p_block_loop(const DevPtrs& P, const Params& p
                 const uint32_t blk = oct == 0 ? b : P.nbh[b * NUM_NBH + oct - 1u];
                 const uint32_t node = (tx - 4u * ox) + 4u * (ty - 4u * oy) + 16u * (tz - 4u * oz);
                 halo_inc[t] = blk == NONE ? make_float4(0.f, 0.f, 0.f, 0.f) : P.nodes_inc[blk * 64u + node];
-                const uint4 nc = blk == NONE ? make_uint4(0u, 0u, NONE, 0u) : P.ncdf[blk * 64u + node];
-                halo_cdf[t] = make_uint2(nc.y, nc.z);
             }
             cx.halo_inc = halo_inc;
             cx.halo_cdf = halo_cdf;
@@ -552,7 +633,11 @@ __device__ __forceinline__ void g2p_block_loop(const DevPtrs& P, const Params& p
                 xm = kr[0];
                 vf = kr[1];
             }
-            g2p_particle(P, prm, halo, pid, reorder ? first + k : pid, xm, vf, key_off, cx, stash);
+#if NXM_CPIC
+            if (cx.halo_cdf) g2p_particle<true>(P, prm, halo, pid, reorder ? first + k : pid, xm, vf, key_off, cx, stash);
+            else
+#endif
+                g2p_particle<false>(P, prm, halo, pid, reorder ? first + k : pid, xm, vf, key_off, cx, stash);
         }
         __syncthreads();
         b = bn;
@@ -798,7 +883,7 @@ __global__ void __launch_bounds__(kG2pThreads, NXM_G2P_MIN_CTAS) k_g2p_range(Dev
                 if (blk >= b && blk - b < cnt) {
                     const int3 key_off =
                         prm.scene_blocks ? scene_base_of_block(prm, P.bvid[blk]) : make_int3(0, 0, 0);
-                    g2p_particle(P, prm, halo + 216u * (blk - b), pid, reorder ? p : pid, xm, vf, key_off, cx,
+                    g2p_particle<false>(P, prm, halo + 216u * (blk - b), pid, reorder ? p : pid, xm, vf, key_off, cx,
                                  stash);
                     pending = false;
                 }

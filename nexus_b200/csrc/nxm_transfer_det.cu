@@ -210,9 +210,11 @@ __global__ void __launch_bounds__(256) k_grid_update_cdf(DevPtrs P) {
                             (float)(vid.z * 4 + (int)(k >> 4))) * dx;
         float dist = MAX_FLT;
         uint32_t aff = 0u, closest = NONE;
+        // the warp's 32 nodes share one block: its analytic colliders in reach
+        const uint32_t near = colliders_near_block(P, cols, ncol, dx, vid, true);
         for (uint32_t i = 0; i < ncol; ++i) {
             const DevCollider& c = cols[i];
-            if (c.type == SHAPE_TRIMESH) continue;
+            if (c.type == SHAPE_TRIMESH || !(near & (1u << i))) continue;
             const quat q = quat{c.rot[0], c.rot[1], c.rot[2], c.rot[3]};
             const v3 tra = mk(c.tra[0], c.tra[1], c.tra[2]);
             const v3 local = qrot(qconj(q), point - tra);
@@ -267,7 +269,11 @@ __global__ void __launch_bounds__(256) k_rigid_transform(DevPtrs P) {
 // ascending-id order gives, and only a strictly closer one replaces the
 // analytic colliders' result.
 __global__ void __launch_bounds__(64) k_p2g_cdf(DevPtrs P) {
-    __shared__ float4 sa[64], sb[64], sc[64];
+    // per staged entry: its triangle's vertices a, b, c, the face normal
+    // n = (b - a) x (c - a) with |n|, and the three edge normals (edge x n);
+    // a node's test then needs only differences and dot products, with the
+    // same operations (and roundings) as forming them per node
+    __shared__ float4 sa[64], sb[64], sc[64], sn[64], seab[64], sebc[64], seac[64];
     __shared__ int4 sassoc[64];  // associated cell, collider
     const float dx = P.params->dx;
     const uint32_t nb = __ldcg(&P.counters->num_blocks);
@@ -306,34 +312,45 @@ __global__ void __launch_bounds__(64) k_p2g_cdf(DevPtrs P) {
                 const v3 a = pose_apply(c, mk(t.v[0][0], t.v[0][1], t.v[0][2]));
                 const v3 bb = pose_apply(c, mk(t.v[1][0], t.v[1][1], t.v[1][2]));
                 const v3 cc = pose_apply(c, mk(t.v[2][0], t.v[2][1], t.v[2][2]));
+                const v3 ab = bb - a, acv = cc - a, bc = cc - bb;
+                const v3 n = cross(ab, acv);
+                const float nl = length(n);
+                const v3 eab = cross(ab, n), ebc = cross(bc, n), eac = cross(acv, n);
                 sa[tid] = make_float4(a.x, a.y, a.z, 0.f);
                 sb[tid] = make_float4(bb.x, bb.y, bb.z, 0.f);
                 sc[tid] = make_float4(cc.x, cc.y, cc.z, 0.f);
+                sn[tid] = make_float4(n.x, n.y, n.z, nl);
+                seab[tid] = make_float4(eab.x, eab.y, eab.z, 0.f);
+                sebc[tid] = make_float4(ebc.x, ebc.y, ebc.z, 0.f);
+                seac[tid] = make_float4(eac.x, eac.y, eac.z, 0.f);
                 const v3 ac = assoc_cell_of(dx, mk(w.x, w.y, w.z));
-                sassoc[tid] = make_int4(f2i_sat(ac.x), f2i_sat(ac.y), f2i_sat(ac.z), (int)(col - col0));
+                // a degenerate triangle (|n| = 0) projects on no node: out of every range
+                sassoc[tid] = nl != 0.f ? make_int4(f2i_sat(ac.x), f2i_sat(ac.y), f2i_sat(ac.z), (int)(col - col0))
+                                        : make_int4(INT32_MIN, INT32_MIN, INT32_MIN, 0);
             }
             __syncthreads();
             const uint32_t len = min(64u, num - chunk);
             for (uint32_t p = 0; p < len; ++p) {
                 const int4 as = sassoc[p];
-                const int sx = cx - as.x, sy = cy - as.y, sz = cz - as.z;
-                if (sx < 0 || sx > 2 || sy < 0 || sy > 2 || sz < 0 || sz > 2) continue;
-                const float4 fa = sa[p], fb = sb[p], fc = sc[p];
-                const v3 a = mk(fa.x, fa.y, fa.z), bb = mk(fb.x, fb.y, fb.z), cc = mk(fc.x, fc.y, fc.z);
-                const v3 ap = cell_pos - a, bp = cell_pos - bb, cp = cell_pos - cc;
-                const v3 ab = bb - a, acv = cc - a, bc = cc - bb;
-                const v3 n = cross(ab, acv);
-                const float nl = length(n);
-                if (nl != 0.f && dot(cross(ab, n), ap) <= 0.f && dot(cross(bc, n), bp) <= 0.f &&
-                    dot(cross(acv, n), cp) >= 0.f) {
-                    const float sd = dot(n, ap) / nl;
-                    const float d = fabsf(sd);
-                    const uint32_t col = (uint32_t)as.w;
-                    aff |= (sd < 0.f ? 0x00010001u : 0x00000001u) << col;
-                    if (d < rbest || (d == rbest && col < rcol)) {
-                        rbest = d;
-                        rcol = col;
-                    }
+                const unsigned sx = (unsigned)cx - (unsigned)as.x, sy = (unsigned)cy - (unsigned)as.y,
+                               sz = (unsigned)cz - (unsigned)as.z;
+                if (sx > 2u || sy > 2u || sz > 2u) continue;
+                const float4 fa = sa[p];
+                const v3 ap = cell_pos - mk(fa.x, fa.y, fa.z);
+                const float4 e0 = seab[p];
+                if (!(dot(mk(e0.x, e0.y, e0.z), ap) <= 0.f)) continue;
+                const float4 fb = sb[p], e1 = sebc[p];
+                if (!(dot(mk(e1.x, e1.y, e1.z), cell_pos - mk(fb.x, fb.y, fb.z)) <= 0.f)) continue;
+                const float4 fc = sc[p], e2 = seac[p];
+                if (!(dot(mk(e2.x, e2.y, e2.z), cell_pos - mk(fc.x, fc.y, fc.z)) >= 0.f)) continue;
+                const float4 fn = sn[p];
+                const float sd = dot(mk(fn.x, fn.y, fn.z), ap) / fn.w;
+                const float d = fabsf(sd);
+                const uint32_t col = (uint32_t)as.w;
+                aff |= (sd < 0.f ? 0x00010001u : 0x00000001u) << col;
+                if (d < rbest || (d == rbest && col < rcol)) {
+                    rbest = d;
+                    rcol = col;
                 }
             }
         }
@@ -359,6 +376,7 @@ __global__ void __launch_bounds__(128) k_g2p_cdf(DevPtrs P) {
     const float dx = prm.dx;
     const uint32_t nbp = min(__ldcg(&P.counters->num_primary), __ldcg(&P.counters->num_blocks));
     for (uint32_t b = blockIdx.x; b < nbp; b += gridDim.x) {
+        uint32_t any = 0u;
         for (uint32_t t = threadIdx.x; t < 216u; t += blockDim.x) {
             const uint32_t tx = t % 6u, ty = (t / 6u) % 6u, tz = t / 36u;
             const uint32_t ox = tx >= 4u, oy = ty >= 4u, oz = tz >= 4u;
@@ -366,13 +384,22 @@ __global__ void __launch_bounds__(128) k_g2p_cdf(DevPtrs P) {
             const uint32_t blk = oct == 0 ? b : P.nbh[b * NUM_NBH + oct - 1u];
             halo[t] = blk == NONE ? make_uint4(__float_as_uint(MAX_FLT), 0u, NONE, 0u)
                                   : P.ncdf[blk * 64u + (tx - 4u * ox) + 4u * (ty - 4u * oy) + 16u * (tz - 4u * oz)];
+            any |= halo[t].y;
         }
-        __syncthreads();
+        // a halo without affinity bits gives every particle of the block the zero record
+        const bool block_aff = __syncthreads_or((int)(any & 0x0000FFFFu)) != 0;
         const uint32_t first = P.first[b], np = P.nprim[b];
         for (uint32_t k = threadIdx.x; k < np; k += blockDim.x) {
             const uint32_t pid = P.sorted[first + k];
             float4* rec = &P.pcdf[3u * pid];
             const uint32_t prev = __float_as_uint(rec[1].w);
+            if (!block_aff) {
+                if (prev != 0u) {
+                    rec[0] = make_float4(0.f, 0.f, 0.f, 0.f);
+                    rec[1] = make_float4(0.f, 0.f, 0.f, __uint_as_float(0u));
+                }
+                continue;
+            }
             const float4 xm = reinterpret_cast<const float4*>(&P.kin[pid])[0];
             const v3 pt = mk(xm.x, xm.y, xm.z);
             const v3 ref = assoc_cell_of(dx, pt) * dx - pt;
@@ -380,31 +407,41 @@ __global__ void __launch_bounds__(128) k_g2p_cdf(DevPtrs P) {
                      w2 = kernel_eval_all(-ref.z / dx);
             const CellInfo ci = cell_info(dx, pt);
             const uint32_t packed = ci.ax + 6u * ci.ay + 36u * ci.az;
+            // the union of the 27 nodes' affinity bits; without any, no node
+            // enters the fit, which is then singular: the record is zeroed
+            // (and a record whose previous affinity word is 0 is zero already)
             uint32_t pa = 0u;
-            float sums[16];
-#pragma unroll
-            for (int ic = 0; ic < 16; ++ic) sums[ic] = 0.f;
             for (int i = 0; i < 27; ++i) {
                 int sx, sy, sz;
                 nbh_shift(i, sx, sy, sz);
-                const uint4 nd = halo[packed + (uint32_t)(sx + 6 * sy + 36 * sz)];
-                pa |= nd.y & 0x0000FFFFu;
-                const float weight = vget(w0, sx) * vget(w1, sy) * vget(w2, sz);
-                const float ndist = __uint_as_float(nd.x);
-#pragma unroll
-                for (int ic = 0; ic < 16; ++ic) {
-                    const float compatible = (nd.y & (1u << ic)) ? 1.0f : 0.0f;
-                    const float sign = ((nd.y >> 16) & (1u << ic)) ? -1.0f : 1.0f;
-                    sums[ic] += compatible * weight * sign * ndist;
-                }
+                pa |= halo[packed + (uint32_t)(sx + 6 * sy + 36 * sz)].y;
             }
-#pragma unroll
-            for (int ic = 0; ic < 16; ++ic) {
-                if (!(prev & (1u << ic))) {
-                    if (sums[ic] < 0.f) pa |= 0x00010000u << ic;
-                } else {
-                    pa |= prev & (0x00010000u << ic);
+            pa &= 0x0000FFFFu;
+            if (pa == 0u) {
+                if (prev != 0u) {
+                    rec[0] = make_float4(0.f, 0.f, 0.f, 0.f);
+                    rec[1] = make_float4(0.f, 0.f, 0.f, __uint_as_float(0u));
                 }
+                continue;
+            }
+            // signs: kept for every collider of the previous affinity (with or
+            // without a node carrying it now); for a new affinity, the sign of
+            // the weighted distances of the nodes carrying that collider's
+            // bit, summed in stencil order (a node without the bit adds zero)
+            pa |= prev & ((prev & 0x0000FFFFu) << 16);
+            for (uint32_t rem = pa & ~prev & 0x0000FFFFu; rem != 0u; rem &= rem - 1u) {
+                const uint32_t bit = rem & (0u - rem);
+                float sum = 0.f;
+                for (int i = 0; i < 27; ++i) {
+                    int sx, sy, sz;
+                    nbh_shift(i, sx, sy, sz);
+                    const uint4 nd = halo[packed + (uint32_t)(sx + 6 * sy + 36 * sz)];
+                    if (!(nd.y & bit)) continue;
+                    const float weight = vget(w0, sx) * vget(w1, sy) * vget(w2, sz);
+                    const float sign = ((nd.y >> 16) & bit) ? -1.0f : 1.0f;
+                    sum += weight * sign * __uint_as_float(nd.x);
+                }
+                if (sum < 0.f) pa |= bit << 16;
             }
             float q[4][4], u[4] = {0.f, 0.f, 0.f, 0.f};
 #pragma unroll

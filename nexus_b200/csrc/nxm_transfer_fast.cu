@@ -49,7 +49,7 @@ constexpr int kP2gRec = 28;  // floats per staged particle
 constexpr size_t kP2gSmem = (size_t)kP2gWarps * 216 * 16 + (size_t)kP2gChunk * kP2gRec * 4 + (64 + 68) * 4 +
                             (size_t)kP2gChunk * (2 + 2 + 1);
 // CPIC adds the warps' incompatible-field tiles and the 216 tile nodes' affinity bits
-constexpr size_t kP2gSmemCpic = kP2gSmem + (size_t)kP2gWarps * 216 * 16 + 216 * 4 + 16;
+constexpr size_t kP2gSmemCpic = kP2gSmem + (size_t)kP2gWarps * 216 * 16 + 218 * 4 + 16;
 static_assert(kP2gChunk <= 65536, "staged particle indices are 16-bit");
 
 __device__ __forceinline__ float4 f4add(float4 a, float4 b) { return make_float4(a.x + b.x, a.y + b.y, a.z + b.z, a.w + b.w); }
@@ -116,6 +116,13 @@ __global__ void __launch_bounds__(kP2gThreads, kCpic ? 2 : NXM_P2G_MIN_CTAS) k_p
     uint16_t* prank = perm + kP2gChunk;
     uint8_t* pcell = reinterpret_cast<uint8_t*>(prank + kP2gChunk);
     uint32_t* node_aff = reinterpret_cast<uint32_t*>(pcell + ((kP2gChunk + 15) & ~15));  // CPIC: 216 tile nodes
+    // CPIC: nonzero when a tile node of the current block carries an affinity
+    // bit; otherwise every particle is compatible with every node and the
+    // block runs the plain accumulation (no incompatible sums, no flush).
+    // Two flags by block parity: the one of the next block is cleared while
+    // the current one is in use (between two end-of-block barriers).
+    volatile uint32_t* blk_aff_pair = node_aff + 216;
+    uint32_t parity = 0u;
 
     const float dx = P.params->dx;
     const float inv_dx = P.params->inv_dx;
@@ -150,6 +157,7 @@ __global__ void __launch_bounds__(kP2gThreads, kCpic ? 2 : NXM_P2G_MIN_CTAS) k_p
     for (uint32_t t = tid; t < (kCpic ? 2u : 1u) * kP2gWarps * 216u; t += kP2gThreads)
         tiles[t] = make_float4(0.f, 0.f, 0.f, 0.f);
     if (tid < 64) cnt[tid] = 0;
+    if (kCpic && tid == 0) blk_aff_pair[0] = 0u;
     P2gHdr h = p2g_load_hdr(P, b, nbp);
     P2gHdr hn = p2g_load_hdr(P, b + stride, nbp);
     P2gHdr hnn = p2g_load_hdr(P, b + 2u * stride, nbp);
@@ -162,8 +170,13 @@ __global__ void __launch_bounds__(kP2gThreads, kCpic ? 2 : NXM_P2G_MIN_CTAS) k_p
             vid.x -= o.x; vid.y -= o.y; vid.z -= o.z;
         }
         const uint32_t fblk = (tid < 216u && foct != 0u) ? __ldg(&P.nbh[b * NUM_NBH + foct - 1u]) : b;
-        if (kCpic && tid < 216u)  // read after the staging barrier below
-            node_aff[tid] = fblk == NONE ? 0u : __ldg(&P.ncdf[fblk * 64u + fnode].y);
+        volatile uint32_t* blk_aff = blk_aff_pair + parity;
+        if (kCpic && tid == 0) blk_aff_pair[parity ^ 1u] = 0u;
+        if (kCpic && tid < 216u) {  // read after the staging barrier below
+            const uint32_t na = fblk == NONE ? 0u : __ldg(&P.ncdf[fblk * 64u + fnode].y);
+            node_aff[tid] = na;
+            if (na & 0x0000FFFFu) *blk_aff = 1u;
+        }
         for (uint32_t base = 0; base < h.np; base += kP2gChunk) {
             const uint32_t m_chunk = min(h.np - base, (uint32_t)kP2gChunk);
             // 1. stage and bin this thread's particle (base + tid)
@@ -226,6 +239,7 @@ __global__ void __launch_bounds__(kP2gThreads, kCpic ? 2 : NXM_P2G_MIN_CTAS) k_p
             __syncthreads();
             if (tid < 64) cnt[tid] = 0;  // counts are consumed; ready for the next chunk
             raw = p2g_load_raw<kCpic>(P, pid_next);
+            const bool split = kCpic && *blk_aff != 0u;
             // 3. one warp per cell, three particles per pass
             for (uint32_t c = warp; c < 64u; c += kP2gWarps) {
                 const int s0 = start[c], s1 = start[c + 1];
@@ -235,7 +249,7 @@ __global__ void __launch_bounds__(kP2gThreads, kCpic ? 2 : NXM_P2G_MIN_CTAS) k_p
                 const uint32_t cx = c & 3u, cy = (c >> 2) & 3u, cz = c >> 4;
                 const uint32_t col = (cx + sxy % 3u) + 6u * (cy + sxy / 3u) + 36u * cz;  // this lane's s.z = 0 node
                 uint32_t na0 = 0u, na1 = 0u, na2 = 0u;
-                if (kCpic && worker) {
+                if (split && worker) {
                     na0 = node_aff[col];
                     na1 = node_aff[col + 36u];
                     na2 = node_aff[col + 72u];
@@ -252,7 +266,7 @@ __global__ void __launch_bounds__(kP2gThreads, kCpic ? 2 : NXM_P2G_MIN_CTAS) k_p
                     float bx = qm.x + k0.x * fx + k1.x * fy;
                     float by = qm.y + k0.y * fx + k1.y * fy;
                     float bz = qm.z + k0.z * fx + k1.z * fy;
-                    if (!kCpic) {
+                    if (!split) {
                         float w = wxy * k0.w;
                         a0.x += w * bx; a0.y += w * by; a0.z += w * bz; a0.w += w * qm.w;
                         bx += k2.x; by += k2.y; bz += k2.z;
@@ -293,7 +307,7 @@ __global__ void __launch_bounds__(kP2gThreads, kCpic ? 2 : NXM_P2G_MIN_CTAS) k_p
                 const float4 t = exchange(a0, a1, a2);
                 const uint32_t node = col + 36u * grp;
                 if (worker) tile[node] = f4add(tile[node], t);
-                if (kCpic) {
+                if (split) {
                     const float4 ti = exchange(i0, i1, i2);
                     if (worker) tile_inc[node] = f4add(tile_inc[node], ti);
                 }
@@ -301,8 +315,9 @@ __global__ void __launch_bounds__(kP2gThreads, kCpic ? 2 : NXM_P2G_MIN_CTAS) k_p
             __syncthreads();
         }
         // 4. sum the warp tiles (clearing them) and flush the block's nodes
+        const int nfields = kCpic && *blk_aff != 0u ? 2 : 1;
         if (tid < 216u) {
-            for (int f = 0; f < (kCpic ? 2 : 1); ++f) {
+            for (int f = 0; f < nfields; ++f) {
                 float4* tt = f ? tiles_inc : tiles;
                 float4 sum = tt[tid];
                 tt[tid] = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -318,6 +333,7 @@ __global__ void __launch_bounds__(kP2gThreads, kCpic ? 2 : NXM_P2G_MIN_CTAS) k_p
             }
         }
         __syncthreads();
+        parity ^= 1u;
         b += stride;
         if (b >= nbp) break;
         h = hn;

@@ -530,6 +530,39 @@ def test_batched_coupled_scenes_step_as_alone(pipe):
     assert np.abs(pose[4:] - mix[0].colliders[int(mix[0].kinematics[0, 0])]["translation"]).max() > 0
 
 
+def _bodies_in_the_box():
+    """A coupled scene (trimesh floor, box walls, sand) whose eight bodies
+    (cuboids, balls, capsules) are rotated, placed on and inside the sand
+    box and move into it, spinning, so that many grid nodes lie within reach
+    of several shapes."""
+    sc = scenes.coupled_scene(0, dx=1.0 / 64.0, n_min=1500, n_max=3000, floor_vertices=21)
+    lo, hi = sc.particles.pos.min(0), sc.particles.pos.max(0)
+    rng = np.random.default_rng(7)
+    for j, row in enumerate(sc.kinematics):
+        i = int(row[0])
+        q = rng.normal(size=4)
+        sc.colliders[i]["rotation"] = (q / np.linalg.norm(q)).astype(np.float32)
+        t = lo + (hi - lo) * rng.uniform(-0.1, 1.1, 3)
+        sc.colliders[i]["translation"] = t.astype(np.float32)
+        sc.colliders[i]["linvel"] = (0.5 * (0.5 * (lo + hi) - t) / np.linalg.norm(0.5 * (lo + hi) - t)).astype(np.float32)
+        sc.colliders[i]["angvel"] = rng.uniform(-3.0, 3.0, 3).astype(np.float32)
+    sc.kinematics = sc.kinematics[:0]  # constant velocities, no driving
+    return sc
+
+
+@pytest.mark.parametrize("deterministic", [False, True])
+def test_rotated_bodies_in_the_sand_match_oracle(pipe, deterministic):
+    """Grid-node collisions with rotated analytic shapes and a trimesh, every
+    node near some shape: the per-block reach test that leaves out far
+    colliders must leave the projections exactly as the oracle's full scan
+    (deterministic bounds as for the trimesh floor: BVH ties)."""
+    sc = _bodies_in_the_box()
+    start = start_state(sc)
+    g, o, o64 = _run_both(sc, deterministic, 60)
+    bounds = dict(DET_BOUNDS, pos=1e-4, vel=1e-3, aff=1e-2, def_grad=1e-3) if deterministic else FAST_BOUNDS
+    assert_run_matches(f"rotated bodies, deterministic={deterministic}", g, o, o64, start, bounds)
+
+
 def test_hash_full_is_reported(pipe):
     """More distinct primary block keys than the hash has slots (a grid of 8
     blocks has a 1024-slot hash; 1331 particles 4 cells apart each sit in a
