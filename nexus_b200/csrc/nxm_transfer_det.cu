@@ -443,6 +443,34 @@ __global__ void __launch_bounds__(128) k_g2p_cdf(DevPtrs P) {
                 }
                 if (sum < 0.f) pa |= bit << 16;
             }
+            // The fit's moment matrix is a weighted sum of p p^T (positive
+            // semi-definite), so its determinant is at most the product of its
+            // diagonal (Hadamard's inequality); the float evaluation of the
+            // determinant stays within a relative 1e-3 above that product, so
+            // a product at or below 1e-8 / 1.01 leaves the fit singular and
+            // the record zero.  The diagonal is summed as in the full pass.
+            {
+                float dg[4] = {0.f, 0.f, 0.f, 0.f};
+                for (int i = 0; i < 27; ++i) {
+                    int sx, sy, sz;
+                    nbh_shift(i, sx, sy, sz);
+                    const uint4 nd = halo[packed + (uint32_t)(sx + 6 * sy + 36 * sz)];
+                    if (!(nd.y & pa & 0x0000FFFFu)) continue;
+                    const v3 dpt = ref + mk((float)sx, (float)sy, (float)sz) * dx;
+                    const float weight = vget(w0, sx) * vget(w1, sy) * vget(w2, sz);
+                    dg[0] += dpt.x * dpt.x * weight;
+                    dg[1] += dpt.y * dpt.y * weight;
+                    dg[2] += dpt.z * dpt.z * weight;
+                    dg[3] += 1.0f * 1.0f * weight;
+                }
+                if (dg[0] * dg[1] * dg[2] * dg[3] * 1.01f <= 1.0e-8f) {
+                    if (prev != 0u) {
+                        rec[0] = make_float4(0.f, 0.f, 0.f, 0.f);
+                        rec[1] = make_float4(0.f, 0.f, 0.f, __uint_as_float(0u));
+                    }
+                    continue;
+                }
+            }
             float q[4][4], u[4] = {0.f, 0.f, 0.f, 0.f};
 #pragma unroll
             for (int r = 0; r < 4; ++r)
