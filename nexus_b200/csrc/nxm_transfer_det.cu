@@ -424,31 +424,13 @@ __global__ void __launch_bounds__(128) k_g2p_cdf(DevPtrs P) {
                 }
                 continue;
             }
-            // signs: kept for every collider of the previous affinity (with or
-            // without a node carrying it now); for a new affinity, the sign of
-            // the weighted distances of the nodes carrying that collider's
-            // bit, summed in stencil order (a node without the bit adds zero)
-            pa |= prev & ((prev & 0x0000FFFFu) << 16);
-            for (uint32_t rem = pa & ~prev & 0x0000FFFFu; rem != 0u; rem &= rem - 1u) {
-                const uint32_t bit = rem & (0u - rem);
-                float sum = 0.f;
-                for (int i = 0; i < 27; ++i) {
-                    int sx, sy, sz;
-                    nbh_shift(i, sx, sy, sz);
-                    const uint4 nd = halo[packed + (uint32_t)(sx + 6 * sy + 36 * sz)];
-                    if (!(nd.y & bit)) continue;
-                    const float weight = vget(w0, sx) * vget(w1, sy) * vget(w2, sz);
-                    const float sign = ((nd.y >> 16) & bit) ? -1.0f : 1.0f;
-                    sum += weight * sign * __uint_as_float(nd.x);
-                }
-                if (sum < 0.f) pa |= bit << 16;
-            }
             // The fit's moment matrix is a weighted sum of p p^T (positive
             // semi-definite), so its determinant is at most the product of its
             // diagonal (Hadamard's inequality); the float evaluation of the
             // determinant stays within a relative 1e-3 above that product, so
             // a product at or below 1e-8 / 1.01 leaves the fit singular and
-            // the record zero.  The diagonal is summed as in the full pass.
+            // the record zero (whatever the signs below).  The diagonal is
+            // summed as in the full pass, over the same nodes (affinity bits).
             {
                 float dg[4] = {0.f, 0.f, 0.f, 0.f};
                 for (int i = 0; i < 27; ++i) {
@@ -470,6 +452,25 @@ __global__ void __launch_bounds__(128) k_g2p_cdf(DevPtrs P) {
                     }
                     continue;
                 }
+            }
+            // signs: kept for every collider of the previous affinity (with or
+            // without a node carrying it now); for a new affinity, the sign of
+            // the weighted distances of the nodes carrying that collider's
+            // bit, summed in stencil order (a node without the bit adds zero)
+            pa |= prev & ((prev & 0x0000FFFFu) << 16);
+            for (uint32_t rem = pa & ~prev & 0x0000FFFFu; rem != 0u; rem &= rem - 1u) {
+                const uint32_t bit = rem & (0u - rem);
+                float sum = 0.f;
+                for (int i = 0; i < 27; ++i) {
+                    int sx, sy, sz;
+                    nbh_shift(i, sx, sy, sz);
+                    const uint4 nd = halo[packed + (uint32_t)(sx + 6 * sy + 36 * sz)];
+                    if (!(nd.y & bit)) continue;
+                    const float weight = vget(w0, sx) * vget(w1, sy) * vget(w2, sz);
+                    const float sign = ((nd.y >> 16) & bit) ? -1.0f : 1.0f;
+                    sum += weight * sign * __uint_as_float(nd.x);
+                }
+                if (sum < 0.f) pa |= bit << 16;
             }
             float q[4][4], u[4] = {0.f, 0.f, 0.f, 0.f};
 #pragma unroll
