@@ -114,7 +114,6 @@ constexpr int kRigidSortLaunches = 5;
 void launch_p2g(const DevPtrs& P, const LaunchCfg& c, cudaStream_t s);
 void launch_grid_update(const DevPtrs& P, const LaunchCfg& c, cudaStream_t s);
 int launch_g2p_update(const DevPtrs& P, const LaunchCfg& c, cudaStream_t s);  // returns the kernels issued
-void launch_colliders_end(const DevPtrs& P, cudaStream_t s);
 // CPIC scatter P2G (compatible and incompatible fields; particles in id order).
 void launch_p2g_cpic(const DevPtrs& P, const LaunchCfg& c, cudaStream_t s);
 // A bulk-copy barrier wait that runs out after `limit` rounds (test of the

@@ -1056,7 +1056,6 @@ int enqueue_step(nxm_state* s, cudaStream_t st, cudaEvent_t* ev /* 5 events or n
     k += exact_path   ? exact::launch_g2p_update(P, c, st)
          : fast_cpic ? fast_cpic::launch_g2p_update(P, c, st)
                      : fast::launch_g2p_update(P, c, st);
-    if (has_col) { fast::launch_colliders_end(P, st); ++k; }
     if (ev) cudaEventRecord(ev[4], st);
     return k;
 }

@@ -482,6 +482,45 @@ __device__ __forceinline__ void g2p_particle(const DevPtrs& P, const Params& prm
     if (P.pid_in) P.pid_out[dst] = P.pid_in[src];
 }
 
+// dynamics/body.rs Velocity::integrate for one-way coupled bodies
+// (rigid_impulses.rs:66-140 with zero impulse and zero inverse mass): the
+// pose of every collider the step moves (all, at most 16, or every scene's
+// in batched mode) advances by its velocities over dt.  Run by the first
+// threads of the G2P launch, one collider each: nothing in G2P reads a
+// collider's rotation or translation (the body velocities it reads use the
+// centre of mass refreshed at the start of the step), and the next reader is
+// the next step's sort.
+__device__ __forceinline__ void integrate_colliders(const DevPtrs& P, const Params& prm) {
+    const uint32_t ncol = prm.scene_blocks ? prm.ncol : min(prm.ncol, (uint32_t)MAX_COLLIDERS);
+    const float dt = prm.dt;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < ncol; i += gridDim.x * blockDim.x) {
+        DevCollider& c = P.colliders[i];
+        const quat q = quat{c.rot[0], c.rot[1], c.rot[2], c.rot[3]};
+        const v3 tra = mk(c.tra[0], c.tra[1], c.tra[2]);
+        const v3 init_com = qrot(q, mk(c.local_com[0], c.local_com[1], c.local_com[2])) + tra;
+        const v3 sa = mk(c.angvel[0], c.angvel[1], c.angvel[2]) * dt;
+        const float ang = length(sa);
+        quat dq;
+        if (ang == 0.f) {
+            dq = quat{0.f, 0.f, 0.f, 1.f};
+        } else {
+            const v3 ax = sa / ang;
+            const float sh = sinf(ang * 0.5f), ch = cosf(ang * 0.5f);
+            dq = quat{ax.x * sh, ax.y * sh, ax.z * sh, ch};
+        }
+        const v3 dl = mk(c.linvel[0], c.linvel[1], c.linvel[2]) * dt;
+        const v3 nt = (init_com + qrot(dq, tra - init_com)) + dl;
+        quat nr;
+        nr.w = dq.w * q.w - dq.x * q.x - dq.y * q.y - dq.z * q.z;
+        nr.x = dq.w * q.x + dq.x * q.w + dq.y * q.z - dq.z * q.y;
+        nr.y = dq.w * q.y - dq.x * q.z + dq.y * q.w + dq.z * q.x;
+        nr.z = dq.w * q.z + dq.x * q.y - dq.y * q.x + dq.z * q.w;
+        const float rl = 1.0f / sqrtf(nr.x * nr.x + nr.y * nr.y + nr.z * nr.z + nr.w * nr.w);
+        c.rot[0] = nr.x * rl; c.rot[1] = nr.y * rl; c.rot[2] = nr.z * rl; c.rot[3] = nr.w * rl;
+        c.tra[0] = nt.x; c.tra[1] = nt.y; c.tra[2] = nt.z;
+    }
+}
+
 // End of a G2P launch: when reordering, the particles the sort could not
 // place (their block was not created: capacity or hash overflow, reported in
 // the status word) are copied unchanged to the slots after the sorted ones;
@@ -662,6 +701,7 @@ __global__ void __launch_bounds__(kG2pThreads, NXM_G2P_MIN_CTAS) k_g2p_update(De
     uint2* halo_cdf = nullptr;
 #endif
     const Params prm = *P.params;
+    integrate_colliders(P, prm);
     g2p_block_loop(P, prm, halo, halo_inc, halo_cdf, stash);
     g2p_finish(P, prm);
 }
@@ -816,6 +856,7 @@ __global__ void __launch_bounds__(kG2pThreads, NXM_G2P_MIN_CTAS) k_g2p_range(Dev
     volatile float* stash = nullptr;
 #endif
     const Params prm = *P.params;
+    integrate_colliders(P, prm);
     const uint32_t nbp = min(__ldcg(&P.counters->num_primary), __ldcg(&P.counters->num_blocks));
     const uint32_t len = min(__ldcg(&P.counters->sorted_len), prm.n);
     const bool sparse = g2p_sparse(P, prm);

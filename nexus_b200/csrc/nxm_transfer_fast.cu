@@ -342,44 +342,6 @@ __global__ void __launch_bounds__(kP2gThreads, kCpic ? 2 : NXM_P2G_MIN_CTAS) k_p
     }
 }
 
-// Colliders a step moves: all (at most 16), or every scene's in batched mode.
-__device__ __forceinline__ uint32_t collider_count(const Params& p) {
-    return p.scene_blocks ? p.ncol : min(p.ncol, (uint32_t)MAX_COLLIDERS);
-}
-
-// dynamics/body.rs Velocity::integrate for one-way coupled bodies
-// (rigid_impulses.rs:66-140 with zero impulse and zero inverse mass).
-__global__ void k_colliders_end(DevPtrs P) {
-    const uint32_t ncol = collider_count(*P.params);
-    const float dt = P.params->dt;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < ncol; i += gridDim.x * blockDim.x) {
-    DevCollider& c = P.colliders[i];
-    quat q = quat{c.rot[0], c.rot[1], c.rot[2], c.rot[3]};
-    v3 tra = mk(c.tra[0], c.tra[1], c.tra[2]);
-    v3 init_com = qrot(q, mk(c.local_com[0], c.local_com[1], c.local_com[2])) + tra;
-    v3 sa = mk(c.angvel[0], c.angvel[1], c.angvel[2]) * dt;
-    float ang = length(sa);
-    quat dq;
-    if (ang == 0.f) {
-        dq = quat{0.f, 0.f, 0.f, 1.f};
-    } else {
-        v3 ax = sa / ang;
-        float sh = sinf(ang * 0.5f), ch = cosf(ang * 0.5f);
-        dq = quat{ax.x * sh, ax.y * sh, ax.z * sh, ch};
-    }
-    v3 dl = mk(c.linvel[0], c.linvel[1], c.linvel[2]) * dt;
-    v3 nt = (init_com + qrot(dq, tra - init_com)) + dl;
-    quat nr;
-    nr.w = dq.w * q.w - dq.x * q.x - dq.y * q.y - dq.z * q.z;
-    nr.x = dq.w * q.x + dq.x * q.w + dq.y * q.z - dq.z * q.y;
-    nr.y = dq.w * q.y - dq.x * q.z + dq.y * q.w + dq.z * q.x;
-    nr.z = dq.w * q.z + dq.x * q.y - dq.y * q.x + dq.z * q.w;
-    float rl = 1.0f / sqrtf(nr.x * nr.x + nr.y * nr.y + nr.z * nr.z + nr.w * nr.w);
-    c.rot[0] = nr.x * rl; c.rot[1] = nr.y * rl; c.rot[2] = nr.z * rl; c.rot[3] = nr.w * rl;
-    c.tra[0] = nt.x; c.tra[1] = nt.y; c.tra[2] = nt.z;
-    }
-}
-
 }  // namespace
 
 void launch_p2g(const DevPtrs& P, const LaunchCfg& c, cudaStream_t s) {
@@ -392,7 +354,6 @@ void launch_p2g_cpic(const DevPtrs& P, const LaunchCfg& c, cudaStream_t s) {
     k_p2g<true><<<c.sm_count * 2, kP2gThreads, kP2gSmemCpic, s>>>(P);
 }
 
-void launch_colliders_end(const DevPtrs& P, cudaStream_t s) { k_colliders_end<<<8, 128, 0, s>>>(P); }
 
 }  // namespace fast
 }  // namespace nxm
