@@ -87,7 +87,7 @@ def test_p2g_fast_matches_within_rounding(pipe, name):
     assert rel_l2(g[..., :3], want[..., :3]) < 1e-5
 
 
-def _run_both(sc, deterministic, steps):
+def _run_states(sc, deterministic, steps):
     from oracle.oracle import OracleScene
     pipe = MpmPipeline()
     st = state_from_scene(sc, deterministic=deterministic)
@@ -97,6 +97,11 @@ def _run_both(sc, deterministic, steps):
     o32, o64 = OracleScene(sc, "f32"), OracleScene(sc, "f64")
     o32.step(steps)
     o64.step(steps)
+    return st, o32, o64
+
+
+def _run_both(sc, deterministic, steps):
+    st, o32, o64 = _run_states(sc, deterministic, steps)
     o64p = o64.particles()
     o64p["pos"] = o64.positions_f64()
     return st.read_particles(), o32.particles(), o64p
@@ -558,9 +563,19 @@ def test_rotated_bodies_in_the_sand_match_oracle(pipe, deterministic):
     (deterministic bounds as for the trimesh floor: BVH ties)."""
     sc = _bodies_in_the_box()
     start = start_state(sc)
-    g, o, o64 = _run_both(sc, deterministic, 60)
+    st, o32, o64 = _run_states(sc, deterministic, 60)
+    o64p = o64.particles()
+    o64p["pos"] = o64.positions_f64()
     bounds = dict(DET_BOUNDS, pos=1e-4, vel=1e-3, aff=1e-2, def_grad=1e-3) if deterministic else FAST_BOUNDS
-    assert_run_matches(f"rotated bodies, deterministic={deterministic}", g, o, o64, start, bounds)
+    assert_run_matches(f"rotated bodies, deterministic={deterministic}", st.read_particles(), o32.particles(), o64p,
+                       start, bounds)
+    # the bodies' poses, integrated once a step by the G2P launch, follow the
+    # oracle's integration: quaternion and translation within float rounding
+    for i in range(6, 14):
+        got, want = st.collider_pose(i), o32.collider_pose(i)
+        want0 = np.concatenate([sc.colliders[i]["rotation"], sc.colliders[i]["translation"]])
+        assert np.abs(want[4:] - want0[4:]).max() > 5e-4, "the body moved"
+        np.testing.assert_allclose(got, want, atol=1e-5, err_msg=f"collider {i}")
 
 
 def test_hash_full_is_reported(pipe):
