@@ -212,7 +212,8 @@ def barrier(world: int):
 
 
 def cpu_oracle_rate(scene, steps: int, warmup: int):
-    """Particle-steps/s of the FP32 oracle (OpenMP, all host cores)."""
+    """Particle-steps/s of the FP32 oracle (OpenMP, all host cores), and the
+    oracle after its warmup + steps steps."""
     from oracle.oracle import OracleScene
     o = OracleScene(scene, "f32")
     if warmup:
@@ -220,7 +221,37 @@ def cpu_oracle_rate(scene, steps: int, warmup: int):
     t0 = time.perf_counter()
     o.step(steps)
     dt = time.perf_counter() - t0
-    return scene.n * steps / dt, dt
+    return scene.n * steps / dt, dt, o
+
+
+def measure_accuracy(scene, o32, steps: int) -> dict:
+    """The GPU path's x, v, C and F after `steps` steps of the scene from its
+    start, in fast and in deterministic mode, against the FP32 oracle of the
+    cpu_baseline leg (which ran the same steps) and an FP64 rerun: per field,
+    the relative L2 of the error over the oracle's own change from the start
+    (change_rel_l2 of tests/parity.py; a result that never moved scores 1)."""
+    from oracle.oracle import OracleScene
+    from nexus_b200.mpm import MpmPipeline, state_from_scene
+    from tests.parity import start_state, state_errors
+    start = start_state(scene)
+    o64 = OracleScene(scene, "f64")
+    o64.step(steps)
+    w64 = o64.particles()
+    w64["pos"] = o64.positions_f64()
+    w32 = o32.particles()
+    out = {"steps": steps, "metric": "||got - want|| / ||want - start|| per field (x, v, C, F)",
+           "oracle_f32_vs_f64": state_errors(w32, w64, start)}
+    pipe = MpmPipeline()
+    for det in (False, True):
+        st = state_from_scene(scene, deterministic=det)
+        for _ in range(steps):
+            pipe.step(st)
+        st.synchronize()
+        got = st.read_particles()
+        out["deterministic" if det else "fast"] = {"vs_f32": state_errors(got, w32, start),
+                                                   "vs_f64": state_errors(got, w64, start)}
+        del st
+    return out
 
 
 def workload_config(scene, world: int) -> dict:
@@ -398,13 +429,16 @@ def run_ours(args, world, rank, local):
 
     if rank != 0:
         return
-    cpu = None
+    cpu = accuracy = None
     if world == 1 and args.cpu_baseline:
         os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count()))
-        rate, secs = cpu_oracle_rate(scene, args.ref_steps, 1)
+        rate, secs, o32 = cpu_oracle_rate(scene, args.ref_steps, 1)
         cpu = {"value": rate, "unit": UNIT, "cores": int(os.environ["OMP_NUM_THREADS"]), "kind": "port",
                "sample": f"{args.ref_steps} full steps of the same {n}-particle scene after 1 warm-up step "
                          f"({secs:.1f} s; C restatement of the reference step, FP32, OpenMP)"}
+        # the oracle as the checker: the same steps on the GPU against it
+        accuracy = measure_accuracy(scene, o32, args.ref_steps + 1)
+        del o32
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -422,6 +456,7 @@ def run_ours(args, world, rank, local):
         "e2e_pageable": e2e_pageable,
         "gpu_launches": launches,
         "cpu_baseline": cpu,
+        "accuracy": accuracy,
         "elastic_cube": cube,
         "batched": batched,
         "serving": serving,
