@@ -6,8 +6,9 @@ budget beside the scenes already running.  Every admitted scene then
 advances in the same batched state as all the others of its cell width, dt
 and gravity: one launch sequence per step for all of them (nxm_step on a
 state with batched scenes).  When a scene has taken its step budget, its
-particles are read back and the scene is removed, freeing memory for the next
-arrivals.  Scenes that arrive while others run start on the next step.
+particles are read back; finished scenes leave the state in batches (a
+removal compacts the whole particle storage), sooner when an arrival needs
+their room.  Scenes that arrive while others run start on the next step.
 
 The host never drains the GPU: a finished scene's positions are read
 asynchronously into pinned memory and its slot is freed at once (both queue
@@ -26,7 +27,8 @@ result read (nxm_state_read_status_async), so that a result is only handed
 out when no step before it reported a bit.  When a state reports one, every
 scene that may have taken part in the failing step (those active on the state
 and those whose final read is still in flight) is evicted and reported in
-``MpmServer.failed`` with the status bits; the bits are cleared, the state's
+``MpmServer.failed`` with the status bits (finished scenes still in the state
+leave with them; their results were handed out before); the bits are cleared, the state's
 grid admission estimate is doubled so that the same mix is not admitted
 again, and serving continues with the other requests.
 """
@@ -95,6 +97,7 @@ class _Group:
         self.state.set_deterministic(deterministic)
         self.state.enable_scenes(scene_blocks)
         self.active = {}  # slot -> [request, remaining steps, admitted time]
+        self.retired = []  # (slot, request): finished, read queued, awaiting removal with others
         self.particles = 0
         self.grid = 0
         self.grid_factor = 1.0  # admission estimate of a scene's grid blocks, doubled after an overflow
@@ -105,13 +108,21 @@ class MpmServer:
     """Request loop over batched states (one per cell width / dt / gravity)."""
 
     def __init__(self, hbm_budget: float = 150e9, particles_capacity: int = 1 << 24,
-                 grid_capacity: int = 1 << 20, deterministic: bool = False, scene_blocks=None):
+                 grid_capacity: int = 1 << 20, deterministic: bool = False, scene_blocks=None,
+                 retire_fraction: float = 0.02):
         self.pipe = MpmPipeline()
         self.budget = hbm_budget
         self.particles_capacity = particles_capacity
         self.grid_capacity = grid_capacity
         self.deterministic = deterministic
         self.scene_blocks = scene_blocks  # None: 64 blocks per scene axis at dx >= 1/128, else 128
+        # Finished scenes leave their state in batches: a removal compacts the
+        # state's whole particle storage, whatever it removes, while a finished
+        # scene left in place only steps along (its result was read at its last
+        # step).  They leave once they hold this fraction of the state's
+        # particles, when their room lets the next arrival in, or when the
+        # state has nothing else to run.
+        self.retire_fraction = float(retire_fraction)
         self.groups = {}
         self.failed = {}  # request id -> Failure
         self.in_use = 0
@@ -151,23 +162,39 @@ class MpmServer:
         for sc in scenes_:
             self._group(sc)
 
-    def _fits(self, sc: Scene, g: _Group) -> bool:
-        return (self.in_use + footprint(sc) <= self.budget and g.particles + sc.n <= self.particles_capacity
-                and g.grid + sc.grid_capacity * g.grid_factor <= self.grid_capacity)
+    def _fits(self, sc: Scene, g: _Group, without_retired: bool = False) -> bool:
+        in_use, particles, grid = self.in_use, g.particles, g.grid
+        if without_retired:  # as it would be once the finished scenes left
+            in_use -= sum(footprint(r.scene) for _, r in g.retired)
+            particles -= sum(r.scene.n for _, r in g.retired)
+            grid -= sum(r.scene.grid_capacity * g.grid_factor for _, r in g.retired)
+        return (in_use + footprint(sc) <= self.budget and particles + sc.n <= self.particles_capacity
+                and grid + sc.grid_capacity * g.grid_factor <= self.grid_capacity)
 
     def _usage(self, g: _Group):
-        g.particles = sum(rec[0].scene.n for rec in g.active.values())
-        g.grid = sum(rec[0].scene.grid_capacity * g.grid_factor for rec in g.active.values())
+        live = [rec[0] for rec in g.active.values()] + [r for _, r in g.retired]
+        g.particles = sum(r.scene.n for r in live)
+        g.grid = sum(r.scene.grid_capacity * g.grid_factor for r in live)
         self.in_use = sum(footprint(rec[0].scene) for gg in self.groups.values() for rec in gg.active.values())
+        self.in_use += sum(footprint(r.scene) for gg in self.groups.values() for _, r in gg.retired)
+
+    def _remove_retired(self, g: _Group):
+        """Removes the finished scenes still in `g` (queued behind their reads)."""
+        if g.retired:
+            g.state.remove_scenes([slot for slot, _ in g.retired])
+            g.retired.clear()
+            self._usage(g)
 
     def _fail(self, g: _Group, bits: int, reads: deque):
         """Evicts every scene of `g` that may have taken part in the failing
         step (see the module docstring) and reports it in self.failed."""
         for slot, (r, left, _) in g.active.items():
             self.failed[r.rid] = Failure(r.rid, bits, r.steps - left)
-        if g.active:
-            g.state.remove_scenes(list(g.active))
+        slots = list(g.active) + [slot for slot, _ in g.retired]  # finished ones leave too
+        if slots:
+            g.state.remove_scenes(slots)
         g.active.clear()
+        g.retired.clear()
         keep = deque()
         for item in reads:
             if item[0] is g:
@@ -204,7 +231,9 @@ class MpmServer:
                     rejected.append(pending.pop(0))  # can never fit, even alone
                     continue
                 if not self._fits(r.scene, g):
-                    break
+                    if not (g.retired and self._fits(r.scene, g, without_retired=True)):
+                        break
+                    self._remove_retired(g)  # the room held by finished scenes lets it in
                 pending.pop(0)
                 slot = g.state.add_scene(r.scene.particles, r.scene.colliders,
                                          r.scene.tri_vertices if r.scene.tri_vertices.size else None)
@@ -260,9 +289,12 @@ class MpmServer:
                     w = self._word()
                     ticket = g.state.read_status_async(self._words.array[w:w + 1])
                     reads.append((g, ticket, r, admitted, buf, w))
-                if done:  # queued behind the reads above
-                    g.state.remove_scenes(done)
-                    self._usage(g)
+                    g.retired.append((slot, r))
+                if g.retired and (not g.active or sum(r.scene.n for _, r in g.retired)
+                                  >= self.retire_fraction * g.particles):
+                    self._remove_retired(g)  # queued behind the reads above
+        for g in self.groups.values():
+            self._remove_retired(g)
         return results, rejected
 
 

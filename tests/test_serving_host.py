@@ -227,3 +227,34 @@ def test_two_gloo_ranks_serve_disjoint_shards_of_one_stream():
     assert all0 == all1 == list(range(20)) and not rej0 and not rej1 and not f0 and not f1
     assert ok0 and ok1
     assert abs(w0 - w1) <= max(w0, w1) // 2
+
+
+@pytest.mark.parametrize("fraction", [0.0, 0.02, 1.0])
+def test_finished_scenes_leave_in_batches(monkeypatch, fraction):
+    """Finished scenes stay in their state (stepping along) until they hold
+    `retire_fraction` of its particles, their room admits the next arrival,
+    or nothing else runs: results stay exact, a tight particle capacity still
+    admits every request, and every scene is gone at the end."""
+    monkeypatch.setattr(serving, "MpmState", FakeState)
+    monkeypatch.setattr(serving, "MpmPipeline", FakePipeline)
+    monkeypatch.setattr(serving, "PinnedArray", FakeArray)
+    rng = np.random.default_rng(5)
+    reqs = [serving.Request(i, _scene(i, int(rng.integers(10, 40))), int(rng.integers(1, 30)), 0.0)
+            for i in range(16)]
+    srv = serving.MpmServer(hbm_budget=1e12, particles_capacity=100, grid_capacity=1 << 12,
+                            retire_fraction=fraction)
+    removals = []
+    orig = FakeState.remove_scenes
+    monkeypatch.setattr(FakeState, "remove_scenes", lambda self, slots: (removals.append(len(slots)),
+                                                                          orig(self, slots))[1])
+    results, rejected = srv.run(reqs, clock=iter(np.arange(0.0, 1e6, 1e-3)).__next__, idle_sleep=0.0, depth=4)
+    assert not rejected and sorted(results) == list(range(16))
+    for r in reqs:
+        np.testing.assert_array_equal(results[r.rid].positions, r.scene.particles.pos + np.float32(r.steps))
+    (g,) = srv.groups.values()
+    while g.state.queue:
+        g.state._run_one()
+    assert not g.state.scenes and not g.retired
+    assert sum(removals) == 16
+    if fraction == 1.0:  # only admissions and the end let finished scenes go
+        assert len(removals) < 16
