@@ -11,9 +11,10 @@ removal compacts the whole particle storage), sooner when an arrival needs
 their room.  Scenes that arrive while others run start on the next step.
 
 The host never drains the GPU: a finished scene's positions are read
-asynchronously into pinned memory and its slot is freed at once (both queue
-behind the steps in flight), and its result is collected when the read's
-ticket completes; each batched state keeps at most a few steps queued ahead.
+asynchronously into pinned memory (queued behind the steps in flight), as is
+the removal of a batch of finished scenes, and a result is collected when its
+read's ticket completes; each batched state keeps at most a few steps queued
+ahead.
 
 Each scene steps exactly as it would alone (scene-local coordinates, its own
 block-key region and colliders), so a result does not depend on what else was
