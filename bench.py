@@ -324,7 +324,7 @@ def phase_rooflines(phases: dict, scene, st, peak: float) -> dict:
 
 
 def measure_cube(torch, steps: int = 100):
-    """the 32,768-particle elastic cube, 100 steps, one graph per step."""
+    """The 32,768-particle elastic cube, 100 steps, one graph per step."""
     from nexus_b200 import scenes
     from nexus_b200.mpm import MpmPipeline, state_from_scene
     sc = scenes.elastic_cube()
@@ -530,7 +530,7 @@ def measure_batched(args, world, rank, torch):
 
 
 def measure_coupled(args, torch, cpic: bool = False):
-    """The coupled batched mix (configs[3]: 64 sand scenes, each with eight
+    """The coupled batched mix (64 sand scenes, each with eight
     kinematic bodies on seeded trajectories driven every step and a
     20,000-triangle height-field floor) in one state, against the same scenes
     stepped one by one with the same driving.  With `cpic`, every scene runs
