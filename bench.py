@@ -215,13 +215,18 @@ def cpu_oracle_rate(scene, steps: int, warmup: int):
     """Particle-steps/s of the FP32 oracle (OpenMP, all host cores), and the
     oracle after its warmup + steps steps."""
     from oracle.oracle import OracleScene
-    o = OracleScene(scene, "f32")
+    o = OracleScene(scene, "f32", native=True)
     if warmup:
         o.step(warmup)
     t0 = time.perf_counter()
     o.step(steps)
     dt = time.perf_counter() - t0
     return scene.n * steps / dt, dt, o
+
+
+def oracle_build(o) -> str:
+    """Which oracle library an OracleScene runs: the host-native build or the portable one."""
+    return "-march=native on this host" if "_build_native_" in o.L.oracle_path else "portable -march=x86-64-v3"
 
 
 def measure_accuracy(scene, o32, steps: int) -> dict:
@@ -274,7 +279,7 @@ def run_reference(args, world, rank):
     from oracle.oracle import OracleScene
     scene = make_scene(args.workload, scale=args.scale)
     cores = int(os.environ["OMP_NUM_THREADS"])
-    o = OracleScene(scene, "f32")
+    o = OracleScene(scene, "f32", native=True)
     warm = min(args.warmup, 2)
     t0 = time.perf_counter()
     if warm:
@@ -296,7 +301,7 @@ def run_reference(args, world, rank):
                          "sample": f"{steps} full steps of the {scene.n}-particle scene after {warm} warm-up "
                                    f"steps (of --steps {args.steps} / --warmup {args.warmup}: at most "
                                    f"{REFERENCE_BUDGET_S:.0f} s of steps; C restatement of the reference step, "
-                                   f"FP32, OpenMP)"},
+                                   f"FP32, OpenMP, {oracle_build(o)})"},
         "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "note": "the reference's own GPU (wgpu) and CPU (Rust) paths cannot run on this box: no Rust toolchain, "
                 "no graphics stack",
@@ -435,7 +440,7 @@ def run_ours(args, world, rank, local):
         rate, secs, o32 = cpu_oracle_rate(scene, args.ref_steps, 1)
         cpu = {"value": rate, "unit": UNIT, "cores": int(os.environ["OMP_NUM_THREADS"]), "kind": "port",
                "sample": f"{args.ref_steps} full steps of the same {n}-particle scene after 1 warm-up step "
-                         f"({secs:.1f} s; C restatement of the reference step, FP32, OpenMP)"}
+                         f"({secs:.1f} s; C restatement of the reference step, FP32, OpenMP, {oracle_build(o32)})"}
         # the oracle as the checker: the same steps on the GPU against it
         accuracy = measure_accuracy(scene, o32, args.ref_steps + 1)
         del o32

@@ -33,13 +33,54 @@ def _ptr(a, t):
     return a.ctypes.data_as(t) if a is not None else None
 
 
-def lib(precision: str = "f32"):
-    if precision in _LIBS:
-        return _LIBS[precision]
-    path = os.path.join(_BUILD, f"liboracle_{precision}.so")
+def _host_key() -> str:
+    """A short fingerprint of this host's CPU (model and feature flags), so
+    that a -march=native build is only ever loaded where it was built."""
+    import hashlib
+    model = flags = ""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if not model and line.startswith("model name"):
+                    model = line.split(":", 1)[1].strip()
+                elif not flags and line.startswith("flags"):
+                    flags = line.split(":", 1)[1].strip()
+                if model and flags:
+                    break
+    except OSError:
+        pass
+    return hashlib.sha256((model + "|" + flags).encode()).hexdigest()[:12]
+
+
+def native_path() -> str | None:
+    """The FP32 oracle built with -march=native for this host (built on first
+    use, a few seconds of gcc), or None when it cannot be built here."""
+    d = os.path.join(_HERE, f"_build_native_{_host_key()}")
+    path = os.path.join(d, "liboracle_f32.so")
     if not os.path.exists(path):
-        build()
+        r = subprocess.run(["make", "-s", "-C", _HERE, "native", f"NATIVE={d}"], capture_output=True)
+        if r.returncode != 0 or not os.path.exists(path):
+            return None
+    return path
+
+
+def lib(precision: str = "f32", native: bool = False):
+    """The oracle library; `native`: the FP32 build for this host's CPU when
+    it can be built (same rounding flags, so the same results), else the
+    portable build."""
+    key = req = precision + ("_native" if native else "")
+    if key in _LIBS:
+        return _LIBS[key]
+    path = native_path() if native and precision == "f32" else None
+    if path is None:
+        key = precision
+        if key in _LIBS:
+            return _LIBS[key]
+        path = os.path.join(_BUILD, f"liboracle_{precision}.so")
+        if not os.path.exists(path):
+            build()
     L = C.CDLL(path)
+    L.oracle_path = path
     L.orc_create.restype = C.c_void_p
     L.orc_create.argtypes = [C.c_uint32, C.c_double, C.c_uint32]
     L.orc_destroy.argtypes = [C.c_void_p]
@@ -88,7 +129,7 @@ def lib(precision: str = "f32"):
     L.orc_project_point.restype = C.c_int
     L.orc_bc_project.argtypes = [C.c_uint32, C.c_float, _f, _f, _f]
     L.orc_prefix_sum.argtypes = [_u, C.c_uint32]
-    _LIBS[precision] = L
+    _LIBS[key] = _LIBS[req] = L
     return L
 
 
@@ -96,10 +137,11 @@ HEADER_FIELDS = 23  # vid[3], first, num, num_extras, cursors[10], nbh[7]
 
 
 class OracleScene:
-    """One scene held by the oracle (``precision`` = "f32" or "f64")."""
+    """One scene held by the oracle (``precision`` = "f32" or "f64"; ``native``:
+    the FP32 build for this host's CPU, where it can be built)."""
 
-    def __init__(self, scene, precision: str = "f32", grid_capacity: int | None = None):
-        self.L = lib(precision)
+    def __init__(self, scene, precision: str = "f32", grid_capacity: int | None = None, native: bool = False):
+        self.L = lib(precision, native)
         self.precision = precision
         p = scene.particles
         self.n = p.n
