@@ -346,6 +346,12 @@ NXM_API int nxm_debug_sort(nxm_pipeline* pipeline, nxm_state* state, int with_p2
  * `limit` rounds, recording NXM_STATUS_COPY_TIMEOUT in the state's status word
  * (nxm_synchronize then returns NXM_E_CUDA until the status is cleared). */
 NXM_API int nxm_debug_copy_wait_timeout(nxm_state* state, uint32_t limit);
+/* Test of the error paths of host calls that allocate device memory (no
+ * counterpart in the reference): with `after` >= 0, the after-th device
+ * allocation the library makes from now on (0: the next one; any state)
+ * fails once with NXM_E_OOM, as a full GPU would make it fail; -1 disarms.
+ * A call that fails this way leaves its state as it was before the call. */
+NXM_API int nxm_debug_fail_allocation(int64_t after);
 
 /* ---- autotuner --------------------------------------------------------------
  * Launch shapes of one state's step.  No counterpart in the reference (its

@@ -11,6 +11,7 @@
 
 #include <algorithm>
 #include <array>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -52,10 +53,24 @@ uint32_t next_pow2(uint32_t v) {
         if (rc_) return rc_;    \
     } while (0)
 
+// Host-side fault injection (nxm_debug_fail_allocation): armed with k >= 0,
+// the k-th device allocation from then on (0: the next one) reports
+// cudaErrorMemoryAllocation once and the hook disarms; -1: off.  Counts the
+// library's own cudaMalloc and pool allocations, every state alike.
+std::atomic<int64_t> g_alloc_fail_in{-1};
+
+bool injected_alloc_failure() {
+    int64_t v = g_alloc_fail_in.load();
+    while (v >= 0)
+        if (g_alloc_fail_in.compare_exchange_weak(v, v - 1)) return v == 0;
+    return false;
+}
+
 template <class T>
 cudaError_t dalloc(T** p, size_t count) {
     *p = nullptr;
     if (count == 0) count = 1;
+    if (injected_alloc_failure()) return cudaErrorMemoryAllocation;
     return cudaMalloc(reinterpret_cast<void**>(p), count * sizeof(T));
 }
 template <class T>
@@ -584,6 +599,8 @@ LaunchCfg launch_cfg(nxm_state* s) {
 // Stream-ordered scratch from the state's pool (freed with cudaFreeAsync).
 template <class T>
 cudaError_t scratch_alloc(nxm_state* s, T** p, size_t bytes) {
+    *p = nullptr;
+    if (injected_alloc_failure()) return cudaErrorMemoryAllocation;
     return cudaMallocFromPoolAsync(reinterpret_cast<void**>(p), bytes, s->pool, s->stream);
 }
 
@@ -798,6 +815,7 @@ struct Slab {
     // Allocates and points every added array into the allocation (or leaves them null).
     cudaError_t alloc(char** base) {
         *base = nullptr;
+        if (injected_alloc_failure()) return cudaErrorMemoryAllocation;
         const cudaError_t e = cudaMalloc(reinterpret_cast<void**>(base), bytes);
         if (e != cudaSuccess) {
             *base = nullptr;
@@ -916,6 +934,8 @@ void free_particles(nxm_state* s) {
     s->d_pcdf = s->d_pcdf_alt = nullptr;
 }
 
+int invalidate_codes(nxm_state* s);
+
 int reserve_particles(nxm_state* s, uint32_t need) {
     if (need <= s->pcap) return NXM_OK;
     int rc = canonicalize(s);
@@ -945,7 +965,10 @@ int reserve_particles(nxm_state* s, uint32_t need) {
     s->pcap = cap;
     invalidate_graph(s);
     s->params_dirty = true;
-    return NXM_OK;
+    // the new arrays hold no cached block keys: the next sort recomputes them
+    // from the positions (an upload that fails after this growth leaves the
+    // state stepping on these arrays)
+    return invalidate_codes(s);
 }
 
 // Deduplicates a model's static words; returns the material index.
@@ -2562,6 +2585,12 @@ int nxm_debug_sort(nxm_pipeline* pipeline, nxm_state* s, int with_p2g) {
     }
     NXM_TRY(cudaGetLastError());
     NXM_TRY(cudaStreamSynchronize(s->stream));
+    return NXM_OK;
+}
+
+int nxm_debug_fail_allocation(int64_t after) {
+    if (after < -1) return NXM_E_INVALID;
+    g_alloc_fail_in.store(after);
     return NXM_OK;
 }
 

@@ -104,6 +104,7 @@ SIGNATURES = {
     "nxm_grid_read_nodes": (C.c_int, [_vp, _f, C.c_uint32]),
     "nxm_debug_sort": (C.c_int, [_vp, _vp, C.c_int]),
     "nxm_debug_copy_wait_timeout": (C.c_int, [_vp, C.c_uint32]),
+    "nxm_debug_fail_allocation": (C.c_int, [C.c_int64]),
     "nxm_state_estimate_timestep_bound": (C.c_int, [_vp, _f, _u]),
     "nxm_read_cdf": (C.c_int, [_vp, _f]),
     "nxm_simulate_frame": (C.c_int, [_vp, _vp, C.c_uint32, C.c_uint32, _u]),
@@ -637,6 +638,12 @@ class MpmState:
     def cuda_stream(self) -> int:
         """The cudaStream_t (as an integer) all of this state's work runs on."""
         return int(self.lib.nxm_state_cuda_stream(self.h) or 0)
+
+
+def debug_fail_allocation(after: int):
+    """Test hook (nxm_debug_fail_allocation): the after-th device allocation of
+    the library from now on fails once with NXM_E_OOM; -1 disarms."""
+    _check(load().nxm_debug_fail_allocation(int(after)), "debug_fail_allocation")
 
 
 def tuning_table() -> list:
